@@ -1,0 +1,229 @@
+/*
+ * cmscan_gpu.h -- C ABI of the B200 covariance-model scan library
+ * (libcmscan_gpu.so).
+ *
+ * The library replaces the QDB-banded CYK / Inside window scanner of infernox
+ * (src/cm_nohmm.rs) behind plain C entry points: POD structs, raw pointers and
+ * sizes, int status codes, no exceptions and no torch types.  A Rust caller
+ * binds these with an `extern "C"` block; the Python
+ * package `infernox_b200` binds them with ctypes.
+ *
+ * Conventions
+ *   - Every entry point returns CMGPU_OK (0) or a negative CMGPU_E* code;
+ *     cmgpu_last_error() returns a message for the calling thread.
+ *   - Digital sequences are "window frames" exactly as the reference passes
+ *     them: dsq[0] = 255 (sentinel), dsq[1..n] residue codes 0..17
+ *     (A0 C1 G2 U3, gap 4, IUPAC 5..15, nonresidue 16, missing 17),
+ *     dsq[n+1] = 255.
+ *   - Coordinates are 1-based window coordinates, as in the reference.
+ *   - Scores are bits.  Integer Inside scores are the reference's
+ *     INTSCALE=1000 fixed point with -INFTY = -987654321.
+ *   - A model handle is read-only after upload and may be shared by threads;
+ *     a workspace handle must be used by one thread at a time.
+ */
+#ifndef CMSCAN_GPU_H
+#define CMSCAN_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CMGPU_OK 0
+#define CMGPU_EINVAL (-1)     /* bad argument                                */
+#define CMGPU_ENOMEM (-2)     /* host or device allocation failed            */
+#define CMGPU_EDEVICE (-3)    /* CUDA error (message in cmgpu_last_error)    */
+#define CMGPU_EOVERFLOW (-4)  /* caller's output array too small; *n_out set */
+#define CMGPU_ERANGE (-5)     /* band calculation did not converge           */
+#define CMGPU_ETIMEOUT (-6)   /* a device-side bounded wait gave up          */
+#define CMGPU_ENOSPACE (-7)   /* request exceeds a fixed capacity            */
+
+#define CMGPU_KP 18           /* digital alphabet size incl. degeneracies    */
+#define CMGPU_MAXCONNECT 6    /* max children of a CM state                  */
+#define CMGPU_ESC_STRIDE 324  /* per-state emission row: 18 (single), 18*18 (pair) */
+#define CMGPU_INFTY 987654321
+
+/* Semirings of the scanner (the reference's `generic_scan::<f32>` and
+ * `generic_scan::<i32>`, src/cm_nohmm.rs:406). */
+#define CMGPU_CYK_F32 0
+#define CMGPU_INSIDE_I32 1
+
+/* Band sets (src/cm_nohmm.rs:261-262 SMX_QDB1_TIGHT / SMX_QDB2_LOOSE; 0 = the
+ * `nonbanded` full d-range of the --max path, src/cm_nohmm.rs:431-437). */
+#define CMGPU_NOQDB 0
+#define CMGPU_QDB1 1
+#define CMGPU_QDB2 2
+
+/* Probability-level covariance model: structure + parameters, as read from a
+ * CM file in global configuration (src/cm.rs:315-563).  Arrays are caller
+ * owned.  t is [M][6], e is [M][16] (pairs a*4+b; singles use [0..4]). */
+typedef struct cmgpu_cm_params {
+    int32_t M, nodes, clen;
+    const int8_t *sttype, *stid, *ndtype;
+    const int32_t *ndidx, *cfirst, *cnum, *plast, *pnum, *nodemap;
+    const float *t, *e;
+    float null[4];
+    float el_selfsc;      /* EL self-transition score (bits)               */
+    float pbegin, pend;   /* local begin / end probabilities (0.05)        */
+    float n3_omega;       /* null3 prior                                   */
+} cmgpu_cm_params;
+
+/* The scanner's view of a configured CM: exactly the fields generic_scan,
+ * report_hits_greedily and the null3 correction read from `&CM`
+ * (src/cm_nohmm.rs:406-812).  Arrays are caller owned; per-state rows:
+ * tsc/itsc [M][6], oesc/ioesc [M][324]. */
+typedef struct cmgpu_cm {
+    int32_t M;
+    int32_t W;            /* window length cm.w                            */
+    uint32_t flags;       /* bit 10 = local begins (CMH_LOCAL_BEGIN)       */
+    const int8_t *sttype, *stid;
+    const int32_t *cfirst, *cnum;
+    const float *tsc, *oesc, *endsc, *beginsc;
+    float el_selfsc;
+    const int32_t *itsc, *ioesc, *iendsc, *ibeginsc;
+    int32_t iel_selfsc;
+    const int32_t *dmin1, *dmax1, *dmin2, *dmax2;
+    float null[4];
+    float n3_omega;
+} cmgpu_cm;
+
+/* Output arrays filled by cmgpu_prep_configure (all caller allocated). */
+typedef struct cmgpu_cm_scores {
+    float *tsc, *oesc, *endsc, *beginsc;     /* [M*6], [M*324], [M], [M]   */
+    int32_t *itsc, *ioesc, *iendsc, *ibeginsc;
+    int32_t *dmin1, *dmax1, *dmin2, *dmax2;   /* [M] each                   */
+    float *t_local;       /* [M*6] transition probs after localisation     */
+    float el_selfsc;      /* out */
+    int32_t iel_selfsc;   /* out */
+    int32_t W;            /* out: dmax of ROOT at beta_W                   */
+    uint32_t flags;       /* out */
+} cmgpu_cm_scores;
+
+typedef struct cmgpu_hit {
+    int32_t i, j;         /* window coordinates                            */
+    float score;          /* null3-corrected bit score                     */
+    float bias;           /* null3 correction                              */
+} cmgpu_hit;
+
+typedef struct cmgpu_envelope {
+    int32_t start, end;
+} cmgpu_envelope;
+
+/* One scan job of a batch: window [i0, j0] of the frame starting at byte
+ * dsq_offset of the batch's residue buffer (frame[0] is the sentinel). */
+typedef struct cmgpu_window {
+    int64_t dsq_offset;
+    int32_t i0, j0;
+} cmgpu_window;
+
+typedef struct cmgpu_batch_hit {
+    int32_t win;          /* index of the window in the batch              */
+    int32_t i, j;
+    float score, bias;
+} cmgpu_batch_hit;
+
+/* Per-call counters (cells = (j,v,d) DP cells computed, terms = child
+ * relaxations, both counted from the bands exactly as the oracle counts). */
+typedef struct cmgpu_stats {
+    double cells, terms, residues;
+    int64_t work_items, candidates;
+    float kernel_ms;      /* device time of the scan kernel(s)             */
+    int32_t kernel_launches;
+    int32_t deck_in_smem; /* 1 when the rolling decks live in shared memory */
+    int32_t ctas;
+} cmgpu_stats;
+
+typedef struct cmgpu_model cmgpu_model;
+typedef struct cmgpu_workspace cmgpu_workspace;
+
+const char *cmgpu_last_error(void);
+const char *cmgpu_version(void);
+
+/* ---- host-side model preparation (no GPU needed) ------------------------
+ * Configures a probability-level CM for scanning, as FaithfulSearcher::new
+ * does (src/cm_search.rs:871-979): QDB bands and W on the global model
+ * (cm_calc_qdb_bands, src/cm_nohmm.rs:374 -> band_calculation_engine,
+ * src/cm_qdband.rs:258), then either the global scores
+ * (cm_configure_scores_global, src/cm_nohmm.rs:264) or the local ones
+ * (cm_configure_scores, src/cp9.rs:4538, plus build_integer_scores,
+ * src/cm_nohmm.rs:279).  local=0/1.  W_in > 0 keeps a file W; 0 computes it. */
+int cmgpu_prep_configure(const cmgpu_cm_params *p, int local, int32_t W_in,
+                         double beta1, double beta2, double betaW,
+                         cmgpu_cm_scores *out);
+
+/* ILogsum table (src/cp9.rs:28-44): tbl[0..n) with n <= 23000. */
+int cmgpu_ilogsum_table(int32_t *tbl, int32_t n);
+/* FLogsum table (src/cp9.rs:5391-5400). */
+int cmgpu_flogsum_table(float *tbl, int32_t n);
+
+/* ---- device model and workspace ---------------------------------------- */
+int cmgpu_model_upload(const cmgpu_cm *cm, int device, cmgpu_model **out);
+void cmgpu_model_free(cmgpu_model *m);
+/* stream: a cudaStream_t or NULL for a library-owned stream. */
+int cmgpu_workspace_create(int device, void *stream, cmgpu_workspace **out);
+void cmgpu_workspace_free(cmgpu_workspace *ws);
+int cmgpu_workspace_stats(const cmgpu_workspace *ws, cmgpu_stats *out);
+/* Launch shape override for tuning: ctas_per_sm <= 0 keeps the tuned value,
+ * threads in {128,256,512}, chunk = residues per work item (0 = auto). */
+int cmgpu_workspace_set_shape(cmgpu_workspace *ws, int ctas_per_sm, int threads, int chunk);
+
+/* ---- scanner entry points ----------------------------------------------- */
+
+/* generic_scan (src/cm_nohmm.rs:406-763): scan window [i0, j0] of dsq and
+ * return the greedily reported, overlap-pruned hits (score order). */
+int cmgpu_qdb_scan(const cmgpu_model *m, cmgpu_workspace *ws, int semiring,
+                   int qdbidx, const uint8_t *dsq, int32_t n, int32_t i0,
+                   int32_t j0, float cutoff, int do_null3, cmgpu_hit *hits,
+                   int32_t cap, int32_t *n_out);
+
+/* cyk_seq_filter (src/cm_nohmm.rs:855-889): QDB1 CYK over [1, n] then hits
+ * padded by W-1 and merged into envelopes (ascending end). */
+int cmgpu_cyk_seq_filter(const cmgpu_model *m, cmgpu_workspace *ws,
+                         const uint8_t *dsq, int32_t n, float cutoff,
+                         int do_null3, cmgpu_envelope *envs, int32_t cap,
+                         int32_t *n_out);
+
+/* final_stage_inside_opt (src/cm_nohmm.rs:919-935): integer Inside over each
+ * envelope (QDB2, or the full d-range when nonbanded != 0); hits of all
+ * envelopes concatenated in envelope order. */
+int cmgpu_final_stage_inside_opt(const cmgpu_model *m, cmgpu_workspace *ws,
+                                 const uint8_t *dsq, int32_t n,
+                                 const cmgpu_envelope *envs, int32_t nenv,
+                                 float cutoff, int do_null3, int nonbanded,
+                                 cmgpu_hit *hits, int32_t cap, int32_t *n_out);
+
+/* Batched scan: every window is scanned as generic_scan would scan it on its
+ * own (same hits, same order), but all windows of the batch share one
+ * cost-ordered persistent launch.  dsq_all is host memory. */
+int cmgpu_scan_batch(const cmgpu_model *m, cmgpu_workspace *ws, int semiring,
+                     int qdbidx, const uint8_t *dsq_all, int64_t dsq_len,
+                     const cmgpu_window *wins, int32_t nwin, float cutoff,
+                     int do_null3, cmgpu_batch_hit *hits, int32_t cap,
+                     int32_t *n_out);
+
+/* As cmgpu_scan_batch with the residue buffer already resident in device
+ * memory (d_dsq_all is a device pointer); windows and hits stay on the host. */
+int cmgpu_scan_batch_device(const cmgpu_model *m, cmgpu_workspace *ws,
+                            int semiring, int qdbidx, const uint8_t *d_dsq_all,
+                            int64_t dsq_len, const cmgpu_window *wins,
+                            int32_t nwin, float cutoff, int do_null3,
+                            cmgpu_batch_hit *hits, int32_t cap, int32_t *n_out);
+
+/* Plain comparator: one launch per window, one CTA per window, no work queue
+ * and no sub-chunking.  Same results as cmgpu_scan_batch. */
+int cmgpu_scan_plain(const cmgpu_model *m, cmgpu_workspace *ws, int semiring,
+                     int qdbidx, const uint8_t *dsq_all, int64_t dsq_len,
+                     const cmgpu_window *wins, int32_t nwin, float cutoff,
+                     int do_null3, cmgpu_batch_hit *hits, int32_t cap,
+                     int32_t *n_out);
+
+/* Exact counts of cells and terms the reference scanner evaluates for a
+ * window of length L (host only; used for Gcells/s). */
+int cmgpu_count_work(const cmgpu_cm *cm, int semiring, int qdbidx, int32_t L,
+                     double *cells, double *terms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CMSCAN_GPU_H */

@@ -1,0 +1,153 @@
+"""ctypes binding of libcmscan_gpu.so (include/cmscan_gpu.h).
+
+The library is built in-tree (infernox_b200/_lib) by infernox_b200.build; it
+is loaded from there and nowhere else.  A missing library is an error: there
+is no CPU fallback for the scanner.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libcmscan_gpu.so")
+
+CMGPU_OK = 0
+CMGPU_EOVERFLOW = -4
+CYK_F32, INSIDE_I32 = 0, 1
+NOQDB, QDB1, QDB2 = 0, 1, 2
+
+P = C.POINTER
+
+
+class CmParams(C.Structure):
+    _fields_ = [
+        ("M", C.c_int32), ("nodes", C.c_int32), ("clen", C.c_int32),
+        ("sttype", P(C.c_int8)), ("stid", P(C.c_int8)), ("ndtype", P(C.c_int8)),
+        ("ndidx", P(C.c_int32)), ("cfirst", P(C.c_int32)), ("cnum", P(C.c_int32)),
+        ("plast", P(C.c_int32)), ("pnum", P(C.c_int32)), ("nodemap", P(C.c_int32)),
+        ("t", P(C.c_float)), ("e", P(C.c_float)),
+        ("null", C.c_float * 4),
+        ("el_selfsc", C.c_float), ("pbegin", C.c_float), ("pend", C.c_float),
+        ("n3_omega", C.c_float),
+    ]
+
+
+class Cm(C.Structure):
+    _fields_ = [
+        ("M", C.c_int32), ("W", C.c_int32), ("flags", C.c_uint32),
+        ("sttype", P(C.c_int8)), ("stid", P(C.c_int8)),
+        ("cfirst", P(C.c_int32)), ("cnum", P(C.c_int32)),
+        ("tsc", P(C.c_float)), ("oesc", P(C.c_float)), ("endsc", P(C.c_float)),
+        ("beginsc", P(C.c_float)), ("el_selfsc", C.c_float),
+        ("itsc", P(C.c_int32)), ("ioesc", P(C.c_int32)), ("iendsc", P(C.c_int32)),
+        ("ibeginsc", P(C.c_int32)), ("iel_selfsc", C.c_int32),
+        ("dmin1", P(C.c_int32)), ("dmax1", P(C.c_int32)),
+        ("dmin2", P(C.c_int32)), ("dmax2", P(C.c_int32)),
+        ("null", C.c_float * 4), ("n3_omega", C.c_float),
+    ]
+
+
+class CmScores(C.Structure):
+    _fields_ = [
+        ("tsc", P(C.c_float)), ("oesc", P(C.c_float)), ("endsc", P(C.c_float)),
+        ("beginsc", P(C.c_float)),
+        ("itsc", P(C.c_int32)), ("ioesc", P(C.c_int32)), ("iendsc", P(C.c_int32)),
+        ("ibeginsc", P(C.c_int32)),
+        ("dmin1", P(C.c_int32)), ("dmax1", P(C.c_int32)),
+        ("dmin2", P(C.c_int32)), ("dmax2", P(C.c_int32)),
+        ("t_local", P(C.c_float)),
+        ("el_selfsc", C.c_float), ("iel_selfsc", C.c_int32), ("W", C.c_int32),
+        ("flags", C.c_uint32),
+    ]
+
+
+class Hit(C.Structure):
+    _fields_ = [("i", C.c_int32), ("j", C.c_int32), ("score", C.c_float), ("bias", C.c_float)]
+
+
+HIT_DTYPE = np.dtype([("i", np.int32), ("j", np.int32), ("score", np.float32), ("bias", np.float32)])
+BATCH_HIT_DTYPE = np.dtype([("win", np.int32), ("i", np.int32), ("j", np.int32),
+                            ("score", np.float32), ("bias", np.float32)])
+ENV_DTYPE = np.dtype([("start", np.int32), ("end", np.int32)])
+WINDOW_DTYPE = np.dtype([("dsq_offset", np.int64), ("i0", np.int32), ("j0", np.int32)])
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("cells", C.c_double), ("terms", C.c_double), ("residues", C.c_double),
+        ("work_items", C.c_int64), ("candidates", C.c_int64),
+        ("kernel_ms", C.c_float), ("kernel_launches", C.c_int32),
+        ("deck_in_smem", C.c_int32), ("ctas", C.c_int32),
+    ]
+
+
+def ptr(a: np.ndarray, ctype):
+    return a.ctypes.data_as(P(ctype))
+
+
+_lib = None
+
+
+class CmgpuError(RuntimeError):
+    def __init__(self, rc: int, msg: str):
+        super().__init__(f"cmgpu error {rc}: {msg}")
+        self.rc = rc
+
+
+def lib() -> C.CDLL:
+    """Load the in-tree library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: run `python -m infernox_b200.build` first")
+    L = C.CDLL(LIB_PATH)
+    vp = C.c_void_p
+    L.cmgpu_last_error.restype = C.c_char_p
+    L.cmgpu_version.restype = C.c_char_p
+    L.cmgpu_prep_configure.argtypes = [P(CmParams), C.c_int, C.c_int32, C.c_double, C.c_double,
+                                       C.c_double, P(CmScores)]
+    L.cmgpu_ilogsum_table.argtypes = [P(C.c_int32), C.c_int32]
+    L.cmgpu_flogsum_table.argtypes = [P(C.c_float), C.c_int32]
+    L.cmgpu_model_upload.argtypes = [P(Cm), C.c_int, P(vp)]
+    L.cmgpu_model_free.argtypes = [vp]
+    L.cmgpu_model_free.restype = None
+    L.cmgpu_workspace_create.argtypes = [C.c_int, vp, P(vp)]
+    L.cmgpu_workspace_free.argtypes = [vp]
+    L.cmgpu_workspace_free.restype = None
+    L.cmgpu_workspace_stats.argtypes = [vp, P(Stats)]
+    L.cmgpu_workspace_set_shape.argtypes = [vp, C.c_int, C.c_int, C.c_int]
+    L.cmgpu_qdb_scan.argtypes = [vp, vp, C.c_int, C.c_int, P(C.c_uint8), C.c_int32, C.c_int32,
+                                 C.c_int32, C.c_float, C.c_int, vp, C.c_int32, P(C.c_int32)]
+    L.cmgpu_cyk_seq_filter.argtypes = [vp, vp, P(C.c_uint8), C.c_int32, C.c_float, C.c_int, vp,
+                                       C.c_int32, P(C.c_int32)]
+    L.cmgpu_final_stage_inside_opt.argtypes = [vp, vp, P(C.c_uint8), C.c_int32, vp, C.c_int32,
+                                               C.c_float, C.c_int, C.c_int, vp, C.c_int32,
+                                               P(C.c_int32)]
+    for name in ("cmgpu_scan_batch", "cmgpu_scan_plain"):
+        getattr(L, name).argtypes = [vp, vp, C.c_int, C.c_int, P(C.c_uint8), C.c_int64, vp,
+                                     C.c_int32, C.c_float, C.c_int, vp, C.c_int32, P(C.c_int32)]
+    L.cmgpu_scan_batch_device.argtypes = [vp, vp, C.c_int, C.c_int, vp, C.c_int64, vp, C.c_int32,
+                                          C.c_float, C.c_int, vp, C.c_int32, P(C.c_int32)]
+    L.cmgpu_count_work.argtypes = [P(Cm), C.c_int, C.c_int, C.c_int32, P(C.c_double),
+                                   P(C.c_double)]
+    _lib = L
+    return L
+
+
+def check(rc: int) -> None:
+    if rc != CMGPU_OK:
+        raise CmgpuError(rc, lib().cmgpu_last_error().decode(errors="replace"))
+
+
+# symbols declared in include/cmscan_gpu.h (checked by the CPU test suite)
+EXPORTED = [
+    "cmgpu_last_error", "cmgpu_version", "cmgpu_prep_configure", "cmgpu_ilogsum_table",
+    "cmgpu_flogsum_table", "cmgpu_model_upload", "cmgpu_model_free", "cmgpu_workspace_create",
+    "cmgpu_workspace_free", "cmgpu_workspace_stats", "cmgpu_workspace_set_shape",
+    "cmgpu_qdb_scan", "cmgpu_cyk_seq_filter", "cmgpu_final_stage_inside_opt",
+    "cmgpu_scan_batch", "cmgpu_scan_batch_device", "cmgpu_scan_plain", "cmgpu_count_work",
+]

@@ -1,0 +1,855 @@
+// C ABI of libcmscan_gpu.so (include/cmscan_gpu.h): model upload, workspaces,
+// batching of windows into work items, the scan launch, and the host-side
+// hit reporting.
+//
+// The device returns every reportable cell: (j, d) with bestsc >= cutoff.
+// The host then replays, per window and column, the reference's greedy
+// report (report_hits_greedily, src/cm_nohmm.rs:769-812) with the null3
+// correction in double precision (score_correction_null3, src/cp9.rs:6516)
+// and the greedy overlap removal (src/cp9.rs:6544-6574).  null3 can only
+// lower a score, so the cells the device returns are a superset of what the
+// reference could report, and the replay sees them in the reference's order
+// (j ascending, d ascending).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/cmscan_gpu.h"
+#include "cm_internal.h"
+#include "qdb_kernel.h"
+#include "qdb_plan.h"
+
+namespace cmx {
+
+static thread_local std::string g_err;
+void set_error(const std::string &msg) { g_err = msg; }
+
+bool build_plan(const cmgpu_cm *cm, int semiring, int qdbidx, Plan &p);
+void count_column_public(const cmgpu_cm *cm, const Plan &p, int qdbidx, int jrow, double &cells, double &terms);
+
+#define CUDA_TRY(call)                                                                          \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess) {                                                                \
+            set_error(std::string(#call) + ": " + cudaGetErrorString(e_));                      \
+            return CMGPU_EDEVICE;                                                               \
+        }                                                                                       \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// host copy of a configured CM
+// ---------------------------------------------------------------------------
+struct HostCM {
+    cmgpu_cm view{};
+    std::vector<int8_t> sttype, stid;
+    std::vector<int32_t> cfirst, cnum, itsc, ioesc, iendsc, ibeginsc, dmin1, dmax1, dmin2, dmax2;
+    std::vector<float> tsc, oesc, endsc, beginsc;
+
+    bool load(const cmgpu_cm *c) {
+        const int M = c->M;
+        if (M < 2 || c->W < 1 || !c->sttype || !c->stid || !c->cfirst || !c->cnum || !c->tsc || !c->oesc ||
+            !c->endsc || !c->beginsc || !c->itsc || !c->ioesc || !c->iendsc || !c->ibeginsc || !c->dmin1 ||
+            !c->dmax1 || !c->dmin2 || !c->dmax2)
+            return false;
+        sttype.assign(c->sttype, c->sttype + M);
+        stid.assign(c->stid, c->stid + M);
+        cfirst.assign(c->cfirst, c->cfirst + M);
+        cnum.assign(c->cnum, c->cnum + M);
+        tsc.assign(c->tsc, c->tsc + (size_t)M * MAXC);
+        oesc.assign(c->oesc, c->oesc + (size_t)M * ESC);
+        endsc.assign(c->endsc, c->endsc + M);
+        beginsc.assign(c->beginsc, c->beginsc + M);
+        itsc.assign(c->itsc, c->itsc + (size_t)M * MAXC);
+        ioesc.assign(c->ioesc, c->ioesc + (size_t)M * ESC);
+        iendsc.assign(c->iendsc, c->iendsc + M);
+        ibeginsc.assign(c->ibeginsc, c->ibeginsc + M);
+        dmin1.assign(c->dmin1, c->dmin1 + M);
+        dmax1.assign(c->dmax1, c->dmax1 + M);
+        dmin2.assign(c->dmin2, c->dmin2 + M);
+        dmax2.assign(c->dmax2, c->dmax2 + M);
+        view = *c;
+        view.sttype = sttype.data();
+        view.stid = stid.data();
+        view.cfirst = cfirst.data();
+        view.cnum = cnum.data();
+        view.tsc = tsc.data();
+        view.oesc = oesc.data();
+        view.endsc = endsc.data();
+        view.beginsc = beginsc.data();
+        view.itsc = itsc.data();
+        view.ioesc = ioesc.data();
+        view.iendsc = iendsc.data();
+        view.ibeginsc = ibeginsc.data();
+        view.dmin1 = dmin1.data();
+        view.dmax1 = dmax1.data();
+        view.dmin2 = dmin2.data();
+        view.dmax2 = dmax2.data();
+        // structural sanity: children inside [0, M), B children valid
+        for (int v = 0; v < M; v++) {
+            int st = sttype[v];
+            if (st < 0 || st > 8) return false;
+            if (st == E_ST) continue;
+            if (st == B_ST) {
+                if (cfirst[v] <= v || cfirst[v] >= M || cnum[v] <= v || cnum[v] >= M) return false;
+                if (stid[cfirst[v]] != BEGL_S) return false;
+            } else {
+                if (cnum[v] < 1 || cnum[v] > MAXC || cfirst[v] < v || cfirst[v] + cnum[v] > M) return false;
+                for (int yo = 0; yo < cnum[v]; yo++) {
+                    int y = cfirst[v] + yo;
+                    if (y == v && st != IL_ST && st != IR_ST) return false;
+                }
+            }
+        }
+        return true;
+    }
+};
+
+struct DevPlan {
+    Plan host;
+    StateDev *states = nullptr;
+    ChunkDev *chunks = nullptr;
+    int32_t *level_start = nullptr, *begin_states = nullptr;
+    uint32_t *tsc = nullptr, *init0 = nullptr, *endsc = nullptr, *beginsc = nullptr, *esc = nullptr,
+             *el_sca = nullptr;
+    std::vector<double> cells_prefix, terms_prefix;  // per jrow, prefix over jrow = 1..W
+    double cells_full = 0, terms_full = 0;
+    ~DevPlan() {
+        cudaFree(states);
+        cudaFree(chunks);
+        cudaFree(level_start);
+        cudaFree(begin_states);
+        cudaFree(tsc);
+        cudaFree(init0);
+        cudaFree(endsc);
+        cudaFree(beginsc);
+        cudaFree(esc);
+        cudaFree(el_sca);
+    }
+};
+
+template <class T>
+static int upload_vec(T **dst, const std::vector<T> &v) {
+    size_t n = std::max<size_t>(v.size(), 1);
+    CUDA_TRY(cudaMalloc((void **)dst, n * sizeof(T)));
+    if (!v.empty()) CUDA_TRY(cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return CMGPU_OK;
+}
+
+}  // namespace cmx
+
+using namespace cmx;
+
+struct cmgpu_model {
+    int device = 0;
+    HostCM cm;
+    std::mutex mu;
+    std::map<int, std::unique_ptr<DevPlan>> plans;  // key semiring*8 + qdbidx
+    uint16_t *ilog = nullptr;
+    int ilog_nz = 0;
+    std::vector<float> flog;  // host FLogsum table for null3
+    ~cmgpu_model() { cudaFree(ilog); }
+};
+
+struct cmgpu_workspace {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // device buffers (grow only)
+    uint8_t *d_dsq = nullptr;
+    size_t dsq_cap = 0;
+    WorkItem *d_items = nullptr;
+    size_t items_cap = 0;
+    Cand *d_cands = nullptr;
+    size_t cands_cap = 0;
+    int *d_counters = nullptr;  // [0] next item, [1] candidate count
+    uint32_t *d_deck = nullptr;
+    size_t deck_cap = 0;  // elements
+    // host staging
+    Cand *h_cands = nullptr;
+    size_t h_cands_cap = 0;
+    int *h_counters = nullptr;
+    // launch shape
+    int threads = 256;
+    int ctas_per_sm = 0;  // 0 = occupancy
+    int chunk = 0;        // 0 = auto
+    int sm_count = 148;
+    cmgpu_stats stats{};
+    ~cmgpu_workspace() {
+        cudaFree(d_dsq);
+        cudaFree(d_items);
+        cudaFree(d_cands);
+        cudaFree(d_counters);
+        cudaFree(d_deck);
+        cudaFreeHost(h_cands);
+        cudaFreeHost(h_counters);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (own_stream && stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace cmx {
+
+static int get_plan(cmgpu_model *m, int semiring, int qdbidx, DevPlan **out) {
+    std::lock_guard<std::mutex> lk(m->mu);
+    int key = semiring * 8 + qdbidx;
+    auto it = m->plans.find(key);
+    if (it != m->plans.end()) {
+        *out = it->second.get();
+        return CMGPU_OK;
+    }
+    std::unique_ptr<DevPlan> dp(new DevPlan());
+    if (!build_plan(&m->cm.view, semiring, qdbidx, dp->host)) return CMGPU_EINVAL;
+    const Plan &p = dp->host;
+    CUDA_TRY(cudaSetDevice(m->device));
+    int rc;
+    if ((rc = upload_vec(&dp->states, p.states))) return rc;
+    if ((rc = upload_vec(&dp->chunks, p.chunks))) return rc;
+    if ((rc = upload_vec(&dp->level_start, p.level_start))) return rc;
+    if ((rc = upload_vec(&dp->begin_states, p.begin_states))) return rc;
+    if ((rc = upload_vec(&dp->tsc, p.tsc))) return rc;
+    if ((rc = upload_vec(&dp->init0, p.init0))) return rc;
+    if ((rc = upload_vec(&dp->endsc, p.endsc))) return rc;
+    if ((rc = upload_vec(&dp->beginsc, p.beginsc))) return rc;
+    if ((rc = upload_vec(&dp->esc, p.esc))) return rc;
+    if ((rc = upload_vec(&dp->el_sca, p.el_sca))) return rc;
+    // per-column work counts by row limit
+    const int W = p.W;
+    dp->cells_prefix.assign(W + 1, 0.0);
+    dp->terms_prefix.assign(W + 1, 0.0);
+    for (int jr = 1; jr <= W; jr++) {
+        double c = 0, t = 0;
+        count_column_public(&m->cm.view, p, qdbidx, jr, c, t);
+        dp->cells_prefix[jr] = dp->cells_prefix[jr - 1] + c;
+        dp->terms_prefix[jr] = dp->terms_prefix[jr - 1] + t;
+        if (jr == W) {
+            dp->cells_full = c;
+            dp->terms_full = t;
+        }
+    }
+    *out = dp.get();
+    m->plans[key] = std::move(dp);
+    return CMGPU_OK;
+}
+
+// exact reference cells/terms of a window of length L
+static void window_work(const DevPlan *dp, int64_t L, double &cells, double &terms) {
+    const int W = dp->host.W;
+    int64_t warm = std::min<int64_t>(L, W - 1);
+    cells = dp->cells_prefix[warm];
+    terms = dp->terms_prefix[warm];
+    if (L > warm) {
+        cells += dp->cells_full * (double)(L - warm);
+        terms += dp->terms_full * (double)(L - warm);
+    }
+}
+
+template <class T>
+static int ensure_dev(T **p, size_t *cap, size_t n) {
+    if (n <= *cap && *p) return CMGPU_OK;
+    size_t nc = std::max<size_t>(n, *cap * 3 / 2 + 16);
+    cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    CUDA_TRY(cudaMalloc((void **)p, nc * sizeof(T)));
+    *cap = nc;
+    return CMGPU_OK;
+}
+
+static int ensure_host_cands(cmgpu_workspace *ws, size_t n) {
+    if (n <= ws->h_cands_cap && ws->h_cands) return CMGPU_OK;
+    size_t nc = std::max<size_t>(n, ws->h_cands_cap * 3 / 2 + 16);
+    cudaFreeHost(ws->h_cands);
+    ws->h_cands = nullptr;
+    ws->h_cands_cap = 0;
+    CUDA_TRY(cudaMallocHost((void **)&ws->h_cands, nc * sizeof(Cand)));
+    ws->h_cands_cap = nc;
+    return CMGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// host-side reporting
+// ---------------------------------------------------------------------------
+static inline double sre_log2d(double x) { return x > 0.0 ? std::log(x) * 1.44269504 : -1.0e36; }
+
+static float flogsum_host(const std::vector<float> &tbl, float s1, float s2) {
+    float mx = std::max(s1, s2), mn = std::min(s1, s2);
+    if (mn == -INFINITY || (mx - mn) >= 23.0f) return mx;
+    return mx + tbl[(size_t)((mx - mn) * 1000.0f)];
+}
+
+// score_correction_null3 (src/cp9.rs:6516-6528)
+static float null3_correction(const cmgpu_model *m, const float *comp, int len) {
+    float score = 0.0f;
+    for (int a = 0; a < 4; a++) {
+        double term = sre_log2d((double)(comp[a] / m->cm.view.null[a])) * (double)comp[a] * (double)len;
+        score = (float)((double)score + term);
+    }
+    score = (float)((double)score + sre_log2d((double)m->cm.view.n3_omega));
+    return flogsum_host(m->flog, 0.0f, score);
+}
+
+static inline float raw_bits(int semiring, uint32_t raw) {
+    if (semiring == CMGPU_INSIDE_I32) {
+        int32_t s = (int32_t)raw;
+        return s == -INFTY ? IMPOSSIBLE : (float)((double)s / INTSCALE);
+    }
+    float f;
+    std::memcpy(&f, &raw, 4);
+    return f;
+}
+
+// remove_overlaps_greedy (src/cp9.rs:6544-6574)
+static void remove_overlaps(std::vector<cmgpu_hit> &h) {
+    std::stable_sort(h.begin(), h.end(), [](const cmgpu_hit &a, const cmgpu_hit &b) {
+        if (a.score != b.score) return a.score > b.score;
+        return a.i < b.i;
+    });
+    std::vector<char> removed(h.size(), 0);
+    for (size_t i = 0; i < h.size(); i++) {
+        if (removed[i]) continue;
+        for (size_t j = i + 1; j < h.size(); j++) {
+            if (removed[j]) continue;
+            if (!(h[j].j < h[i].i) && !(h[i].j < h[j].i)) removed[j] = 1;
+        }
+    }
+    size_t o = 0;
+    for (size_t i = 0; i < h.size(); i++)
+        if (!removed[i]) h[o++] = h[i];
+    h.resize(o);
+}
+
+// Replays report_hits_greedily for one window from its candidate cells
+// (sorted by j, d).  frame = window frame (host), needed for null3.
+static void report_window(const cmgpu_model *m, int semiring, const Cand *c, size_t n, const uint8_t *frame,
+                          int32_t i0, float cutoff, int do_null3, std::vector<cmgpu_hit> &out) {
+    std::vector<cmgpu_hit> tmp;
+    // prefix counts of canonical residues over the candidates' span
+    std::vector<int32_t> pre;
+    int32_t lo = 0;
+    if (do_null3 && n) {
+        int32_t mini = c[0].j, maxj = c[0].j;
+        for (size_t k = 0; k < n; k++) {
+            mini = std::min(mini, c[k].j - c[k].d + 1);
+            maxj = std::max(maxj, c[k].j);
+        }
+        lo = std::max(i0, mini) - 1;
+        pre.assign((size_t)(maxj - lo + 1) * 4, 0);
+        for (int32_t p = lo + 1; p <= maxj; p++) {
+            for (int a = 0; a < 4; a++) pre[(size_t)(p - lo) * 4 + a] = pre[(size_t)(p - 1 - lo) * 4 + a];
+            uint8_t r = frame[p];
+            if (r < 4) pre[(size_t)(p - lo) * 4 + r]++;
+        }
+    }
+    size_t k = 0;
+    while (k < n) {
+        int32_t j = c[k].j;
+        float max_reported = IMPOSSIBLE;
+        for (; k < n && c[k].j == j; k++) {
+            int32_t d = c[k].d, i = j - d + 1;
+            float hit_sc = raw_bits(semiring, c[k].raw);
+            float bias = 0.0f;
+            if (!(hit_sc > max_reported && hit_sc >= cutoff && hit_sc > IMPOSSIBLE + 1.0f)) continue;
+            bool do_report = true;
+            if (do_null3) {
+                float comp[4];
+                for (int a = 0; a < 4; a++) {
+                    int32_t cnt = pre[(size_t)(j - lo) * 4 + a] - pre[(size_t)(i - 1 - lo) * 4 + a];
+                    comp[a] = (float)(double)cnt;
+                }
+                float sum = 0.0f;
+                for (int a = 0; a < 4; a++) sum += comp[a];
+                if (sum > 0.0f)
+                    for (int a = 0; a < 4; a++) comp[a] /= sum;
+                else
+                    for (int a = 0; a < 4; a++) comp[a] = 1.0f / 4.0f;
+                float corr = null3_correction(m, comp, d);
+                hit_sc -= corr;
+                bias = corr;
+                do_report = hit_sc > max_reported && hit_sc >= cutoff;
+            }
+            if (do_report) {
+                tmp.push_back(cmgpu_hit{i, j, hit_sc, bias});
+                max_reported = hit_sc;
+            }
+        }
+    }
+    remove_overlaps(tmp);
+    out.insert(out.end(), tmp.begin(), tmp.end());
+}
+
+// ---------------------------------------------------------------------------
+// the batched scan
+// ---------------------------------------------------------------------------
+struct WinDesc {
+    int64_t off;
+    int32_t i0, j0;
+};
+
+static int run_scan(cmgpu_model *m, cmgpu_workspace *ws, int semiring, int qdbidx, const uint8_t *d_dsq,
+                    const uint8_t *h_dsq, int64_t dsq_len, const std::vector<WinDesc> &wins, float cutoff,
+                    int do_null3, bool plain, std::vector<std::vector<cmgpu_hit>> &hits_per_win) {
+    if (semiring != CMGPU_CYK_F32 && semiring != CMGPU_INSIDE_I32) {
+        set_error("unknown semiring");
+        return CMGPU_EINVAL;
+    }
+    if (qdbidx < 0 || qdbidx > 2) {
+        set_error("unknown band set");
+        return CMGPU_EINVAL;
+    }
+    DevPlan *dp = nullptr;
+    int rc = get_plan(m, semiring, qdbidx, &dp);
+    if (rc) return rc;
+    const Plan &pl = dp->host;
+    CUDA_TRY(cudaSetDevice(ws->device));
+    hits_per_win.assign(wins.size(), {});
+    memset(&ws->stats, 0, sizeof(ws->stats));
+
+    ScanParams sp{};
+    sp.states = dp->states;
+    sp.chunks = dp->chunks;
+    sp.level_start = dp->level_start;
+    sp.nlev = (int)pl.level_start.size() - 1;
+    sp.tsc = dp->tsc;
+    sp.init0 = dp->init0;
+    sp.endsc = dp->endsc;
+    sp.beginsc = dp->beginsc;
+    sp.esc = dp->esc;
+    sp.el_sca = dp->el_sca;
+    sp.begin_states = dp->begin_states;
+    sp.nbegin = (int)pl.begin_states.size();
+    sp.M = pl.M;
+    sp.W = pl.W;
+    sp.root_dn = pl.root_dn;
+    sp.root_dxcap = pl.root_dxcap;
+    sp.root_cfirst = pl.root_cfirst;
+    sp.root_cnum = pl.root_cnum;
+    sp.local = pl.local ? 1 : 0;
+    sp.inside = semiring == CMGPU_INSIDE_I32;
+    sp.deck_elems = pl.deck_elems;
+    sp.ilog = m->ilog;
+    sp.ilog_nz = m->ilog_nz;
+    sp.dsq = d_dsq;
+    sp.cutoff = cutoff;
+
+    // launch shape
+    const int threads = ws->threads;
+    bool deck_smem = scan_smem_bytes(sp, true) <= 227 * 1024 - 1024;
+    int occ = scan_occupancy(sp, deck_smem, threads);
+    if (deck_smem && occ < 1) {
+        deck_smem = false;
+        occ = scan_occupancy(sp, false, threads);
+    }
+    if (occ < 1) {
+        set_error("scan kernel cannot be resident with this shape");
+        return CMGPU_EDEVICE;
+    }
+    int per_sm = ws->ctas_per_sm > 0 ? std::min(ws->ctas_per_sm, occ) : occ;
+    int max_ctas = ws->sm_count * per_sm;
+
+    // work items
+    std::vector<WorkItem> items;
+    int64_t total_cols = 0;
+    for (auto &w : wins) total_cols += std::max<int64_t>(0, (int64_t)w.j0 - w.i0 + 1);
+    const int W = pl.W;
+    int64_t chunk = ws->chunk;
+    if (chunk <= 0) {
+        chunk = total_cols / std::max<int64_t>(1, (int64_t)max_ctas * 4);
+        chunk = std::max<int64_t>(chunk, 4 * (int64_t)W);
+        chunk = std::min<int64_t>(chunk, 32768);
+    }
+    for (size_t wi = 0; wi < wins.size(); wi++) {
+        const WinDesc &w = wins[wi];
+        if (w.j0 < w.i0) continue;
+        double c = 0, t = 0;
+        window_work(dp, (int64_t)w.j0 - w.i0 + 1, c, t);
+        ws->stats.cells += c;
+        ws->stats.terms += t;
+        ws->stats.residues += (double)w.j0 - w.i0 + 1;
+        if (plain) {
+            items.push_back(WorkItem{w.off, w.i0, w.j0, w.i0, (int32_t)wi});
+            continue;
+        }
+        for (int64_t r0 = w.i0; r0 <= w.j0; r0 += chunk) {
+            int64_t r1 = std::min<int64_t>(w.j0, r0 + chunk - 1);
+            int64_t js = std::max<int64_t>(w.i0, r0 - (W - 1));
+            items.push_back(WorkItem{w.off, (int32_t)js, (int32_t)r1, (int32_t)r0, (int32_t)wi});
+        }
+    }
+    if (!plain)
+        std::stable_sort(items.begin(), items.end(), [](const WorkItem &a, const WorkItem &b) {
+            return (a.jend - a.jstart) > (b.jend - b.jstart);
+        });
+    ws->stats.work_items = (int64_t)items.size();
+    ws->stats.deck_in_smem = deck_smem ? 1 : 0;
+    if (items.empty()) return CMGPU_OK;
+
+    if ((rc = ensure_dev(&ws->d_items, &ws->items_cap, items.size()))) return rc;
+    CUDA_TRY(cudaMemcpyAsync(ws->d_items, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice,
+                             ws->stream));
+    size_t cand_cap = std::max<size_t>(ws->cands_cap, 1 << 16);
+    if ((rc = ensure_dev(&ws->d_cands, &ws->cands_cap, cand_cap))) return rc;
+    int ctas = plain ? 1 : (int)std::min<int64_t>((int64_t)items.size(), max_ctas);
+    ws->stats.ctas = ctas;
+    if (!deck_smem) {
+        size_t stride = ((size_t)pl.deck_elems + 31) & ~(size_t)31;
+        if ((rc = ensure_dev(&ws->d_deck, &ws->deck_cap, stride * (size_t)ctas))) return rc;
+        sp.deck_global = ws->d_deck;
+        sp.deck_stride = (int64_t)stride;
+    }
+    sp.items = ws->d_items;
+    sp.next_item = ws->d_counters;
+    sp.cand_count = ws->d_counters + 1;
+
+    size_t ncand = 0;
+    for (int attempt = 0; attempt < 3; attempt++) {
+        sp.cands = ws->d_cands;
+        sp.cand_cap = (int)std::min<size_t>(ws->cands_cap, (size_t)INT32_MAX);
+        CUDA_TRY(cudaMemsetAsync(ws->d_counters, 0, 2 * sizeof(int), ws->stream));
+        CUDA_TRY(cudaEventRecord(ws->ev0, ws->stream));
+        if (plain) {
+            // one launch per window, one CTA: the per-window comparator
+            for (size_t k = 0; k < items.size(); k++) {
+                sp.items = ws->d_items + k;
+                sp.nitems = 1;
+                sp.item_base = (int)k;
+                CUDA_TRY(cudaMemsetAsync(ws->d_counters, 0, sizeof(int), ws->stream));
+                CUDA_TRY(scan_launch(sp, deck_smem, 1, threads, ws->stream));
+            }
+            ws->stats.kernel_launches = (int)items.size();
+        } else {
+            sp.nitems = (int)items.size();
+            sp.item_base = 0;
+            CUDA_TRY(scan_launch(sp, deck_smem, ctas, threads, ws->stream));
+            ws->stats.kernel_launches = 1;
+        }
+        CUDA_TRY(cudaEventRecord(ws->ev1, ws->stream));
+        CUDA_TRY(cudaMemcpyAsync(ws->h_counters, ws->d_counters, 2 * sizeof(int), cudaMemcpyDeviceToHost,
+                                 ws->stream));
+        CUDA_TRY(cudaStreamSynchronize(ws->stream));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ws->ev0, ws->ev1);
+        ws->stats.kernel_ms += ms;
+        ncand = (size_t)(unsigned)ws->h_counters[1];
+        if (ncand <= ws->cands_cap) break;
+        if ((rc = ensure_dev(&ws->d_cands, &ws->cands_cap, ncand + ncand / 4 + 1024))) return rc;
+        if (attempt == 2) {
+            set_error("candidate buffer overflow");
+            return CMGPU_ENOSPACE;
+        }
+        if (plain) sp.items = ws->d_items;
+    }
+    ws->stats.candidates = (int64_t)ncand;
+    if ((rc = ensure_host_cands(ws, ncand + 1))) return rc;
+    if (ncand)
+        CUDA_TRY(cudaMemcpyAsync(ws->h_cands, ws->d_cands, ncand * sizeof(Cand), cudaMemcpyDeviceToHost,
+                                 ws->stream));
+    CUDA_TRY(cudaStreamSynchronize(ws->stream));
+
+    // map items to windows, order by (window, j, d)
+    std::vector<Cand> cs(ws->h_cands, ws->h_cands + ncand);
+    for (auto &c : cs) c.item = items[c.item].win;
+    std::sort(cs.begin(), cs.end(), [](const Cand &a, const Cand &b) {
+        if (a.item != b.item) return a.item < b.item;
+        if (a.j != b.j) return a.j < b.j;
+        return a.d < b.d;
+    });
+    std::vector<uint8_t> frame_buf;
+    size_t k = 0;
+    while (k < cs.size()) {
+        size_t e = k;
+        while (e < cs.size() && cs[e].item == cs[k].item) e++;
+        const WinDesc &w = wins[cs[k].item];
+        const uint8_t *frame = nullptr;
+        if (do_null3) {
+            if (h_dsq) {
+                frame = h_dsq + w.off;
+            } else {
+                frame_buf.resize((size_t)w.j0 + 2);
+                CUDA_TRY(cudaMemcpy(frame_buf.data(), d_dsq + w.off, (size_t)w.j0 + 1, cudaMemcpyDeviceToHost));
+                frame = frame_buf.data();
+            }
+        }
+        report_window(m, semiring, cs.data() + k, e - k, frame, w.i0, cutoff, do_null3,
+                      hits_per_win[cs[k].item]);
+        k = e;
+    }
+    (void)dsq_len;
+    return CMGPU_OK;
+}
+
+static bool check_codes(const uint8_t *dsq, int32_t n);
+
+// Copies a host residue buffer to the workspace.  frame=true: the buffer is
+// one window frame, whose residues 1..len-2 are checked to be codes 0..17.
+static int stage_dsq(cmgpu_workspace *ws, const uint8_t *h, int64_t len, bool frame = true) {
+    if (frame && len >= 2 && !check_codes(h, (int32_t)(len - 2))) {
+        set_error("residue code > 17 in the sequence");
+        return CMGPU_EINVAL;
+    }
+    int rc = ensure_dev(&ws->d_dsq, &ws->dsq_cap, (size_t)len);
+    if (rc) return rc;
+    CUDA_TRY(cudaMemcpyAsync(ws->d_dsq, h, (size_t)len, cudaMemcpyHostToDevice, ws->stream));
+    return CMGPU_OK;
+}
+
+static bool check_windows(const cmgpu_window *wins, int32_t nwin, int64_t dsq_len, const uint8_t *h_dsq) {
+    for (int32_t k = 0; k < nwin; k++) {
+        const cmgpu_window &w = wins[k];
+        if (w.dsq_offset < 0 || w.i0 < 1 || w.j0 < w.i0 - 1) return false;
+        if (w.dsq_offset + (int64_t)w.j0 + 1 > dsq_len) return false;
+        if (h_dsq)
+            for (int32_t x = w.i0; x <= w.j0; x++)
+                if (h_dsq[w.dsq_offset + x] > 17) return false;
+    }
+    return true;
+}
+
+static bool check_codes(const uint8_t *dsq, int32_t n) {
+    for (int32_t x = 1; x <= n; x++)
+        if (dsq[x] > 17) return false;
+    return true;
+}
+
+}  // namespace cmx
+
+// ===========================================================================
+// exported entry points
+// ===========================================================================
+extern "C" {
+
+const char *cmgpu_last_error(void) { return cmx::g_err.c_str(); }
+const char *cmgpu_version(void) { return "cmscan_gpu 0.1 (sm_100a)"; }
+
+int cmgpu_model_upload(const cmgpu_cm *cm, int device, cmgpu_model **out) {
+    if (!cm || !out) return CMGPU_EINVAL;
+    *out = nullptr;
+    std::unique_ptr<cmgpu_model> m(new cmgpu_model());
+    m->device = device;
+    if (!m->cm.load(cm)) {
+        set_error("cmgpu_model_upload: inconsistent model arrays");
+        return CMGPU_EINVAL;
+    }
+    CUDA_TRY(cudaSetDevice(device));
+    std::vector<int32_t> t(LOGSUM_TBL);
+    cmgpu_ilogsum_table(t.data(), LOGSUM_TBL);
+    int nz = 0;
+    for (int i = 0; i < LOGSUM_TBL; i++)
+        if (t[i] != 0) nz = i + 1;
+    std::vector<uint16_t> t16(nz);
+    for (int i = 0; i < nz; i++) t16[i] = (uint16_t)t[i];
+    m->ilog_nz = nz;
+    int rc = upload_vec(&m->ilog, t16);
+    if (rc) return rc;
+    m->flog.resize(LOGSUM_TBL);
+    cmgpu_flogsum_table(m->flog.data(), LOGSUM_TBL);
+    *out = m.release();
+    return CMGPU_OK;
+}
+
+void cmgpu_model_free(cmgpu_model *m) { delete m; }
+
+int cmgpu_workspace_create(int device, void *stream, cmgpu_workspace **out) {
+    if (!out) return CMGPU_EINVAL;
+    *out = nullptr;
+    std::unique_ptr<cmgpu_workspace> ws(new cmgpu_workspace());
+    ws->device = device;
+    CUDA_TRY(cudaSetDevice(device));
+    if (stream) {
+        ws->stream = (cudaStream_t)stream;
+    } else {
+        CUDA_TRY(cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking));
+        ws->own_stream = true;
+    }
+    CUDA_TRY(cudaEventCreate(&ws->ev0));
+    CUDA_TRY(cudaEventCreate(&ws->ev1));
+    CUDA_TRY(cudaMalloc((void **)&ws->d_counters, 4 * sizeof(int)));
+    CUDA_TRY(cudaMallocHost((void **)&ws->h_counters, 4 * sizeof(int)));
+    cudaDeviceProp prop;
+    CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+    ws->sm_count = prop.multiProcessorCount;
+    *out = ws.release();
+    return CMGPU_OK;
+}
+
+void cmgpu_workspace_free(cmgpu_workspace *ws) { delete ws; }
+
+int cmgpu_workspace_stats(const cmgpu_workspace *ws, cmgpu_stats *out) {
+    if (!ws || !out) return CMGPU_EINVAL;
+    *out = ws->stats;
+    return CMGPU_OK;
+}
+
+int cmgpu_workspace_set_shape(cmgpu_workspace *ws, int ctas_per_sm, int threads, int chunk) {
+    if (!ws) return CMGPU_EINVAL;
+    if (threads != 0 && threads != 128 && threads != 256 && threads != 512) return CMGPU_EINVAL;
+    ws->ctas_per_sm = ctas_per_sm;
+    if (threads) ws->threads = threads;
+    ws->chunk = chunk;
+    return CMGPU_OK;
+}
+
+static int finish_single(const std::vector<std::vector<cmgpu_hit>> &hpw, cmgpu_hit *hits, int32_t cap,
+                         int32_t *n_out) {
+    size_t n = 0;
+    for (auto &v : hpw) n += v.size();
+    *n_out = (int32_t)n;
+    if ((int64_t)n > cap) {
+        set_error("output array too small");
+        return CMGPU_EOVERFLOW;
+    }
+    size_t o = 0;
+    for (auto &v : hpw)
+        for (auto &h : v) hits[o++] = h;
+    return CMGPU_OK;
+}
+
+int cmgpu_qdb_scan(const cmgpu_model *mc, cmgpu_workspace *ws, int semiring, int qdbidx, const uint8_t *dsq,
+                   int32_t n, int32_t i0, int32_t j0, float cutoff, int do_null3, cmgpu_hit *hits, int32_t cap,
+                   int32_t *n_out) {
+    cmgpu_model *m = const_cast<cmgpu_model *>(mc);
+    if (!m || !ws || !dsq || !n_out || n < 0 || i0 < 1 || j0 > n || (cap > 0 && !hits)) return CMGPU_EINVAL;
+    *n_out = 0;
+    int rc = stage_dsq(ws, dsq, (int64_t)n + 2);
+    if (rc) return rc;
+    std::vector<WinDesc> wins{{0, i0, j0}};
+    std::vector<std::vector<cmgpu_hit>> hpw;
+    rc = run_scan(m, ws, semiring, qdbidx, ws->d_dsq, dsq, (int64_t)n + 2, wins, cutoff, do_null3, false, hpw);
+    if (rc) return rc;
+    return finish_single(hpw, hits, cap, n_out);
+}
+
+int cmgpu_cyk_seq_filter(const cmgpu_model *mc, cmgpu_workspace *ws, const uint8_t *dsq, int32_t n, float cutoff,
+                         int do_null3, cmgpu_envelope *envs, int32_t cap, int32_t *n_out) {
+    cmgpu_model *m = const_cast<cmgpu_model *>(mc);
+    if (!m || !ws || !dsq || !n_out || n < 0 || (cap > 0 && !envs)) return CMGPU_EINVAL;
+    *n_out = 0;
+    if (n == 0) return CMGPU_OK;
+    int rc = stage_dsq(ws, dsq, (int64_t)n + 2);
+    if (rc) return rc;
+    std::vector<WinDesc> wins{{0, 1, n}};
+    std::vector<std::vector<cmgpu_hit>> hpw;
+    rc = run_scan(m, ws, CMGPU_CYK_F32, CMGPU_QDB1, ws->d_dsq, dsq, (int64_t)n + 2, wins, cutoff, do_null3, false,
+                  hpw);
+    if (rc) return rc;
+    // pad each hit by W-1 and merge (src/cm_nohmm.rs:858-888)
+    const int W = m->cm.view.W;
+    std::vector<std::pair<int32_t, int32_t>> pad;
+    for (auto &h : hpw[0]) pad.push_back({std::max(1, h.j - (W - 1)), std::min(n, h.i + (W - 1))});
+    std::sort(pad.begin(), pad.end(), [](const std::pair<int32_t, int32_t> &a, const std::pair<int32_t, int32_t> &b) {
+        if (a.second != b.second) return a.second < b.second;
+        return a.first < b.first;
+    });
+    std::vector<cmgpu_envelope> out;
+    size_t h = 0;
+    while (h < pad.size()) {
+        int32_t iw = pad[h].first, jw = pad[h].second;
+        while (h + 1 < pad.size() && pad[h + 1].first <= jw) {
+            h++;
+            jw = std::max(jw, pad[h].second);
+        }
+        out.push_back(cmgpu_envelope{iw, jw});
+        h++;
+    }
+    *n_out = (int32_t)out.size();
+    if ((int64_t)out.size() > cap) {
+        set_error("output array too small");
+        return CMGPU_EOVERFLOW;
+    }
+    std::copy(out.begin(), out.end(), envs);
+    return CMGPU_OK;
+}
+
+int cmgpu_final_stage_inside_opt(const cmgpu_model *mc, cmgpu_workspace *ws, const uint8_t *dsq, int32_t n,
+                                 const cmgpu_envelope *envs, int32_t nenv, float cutoff, int do_null3, int nonbanded,
+                                 cmgpu_hit *hits, int32_t cap, int32_t *n_out) {
+    cmgpu_model *m = const_cast<cmgpu_model *>(mc);
+    if (!m || !ws || !dsq || !n_out || n < 0 || nenv < 0 || (nenv > 0 && !envs) || (cap > 0 && !hits))
+        return CMGPU_EINVAL;
+    *n_out = 0;
+    std::vector<WinDesc> wins;
+    for (int32_t k = 0; k < nenv; k++) {
+        if (envs[k].start < 1 || envs[k].end > n) {
+            set_error("envelope outside the sequence");
+            return CMGPU_EINVAL;
+        }
+        wins.push_back(WinDesc{0, envs[k].start, envs[k].end});
+    }
+    if (wins.empty()) return CMGPU_OK;
+    int rc = stage_dsq(ws, dsq, (int64_t)n + 2);
+    if (rc) return rc;
+    std::vector<std::vector<cmgpu_hit>> hpw;
+    rc = run_scan(m, ws, CMGPU_INSIDE_I32, nonbanded ? CMGPU_NOQDB : CMGPU_QDB2, ws->d_dsq, dsq, (int64_t)n + 2,
+                  wins, cutoff, do_null3, false, hpw);
+    if (rc) return rc;
+    return finish_single(hpw, hits, cap, n_out);
+}
+
+static int batch_common(const cmgpu_model *mc, cmgpu_workspace *ws, int semiring, int qdbidx, const uint8_t *h_dsq,
+                        const uint8_t *d_dsq, int64_t dsq_len, const cmgpu_window *wins, int32_t nwin, float cutoff,
+                        int do_null3, bool plain, cmgpu_batch_hit *hits, int32_t cap, int32_t *n_out) {
+    cmgpu_model *m = const_cast<cmgpu_model *>(mc);
+    if (!m || !ws || !n_out || nwin < 0 || (nwin > 0 && !wins) || (cap > 0 && !hits)) return CMGPU_EINVAL;
+    *n_out = 0;
+    if (!check_windows(wins, nwin, dsq_len, h_dsq)) {
+        set_error("window outside the residue buffer, or residue code > 17");
+        return CMGPU_EINVAL;
+    }
+    if (nwin == 0) return CMGPU_OK;
+    std::vector<WinDesc> wv;
+    for (int32_t k = 0; k < nwin; k++) wv.push_back(WinDesc{wins[k].dsq_offset, wins[k].i0, wins[k].j0});
+    int rc;
+    if (h_dsq) {
+        if ((rc = stage_dsq(ws, h_dsq, dsq_len, false))) return rc;
+        d_dsq = ws->d_dsq;
+    }
+    std::vector<std::vector<cmgpu_hit>> hpw;
+    rc = run_scan(m, ws, semiring, qdbidx, d_dsq, h_dsq, dsq_len, wv, cutoff, do_null3, plain, hpw);
+    if (rc) return rc;
+    size_t n = 0;
+    for (auto &v : hpw) n += v.size();
+    *n_out = (int32_t)n;
+    if ((int64_t)n > cap) {
+        set_error("output array too small");
+        return CMGPU_EOVERFLOW;
+    }
+    size_t o = 0;
+    for (size_t w = 0; w < hpw.size(); w++)
+        for (auto &h : hpw[w]) hits[o++] = cmgpu_batch_hit{(int32_t)w, h.i, h.j, h.score, h.bias};
+    return CMGPU_OK;
+}
+
+int cmgpu_scan_batch(const cmgpu_model *m, cmgpu_workspace *ws, int semiring, int qdbidx, const uint8_t *dsq_all,
+                     int64_t dsq_len, const cmgpu_window *wins, int32_t nwin, float cutoff, int do_null3,
+                     cmgpu_batch_hit *hits, int32_t cap, int32_t *n_out) {
+    if (!dsq_all) return CMGPU_EINVAL;
+    return batch_common(m, ws, semiring, qdbidx, dsq_all, nullptr, dsq_len, wins, nwin, cutoff, do_null3, false, hits,
+                        cap, n_out);
+}
+
+int cmgpu_scan_batch_device(const cmgpu_model *m, cmgpu_workspace *ws, int semiring, int qdbidx,
+                            const uint8_t *d_dsq_all, int64_t dsq_len, const cmgpu_window *wins, int32_t nwin,
+                            float cutoff, int do_null3, cmgpu_batch_hit *hits, int32_t cap, int32_t *n_out) {
+    if (!d_dsq_all) return CMGPU_EINVAL;
+    return batch_common(m, ws, semiring, qdbidx, nullptr, d_dsq_all, dsq_len, wins, nwin, cutoff, do_null3, false,
+                        hits, cap, n_out);
+}
+
+int cmgpu_scan_plain(const cmgpu_model *m, cmgpu_workspace *ws, int semiring, int qdbidx, const uint8_t *dsq_all,
+                     int64_t dsq_len, const cmgpu_window *wins, int32_t nwin, float cutoff, int do_null3,
+                     cmgpu_batch_hit *hits, int32_t cap, int32_t *n_out) {
+    if (!dsq_all) return CMGPU_EINVAL;
+    return batch_common(m, ws, semiring, qdbidx, dsq_all, nullptr, dsq_len, wins, nwin, cutoff, do_null3, true, hits,
+                        cap, n_out);
+}
+
+}  // extern "C"

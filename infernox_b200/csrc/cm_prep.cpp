@@ -1,0 +1,443 @@
+// Host-side model preparation: turns a probability-level CM into the score
+// tables and query-dependent bands the scanner reads.
+//
+// Each routine follows the arithmetic of the reference routine it names
+// (operand types, rounding points and loop order), because every score it
+// produces feeds the bit-exact scan:
+//   logoddsify          src/cp9.rs:4263-4368  (CMLogoddsify + FCalcOptimizedEmitScores)
+//   integer scores      src/cm_nohmm.rs:279-369 (build_integer_scores)
+//   localisation        src/cp9.rs:4193-4258  (cm_config_local)
+//   QDB band engine     src/cm_qdband.rs:258-549, wrapper :554-592
+//   ILogsum / FLogsum   src/cp9.rs:28-44, :5391-5400
+// Compiled with -ffp-contract=off: no multiply-add is fused, as in Rust.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "cm_internal.h"
+#include "../../include/cmscan_gpu.h"
+
+using namespace cmx;
+
+namespace cmx {
+void set_error(const std::string &msg);
+}
+
+namespace {
+
+// Prob2Score of cm_nohmm (src/cm_nohmm.rs:27-33): floor(0.5 + 1000*log2(p/null)).
+int prob2score(float p, float null) {
+    if (p == 0.0f) return -INFTY;
+    return (int)std::floor(0.5 + INTSCALE * std::log2((double)p / (double)null));
+}
+
+// esl_abc_FAvgScore (src/cm.rs:84-96)
+float favg_score(int x, const float *sc) {
+    if (!is_residue(x)) return 0.0f;
+    float r = 0.0f;
+    for (int i = 0; i < K; i++)
+        if (degen(x, i)) r += sc[i];
+    return r / (float)ndegen(x);
+}
+
+// esl_abc_IAvgScore (src/cm.rs:101-117)
+int iavg_score(int x, const int *sc) {
+    if (!is_residue(x)) return 0;
+    float r = 0.0f;
+    for (int i = 0; i < K; i++)
+        if (degen(x, i)) r += (float)sc[i];
+    r /= (float)ndegen(x);
+    return r < 0.0f ? (int)(r - 0.5f) : (int)(r + 0.5f);
+}
+
+// esl_vec_FSum with Kahan compensation (src/cp9.rs:451-461)
+float kahan_fsum(const float *v, int n) {
+    float sum = 0.0f, c = 0.0f;
+    for (int i = 0; i < n; i++) {
+        float y = v[i] - c;
+        float t = sum + y;
+        c = (t - sum) - y;
+        sum = t;
+    }
+    return sum;
+}
+
+struct Model {
+    int M, nodes, clen;
+    std::vector<int8_t> sttype, stid, ndtype;
+    std::vector<int32_t> cfirst, cnum, nodemap;
+    std::vector<float> t, e, begin, end;
+    float null[4];
+    float el_selfsc, pbegin, pend;
+    uint32_t flags = 0;
+};
+
+Model load(const cmgpu_cm_params *p) {
+    Model m;
+    m.M = p->M;
+    m.nodes = p->nodes;
+    m.clen = p->clen;
+    m.sttype.assign(p->sttype, p->sttype + m.M);
+    m.stid.assign(p->stid, p->stid + m.M);
+    m.ndtype.assign(p->ndtype, p->ndtype + m.nodes);
+    m.cfirst.assign(p->cfirst, p->cfirst + m.M);
+    m.cnum.assign(p->cnum, p->cnum + m.M);
+    m.nodemap.assign(p->nodemap, p->nodemap + m.nodes);
+    m.t.assign(p->t, p->t + (size_t)m.M * MAXC);
+    m.e.assign(p->e, p->e + (size_t)m.M * 16);
+    m.begin.assign(m.M, 0.0f);
+    m.end.assign(m.M, 0.0f);
+    std::memcpy(m.null, p->null, sizeof(m.null));
+    m.el_selfsc = p->el_selfsc;
+    m.pbegin = p->pbegin;
+    m.pend = p->pend;
+    return m;
+}
+
+// cm_config_local (src/cp9.rs:4193-4258)
+void config_local(Model &cm) {
+    const float p_internal_start = cm.pbegin, p_internal_exit = cm.pend;
+    int nstarts = 0;
+    for (int nd = 2; nd < cm.nodes; nd++) {
+        int t = cm.ndtype[nd];
+        if (t == MATP_ND || t == MATL_ND || t == MATR_ND || t == BIF_ND) nstarts++;
+    }
+    std::fill(cm.begin.begin(), cm.begin.end(), 0.0f);
+    cm.begin[cm.nodemap[1]] = 1.0f - p_internal_start;
+    float p = p_internal_start / (float)nstarts;
+    for (int nd = 2; nd < cm.nodes; nd++) {
+        int t = cm.ndtype[nd];
+        if (t == MATP_ND || t == MATL_ND || t == MATR_ND || t == BIF_ND) cm.begin[cm.nodemap[nd]] = p;
+    }
+    for (int y = 0; y < cm.cnum[0]; y++) cm.t[y] = 0.0f;  // state 0 row
+    cm.flags |= 1u << 10;
+
+    auto is_exit = [&](int nd) {
+        int t = cm.ndtype[nd];
+        return (t == MATP_ND || t == MATL_ND || t == MATR_ND || t == BEGL_ND || t == BEGR_ND) &&
+               cm.ndtype[nd + 1] != END_ND;
+    };
+    int nexits = 0;
+    for (int nd = 1; nd < cm.nodes; nd++)
+        if (is_exit(nd)) nexits++;
+    std::fill(cm.end.begin(), cm.end.end(), 0.0f);
+    for (int nd = 1; nd < cm.nodes; nd++) {
+        if (!is_exit(nd)) continue;
+        int v = cm.nodemap[nd];
+        cm.end[v] = p_internal_exit / (float)nexits;
+        int cnum = cm.cnum[v];
+        float denom = kahan_fsum(&cm.t[(size_t)v * MAXC], cnum);
+        denom += cm.end[v];
+        float inv = 1.0f / denom;
+        for (int x = 0; x < cnum; x++) cm.t[(size_t)v * MAXC + x] *= inv;
+    }
+    cm.flags |= 1u << 11;
+}
+
+// cm_logoddsify (src/cp9.rs:4263-4368), scan-relevant outputs.
+void logoddsify(const Model &cm, cmgpu_cm_scores *o) {
+    for (int v = 0; v < cm.M; v++) {
+        int st = cm.sttype[v];
+        float *tsc = o->tsc + (size_t)v * MAXC;
+        float *oesc = o->oesc + (size_t)v * ESC;
+        for (int x = 0; x < MAXC; x++) tsc[x] = IMPOSSIBLE;
+        for (int x = 0; x < ESC; x++) oesc[x] = IMPOSSIBLE;
+        if (st != B_ST && st != E_ST) {
+            for (int x = 0; x < cm.cnum[v]; x++)
+                tsc[x] = (float)sre_log2((double)cm.t[(size_t)v * MAXC + x]);
+        }
+        const float *e = &cm.e[(size_t)v * 16];
+        if (st == MP_ST) {
+            float esc[16];
+            for (int x = 0; x < K; x++)
+                for (int y = 0; y < K; y++) {
+                    float arg = e[x * K + y] / (cm.null[x] * cm.null[y]);
+                    esc[x * K + y] = (float)sre_log2((double)arg);
+                }
+            for (int a = 0; a < K; a++)
+                for (int b = 0; b < K; b++) oesc[a * KP + b] = esc[a * K + b];
+            for (int a = K + 1; a < KP - 1; a++)
+                for (int b = 0; b < K; b++) {
+                    float sc = 0.0f;
+                    for (int l = 0; l < K; l++) sc += esc[l * K + b] * fcount_frac(a, l);
+                    oesc[a * KP + b] = sc;
+                }
+            for (int a = 0; a < K; a++)
+                for (int b = K + 1; b < KP - 1; b++) {
+                    float sc = 0.0f;
+                    for (int r = 0; r < K; r++) sc += esc[a * K + r] * fcount_frac(b, r);
+                    oesc[a * KP + b] = sc;
+                }
+            for (int a = K + 1; a < KP - 1; a++)
+                for (int b = K + 1; b < KP - 1; b++) {
+                    float sc = 0.0f;
+                    for (int l = 0; l < K; l++)
+                        for (int r = 0; r < K; r++)
+                            sc += esc[l * K + r] * fcount_frac(a, l) * fcount_frac(b, r);
+                    oesc[a * KP + b] = sc;
+                }
+        } else if (st == ML_ST || st == MR_ST || st == IL_ST || st == IR_ST) {
+            float esc[K];
+            for (int x = 0; x < K; x++) {
+                float arg = e[x] / cm.null[x];
+                esc[x] = (float)sre_log2((double)arg);
+            }
+            for (int a = 0; a < K; a++) oesc[a] = esc[a];
+            for (int a = K + 1; a < KP - 1; a++) oesc[a] = favg_score(a, esc);
+        }
+        o->beginsc[v] = (float)sre_log2((double)cm.begin[v]);
+        o->endsc[v] = (float)sre_log2((double)cm.end[v]);
+    }
+}
+
+// build_integer_scores (src/cm_nohmm.rs:279-369)
+void integer_scores(const Model &cm, float el_selfsc, cmgpu_cm_scores *o) {
+    for (int v = 0; v < cm.M; v++) {
+        int st = cm.sttype[v];
+        int32_t *itsc = o->itsc + (size_t)v * MAXC;
+        int32_t *ioesc = o->ioesc + (size_t)v * ESC;
+        for (int x = 0; x < MAXC; x++) itsc[x] = -INFTY;
+        for (int x = 0; x < ESC; x++) ioesc[x] = -INFTY;
+        if (st != B_ST && st != E_ST)
+            for (int x = 0; x < cm.cnum[v]; x++) itsc[x] = prob2score(cm.t[(size_t)v * MAXC + x], 1.0f);
+        const float *e = &cm.e[(size_t)v * 16];
+        if (st == MP_ST) {
+            int iesc[16];
+            for (int a = 0; a < K; a++)
+                for (int b = 0; b < K; b++) iesc[a * K + b] = prob2score(e[a * K + b], cm.null[a] * cm.null[b]);
+            for (int a = 0; a < K; a++)
+                for (int b = 0; b < K; b++) ioesc[a * KP + b] = iesc[a * K + b];
+            for (int a = K + 1; a < KP - 1; a++)
+                for (int b = 0; b < K; b++) {
+                    float sc = 0.0f;
+                    for (int l = 0; l < K; l++) sc += (float)iesc[l * K + b] * fcount_frac(a, l);
+                    ioesc[a * KP + b] = (int)sc;
+                }
+            for (int a = 0; a < K; a++)
+                for (int b = K + 1; b < KP - 1; b++) {
+                    float sc = 0.0f;
+                    for (int r = 0; r < K; r++) sc += (float)iesc[a * K + r] * fcount_frac(b, r);
+                    ioesc[a * KP + b] = (int)sc;
+                }
+            for (int a = K + 1; a < KP - 1; a++)
+                for (int b = K + 1; b < KP - 1; b++) {
+                    float sc = 0.0f;
+                    for (int l = 0; l < K; l++)
+                        for (int r = 0; r < K; r++)
+                            sc += (float)iesc[l * K + r] * fcount_frac(a, l) * fcount_frac(b, r);
+                    ioesc[a * KP + b] = (int)sc;
+                }
+        } else if (st == ML_ST || st == MR_ST || st == IL_ST || st == IR_ST) {
+            int iesc[K];
+            for (int a = 0; a < K; a++) iesc[a] = prob2score(e[a], cm.null[a]);
+            for (int a = 0; a < K; a++) ioesc[a] = iesc[a];
+            for (int a = K + 1; a < KP - 1; a++) ioesc[a] = iavg_score(a, iesc);
+        }
+        o->ibeginsc[v] = prob2score(cm.begin[v], 1.0f);
+        o->iendsc[v] = prob2score(cm.end[v], 1.0f);
+    }
+    o->iel_selfsc = prob2score(std::pow(2.0f, el_selfsc), 1.0f);
+}
+
+// BandTruncationNegligible (src/cm_qdband.rs:217-242)
+bool band_truncation_negligible(const std::vector<double> &density, size_t b, size_t z) {
+    if (b + 1 >= z) return false;
+    double c = 0.0;
+    for (size_t i = b + 1; i <= z; i++) c += density[i];
+    double logbeta = (std::log(density[z]) - std::log(density[b + 1])) / (double)(z - b - 1);
+    double beta = std::exp(logbeta);
+    double d = (beta / (1.0 - beta)) * density[z];
+    return d < c * 2.220446049250313e-16;
+}
+
+struct BandResult {
+    int W;
+    std::vector<int32_t> dmin1, dmax1, dmin2, dmax2;
+};
+
+// band_calculation_engine (src/cm_qdband.rs:258-549) on a global-config
+// model; returns 1 when Z is too small (the caller doubles Z), 0 on success.
+int band_engine(const Model &cm, size_t z, double beta1, double beta2, double beta_w, BandResult &r) {
+    const int m = cm.M;
+    double max_beta = std::max(std::max(beta_w, beta1), beta2);
+    std::vector<float> tc((size_t)m * MAXC, 0.0f);
+    for (int v = 0; v < m; v++)
+        for (int k = 0; k < std::min(cm.cnum[v], MAXC); k++) tc[(size_t)v * MAXC + k] = cm.t[(size_t)v * MAXC + k];
+    // local begin probabilities (src/cm_qdband.rs:151-183)
+    std::vector<float> begin_copy(m, 0.0f);
+    {
+        int nstarts = 0;
+        for (int nd = 2; nd < cm.nodes; nd++) {
+            int t = cm.ndtype[nd];
+            if (t == MATP_ND || t == MATL_ND || t == MATR_ND || t == BIF_ND) nstarts++;
+        }
+        double pis = (double)cm.pbegin;
+        if (cm.nodes > 1) begin_copy[cm.nodemap[1]] = (float)(1.0 - pis);
+        if (nstarts > 0) {
+            float p = (float)(pis / (double)nstarts);
+            for (int nd = 2; nd < cm.nodes; nd++) {
+                int t = cm.ndtype[nd];
+                if (t == MATP_ND || t == MATL_ND || t == MATR_ND || t == BIF_ND) begin_copy[cm.nodemap[nd]] = p;
+            }
+        }
+    }
+    std::vector<std::vector<double>> gamma(m, std::vector<double>(z + 1, 0.0));
+    gamma[m - 1][0] = 1.0;
+    r.dmin1.assign(m, 0);
+    r.dmin2.assign(m, 0);
+    r.dmax1.assign(m, cm.clen * 2);
+    r.dmax2.assign(m, cm.clen * 2);
+    int w = 0;
+    for (int v = m - 1; v >= 0; v--) {
+        int st = cm.sttype[v];
+        if (st == E_ST) {
+            gamma[v][0] = 1.0;
+            r.dmin1[v] = r.dmax1[v] = r.dmin2[v] = r.dmax2[v] = 0;
+            continue;
+        }
+        double pdf = 0.0;
+        std::vector<double> &gv = gamma[v];
+        if (st == B_ST) {
+            const std::vector<double> &gl = gamma[cm.cfirst[v]];
+            const std::vector<double> &gr = gamma[cm.cnum[v]];
+            for (size_t n = 0; n <= z; n++) {
+                for (size_t ln = 0; ln <= n; ln++) gv[n] += gl[ln] * gr[n - ln];
+                pdf += gv[n];
+            }
+        } else if (v != 0) {
+            size_t dv = (size_t)state_delta(st);
+            int cf = cm.cfirst[v], cn = cm.cnum[v];
+            // Element-wise the accumulation is over yoffset ascending in both
+            // forms of the reference (src/cm_qdband.rs:368-399).
+            for (size_t n = dv; n <= z; n++) {
+                for (int yo = 0; yo < cn; yo++) {
+                    int y = cf + yo;
+                    gv[n] += (double)tc[(size_t)v * MAXC + yo] * gamma[y][n - dv];
+                }
+                pdf += gv[n];
+            }
+        }
+        if (begin_copy[v] > 0.0f && v != 0) {
+            for (size_t n = 0; n <= z; n++) gamma[0][n] += (double)begin_copy[v] * gv[n];
+        }
+        if (v == 0) {
+            pdf = 0.0;
+            for (size_t n = 0; n <= z; n++) pdf += gamma[0][n];
+        }
+        if (pdf <= 0.999 || gv[z] > max_beta * 2.220446049250313e-16) return 1;
+        if (pdf > 1.0)
+            for (double &x : gv) x /= pdf;
+        {
+            double cum = 0.0;
+            bool set2 = false;
+            for (size_t n = 0; n <= z; n++) {
+                cum += gv[n];
+                if (!set2 && cum > beta2) {
+                    r.dmin2[v] = (int)n;
+                    set2 = true;
+                }
+                if (set2 && cum > beta1) {
+                    r.dmin1[v] = (int)n;
+                    break;
+                }
+            }
+            cum = 0.0;
+            set2 = false;
+            for (size_t n = z + 1; n-- > 0;) {
+                cum += gv[n];
+                if (!set2 && cum > beta2) {
+                    r.dmax2[v] = (int)n;
+                    set2 = true;
+                }
+                if (set2 && cum > beta1) {
+                    r.dmax1[v] = (int)n;
+                    break;
+                }
+            }
+        }
+        if (v == 0) {
+            double cum = 0.0;
+            for (size_t n = z + 1; n-- > 0;) {
+                cum += gamma[0][n];
+                if (cum > beta_w) {
+                    w = (int)n;
+                    break;
+                }
+            }
+        }
+    }
+    if (!band_truncation_negligible(gamma[0], (size_t)w, z)) return 1;
+    if (!band_truncation_negligible(gamma[0], (size_t)r.dmax1[0], z)) return 1;
+    if (!band_truncation_negligible(gamma[0], (size_t)r.dmax2[0], z)) return 1;
+    r.W = w;
+    return 0;
+}
+
+}  // namespace
+
+extern "C" int cmgpu_prep_configure(const cmgpu_cm_params *p, int local, int32_t W_in, double beta1,
+                                    double beta2, double betaW, cmgpu_cm_scores *out) {
+    if (!p || !out || p->M < 2 || p->nodes < 2 || !p->sttype || !p->t || !p->e) {
+        cmx::set_error("cmgpu_prep_configure: bad arguments");
+        return CMGPU_EINVAL;
+    }
+    if (beta2 - beta1 > 1e-20) {
+        cmx::set_error("cmgpu_prep_configure: beta1 must be >= beta2");
+        return CMGPU_EINVAL;
+    }
+    Model cm = load(p);
+    // QDB bands + W on the un-localised model (src/cm_search.rs:899-912,
+    // src/cm_qdband.rs:554-592).
+    BandResult br;
+    size_t z = (size_t)cm.clen * 4;
+    for (;;) {
+        int rc = band_engine(cm, z, beta1, beta2, betaW, br);
+        if (rc == 0) break;
+        z *= 2;
+        if (z > (size_t)cm.clen * 1000) {
+            cmx::set_error("cmgpu_prep_configure: QDB band calculation: Z got insanely large (> 1000*clen)");
+            return CMGPU_ERANGE;
+        }
+    }
+    int W = W_in > 0 ? W_in : br.W;
+    std::copy(br.dmin1.begin(), br.dmin1.end(), out->dmin1);
+    std::copy(br.dmax1.begin(), br.dmax1.end(), out->dmax1);
+    std::copy(br.dmin2.begin(), br.dmin2.end(), out->dmin2);
+    std::copy(br.dmax2.begin(), br.dmax2.end(), out->dmax2);
+
+    float el = cm.el_selfsc;
+    if (local) {
+        // cm_configure_scores (src/cp9.rs:4538-4545)
+        config_local(cm);
+    }
+    if (el * (float)W < IMPOSSIBLE) el = IMPOSSIBLE / ((float)W + 1.0f);
+    logoddsify(cm, out);
+    integer_scores(cm, el, out);
+    if (out->t_local) std::copy(cm.t.begin(), cm.t.end(), out->t_local);
+    out->el_selfsc = el;
+    out->W = W;
+    out->flags = cm.flags;
+    return CMGPU_OK;
+}
+
+// init_ilogsum (src/cp9.rs:28-44): rint(1000 * log2(1 + 2^(-i/1000))).
+extern "C" int cmgpu_ilogsum_table(int32_t *tbl, int32_t n) {
+    if (!tbl || n < 0 || n > LOGSUM_TBL) return CMGPU_EINVAL;
+    for (int i = 0; i < n; i++) {
+        double v = INTSCALE * std::log2(1.0 + std::pow(2.0, -(double)i / INTSCALE));
+        tbl[i] = (int32_t)std::nearbyint(v);
+    }
+    return CMGPU_OK;
+}
+
+// flogsum_lookup (src/cp9.rs:5391-5400): sreLOG2(1 + sreEXP2(-i/1000)).
+extern "C" int cmgpu_flogsum_table(float *tbl, int32_t n) {
+    if (!tbl || n < 0 || n > LOGSUM_TBL) return CMGPU_EINVAL;
+    for (int i = 0; i < n; i++) {
+        double ex = std::exp((-(double)i / 1000.0) * 0.69314718);
+        tbl[i] = (float)sre_log2(1.0 + ex);
+    }
+    return CMGPU_OK;
+}

@@ -1,0 +1,311 @@
+// Builds the device plan (qdb_plan.h) of a configured CM for one semiring
+// and band set, and counts the exact DP work of a scan.
+//
+// Band selection and per-state dn/dxcap follow generic_scan
+// (src/cm_nohmm.rs:431-456); the d = 0 base values follow the reference's
+// scan-matrix initialisation (src/cm_nohmm.rs:489-537); el_sca is built by
+// repeated addition (src/cm_nohmm.rs:471-474).
+#include <algorithm>
+#include <cstring>
+#include <string>
+
+#include "../../include/cmscan_gpu.h"
+#include "cm_internal.h"
+#include "qdb_plan.h"
+
+namespace cmx {
+
+void set_error(const std::string &msg);
+
+namespace {
+
+inline uint32_t fbits(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    return u;
+}
+inline float bitsf(uint32_t u) {
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+inline int32_t wadd(int32_t a, int32_t b) { return (int32_t)((uint32_t)a + (uint32_t)b); }
+
+struct Bands {
+    std::vector<int32_t> dmin, dmax, dn, dxcap;
+};
+
+Bands select_bands(const cmgpu_cm *cm, int qdbidx) {
+    Bands b;
+    const int M = cm->M, W = cm->W;
+    b.dmin.resize(M);
+    b.dmax.resize(M);
+    b.dn.resize(M);
+    b.dxcap.resize(M);
+    for (int v = 0; v < M; v++) {
+        if (qdbidx == CMGPU_NOQDB) {
+            b.dmin[v] = 0;
+            b.dmax[v] = W;
+        } else if (qdbidx == CMGPU_QDB1) {
+            b.dmin[v] = cm->dmin1[v];
+            b.dmax[v] = cm->dmax1[v];
+        } else {
+            b.dmin[v] = cm->dmin2[v];
+            b.dmax[v] = cm->dmax2[v];
+        }
+        int base = cm->sttype[v] == MP_ST ? 2 : 1;
+        int dn = std::max(b.dmin[v], base);
+        if (dn > W) dn = W;
+        b.dn[v] = dn;
+        b.dxcap[v] = std::min(b.dmax[v], W);
+    }
+    return b;
+}
+
+}  // namespace
+
+bool build_plan(const cmgpu_cm *cm, int semiring, int qdbidx, Plan &p) {
+    const int M = cm->M, W = cm->W;
+    if (M < 2 || W < 1 || M > 32767 || W > 32000) {
+        set_error("model too large for the scan plan (M <= 32767, W <= 32000)");
+        return false;
+    }
+    const bool inside = semiring == CMGPU_INSIDE_I32;
+    p = Plan();
+    p.M = M;
+    p.W = W;
+    p.semiring = semiring;
+    p.qdbidx = qdbidx;
+    p.local = (cm->flags & (1u << 10)) != 0;
+    Bands b = select_bands(cm, qdbidx);
+
+    const uint32_t ZERO = inside ? (uint32_t)(-INFTY) : fbits(IMPOSSIBLE);
+    auto add = [&](uint32_t a, uint32_t c) -> uint32_t {
+        if (inside) return (uint32_t)wadd((int32_t)a, (int32_t)c);
+        return fbits(bitsf(a) + bitsf(c));
+    };
+    auto vmax = [&](uint32_t a, uint32_t c) -> uint32_t {
+        if (inside) return (int32_t)a >= (int32_t)c ? a : c;
+        return bitsf(a) >= bitsf(c) ? a : c;
+    };
+    auto possible_bits = [&](uint32_t x) -> bool {
+        // not_impossible(scbits(x)) (src/cm_nohmm.rs:20-22, :148-150)
+        if (inside) {
+            int32_t s = (int32_t)x;
+            if (s == -INFTY) return false;
+            float f = (float)((double)s / INTSCALE);
+            return f > IMPOSSIBLE + 1.0f;
+        }
+        return bitsf(x) > IMPOSSIBLE + 1.0f;
+    };
+    auto begin_possible = [&](uint32_t x) -> bool {
+        // Sr::is_possible: NOT_IMPOSSIBLE for f32, != -INFTY for i32
+        if (inside) return (int32_t)x != -INFTY;
+        return bitsf(x) > IMPOSSIBLE + 1.0f;
+    };
+
+    // score tables
+    p.tsc.assign((size_t)M * MAXC, ZERO);
+    p.endsc.assign(M, ZERO);
+    p.beginsc.assign(M, ZERO);
+    p.esc.assign((size_t)M * ESC, ZERO);
+    for (int v = 0; v < M; v++) {
+        for (int x = 0; x < MAXC; x++)
+            p.tsc[(size_t)v * MAXC + x] = inside ? (uint32_t)cm->itsc[(size_t)v * MAXC + x]
+                                                 : fbits(cm->tsc[(size_t)v * MAXC + x]);
+        p.endsc[v] = inside ? (uint32_t)cm->iendsc[v] : fbits(cm->endsc[v]);
+        p.beginsc[v] = inside ? (uint32_t)cm->ibeginsc[v] : fbits(cm->beginsc[v]);
+        for (int x = 0; x < ESC; x++)
+            p.esc[(size_t)v * ESC + x] =
+                inside ? (uint32_t)cm->ioesc[(size_t)v * ESC + x] : fbits(cm->oesc[(size_t)v * ESC + x]);
+    }
+    const uint32_t el_self = inside ? (uint32_t)cm->iel_selfsc : fbits(cm->el_selfsc);
+    p.el_sca.assign((size_t)W + 1, 0u);
+    p.el_sca[0] = inside ? 0u : fbits(0.0f);
+    for (int d = 1; d <= W; d++) p.el_sca[d] = add(p.el_sca[d - 1], el_self);
+
+    // d = 0 base values (src/cm_nohmm.rs:489-537)
+    p.init0.assign(M, ZERO);
+    for (int v = M - 1; v >= 0; v--) {
+        int st = cm->sttype[v];
+        if (st == E_ST) {
+            p.init0[v] = inside ? 0u : fbits(0.0f);
+        } else if (st == S_ST || st == D_ST) {  // includes BEGL_S
+            uint32_t a0 = p.endsc[v];
+            for (int yo = 0; yo < cm->cnum[v]; yo++)
+                a0 = vmax(a0, add(p.init0[cm->cfirst[v] + yo], p.tsc[(size_t)v * MAXC + yo]));
+            a0 = vmax(a0, ZERO);
+            p.init0[v] = a0;
+        } else if (st == B_ST) {
+            p.init0[v] = add(p.init0[cm->cfirst[v]], p.init0[cm->cnum[v]]);
+        } else {
+            p.init0[v] = ZERO;
+        }
+    }
+
+    // states, deck layout
+    p.states.assign(M, StateDev());
+    int64_t off = 0;
+    for (int v = 0; v < M; v++) {
+        StateDev &s = p.states[v];
+        int st = cm->sttype[v];
+        s.type = (uint8_t)st;
+        s.flags = 0;
+        s.cfirst = (int16_t)cm->cfirst[v];
+        s.cnum = (int16_t)cm->cnum[v];
+        s.dn = (int16_t)b.dn[v];
+        s.dxcap = (int16_t)b.dxcap[v];
+        int width = std::max(0, b.dxcap[v] - b.dn[v] + 1);
+        if (st == E_ST || v == 0) width = 0;  // E cells are constants; ROOT_S is never read
+        s.width = (int16_t)width;
+        s.esc_off = v * ESC;
+        if (cm->stid[v] == BEGL_S) s.flags |= SF_BEGL;
+        if (right_emitter(st)) s.flags |= SF_TWO_SLOT;
+        if (possible_bits(p.endsc[v])) s.flags |= SF_ENDSC;
+        if (p.local && v >= 1 && begin_possible(p.beginsc[v])) s.flags |= SF_BEGIN;
+        if (st == B_ST) {
+            int wl = cm->cfirst[v], y = cm->cnum[v];
+            s.kdn_y = (int16_t)std::min(b.dmin[y], W);
+            s.kdx_y = (int16_t)std::min(b.dmax[y], W);
+            s.kdn_w = (int16_t)std::min(b.dmin[wl], W);
+            s.kdx_w = (int16_t)std::min(b.dmax[wl], W);
+        }
+        int64_t slots = (s.flags & SF_BEGL) ? (int64_t)W + 1 : (s.flags & SF_TWO_SLOT) ? 2 : 1;
+        s.base = (int32_t)(off - s.dn);
+        off += slots * width;
+        if (off > (int64_t)1 << 30) {
+            set_error("deck exceeds 2^30 cells");
+            return false;
+        }
+    }
+    p.deck_elems = off;
+    p.root_dn = b.dn[0];
+    p.root_dxcap = b.dxcap[0];
+    p.root_cfirst = cm->cfirst[0];
+    p.root_cnum = cm->cnum[0];
+    for (int v = 1; v < M; v++)
+        if (p.states[v].flags & SF_BEGIN) p.begin_states.push_back(v);
+
+    // levels: right emitters read only the previous column -> level 0; every
+    // other state sits one level above its deepest same-column child.
+    std::vector<int> level(M, -1);
+    int nlev = 1;
+    for (int v = M - 1; v >= 1; v--) {
+        int st = cm->sttype[v];
+        if (st == E_ST) continue;
+        if (right_emitter(st)) {
+            level[v] = 0;
+            continue;
+        }
+        int lv = 1;
+        if (st == B_ST) {
+            lv = std::max(lv, level[cm->cfirst[v]] + 1);
+            lv = std::max(lv, level[cm->cnum[v]] + 1);
+        } else {
+            for (int yo = 0; yo < cm->cnum[v]; yo++) {
+                int y = cm->cfirst[v] + yo;
+                if (y == v || cm->sttype[y] == E_ST) continue;
+                lv = std::max(lv, level[y] + 1);
+            }
+        }
+        level[v] = lv;
+        nlev = std::max(nlev, lv + 1);
+    }
+    p.level_start.assign(1, 0);
+    p.chunks.clear();
+    for (int l = 0; l < nlev; l++) {
+        std::vector<std::pair<double, ChunkDev>> lc;
+        for (int v = 1; v < M; v++) {
+            if (level[v] != l) continue;
+            const StateDev &s = p.states[v];
+            if (s.width <= 0) continue;
+            int st = s.type;
+            if (st == IL_ST) {
+                lc.push_back({1e9 + s.width, ChunkDev{v, -1}});
+            } else {
+                for (int d0 = s.dn; d0 <= s.dxcap; d0 += 32) {
+                    double cost = st == B_ST ? 1e6 + d0 : (double)s.cnum;
+                    lc.push_back({cost, ChunkDev{v, d0}});
+                }
+            }
+        }
+        std::stable_sort(lc.begin(), lc.end(),
+                         [](const std::pair<double, ChunkDev> &a, const std::pair<double, ChunkDev> &c) {
+                             return a.first > c.first;
+                         });
+        for (auto &x : lc) p.chunks.push_back(x.second);
+        p.max_level_chunks = std::max(p.max_level_chunks, (int)lc.size());
+        p.level_start.push_back((int32_t)p.chunks.size());
+    }
+    return true;
+}
+
+// Exact cells / terms of one column at row limit jrow, counted the way the
+// oracle's counters count them.
+void count_column(const cmgpu_cm *cm, const Plan &p, const Bands &b, int jrow, double &cells, double &terms) {
+    const int M = cm->M, W = cm->W;
+    for (int v = 1; v < M; v++) {
+        int st = cm->sttype[v];
+        if (st == E_ST) continue;
+        int dn = b.dn[v], dx = std::min(jrow, b.dxcap[v]);
+        if (dx < dn) continue;
+        int n = dx - dn + 1;
+        cells += n;
+        if (st == B_ST) {
+            int wl = cm->cfirst[v], y = cm->cnum[v];
+            int dn_y = std::min(b.dmin[y], W), dx_y = std::min(b.dmax[y], W);
+            int dn_w = std::min(b.dmin[wl], W), dx_w = std::min(b.dmax[wl], W);
+            for (int d = dn; d <= dx; d++) {
+                int kmin = std::max(0, std::max(dn_y, d - dx_w));
+                int kmax = std::min(dx_y, d - dn_w);
+                if (kmax >= kmin) terms += kmax - kmin + 1;
+            }
+        } else {
+            terms += (double)n * cm->cnum[v];
+        }
+    }
+    int dn0 = b.dn[0], dx0 = std::min(jrow, b.dxcap[0]);
+    if (dx0 >= dn0) {
+        cells += dx0 - dn0 + 1;
+        terms += (double)(dx0 - dn0 + 1) * cm->cnum[0];
+        for (int y : p.begin_states) {
+            int dn = std::max(dn0, b.dn[y]);
+            int dx = std::min(dx0, std::min(jrow, b.dxcap[y]));
+            if (dx >= dn) terms += dx - dn + 1;
+        }
+    }
+}
+
+void count_column_public(const cmgpu_cm *cm, const Plan &p, int qdbidx, int jrow, double &cells, double &terms) {
+    Bands b = select_bands(cm, qdbidx);
+    count_column(cm, p, b, jrow, cells, terms);
+}
+
+bool count_work(const cmgpu_cm *cm, int semiring, int qdbidx, int64_t L, double &cells, double &terms) {
+    Plan p;
+    if (!build_plan(cm, semiring, qdbidx, p)) return false;
+    Bands b = select_bands(cm, qdbidx);
+    cells = terms = 0;
+    const int W = cm->W;
+    int64_t warm = std::min<int64_t>(L, W - 1);
+    for (int64_t j = 1; j <= warm; j++) count_column(cm, p, b, (int)j, cells, terms);
+    if (L > warm) {
+        double c = 0, t = 0;
+        count_column(cm, p, b, W, c, t);
+        cells += c * (double)(L - warm);
+        terms += t * (double)(L - warm);
+    }
+    return true;
+}
+
+}  // namespace cmx
+
+extern "C" int cmgpu_count_work(const cmgpu_cm *cm, int semiring, int qdbidx, int32_t L, double *cells,
+                                double *terms) {
+    if (!cm || !cells || !terms || L < 0) return CMGPU_EINVAL;
+    double c = 0, t = 0;
+    if (L > 0 && !cmx::count_work(cm, semiring, qdbidx, L, c, t)) return CMGPU_EINVAL;
+    *cells = c;
+    *terms = t;
+    return CMGPU_OK;
+}

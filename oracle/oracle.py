@@ -1,0 +1,124 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes binding of the oracle (qdb_oracle.c).
+
+Used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as
+the checker of the GPU scanner.  The product package never imports it.
+Build with `make -C oracle` (or oracle.build()).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+
+HIT_DTYPE = np.dtype([("i", np.int32), ("j", np.int32), ("score", np.float32), ("bias", np.float32)])
+ENV_DTYPE = np.dtype([("start", np.int32), ("end", np.int32)])
+
+_lib = None
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(
+                os.path.join(HERE, "qdb_oracle.c")):
+            build()
+        L = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        P = C.POINTER
+        L.oracle_qdb_scan.argtypes = [vp, C.c_int, C.c_int, P(C.c_uint8), C.c_int32, C.c_int32,
+                                      C.c_float, C.c_int, vp, C.c_int32, P(C.c_int32), vp, vp, vp,
+                                      C.c_int32, P(C.c_int32), P(C.c_double), P(C.c_double)]
+        L.oracle_cyk_seq_filter.argtypes = [vp, P(C.c_uint8), C.c_int32, C.c_float, C.c_int, vp,
+                                            C.c_int32, P(C.c_int32)]
+        L.oracle_final_stage_inside_opt.argtypes = [vp, P(C.c_uint8), vp, C.c_int32, C.c_float,
+                                                    C.c_int, C.c_int, vp, C.c_int32, P(C.c_int32)]
+        L.oracle_ilogsum_table.argtypes = [P(C.c_int32), C.c_int]
+        L.oracle_ilogsum.argtypes = [C.c_int32, C.c_int32]
+        L.oracle_ilogsum.restype = C.c_int32
+        _lib = L
+    return _lib
+
+
+def _u8(a):
+    a = np.ascontiguousarray(a, np.uint8)
+    return a, a.ctypes.data_as(C.POINTER(C.c_uint8))
+
+
+def qdb_scan(cm, semiring, qdbidx, dsq, i0, j0, cutoff, do_null3, want_cands=False):
+    """generic_scan restated: returns (hits, cands, cells, terms)."""
+    L = lib()
+    a, pa = _u8(dsq)
+    cap = max(64, (j0 - i0 + 1) + 64)
+    hits = np.zeros(cap, HIT_DTYPE)
+    n = C.c_int32()
+    cells, terms = C.c_double(), C.c_double()
+    ccap = 0
+    cj = cd = cs = None
+    ncand = C.c_int32()
+    if want_cands:
+        ccap = max(1024, (j0 - i0 + 1) * (cm.W + 2))
+        cj = np.zeros(ccap, np.int32)
+        cd = np.zeros(ccap, np.int32)
+        cs = np.zeros(ccap, np.float32)
+    rc = L.oracle_qdb_scan(C.byref(cm.as_struct()), semiring, qdbidx, pa, i0, j0, float(cutoff),
+                           int(bool(do_null3)), hits.ctypes.data, cap, C.byref(n),
+                           cj.ctypes.data if want_cands else None,
+                           cd.ctypes.data if want_cands else None,
+                           cs.ctypes.data if want_cands else None, ccap,
+                           C.byref(ncand) if want_cands else None, C.byref(cells), C.byref(terms))
+    if rc != 0:
+        raise RuntimeError(f"oracle overflow rc={rc}")
+    out = [(int(h["i"]), int(h["j"]), float(h["score"]), float(h["bias"])) for h in hits[: n.value]]
+    cands = None
+    if want_cands:
+        k = ncand.value
+        cands = list(zip(cj[:k].tolist(), cd[:k].tolist(), cs[:k].tolist()))
+    return out, cands, cells.value, terms.value
+
+
+def cyk_seq_filter(cm, dsq, n, cutoff, do_null3):
+    L = lib()
+    a, pa = _u8(dsq)
+    cap = 4096
+    envs = np.zeros(cap, ENV_DTYPE)
+    nout = C.c_int32()
+    rc = L.oracle_cyk_seq_filter(C.byref(cm.as_struct()), pa, n, float(cutoff), int(bool(do_null3)),
+                                 envs.ctypes.data, cap, C.byref(nout))
+    if rc != 0:
+        raise RuntimeError("oracle envelope overflow")
+    return [(int(e["start"]), int(e["end"])) for e in envs[: nout.value]]
+
+
+def final_stage_inside_opt(cm, dsq, envs, cutoff, do_null3, nonbanded):
+    L = lib()
+    a, pa = _u8(dsq)
+    ev = np.asarray([tuple(e) for e in envs], ENV_DTYPE) if len(envs) else np.zeros(1, ENV_DTYPE)
+    cap = 1 << 16
+    hits = np.zeros(cap, HIT_DTYPE)
+    nout = C.c_int32()
+    rc = L.oracle_final_stage_inside_opt(C.byref(cm.as_struct()), pa, ev.ctypes.data, len(envs),
+                                         float(cutoff), int(bool(do_null3)), int(bool(nonbanded)),
+                                         hits.ctypes.data, cap, C.byref(nout))
+    if rc != 0:
+        raise RuntimeError("oracle hit overflow")
+    return [(int(h["i"]), int(h["j"]), float(h["score"]), float(h["bias"])) for h in hits[: nout.value]]
+
+
+def ilogsum_table(n=23000):
+    t = np.zeros(n, np.int32)
+    lib().oracle_ilogsum_table(t.ctypes.data_as(C.POINTER(C.c_int32)), n)
+    return t
+
+
+def ilogsum(a, b):
+    return int(lib().oracle_ilogsum(a, b))

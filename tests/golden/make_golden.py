@@ -1,0 +1,81 @@
+"""Regenerates the fixtures in tests/golden/.
+
+* ilogsum_kat.json, state_delta_kat.json: the known answers of the
+  reference's own unit tests, parsed from its sources (src/cp9.rs tests
+  `ilogsum_sentinel_and_bounds`, `ilogsum_table_matches_c_dump`,
+  `ilogsum_table_endpoints_match_c_formula`; src/cm_qdband.rs
+  `test_state_delta`).  Needs the reference checkout (REFERENCE_ROOT, default
+  /root/reference); run it only where that exists.
+* scan_small.json: the oracle's hits on one fixed seeded model and sequence,
+  a regression lock for the oracle itself.
+
+Usage: python tests/golden/make_golden.py
+"""
+import json
+import os
+import re
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+REF = os.environ.get("REFERENCE_ROOT", "/root/reference")
+
+
+def ilogsum_kats():
+    src = open(os.path.join(REF, "src", "cp9.rs")).read()
+    body = src[src.index("fn ilogsum_table_matches_c_dump"):]
+    body = body[: body.index("}\n\n")]
+    table = [[int(a), int(b)] for a, b in re.findall(r"\((\d+),\s*(\d+)\)", body)]
+    calls = []
+    sent = src[src.index("fn ilogsum_sentinel_and_bounds"):]
+    sent = sent[: sent.index("}\n\n")]
+    end = src[src.index("fn ilogsum_table_endpoints_match_c_formula"):]
+    end = end[: end.index("}\n}")]
+    for blk in (sent, end):
+        for a, b, w in re.findall(r"assert_eq!\(ilogsum\(([^,]+),\s*([^)]+)\),\s*([^)]+)\)", blk):
+            def val(x):
+                x = x.strip()
+                return -987654321 if x == "-INFTY" else int(x)
+            calls.append([val(a), val(b), val(w)])
+    return {"source": "src/cp9.rs:81-117", "table": table, "calls": calls}
+
+
+def state_delta_kats():
+    src = open(os.path.join(REF, "src", "cm_qdband.rs")).read()
+    body = src[src.index("fn test_state_delta()"):]
+    body = body[: body.index("}\n")]
+    codes = {"D_ST": 0, "MP_ST": 1, "ML_ST": 2, "MR_ST": 3, "IL_ST": 4, "IR_ST": 5, "S_ST": 6,
+             "E_ST": 7, "B_ST": 8, "EL_ST": 9}
+    pairs = [[codes[s], int(d)] for s, d in re.findall(r"state_delta\((\w+)\),\s*(\d+)", body)]
+    return {"source": "src/cm_qdband.rs:639-652", "state_delta": pairs}
+
+
+def scan_small():
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle
+    from helpers import frame, models, planted_seq
+    name, n, nplant, seed = "small2", 1500, 2, 77
+    cm, g, l = models(name)
+    dsq = frame(planted_seq(cm, n, 0.5, nplant, seed=seed))
+    cases = []
+    for sr, band, cutoff in ((0, 1, 0.0), (1, 2, 0.0), (1, 0, 2.0)):
+        hits, _, _, _ = oracle.qdb_scan(l, sr, band, dsq, 1, n, cutoff, True)
+        cases.append({"semiring": sr, "band": band, "cutoff": cutoff,
+                      "hits": [[h[0], h[1], round(h[2], 4), round(h[3], 6)] for h in hits]})
+    return {"model": name, "local": True, "n": n, "nplant": nplant, "seed": seed, "cases": cases}
+
+
+def main():
+    if os.path.isdir(REF):
+        with open(os.path.join(HERE, "ilogsum_kat.json"), "w") as f:
+            json.dump(ilogsum_kats(), f, indent=1)
+        with open(os.path.join(HERE, "state_delta_kat.json"), "w") as f:
+            json.dump(state_delta_kats(), f, indent=1)
+    with open(os.path.join(HERE, "scan_small.json"), "w") as f:
+        json.dump(scan_small(), f, indent=1)
+
+
+if __name__ == "__main__":
+    main()

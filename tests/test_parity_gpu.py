@@ -1,0 +1,138 @@
+"""GPU scanner vs the oracle: hits must be bit-identical.
+
+CYK (f32 max-plus) and integer Inside (ILogsum) are both held to exact
+equality of (i, j, score, bias) -- the kernel keeps the reference's
+per-cell operand order, so no tolerance is needed.  Sizes are small enough
+for the oracle to finish in seconds."""
+import numpy as np
+import pytest
+
+import oracle
+from infernox_b200 import scan
+from infernox_b200.scan import CYK_F32, INSIDE_I32, NOQDB, QDB1, QDB2
+
+from helpers import frame, models, planted_seq
+
+pytestmark = pytest.mark.gpu
+
+
+def hits_equal(gpu, ref):
+    g = [(h.i, h.j, np.float32(h.score).tobytes(), np.float32(h.bias).tobytes()) for h in gpu]
+    r = [(h[0], h[1], np.float32(h[2]).tobytes(), np.float32(h[3]).tobytes()) for h in ref]
+    return g == r
+
+
+CASES = [
+    # model, local, semiring, band, n, cutoff, null3, degenerate
+    ("trna", True, CYK_F32, QDB1, 2500, 0.0, True, 0.0),
+    ("trna", False, CYK_F32, QDB1, 2500, 0.0, True, 0.0),
+    ("trna", True, INSIDE_I32, QDB2, 2500, 0.0, True, 0.0),
+    ("trna", False, INSIDE_I32, QDB2, 2500, -5.0, True, 0.0),
+    ("trna", True, INSIDE_I32, NOQDB, 1500, 0.0, True, 0.0),
+    ("trna", True, CYK_F32, NOQDB, 1500, 0.0, False, 0.0),
+    ("small0", True, CYK_F32, QDB1, 3000, -2.0, True, 0.01),
+    ("small0", True, INSIDE_I32, QDB2, 3000, -2.0, True, 0.01),
+    ("small2", True, INSIDE_I32, NOQDB, 2000, 0.0, True, 0.0),
+    ("small2", False, CYK_F32, QDB2, 2000, 0.0, False, 0.02),
+    ("mb3", True, CYK_F32, QDB1, 2000, 0.0, True, 0.0),
+    ("mb3", True, INSIDE_I32, QDB2, 2000, 0.0, True, 0.0),
+    ("cfg2", True, INSIDE_I32, NOQDB, 1200, 0.0, True, 0.0),
+    ("cfg2", True, CYK_F32, QDB1, 1200, 0.0, True, 0.0),
+]
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: f"{c[0]}-{'L' if c[1] else 'G'}-s{c[2]}-b{c[3]}")
+def test_generic_scan_matches_oracle(case):
+    name, local, sr, band, n, cutoff, null3, degen = case
+    cm, g, l = models(name)
+    c = l if local else g
+    seq = planted_seq(cm, n, 0.5, 3, seed=17 + CASES.index(case), degenerate=degen)
+    dsq = frame(seq)
+    ref, _, _, _ = oracle.qdb_scan(c, sr, band, dsq, 1, n, cutoff, null3)
+    s = scan.Scanner(c)
+    got = s.generic_scan(sr, band, dsq, 1, n, cutoff, null3)
+    assert len(ref) > 0
+    assert hits_equal(got, ref), (got[:5], ref[:5])
+
+
+@pytest.mark.parametrize("chunk", [0, 200, 1000])
+def test_subchunked_windows_match(chunk):
+    """Forced small work items: warm-up restarts must not change any hit."""
+    cm, g, l = models("trna")
+    n = 6000
+    dsq = frame(planted_seq(cm, n, 0.45, 6, seed=7))
+    s = scan.Scanner(l)
+    s.set_shape(chunk=chunk)
+    for sr, band in ((CYK_F32, QDB1), (INSIDE_I32, QDB2)):
+        ref, _, _, _ = oracle.qdb_scan(l, sr, band, dsq, 1, n, -3.0, True)
+        got = s.generic_scan(sr, band, dsq, 1, n, -3.0, True)
+        assert hits_equal(got, ref)
+
+
+def test_window_inside_frame():
+    """Windows [i0, j0] strictly inside the frame (as envelopes are)."""
+    cm, g, l = models("small2")
+    n = 3000
+    dsq = frame(planted_seq(cm, n, 0.5, 4, seed=9))
+    s = scan.Scanner(l)
+    for (i0, j0) in ((1, 1), (5, 40), (700, 1900), (2990, 3000), (1, 3000)):
+        ref, _, _, _ = oracle.qdb_scan(l, INSIDE_I32, QDB2, dsq, i0, j0, -10.0, True)
+        got = s.generic_scan(INSIDE_I32, QDB2, dsq, i0, j0, -10.0, True)
+        assert hits_equal(got, ref), (i0, j0)
+
+
+def test_cyk_filter_and_final_stage():
+    """The --nohmm pair: QDB1 CYK envelopes, then QDB2 Inside per envelope."""
+    cm, g, l = models("trna")
+    n = 8000
+    dsq = frame(planted_seq(cm, n, 0.5, 8, seed=3))
+    s = scan.Scanner(l)
+    env_ref = oracle.cyk_seq_filter(l, dsq, n, 5.0, True)
+    env = s.cyk_seq_filter(dsq, n, 5.0, True)
+    assert env == env_ref and len(env) > 0
+    for nonbanded in (False, True):
+        ref = oracle.final_stage_inside_opt(l, dsq, env, 8.0, True, nonbanded)
+        got = s.final_stage_inside_opt(dsq, env, 8.0, True, nonbanded)
+        assert hits_equal(got, ref)
+
+
+def test_batch_uneven_windows_match_per_window():
+    """Many windows of uneven length in one launch == each window alone."""
+    cm, g, l = models("small2")
+    rng = np.random.default_rng(42)
+    lens = np.clip(rng.lognormal(np.log(300), 1.0, 40).astype(int), 1, 3000)
+    frames, wins, off = [], [], 0
+    for k, L in enumerate(lens):
+        f = frame(planted_seq(cm, int(L), 0.45, 1 if L > 200 else 0, seed=100 + k))
+        frames.append(f)
+        wins.append((off, 1, int(L)))
+        off += len(f)
+    buf = np.concatenate(frames)
+    W = np.array(wins, dtype=[("dsq_offset", np.int64), ("i0", np.int32), ("j0", np.int32)])
+    s = scan.Scanner(l)
+    for sr, band in ((INSIDE_I32, NOQDB), (CYK_F32, QDB1)):
+        got = s.scan_batch(sr, band, buf, W, 0.0, True)
+        plain = s.scan_batch(sr, band, buf, W, 0.0, True, plain=True)
+        assert np.array_equal(got, plain)
+        k = 0
+        for w, (o, i0, j0) in enumerate(wins):
+            f = buf[o:o + j0 + 2]
+            ref, _, _, _ = oracle.qdb_scan(l, sr, band, f, i0, j0, 0.0, True)
+            mine = got[got["win"] == w]
+            assert [(int(h["i"]), int(h["j"]), h["score"].tobytes(), h["bias"].tobytes()) for h in mine] == \
+                   [(r[0], r[1], np.float32(r[2]).tobytes(), np.float32(r[3]).tobytes()) for r in ref]
+            k += len(mine)
+        assert k == len(got)
+
+
+def test_counts_match_oracle_counters():
+    cm, g, l = models("mb3")
+    n = 1500
+    dsq = frame(planted_seq(cm, n, 0.5, 1, seed=5))
+    s = scan.Scanner(l)
+    for sr, band in ((CYK_F32, QDB1), (INSIDE_I32, NOQDB)):
+        _, _, cells, terms = oracle.qdb_scan(l, sr, band, dsq, 1, n, 0.0, False)
+        s.generic_scan(sr, band, dsq, 1, n, 0.0, False)
+        st = s.stats()
+        assert st["cells"] == cells and st["terms"] == terms
+        assert st["kernel_launches"] >= 1
