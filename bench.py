@@ -1,0 +1,352 @@
+"""Benchmark of the batched QDB/Inside window scan (one JSON line on rank 0).
+
+Workload (default "batched-uneven-max"): the batched uneven-window Inside scan
+of the --max path.  One 120-consensus-column CM with 3 bifurcations (seeded
+synthetic, local configuration), sequences with log-normal lengths clipped to
+[200, 20000] nt (median 1.5 kb, i.i.d. 45% GC), both strands, every window
+scanned with the non-banded integer Inside scanner (final_stage_inside_opt
+with nonbanded=true).  A step is one pass over a batch of --batch sequences
+(both strands) drawn from that distribution; each rank scans its own batch
+(weak scaling).  The metric is DP cells per second (the reference's cells,
+counted exactly from the bands), whole job.
+
+value   device-resident batch: residues already in HBM, hits returned to the host.
+e2e     the public API with host buffers: residues copied host->device inside
+        the timed region, hit list copied back.
+Timing: CUDA events on the stream the library launches on, W warm-up steps,
+L2 flushed (256 MB write) before every timed step, max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (clen, paired fraction, bifurcations, structure seed, param seed,
+    #        semiring, band set, median length, sigma, lo, hi, gc)
+    "batched-uneven-max": dict(clen=120, paired=0.5, nbif=3, sseed=5, pseed=23, semiring=1, band=0,
+                               median=1500, sigma=1.0, lo=200, hi=20000, gc=0.45),
+    "nohmm-cyk-filter": dict(clen=72, paired=None, nbif=2, sseed=0, pseed=11, semiring=0, band=1,
+                             median=100000, sigma=0.0, lo=100000, hi=100000, gc=0.50),
+}
+OPS_PER_TERM = {0: 2.0, 1: 7.0}   # CYK: FADD + select; Inside: 6 INT + 1 LDS
+OPS_PER_CELL = 2.0                # emission add + store
+CUTOFF_BITS = 15.0                # stands in for the E-value threshold
+
+
+def env_rank():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def make_model(w):
+    from infernox_b200 import model, synth
+    if w["paired"] is None:
+        ss = synth.trna_like()
+    else:
+        ss = synth.structure(w["clen"], w["paired"], w["nbif"], w["sseed"])
+    cm = synth.synth_cm(ss, w["pseed"], name="bench")
+    return model.configure(cm, local=True)
+
+
+def make_batch(w, nseq, seed):
+    """Concatenated window frames for nseq sequences, top and bottom strand."""
+    from infernox_b200 import synth
+    rng = np.random.default_rng(seed)
+    if w["sigma"] > 0:
+        lens = np.clip(rng.lognormal(np.log(w["median"]), w["sigma"], nseq), w["lo"], w["hi"]).astype(int)
+    else:
+        lens = np.full(nseq, w["median"], int)
+    frames, wins, off = [], [], 0
+    for L in lens:
+        top = synth.random_dsq(int(L), w["gc"], rng)
+        for s in (top, synth.revcomp(top)):
+            f = np.concatenate([[255], s, [255]]).astype(np.uint8)
+            frames.append(f)
+            wins.append((off, 1, int(L)))
+            off += len(f)
+    buf = np.concatenate(frames)
+    W = np.array(wins, dtype=[("dsq_offset", np.int64), ("i0", np.int32), ("j0", np.int32)])
+    return buf, W, lens
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": len(self.rows)}
+        sm = [float(r[1]) for r in self.rows if len(r) >= 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 8 and r[2].replace(".", "").isdigit()]
+        if sm:
+            out["sm_mhz"] = statistics.median(sm)
+            out["sm_max_mhz"] = max(mx) if mx else None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for k, n in enumerate(names):
+            if any(len(r) >= 8 and r[4 + k].lower() == "active" for r in self.rows):
+                out["reasons"].append(n)
+        return out
+
+
+def cpu_baseline(cm, w, buf, wins, budget_s):
+    """The oracle (C restatement of the reference scanner) on the host cores,
+    threads over windows, on a bounded prefix of the batch."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from concurrent.futures import ThreadPoolExecutor
+    oracle.lib()
+    cores = os.cpu_count() or 1
+    # calibrate on the first window
+    o, i0, j0 = wins[0]
+    t0 = time.perf_counter()
+    oracle.qdb_scan(cm, w["semiring"], w["band"], buf[o:o + j0 + 2], i0, j0, CUTOFF_BITS, True)
+    t1 = time.perf_counter() - t0
+    cells0, _ = cm.count_work(w["semiring"], w["band"], j0 - i0 + 1)
+    rate1 = cells0 / max(t1, 1e-6)
+    target_cells = rate1 * cores * budget_s
+    take, tot = [], 0.0
+    for k, (o, i0, j0) in enumerate(wins):
+        c, _ = cm.count_work(w["semiring"], w["band"], j0 - i0 + 1)
+        take.append(k)
+        tot += c
+        if tot >= target_cells:
+            break
+
+    def run(k):
+        o, i0, j0 = wins[k]
+        oracle.qdb_scan(cm, w["semiring"], w["band"], buf[o:o + j0 + 2], i0, j0, CUTOFF_BITS, True)
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=cores) as ex:
+        list(ex.map(run, take))
+    dt = time.perf_counter() - t0
+    res = int(sum(wins[k][2] - wins[k][1] + 1 for k in take))
+    return {"value": tot / dt / 1e9, "unit": "Gcells/s", "cores": cores, "kind": "port",
+            "sample": f"{len(take)} windows ({res} residues, {tot:.3e} cells) of the same batch, "
+                      f"{dt:.1f} s on {cores} threads",
+            "windows_per_s": len(take) / dt}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="batched-uneven-max", choices=sorted(WORKLOADS))
+    ap.add_argument("--batch", type=int, default=200, help="sequences per step per rank")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--plain-windows", type=int, default=16)
+    args = ap.parse_args()
+    w = WORKLOADS[args.workload]
+    rank, world, local_rank = env_rank()
+    cm = make_model(w)
+    buf, wins, lens = make_batch(w, args.batch, seed=1000 + rank)
+    config = {"workload": args.workload, "model": f"synthetic CM clen={cm.clen} M={cm.M} W={cm.W}",
+              "scan": {0: "CYK f32", 1: "Inside i32"}[w["semiring"]] + " " +
+                      {0: "non-banded", 1: "QDB1", 2: "QDB2"}[w["band"]],
+              "sequences_per_step_per_rank": int(args.batch), "windows_per_step_per_rank": int(len(wins)),
+              "residues_per_step_per_rank": int(2 * lens.sum()), "cutoff_bits": CUTOFF_BITS,
+              "parallelism": f"dp{world}", "l2": "flushed (256 MB write) before each timed step"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        cb = cpu_baseline(cm, w, buf, [tuple(x) for x in wins], args.cpu_seconds)
+        line = {"impl": "reference", "metric": "CYK/Inside scan Gcells/s", "value": cb["value"],
+                "unit": "Gcells/s", "n_gpus": world, "steps": 1, "warmup": 0,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+                "data": "synthetic", "config": config, "cpu_baseline": cb,
+                "e2e": {"value": cb["value"], "unit": "Gcells/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from infernox_b200 import scan
+    stream = torch.cuda.current_stream()
+    sc = scan.Scanner(cm, device=local_rank, stream=stream.cuda_stream)
+    d_buf = torch.from_numpy(buf).cuda()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device="cuda")
+    sr, band = w["semiring"], w["band"]
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def step_device():
+        return sc.scan_batch(sr, band, buf, wins, CUTOFF_BITS, True, device_buf=d_buf.data_ptr())
+
+    def step_e2e():
+        return sc.scan_batch(sr, band, buf, wins, CUTOFF_BITS, True)
+
+    for _ in range(args.warmup):
+        hits = step_device()
+    ref_hits = hits
+    clocks = ClockSampler(local_rank)
+    barrier()
+    clocks.start()
+    times, kms, cells, terms, launches, ncand = [], [], 0.0, 0.0, 0, 0
+    for _ in range(args.steps):
+        flush.fill_(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        hits = step_device()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+        st = sc.stats()
+        kms.append(st["kernel_ms"])
+        cells += st["cells"]
+        terms += st["terms"]
+        launches += st["kernel_launches"]
+        ncand += st["candidates"]
+    barrier()
+    clk = clocks.stop()
+    if not np.array_equal(hits, ref_hits):
+        raise RuntimeError("hit lists differ between steps")
+    total_ms = sum(times)
+    # e2e through the host-buffer API
+    for _ in range(1):
+        step_e2e()
+    barrier()
+    etimes = []
+    for _ in range(args.steps):
+        flush.fill_(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        eh = step_e2e()
+        e1.record(stream)
+        e1.synchronize()
+        etimes.append(e0.elapsed_time(e1))
+    barrier()
+    if not np.array_equal(eh, ref_hits):
+        raise RuntimeError("e2e hits differ from the device-resident path")
+    e2e_ms = sum(etimes)
+
+    t = torch.tensor([total_ms, e2e_ms, cells, float(sum(kms))], dtype=torch.float64, device="cuda")
+    if dist:
+        tmax = t.clone()
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        tsum = t.clone()
+        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+        total_ms_all, e2e_ms_all, cells_all = tmax[0].item(), tmax[1].item(), tsum[2].item()
+    else:
+        total_ms_all, e2e_ms_all, cells_all = total_ms, e2e_ms, cells
+
+    plain = None
+    cb = None
+    if rank == 0:
+        # plain comparator: one launch and one CTA per window, same windows
+        k = min(args.plain_windows, len(wins))
+        sub = wins[:k]
+        sc.scan_batch(sr, band, buf, sub, CUTOFF_BITS, True, plain=True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ph = sc.scan_batch(sr, band, buf, sub, CUTOFF_BITS, True, plain=True)
+        e1.record(stream)
+        e1.synchronize()
+        pst = sc.stats()
+        pms = e0.elapsed_time(e1)
+        bh = sc.scan_batch(sr, band, buf, sub, CUTOFF_BITS, True)
+        if not np.array_equal(ph, bh):
+            raise RuntimeError("plain and batched scans differ")
+        plain = {"value": pst["cells"] / (pms / 1e3) / 1e9, "unit": "Gcells/s", "windows": k,
+                 "launches": pst["kernel_launches"], "ms": pms}
+        if not args.no_cpu:
+            cb = cpu_baseline(cm, w, buf, [tuple(x) for x in wins], args.cpu_seconds)
+
+    if rank == 0:
+        value = cells_all / (total_ms_all / 1e3) / 1e9
+        e2e = cells_all / (e2e_ms_all / 1e3) / 1e9
+        kernel_ms = sum(kms) / max(1, launches)
+        ops_launch = (terms * OPS_PER_TERM[sr] + cells * OPS_PER_CELL) / max(1, launches)
+        sm_mhz = clk["sm_mhz"]
+        peak_src = "measured SM clock during the timed region"
+        if not sm_mhz:
+            try:
+                sm_mhz = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["sm_max_mhz"]
+                peak_src = "MEASURED_PEAKS.json sm_max_mhz"
+            except (OSError, KeyError, ValueError):
+                sm_mhz, peak_src = 1965.0, "nominal max SM clock"
+        nsm = torch.cuda.get_device_properties(local_rank).multi_processor_count
+        peak = nsm * 128 * sm_mhz * 1e6 / 1e9  # Gop/s
+        achieved = ops_launch / (kernel_ms / 1e3) / 1e9
+        step_lat = sorted(times)
+        line = {
+            "metric": "CYK/Inside scan Gcells/s", "value": value, "unit": "Gcells/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total_ms_all / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": {0: "f32", 1: "int32"}[sr], "data": "synthetic",
+            "config": config,
+            "e2e": {"value": e2e, "unit": "Gcells/s",
+                    "h2d_bytes_per_step": int(buf.nbytes + len(wins) * 24),
+                    "d2h_bytes_per_step": int(ncand / max(1, args.steps) * 16 + len(ref_hits) * 20)},
+            "seq_per_s": world * args.batch * args.steps / (total_ms_all / 1e3),
+            "step_latency_ms": {"p50": statistics.median(step_lat),
+                                "p99": step_lat[min(len(step_lat) - 1, int(0.99 * len(step_lat)))]},
+            "gpu_launches": launches,
+            "roofline": {"bound": "issue", "achieved": achieved, "peak": peak, "unit": "Gop/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "note": f"INT32/FP32 lane-op issue: {nsm} SMs x 128 lanes x {sm_mhz:.0f} MHz "
+                                 f"({peak_src}); ops = {OPS_PER_TERM[sr]:.0f}/term + 2/cell"},
+            "plain_gpu": plain,
+            "batched_over_plain": (value / plain["value"]) if plain else None,
+            "cpu_baseline": cb,
+            "clocks": clk,
+            "hits_per_step": int(len(ref_hits)),
+        }
+        print(json.dumps(line))
+    sc.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

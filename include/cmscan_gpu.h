@@ -177,6 +177,14 @@ int cmgpu_qdb_scan(const cmgpu_model *m, cmgpu_workspace *ws, int semiring,
                    int32_t j0, float cutoff, int do_null3, cmgpu_hit *hits,
                    int32_t cap, int32_t *n_out);
 
+/* Test hook, the analogue of the reference's DUMP_* value dumps: every
+ * reportable cell (j, d) of a generic_scan of [i0, j0] with bestsc >= cutoff,
+ * sorted by (j, d), with its bit score, before null3 and greedy reporting. */
+int cmgpu_qdb_scan_cells(const cmgpu_model *m, cmgpu_workspace *ws, int semiring,
+                         int qdbidx, const uint8_t *dsq, int32_t n, int32_t i0,
+                         int32_t j0, float cutoff, int32_t *cj, int32_t *cd,
+                         float *csc, int32_t cap, int32_t *n_out);
+
 /* cyk_seq_filter (src/cm_nohmm.rs:855-889): QDB1 CYK over [1, n] then hits
  * padded by W-1 and merged into envelopes (ascending end). */
 int cmgpu_cyk_seq_filter(const cmgpu_model *m, cmgpu_workspace *ws,

@@ -397,7 +397,8 @@ struct WinDesc {
 
 static int run_scan(cmgpu_model *m, cmgpu_workspace *ws, int semiring, int qdbidx, const uint8_t *d_dsq,
                     const uint8_t *h_dsq, int64_t dsq_len, const std::vector<WinDesc> &wins, float cutoff,
-                    int do_null3, bool plain, std::vector<std::vector<cmgpu_hit>> &hits_per_win) {
+                    int do_null3, bool plain, std::vector<std::vector<cmgpu_hit>> &hits_per_win,
+                    std::vector<Cand> *cells_out = nullptr) {
     if (semiring != CMGPU_CYK_F32 && semiring != CMGPU_INSIDE_I32) {
         set_error("unknown semiring");
         return CMGPU_EINVAL;
@@ -563,6 +564,10 @@ static int run_scan(cmgpu_model *m, cmgpu_workspace *ws, int semiring, int qdbid
         if (a.j != b.j) return a.j < b.j;
         return a.d < b.d;
     });
+    if (cells_out) {
+        *cells_out = cs;
+        return CMGPU_OK;
+    }
     std::vector<uint8_t> frame_buf;
     size_t k = 0;
     while (k < cs.size()) {
@@ -726,6 +731,33 @@ int cmgpu_qdb_scan(const cmgpu_model *mc, cmgpu_workspace *ws, int semiring, int
     rc = run_scan(m, ws, semiring, qdbidx, ws->d_dsq, dsq, (int64_t)n + 2, wins, cutoff, do_null3, false, hpw);
     if (rc) return rc;
     return finish_single(hpw, hits, cap, n_out);
+}
+
+int cmgpu_qdb_scan_cells(const cmgpu_model *mc, cmgpu_workspace *ws, int semiring, int qdbidx, const uint8_t *dsq,
+                         int32_t n, int32_t i0, int32_t j0, float cutoff, int32_t *cj, int32_t *cd, float *csc,
+                         int32_t cap, int32_t *n_out) {
+    cmgpu_model *m = const_cast<cmgpu_model *>(mc);
+    if (!m || !ws || !dsq || !n_out || n < 0 || i0 < 1 || j0 > n || (cap > 0 && (!cj || !cd || !csc)))
+        return CMGPU_EINVAL;
+    *n_out = 0;
+    int rc = stage_dsq(ws, dsq, (int64_t)n + 2);
+    if (rc) return rc;
+    std::vector<WinDesc> wins{{0, i0, j0}};
+    std::vector<std::vector<cmgpu_hit>> hpw;
+    std::vector<Cand> cells;
+    rc = run_scan(m, ws, semiring, qdbidx, ws->d_dsq, dsq, (int64_t)n + 2, wins, cutoff, 0, false, hpw, &cells);
+    if (rc) return rc;
+    *n_out = (int32_t)cells.size();
+    if ((int64_t)cells.size() > cap) {
+        set_error("output array too small");
+        return CMGPU_EOVERFLOW;
+    }
+    for (size_t k = 0; k < cells.size(); k++) {
+        cj[k] = cells[k].j;
+        cd[k] = cells[k].d;
+        csc[k] = raw_bits(semiring, cells[k].raw);
+    }
+    return CMGPU_OK;
 }
 
 int cmgpu_cyk_seq_filter(const cmgpu_model *mc, cmgpu_workspace *ws, const uint8_t *dsq, int32_t n, float cutoff,

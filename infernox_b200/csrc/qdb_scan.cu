@@ -15,7 +15,8 @@
 //             src/cm_nohmm.rs:700-746) and candidate emission.
 // Warps take (state, 32 cells) chunks; lanes are consecutive d.  Cells are
 // evaluated with the reference's operand order (reduce_c_order,
-// src/cm_nohmm.rs:187-242; ascending k for bifurcations) so integer ILogsum
+// src/cm_nohmm.rs:187-242, for emitters, S and D states; natural child order
+// for BEGL_S, :601-611; ascending k for bifurcations) so integer ILogsum
 // results are bit-identical; f32 adds use __fadd_rn (no contraction).
 //
 // IL states read their own cell d-1 (self loop, src/cm_nohmm.rs:622-649), a
@@ -245,7 +246,14 @@ __device__ __forceinline__ void do_chunk(const Ctx &c, int v, int d0, int lane) 
     int idx = d - sd;
     T terms[6];
     child_terms<S>(c, sv, v, idx, slot_y, terms, 0);
-    T sc = reduce_c<S>(sv.cnum, terms, init_sc<S>(c, sv, v, idx), c.tbl, p.ilog_nz);
+    T sc;
+    if (sv.flags & SF_BEGL) {
+        // BEGL_S folds its children in natural order (src/cm_nohmm.rs:601-611)
+        sc = init_sc<S>(c, sv, v, idx);
+        for (int yo = 0; yo < sv.cnum; yo++) sc = S::comb(sc, terms[yo], c.tbl, p.ilog_nz);
+    } else {
+        sc = reduce_c<S>(sv.cnum, terms, init_sc<S>(c, sv, v, idx), c.tbl, p.ilog_nz);
+    }
     int esc_off = v * 324;
     if (t == 2 || t == 4) {  // ML, IL: residue i = j-d+1
         sc = S::add(sc, S::ldg(p.esc + esc_off + res(c.frame, c.j - d + 1)));

@@ -97,6 +97,22 @@ class Scanner:
             return [RawHit(int(h["i"]), int(h["j"]), float(h["score"]), float(h["bias"]))
                     for h in out[: nout.value]]
 
+    def scan_cells(self, semiring: int, qdbidx: int, dsq, i0: int, j0: int, cutoff: float):
+        """Reportable cells (j, d, bits) of a window scan, sorted by (j, d)."""
+        a = _frame(dsq)
+        n = a.size - 2
+        cap = max(1024, (j0 - i0 + 1) * (self.cm.W + 2))
+        cj = np.zeros(cap, np.int32)
+        cd = np.zeros(cap, np.int32)
+        cs = np.zeros(cap, np.float32)
+        nout = C.c_int32()
+        N.check(N.lib().cmgpu_qdb_scan_cells(self._model, self._ws, semiring, qdbidx,
+                                             N.ptr(a, C.c_uint8), n, i0, j0, float(cutoff),
+                                             cj.ctypes.data, cd.ctypes.data, cs.ctypes.data, cap,
+                                             C.byref(nout)))
+        k = nout.value
+        return list(zip(cj[:k].tolist(), cd[:k].tolist(), cs[:k].tolist()))
+
     def cyk_seq_filter(self, dsq, n: int, cutoff: float, do_null3: bool) -> list:
         a = _frame(dsq)
         if n != a.size - 2:

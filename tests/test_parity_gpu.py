@@ -136,3 +136,27 @@ def test_counts_match_oracle_counters():
         st = s.stats()
         assert st["cells"] == cells and st["terms"] == terms
         assert st["kernel_launches"] >= 1
+
+
+CELL_CASES = [
+    ("trna", True, INSIDE_I32, QDB2), ("trna", False, INSIDE_I32, QDB2),
+    ("trna", True, INSIDE_I32, NOQDB), ("small0", True, INSIDE_I32, QDB2),
+    ("trna", True, CYK_F32, QDB1), ("mb3", False, INSIDE_I32, NOQDB),
+]
+
+
+@pytest.mark.parametrize("case", CELL_CASES, ids=lambda c: f"{c[0]}-{'L' if c[1] else 'G'}-s{c[2]}-b{c[3]}")
+def test_all_cells_match_oracle(case):
+    """Every ROOT cell (j, d) above a very low cutoff, bit for bit."""
+    name, local, sr, band = case
+    cm, g, l = models(name)
+    c = l if local else g
+    n = 400
+    dsq = frame(planted_seq(cm, n, 0.5, 1, seed=55))
+    _, ref, _, _ = oracle.qdb_scan(c, sr, band, dsq, 1, n, -1e30, False, want_cands=True)
+    got = scan.Scanner(c).scan_cells(sr, band, dsq, 1, n, -1e30)
+    rmap = {(j, d): s for j, d, s in ref}
+    gmap = {(j, d): s for j, d, s in got}
+    bad = [(k, gmap.get(k), rmap.get(k)) for k in sorted(set(rmap) | set(gmap))
+           if np.float32(gmap.get(k, np.nan)).tobytes() != np.float32(rmap.get(k, np.nan)).tobytes()]
+    assert not bad, (len(bad), len(ref), bad[:8])
