@@ -132,6 +132,7 @@ typedef struct cmgpu_stats {
     int32_t kernel_launches;
     int32_t deck_in_smem; /* 1 when the rolling decks live in shared memory */
     int32_t ctas;
+    int32_t lanes;        /* work items per CTA                            */
 } cmgpu_stats;
 
 typedef struct cmgpu_model cmgpu_model;
@@ -164,9 +165,11 @@ void cmgpu_model_free(cmgpu_model *m);
 int cmgpu_workspace_create(int device, void *stream, cmgpu_workspace **out);
 void cmgpu_workspace_free(cmgpu_workspace *ws);
 int cmgpu_workspace_stats(const cmgpu_workspace *ws, cmgpu_stats *out);
-/* Launch shape override for tuning: ctas_per_sm <= 0 keeps the tuned value,
- * threads in {128,256,512}, chunk = residues per work item (0 = auto). */
-int cmgpu_workspace_set_shape(cmgpu_workspace *ws, int ctas_per_sm, int threads, int chunk);
+/* Launch shape override for tuning (0 keeps the tuned value): CTAs per SM
+ * (1..4), threads in {128,256,512}, residues per work item, work items
+ * scanned side by side per CTA (1..8). */
+int cmgpu_workspace_set_shape(cmgpu_workspace *ws, int ctas_per_sm, int threads, int chunk,
+                              int lanes);
 
 /* ---- scanner entry points ----------------------------------------------- */
 

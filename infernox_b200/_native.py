@@ -80,7 +80,7 @@ class Stats(C.Structure):
         ("cells", C.c_double), ("terms", C.c_double), ("residues", C.c_double),
         ("work_items", C.c_int64), ("candidates", C.c_int64),
         ("kernel_ms", C.c_float), ("kernel_launches", C.c_int32),
-        ("deck_in_smem", C.c_int32), ("ctas", C.c_int32),
+        ("deck_in_smem", C.c_int32), ("ctas", C.c_int32), ("lanes", C.c_int32),
     ]
 
 
@@ -119,7 +119,7 @@ def lib() -> C.CDLL:
     L.cmgpu_workspace_free.argtypes = [vp]
     L.cmgpu_workspace_free.restype = None
     L.cmgpu_workspace_stats.argtypes = [vp, P(Stats)]
-    L.cmgpu_workspace_set_shape.argtypes = [vp, C.c_int, C.c_int, C.c_int]
+    L.cmgpu_workspace_set_shape.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int]
     L.cmgpu_qdb_scan.argtypes = [vp, vp, C.c_int, C.c_int, P(C.c_uint8), C.c_int32, C.c_int32,
                                  C.c_int32, C.c_float, C.c_int, vp, C.c_int32, P(C.c_int32)]
     L.cmgpu_qdb_scan_cells.argtypes = [vp, vp, C.c_int, C.c_int, P(C.c_uint8), C.c_int32, C.c_int32,

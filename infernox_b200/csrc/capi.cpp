@@ -116,22 +116,27 @@ struct DevPlan {
     Plan host;
     StateDev *states = nullptr;
     ChunkDev *chunks = nullptr;
-    int32_t *level_start = nullptr, *begin_states = nullptr;
-    uint32_t *tsc = nullptr, *init0 = nullptr, *endsc = nullptr, *beginsc = nullptr, *esc = nullptr,
-             *el_sca = nullptr;
+    BeginDev *begins = nullptr;
+    int32_t *level_start = nullptr, *wb = nullptr, *cb = nullptr, *init_off = nullptr;
+    uint32_t *tsc = nullptr, *endsc = nullptr, *beginsc = nullptr, *esc = nullptr, *el_sca = nullptr,
+             *esc_c = nullptr, *init_val = nullptr;
     std::vector<double> cells_prefix, terms_prefix;  // per jrow, prefix over jrow = 1..W
     double cells_full = 0, terms_full = 0;
     ~DevPlan() {
         cudaFree(states);
         cudaFree(chunks);
+        cudaFree(begins);
         cudaFree(level_start);
-        cudaFree(begin_states);
+        cudaFree(wb);
+        cudaFree(cb);
+        cudaFree(init_off);
         cudaFree(tsc);
-        cudaFree(init0);
         cudaFree(endsc);
         cudaFree(beginsc);
         cudaFree(esc);
         cudaFree(el_sca);
+        cudaFree(esc_c);
+        cudaFree(init_val);
     }
 };
 
@@ -178,9 +183,10 @@ struct cmgpu_workspace {
     size_t h_cands_cap = 0;
     int *h_counters = nullptr;
     // launch shape
-    int threads = 256;
-    int ctas_per_sm = 0;  // 0 = occupancy
+    int threads = 512;
+    int ctas_per_sm = 0;  // 0 = tuned
     int chunk = 0;        // 0 = auto
+    int lanes = 0;        // 0 = tuned
     int sm_count = 148;
     cmgpu_stats stats{};
     ~cmgpu_workspace() {
@@ -214,14 +220,18 @@ static int get_plan(cmgpu_model *m, int semiring, int qdbidx, DevPlan **out) {
     int rc;
     if ((rc = upload_vec(&dp->states, p.states))) return rc;
     if ((rc = upload_vec(&dp->chunks, p.chunks))) return rc;
+    if ((rc = upload_vec(&dp->begins, p.begins))) return rc;
     if ((rc = upload_vec(&dp->level_start, p.level_start))) return rc;
-    if ((rc = upload_vec(&dp->begin_states, p.begin_states))) return rc;
+    if ((rc = upload_vec(&dp->wb, p.wb))) return rc;
+    if ((rc = upload_vec(&dp->cb, p.cb))) return rc;
+    if ((rc = upload_vec(&dp->init_off, p.init_off))) return rc;
+    if ((rc = upload_vec(&dp->init_val, p.init_val))) return rc;
     if ((rc = upload_vec(&dp->tsc, p.tsc))) return rc;
-    if ((rc = upload_vec(&dp->init0, p.init0))) return rc;
     if ((rc = upload_vec(&dp->endsc, p.endsc))) return rc;
     if ((rc = upload_vec(&dp->beginsc, p.beginsc))) return rc;
     if ((rc = upload_vec(&dp->esc, p.esc))) return rc;
     if ((rc = upload_vec(&dp->el_sca, p.el_sca))) return rc;
+    if ((rc = upload_vec(&dp->esc_c, p.esc_c))) return rc;
     // per-column work counts by row limit
     const int W = p.W;
     dp->cells_prefix.assign(W + 1, 0.0);
@@ -417,22 +427,28 @@ static int run_scan(cmgpu_model *m, cmgpu_workspace *ws, int semiring, int qdbid
 
     ScanParams sp{};
     sp.states = dp->states;
+    sp.wb = dp->wb;
+    sp.cb = dp->cb;
     sp.chunks = dp->chunks;
     sp.level_start = dp->level_start;
     sp.nlev = (int)pl.level_start.size() - 1;
+    sp.nchunks = (int)pl.chunks.size();
     sp.tsc = dp->tsc;
-    sp.init0 = dp->init0;
     sp.endsc = dp->endsc;
-    sp.beginsc = dp->beginsc;
     sp.esc = dp->esc;
     sp.el_sca = dp->el_sca;
-    sp.begin_states = dp->begin_states;
-    sp.nbegin = (int)pl.begin_states.size();
+    sp.esc_c = dp->esc_c;
+    sp.n_esc_c = (int)pl.esc_c.size();
+    sp.begins = dp->begins;
+    sp.beginsc = dp->beginsc;
+    sp.nbegin = (int)pl.begins.size();
+    sp.init_off = dp->init_off;
+    sp.init_val = dp->init_val;
+    sp.ninit = (int)pl.init_off.size();
     sp.M = pl.M;
     sp.W = pl.W;
     sp.root_dn = pl.root_dn;
     sp.root_dxcap = pl.root_dxcap;
-    sp.root_cfirst = pl.root_cfirst;
     sp.root_cnum = pl.root_cnum;
     sp.local = pl.local ? 1 : 0;
     sp.inside = semiring == CMGPU_INSIDE_I32;
@@ -442,19 +458,52 @@ static int run_scan(cmgpu_model *m, cmgpu_workspace *ws, int semiring, int qdbid
     sp.dsq = d_dsq;
     sp.cutoff = cutoff;
 
-    // launch shape
+    // launch shape: lanes (work items per CTA) x CTAs per SM.  Decks go to
+    // shared memory when at least 3 lanes fit per SM; otherwise to global
+    // memory (L2-resident) with 8 lanes per CTA, which keeps more
+    // independent work in flight per SM.
     const int threads = ws->threads;
-    bool deck_smem = scan_smem_bytes(sp, true) <= 227 * 1024 - 1024;
-    int occ = scan_occupancy(sp, deck_smem, threads);
-    if (deck_smem && occ < 1) {
-        deck_smem = false;
-        occ = scan_occupancy(sp, false, threads);
+    const size_t SMEM_CAP = 227 * 1024 - 1024, SM_CAP = 228 * 1024;
+    int best_c = 0, best_l = 0;
+    bool deck_smem = false;
+    auto occ_for = [&](int l, bool smem_deck) {
+        sp.lanes = l;
+        sp.deck_smem = smem_deck ? 1 : 0;
+        sp.lay = scan_layout(sp, l, smem_deck);
+        return scan_occupancy(sp, threads);
+    };
+    if (!plain) {
+        for (int c = 1; c <= 4; c++) {
+            if (ws->ctas_per_sm > 0 && c != ws->ctas_per_sm) continue;
+            size_t cap = std::min(SMEM_CAP, SM_CAP / c - 1024);
+            for (int t = MAX_LANES; t >= 1; t--) {
+                if (ws->lanes > 0 && t != ws->lanes) continue;
+                if ((size_t)scan_layout(sp, t, true).words * 4 > cap) continue;
+                if (occ_for(t, true) >= c && c * t > best_c * best_l) {
+                    best_c = c;
+                    best_l = t;
+                }
+                break;
+            }
+        }
+        bool forced = ws->lanes > 0 || ws->ctas_per_sm > 0;
+        if (best_c * best_l < 3 && !(forced && best_c > 0)) best_c = 0;
+    } else if ((size_t)scan_layout(sp, 1, true).words * 4 <= SMEM_CAP) {
+        best_c = 1;
+        best_l = 1;
     }
+    if (best_c > 0) {
+        deck_smem = true;
+    } else {
+        best_l = plain ? 1 : (ws->lanes > 0 ? ws->lanes : MAX_LANES);
+        best_c = ws->ctas_per_sm > 0 ? ws->ctas_per_sm : 1;
+    }
+    int occ = occ_for(best_l, deck_smem);
     if (occ < 1) {
         set_error("scan kernel cannot be resident with this shape");
         return CMGPU_EDEVICE;
     }
-    int per_sm = ws->ctas_per_sm > 0 ? std::min(ws->ctas_per_sm, occ) : occ;
+    int per_sm = std::min(best_c, occ);
     int max_ctas = ws->sm_count * per_sm;
 
     // work items
@@ -464,7 +513,7 @@ static int run_scan(cmgpu_model *m, cmgpu_workspace *ws, int semiring, int qdbid
     const int W = pl.W;
     int64_t chunk = ws->chunk;
     if (chunk <= 0) {
-        chunk = total_cols / std::max<int64_t>(1, (int64_t)max_ctas * 4);
+        chunk = total_cols / std::max<int64_t>(1, (int64_t)max_ctas * best_l * 4);
         chunk = std::max<int64_t>(chunk, 4 * (int64_t)W);
         chunk = std::min<int64_t>(chunk, 32768);
     }
@@ -492,6 +541,7 @@ static int run_scan(cmgpu_model *m, cmgpu_workspace *ws, int semiring, int qdbid
         });
     ws->stats.work_items = (int64_t)items.size();
     ws->stats.deck_in_smem = deck_smem ? 1 : 0;
+    ws->stats.lanes = best_l;
     if (items.empty()) return CMGPU_OK;
 
     if ((rc = ensure_dev(&ws->d_items, &ws->items_cap, items.size()))) return rc;
@@ -499,11 +549,11 @@ static int run_scan(cmgpu_model *m, cmgpu_workspace *ws, int semiring, int qdbid
                              ws->stream));
     size_t cand_cap = std::max<size_t>(ws->cands_cap, 1 << 16);
     if ((rc = ensure_dev(&ws->d_cands, &ws->cands_cap, cand_cap))) return rc;
-    int ctas = plain ? 1 : (int)std::min<int64_t>((int64_t)items.size(), max_ctas);
+    int ctas = plain ? 1 : (int)std::min<int64_t>(((int64_t)items.size() + best_l - 1) / best_l, max_ctas);
     ws->stats.ctas = ctas;
     if (!deck_smem) {
         size_t stride = ((size_t)pl.deck_elems + 31) & ~(size_t)31;
-        if ((rc = ensure_dev(&ws->d_deck, &ws->deck_cap, stride * (size_t)ctas))) return rc;
+        if ((rc = ensure_dev(&ws->d_deck, &ws->deck_cap, stride * (size_t)ctas * (size_t)best_l))) return rc;
         sp.deck_global = ws->d_deck;
         sp.deck_stride = (int64_t)stride;
     }
@@ -524,13 +574,13 @@ static int run_scan(cmgpu_model *m, cmgpu_workspace *ws, int semiring, int qdbid
                 sp.nitems = 1;
                 sp.item_base = (int)k;
                 CUDA_TRY(cudaMemsetAsync(ws->d_counters, 0, sizeof(int), ws->stream));
-                CUDA_TRY(scan_launch(sp, deck_smem, 1, threads, ws->stream));
+                CUDA_TRY(scan_launch(sp, 1, threads, ws->stream));
             }
             ws->stats.kernel_launches = (int)items.size();
         } else {
             sp.nitems = (int)items.size();
             sp.item_base = 0;
-            CUDA_TRY(scan_launch(sp, deck_smem, ctas, threads, ws->stream));
+            CUDA_TRY(scan_launch(sp, ctas, threads, ws->stream));
             ws->stats.kernel_launches = 1;
         }
         CUDA_TRY(cudaEventRecord(ws->ev1, ws->stream));
@@ -694,12 +744,14 @@ int cmgpu_workspace_stats(const cmgpu_workspace *ws, cmgpu_stats *out) {
     return CMGPU_OK;
 }
 
-int cmgpu_workspace_set_shape(cmgpu_workspace *ws, int ctas_per_sm, int threads, int chunk) {
+int cmgpu_workspace_set_shape(cmgpu_workspace *ws, int ctas_per_sm, int threads, int chunk, int lanes) {
     if (!ws) return CMGPU_EINVAL;
     if (threads != 0 && threads != 128 && threads != 256 && threads != 512) return CMGPU_EINVAL;
+    if (lanes < 0 || lanes > MAX_LANES || ctas_per_sm < 0 || ctas_per_sm > 4) return CMGPU_EINVAL;
     ws->ctas_per_sm = ctas_per_sm;
     if (threads) ws->threads = threads;
     ws->chunk = chunk;
+    ws->lanes = lanes;
     return CMGPU_OK;
 }
 

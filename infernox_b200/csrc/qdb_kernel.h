@@ -9,7 +9,9 @@
 
 namespace cmx {
 
-constexpr int IL_KMAX = 8;  // IL cells per lane kept in registers (W <= 255)
+constexpr int IL_KMAX = 8;     // IL cells per lane kept in registers (W <= 255)
+constexpr int COL_BLOCK = 32;  // columns a lane advances between refills
+constexpr int MAX_LANES = 8;   // work items one CTA scans side by side
 
 // A piece of one window: columns jstart..jend are scanned, candidates are
 // emitted for columns >= jreport (the first W-1 are warm-up).
@@ -24,17 +26,31 @@ struct Cand {
     uint32_t raw;
 };
 
+// Shared-memory layout of one CTA, in 32-bit words from the start of the
+// dynamic shared memory.  Computed once on the host (scan_layout).
+struct SmemLayout {
+    int el, tbl, info, wb, cb, tsc, endsc, escc, chunks, lvl, begin, beginsc, ring, lane, deck;
+    int ring_len;      // residues per lane ring (power of two >= W + 64)
+    int64_t words;     // total
+};
+
 struct ScanParams {
-    // plan (device)
+    // plan (device, global memory; copied to shared memory at kernel start)
     const StateDev *states;
+    const int32_t *wb, *cb;
     const ChunkDev *chunks;
     const int32_t *level_start;
-    int nlev;
-    const uint32_t *tsc, *init0, *endsc, *beginsc, *esc, *el_sca;
-    const int32_t *begin_states;
+    int nlev, nchunks;
+    const uint32_t *tsc, *endsc, *esc, *el_sca, *esc_c;
+    int n_esc_c;
+    const BeginDev *begins;
+    const uint32_t *beginsc;
     int nbegin;
+    const int32_t *init_off;
+    const uint32_t *init_val;
+    int ninit;
     int M, W;
-    int root_dn, root_dxcap, root_cfirst, root_cnum;
+    int root_dn, root_dxcap, root_cnum;
     int local;
     int inside;
     int64_t deck_elems;
@@ -51,13 +67,16 @@ struct ScanParams {
     int cand_cap;
     int *cand_count;
     float cutoff;
-    // global deck fallback
-    uint32_t *deck_global;
+    // lanes per CTA and deck placement
+    int lanes;
+    int deck_smem;
+    uint32_t *deck_global;  // when !deck_smem: [ctas][lanes][deck_stride]
     int64_t deck_stride;
+    SmemLayout lay;
 };
 
-size_t scan_smem_bytes(const ScanParams &p, bool deck_smem);
-int scan_occupancy(const ScanParams &p, bool deck_smem, int threads);
-cudaError_t scan_launch(const ScanParams &p, bool deck_smem, int ctas, int threads, cudaStream_t s);
+SmemLayout scan_layout(const ScanParams &p, int lanes, bool deck_smem);
+int scan_occupancy(const ScanParams &p, int threads);
+cudaError_t scan_launch(const ScanParams &p, int ctas, int threads, cudaStream_t s);
 
 }  // namespace cmx

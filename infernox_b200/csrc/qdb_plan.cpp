@@ -107,17 +107,31 @@ bool build_plan(const cmgpu_cm *cm, int semiring, int qdbidx, Plan &p) {
     // score tables
     p.tsc.assign((size_t)M * MAXC, ZERO);
     p.endsc.assign(M, ZERO);
-    p.beginsc.assign(M, ZERO);
+    p.beginsc_all.assign(M, ZERO);
     p.esc.assign((size_t)M * ESC, ZERO);
     for (int v = 0; v < M; v++) {
         for (int x = 0; x < MAXC; x++)
             p.tsc[(size_t)v * MAXC + x] = inside ? (uint32_t)cm->itsc[(size_t)v * MAXC + x]
                                                  : fbits(cm->tsc[(size_t)v * MAXC + x]);
         p.endsc[v] = inside ? (uint32_t)cm->iendsc[v] : fbits(cm->endsc[v]);
-        p.beginsc[v] = inside ? (uint32_t)cm->ibeginsc[v] : fbits(cm->beginsc[v]);
+        p.beginsc_all[v] = inside ? (uint32_t)cm->ibeginsc[v] : fbits(cm->beginsc[v]);
         for (int x = 0; x < ESC; x++)
             p.esc[(size_t)v * ESC + x] =
                 inside ? (uint32_t)cm->ioesc[(size_t)v * ESC + x] : fbits(cm->oesc[(size_t)v * ESC + x]);
+    }
+    // compact canonical emission table (codes 0..3) for shared memory
+    p.escoff.assign(M, -1);
+    p.esc_c.clear();
+    for (int v = 0; v < M; v++) {
+        int st = cm->sttype[v];
+        if (st == MP_ST) {
+            p.escoff[v] = (int32_t)p.esc_c.size();
+            for (int a = 0; a < 4; a++)
+                for (int c2 = 0; c2 < 4; c2++) p.esc_c.push_back(p.esc[(size_t)v * ESC + a * KP + c2]);
+        } else if (st == ML_ST || st == MR_ST || st == IL_ST || st == IR_ST) {
+            p.escoff[v] = (int32_t)p.esc_c.size();
+            for (int a = 0; a < 4; a++) p.esc_c.push_back(p.esc[(size_t)v * ESC + a]);
+        }
     }
     const uint32_t el_self = inside ? (uint32_t)cm->iel_selfsc : fbits(cm->el_selfsc);
     p.el_sca.assign((size_t)W + 1, 0u);
@@ -143,48 +157,128 @@ bool build_plan(const cmgpu_cm *cm, int semiring, int qdbidx, Plan &p) {
         }
     }
 
-    // states, deck layout
+    // per-state metadata
     p.states.assign(M, StateDev());
-    int64_t off = 0;
+    std::vector<int> width(M, 0);
     for (int v = 0; v < M; v++) {
         StateDev &s = p.states[v];
         int st = cm->sttype[v];
         s.type = (uint8_t)st;
         s.flags = 0;
-        s.cfirst = (int16_t)cm->cfirst[v];
-        s.cnum = (int16_t)cm->cnum[v];
+        s.cnum = (uint8_t)(st == B_ST ? 2 : cm->cnum[v]);
+        s.sd = (uint8_t)state_delta(st);
         s.dn = (int16_t)b.dn[v];
         s.dxcap = (int16_t)b.dxcap[v];
-        int width = std::max(0, b.dxcap[v] - b.dn[v] + 1);
-        if (st == E_ST || v == 0) width = 0;  // E cells are constants; ROOT_S is never read
-        s.width = (int16_t)width;
-        s.esc_off = v * ESC;
+        s.escoff = p.escoff[v];
+        width[v] = std::max(0, b.dxcap[v] - b.dn[v] + 1);
+        if (st == E_ST || v == 0) width[v] = 0;  // E cells are constants; ROOT_S is never read
         if (cm->stid[v] == BEGL_S) s.flags |= SF_BEGL;
         if (right_emitter(st)) s.flags |= SF_TWO_SLOT;
         if (possible_bits(p.endsc[v])) s.flags |= SF_ENDSC;
-        if (p.local && v >= 1 && begin_possible(p.beginsc[v])) s.flags |= SF_BEGIN;
+        if (p.local && v >= 1 && begin_possible(p.beginsc_all[v])) s.flags |= SF_BEGIN;
+    }
+    // index range every state's deck must cover: own band + all reads
+    std::vector<int> lo(M, 1 << 30), hi(M, -1);
+    auto cover = [&](int y, int a, int c) {
+        if (c < a) return;
+        lo[y] = std::min(lo[y], a);
+        hi[y] = std::max(hi[y], c);
+    };
+    for (int v = 0; v < M; v++) {
+        if (width[v] > 0) cover(v, b.dn[v], b.dxcap[v]);
+        int st = cm->sttype[v];
+        if (st == E_ST) continue;
+        if (v == 0) {
+            for (int yo = 0; yo < cm->cnum[0]; yo++) cover(cm->cfirst[0] + yo, b.dn[0], b.dxcap[0]);
+            continue;
+        }
+        if (width[v] <= 0) continue;
         if (st == B_ST) {
             int wl = cm->cfirst[v], y = cm->cnum[v];
-            s.kdn_y = (int16_t)std::min(b.dmin[y], W);
-            s.kdx_y = (int16_t)std::min(b.dmax[y], W);
-            s.kdn_w = (int16_t)std::min(b.dmin[wl], W);
-            s.kdx_w = (int16_t)std::min(b.dmax[wl], W);
+            cover(y, std::max(0, std::min(b.dmin[y], W)), std::min(b.dmax[y], W));
+            cover(wl, std::max(0, std::min(b.dmin[wl], W)), std::min(b.dmax[wl], W));
+        } else {
+            int sd = state_delta(st);
+            for (int yo = 0; yo < cm->cnum[v]; yo++) cover(cm->cfirst[v] + yo, b.dn[v] - sd, b.dxcap[v] - sd);
         }
+    }
+    // deck layout
+    std::vector<int32_t> base(M, 0);
+    int64_t off = 0;
+    for (int v = 0; v < M; v++) {
+        StateDev &s = p.states[v];
+        if (hi[v] < lo[v]) {
+            s.span = 0;
+            continue;
+        }
+        int span = hi[v] - lo[v] + 1;
+        s.span = span;
         int64_t slots = (s.flags & SF_BEGL) ? (int64_t)W + 1 : (s.flags & SF_TWO_SLOT) ? 2 : 1;
-        s.base = (int32_t)(off - s.dn);
-        off += slots * width;
-        if (off > (int64_t)1 << 30) {
+        base[v] = (int32_t)(off - lo[v]);
+        if (lo[v] <= 0 && 0 <= hi[v] && p.init0[v] != ZERO)
+            for (int64_t q = 0; q < slots; q++) {
+                p.init_off.push_back((int32_t)(base[v] + q * span));
+                p.init_val.push_back(p.init0[v]);
+            }
+        off += slots * span;
+        if (off > ((int64_t)1 << 30)) {
             set_error("deck exceeds 2^30 cells");
             return false;
         }
     }
     p.deck_elems = off;
+    // own write bases and child read bases by column parity
+    p.wb.assign((size_t)M * 2, 0);
+    p.cb.assign((size_t)M * 12, 0);
+    auto slot_base = [&](int y, int slot) -> int32_t {
+        const StateDev &s = p.states[y];
+        return base[y] + ((s.flags & SF_TWO_SLOT) ? slot * s.span : 0);
+    };
+    for (int v = 0; v < M; v++) {
+        int st = cm->sttype[v];
+        for (int par = 0; par < 2; par++) p.wb[(size_t)v * 2 + par] = slot_base(v, par);
+        if (st == E_ST) continue;
+        if (st == B_ST) {
+            int wl = cm->cfirst[v], y = cm->cnum[v];
+            int32_t *c = &p.cb[(size_t)v * 12];
+            c[0] = c[1] = base[wl];
+            c[2] = c[3] = base[y];
+            c[4] = std::min(b.dmin[y], W);
+            c[5] = std::min(b.dmax[y], W);
+            c[6] = std::min(b.dmin[wl], W);
+            c[7] = std::min(b.dmax[wl], W);
+            c[8] = p.states[wl].span;
+            continue;
+        }
+        bool rem = right_emitter(st);
+        int sd = v == 0 ? 0 : state_delta(st);
+        for (int yo = 0; yo < cm->cnum[v]; yo++) {
+            int y = cm->cfirst[v] + yo;
+            for (int par = 0; par < 2; par++) {
+                int slot = rem ? (par ^ 1) : par;  // prv for right emitters, cur otherwise
+                p.cb[(size_t)v * 12 + yo * 2 + par] = slot_base(y, slot) - sd;
+            }
+        }
+    }
     p.root_dn = b.dn[0];
     p.root_dxcap = b.dxcap[0];
-    p.root_cfirst = cm->cfirst[0];
     p.root_cnum = cm->cnum[0];
-    for (int v = 1; v < M; v++)
-        if (p.states[v].flags & SF_BEGIN) p.begin_states.push_back(v);
+    for (int v = 1; v < M; v++) {
+        if (!(p.states[v].flags & SF_BEGIN)) continue;
+        BeginDev bd;
+        bd.v = v;
+        if (p.states[v].flags & SF_BEGL) {
+            bd.base0 = bd.base1 = base[v];
+        } else {
+            bd.base0 = slot_base(v, 0);
+            bd.base1 = slot_base(v, 1);
+        }
+        bd.dn = (int16_t)b.dn[v];
+        bd.dxcap = (int16_t)b.dxcap[v];
+        if (width[v] <= 0) continue;
+        p.begins.push_back(bd);
+        p.beginsc.push_back(p.beginsc_all[v]);
+    }
 
     // levels: right emitters read only the previous column -> level 0; every
     // other state sits one level above its deepest same-column child.
@@ -218,10 +312,10 @@ bool build_plan(const cmgpu_cm *cm, int semiring, int qdbidx, Plan &p) {
         for (int v = 1; v < M; v++) {
             if (level[v] != l) continue;
             const StateDev &s = p.states[v];
-            if (s.width <= 0) continue;
+            if (width[v] <= 0) continue;
             int st = s.type;
             if (st == IL_ST) {
-                lc.push_back({1e9 + s.width, ChunkDev{v, -1}});
+                lc.push_back({1e9 + width[v], ChunkDev{v, -1}});
             } else {
                 for (int d0 = s.dn; d0 <= s.dxcap; d0 += 32) {
                     double cost = st == B_ST ? 1e6 + d0 : (double)s.cnum;
@@ -268,7 +362,8 @@ void count_column(const cmgpu_cm *cm, const Plan &p, const Bands &b, int jrow, d
     if (dx0 >= dn0) {
         cells += dx0 - dn0 + 1;
         terms += (double)(dx0 - dn0 + 1) * cm->cnum[0];
-        for (int y : p.begin_states) {
+        for (const BeginDev &bd : p.begins) {
+            int y = bd.v;
             int dn = std::max(dn0, b.dn[y]);
             int dx = std::min(dx0, std::min(jrow, b.dxcap[y]));
             if (dx >= dn) terms += dx - dn + 1;

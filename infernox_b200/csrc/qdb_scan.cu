@@ -1,35 +1,40 @@
 // QDB-banded CYK / Inside window scanner for sm_100a.
 //
-// One persistent CTA scans one work item at a time: a piece of a window plus
-// W-1 warm-up columns, pulled from a cost-ordered device queue.  A cell (j,d)
-// depends only on residues j-d+1..j, so a piece started W-1 columns early
-// reproduces the reference's cells bit for bit (src/cm_nohmm.rs:549-763
-// computes them with jrow = min(j-i0+1, W)).
+// Work decomposition.  A window is cut into work items: a piece of the
+// window plus W-1 warm-up columns.  A cell (j,d) depends only on residues
+// j-d+1..j, so a piece started W-1 columns early reproduces the reference's
+// cells bit for bit (src/cm_nohmm.rs:549-763 computes them with
+// jrow = min(j-i0+1, W)).  Items sit in a cost-ordered device queue; each
+// persistent CTA runs `lanes` items side by side (one deck per lane, one copy
+// of the model metadata), refilling a lane from the queue when its item ends.
 //
-// Per column j the CTA walks the plan's levels:
+// Per column the CTA walks the plan's levels for every lane at once:
 //   level 0   every right emitter (MP, MR, IR).  They read only column j-1
 //             (jp_y = prv, src/cm_nohmm.rs:575), so all of them are
 //             independent and run in one phase;
 //   level l   states whose same-column children sit in levels < l;
 //   root      ROOT_S transitions, local begins (MAX in both semirings,
 //             src/cm_nohmm.rs:700-746) and candidate emission.
-// Warps take (state, 32 cells) chunks; lanes are consecutive d.  Cells are
-// evaluated with the reference's operand order (reduce_c_order,
+// Warps take (lane, state, 32 cells) units; lanes of a warp are consecutive
+// d.  Cells are evaluated in the reference's operand order (reduce_c_order,
 // src/cm_nohmm.rs:187-242, for emitters, S and D states; natural child order
-// for BEGL_S, :601-611; ascending k for bifurcations) so integer ILogsum
+// for BEGL_S, :601-611; ascending k for bifurcations), so integer ILogsum
 // results are bit-identical; f32 adds use __fadd_rn (no contraction).
 //
 // IL states read their own cell d-1 (self loop, src/cm_nohmm.rs:622-649), a
-// serial chain in d.  A warp resolves it by blocked fixed-point iteration:
+// serial chain in d.  One warp resolves it by blocked fixed-point iteration:
 // lane l owns a block of consecutive d, walks it serially from an incoming
-// value, and passes its last value to lane l+1; the warp repeats until no
-// incoming value changes.  The step x -> comb(c, x + t0) + e is monotone, so
-// the fixed point is the serial result exactly, and 33 rounds always reach it.
+// value and passes its last value to lane l+1; the warp repeats until no
+// incoming value changes.  When nothing changes the values satisfy the
+// serial recurrence everywhere, so they are the serial result; after r rounds
+// lanes 0..r are exact, so 33 rounds always suffice.
 //
 // Decks: right emitters keep two column slots (j & 1), BEGL_S states a ring
 // of W+1 columns, every other state one slot that level 0 of column j reads
-// (as column j-1) before levels >= 1 overwrite it.  All decks live in shared
-// memory when they fit; otherwise in a per-CTA region of global memory.
+// (as column j-1) before levels >= 1 overwrite it.  Decks live in shared
+// memory when they fit, else in a per-(CTA, lane) region of global memory.
+// Metadata, score tables (canonical residues), the ILogsum table and a
+// residue ring per lane always live in shared memory.
 #include <cuda_runtime.h>
 #include <cstdint>
 
@@ -82,54 +87,64 @@ struct Sem<true> {  // Inside: i32 wrapping adds, ILogsum
     }
 };
 
-struct SInfo {  // the first 16 bytes of StateDev
-    int32_t base;
-    int16_t dn, dxcap, width;
-    uint8_t flags, type;
-    int16_t cfirst, cnum;
+struct SInfo {  // unpacked StateDev
+    int dn, dxcap, cnum, type, flags, sd, escoff, span;
 };
 
-__device__ __forceinline__ SInfo load_info(const StateDev *st, int v) {
-    int4 q = __ldg(reinterpret_cast<const int4 *>(st + v));
+__device__ __forceinline__ SInfo unpack(int4 q) {
     SInfo s;
-    s.base = q.x;
-    s.dn = (int16_t)(q.y & 0xffff);
-    s.dxcap = (int16_t)((uint32_t)q.y >> 16);
-    s.width = (int16_t)(q.z & 0xffff);
-    s.flags = (uint8_t)(((uint32_t)q.z >> 16) & 0xff);
-    s.type = (uint8_t)((uint32_t)q.z >> 24);
-    s.cfirst = (int16_t)(q.w & 0xffff);
-    s.cnum = (int16_t)((uint32_t)q.w >> 16);
+    s.dn = (int16_t)(q.x & 0xffff);
+    s.dxcap = (int16_t)((uint32_t)q.x >> 16);
+    s.cnum = q.y & 0xff;
+    s.type = (q.y >> 8) & 0xff;
+    s.flags = (q.y >> 16) & 0xff;
+    s.sd = ((uint32_t)q.y >> 24) & 0xff;
+    s.escoff = q.z;
+    s.span = q.w;
     return s;
 }
 
-// Residue code at frame position x.  Codes above 17 (not produced by the
-// digitiser) read as 17 (missing), so a malformed buffer cannot index past an
-// emission row; the host rejects such buffers before launch when it can.
-__device__ __forceinline__ int res(const uint8_t *frame, int x) {
-    int c = __ldg(frame + x);
-    return c > 17 ? 17 : c;
-}
+// Shared-memory views of the model and the per-lane state.
+struct Smem {
+    const uint32_t *el;
+    const uint16_t *tbl;
+    const int4 *info;
+    const int32_t *wb, *cb;
+    const uint32_t *tsc, *endsc, *escc, *beginsc;
+    const int32_t *lvl;
+    const int4 *begin;
+    const int2 *chunks;
+    uint8_t *ring;
+    int32_t *lane;  // [MAX_LANES][8]
+};
 
-__device__ __forceinline__ int state_delta(int t) {
-    return t == 1 ? 2 : (t >= 2 && t <= 5) ? 1 : 0;  // MP 2; ML MR IL IR 1
-}
-__device__ __forceinline__ bool right_em(int t) { return t == 1 || t == 3 || t == 5; }
+// Per-lane view of one column.
+struct Lane {
+    uint32_t *deck;
+    const uint8_t *ring;  // residue at position x: ring[x & rmask]
+    int j, par, jm, jrow;
+};
 
-// Value of cell idx of state Y in column slot `slot` (parity for two-slot
-// states, ring column for BEGL_S, ignored otherwise).
+struct K {
+    const ScanParams *p;
+    Smem s;
+    int nz;
+    int rmask;
+};
+
+// Emission score of a single residue / a pair; canonical residues come from
+// shared memory, IUPAC codes from the full 18 / 18x18 rows in global memory.
 template <class S>
-__device__ __forceinline__ typename S::T rd(const SInfo &Y, const uint32_t *deck, int slot, int idx,
-                                            const uint32_t *init0, int y) {
-    if ((unsigned)(idx - Y.dn) <= (unsigned)(Y.dxcap - Y.dn) && Y.width > 0) {
-        int so = (Y.flags & (SF_TWO_SLOT | SF_BEGL)) ? slot * Y.width : 0;
-        return S::ld(deck + Y.base + so + idx);
-    }
-    if (idx == 0) return S::ldg(init0 + y);
-    return S::zero();
+__device__ __forceinline__ typename S::T esc1(const K &k, int v, int escoff, int c) {
+    if (c < 4) return S::ld(k.s.escc + escoff + c);
+    return S::ldg(k.p->esc + v * 324 + c);
+}
+template <class S>
+__device__ __forceinline__ typename S::T esc2(const K &k, int v, int escoff, int a, int b) {
+    if ((a | b) < 4) return S::ld(k.s.escc + escoff + a * 4 + b);
+    return S::ldg(k.p->esc + v * 324 + a * 18 + b);
 }
 
-// reduce_c_order (src/cm_nohmm.rs:187-242); t[] are the child terms.
 template <class S>
 __device__ __forceinline__ typename S::T reduce_c(int cnum, const typename S::T *t, typename S::T init,
                                                   const uint16_t *tb, int nz) {
@@ -160,14 +175,13 @@ __device__ __forceinline__ typename S::T reduce_c(int cnum, const typename S::T 
         s = S::comb(s, t[1], tb, nz);
         s = S::comb(s, t[0], tb, nz);
         break;
-    default:
+    default:  // cnum is 1..6 for every non-B, non-E state of a CM
         s = init;
-        for (int q = 0; q < cnum; q++) s = S::comb(s, t[q], tb, nz);
     }
     return s;
 }
 
-// The same order with the self term t[0] left out: the IL step is then
+// reduce_c_order with the self term t[0] left out: the IL step is then
 // comb(c, x + t0) (t[0] is combined last for every cnum).
 template <class S>
 __device__ __forceinline__ typename S::T reduce_c_noself(int cnum, const typename S::T *t, typename S::T init,
@@ -196,182 +210,172 @@ __device__ __forceinline__ typename S::T reduce_c_noself(int cnum, const typenam
         s = S::comb(s, t[2], tb, nz);
         s = S::comb(s, t[1], tb, nz);
         break;
-    default:
+    default:  // cnum is 1..6 for every non-B, non-E state of a CM
         s = init;
-        for (int q = 1; q < cnum; q++) s = S::comb(s, t[q], tb, nz);
     }
     return s;
 }
 
-struct Ctx {
-    const ScanParams *p;
-    uint32_t *deck;
-    const uint32_t *el_sca;   // shared
-    const uint16_t *tbl;      // shared ILogsum table (Inside)
-    const uint8_t *frame;     // window frame of the current item
-    int j, cur, prv, jm, jrow;
-};
-
-// Children terms of cell (v, d) for a non-B state: terms[yo] = child + tsc.
+// Child terms of cell d: deck[cb[v][yo][par] + d] + tsc[v][yo].  The padded
+// deck layout makes every read a plain load (no band test).
 template <class S>
-__device__ __forceinline__ void child_terms(const Ctx &c, const SInfo &sv, int v, int idx, int slot,
+__device__ __forceinline__ void child_terms(const K &k, int v, int cnum, const uint32_t *deck, int par, int d,
                                             typename S::T *terms, int first) {
-    const ScanParams &p = *c.p;
-    for (int yo = first; yo < sv.cnum; yo++) {
-        int y = sv.cfirst + yo;
-        SInfo sy = load_info(p.states, y);
-        terms[yo] = S::add(rd<S>(sy, c.deck, slot, idx, p.init0, y), S::ldg(p.tsc + v * 6 + yo));
-    }
+    const int32_t *cb = k.s.cb + v * 12 + par;
+    const uint32_t *tsc = k.s.tsc + v * 6;
+#pragma unroll
+    for (int yo = 0; yo < 6; yo++)
+        if (yo >= first && yo < cnum) terms[yo] = S::add(S::ld(deck + cb[2 * yo] + d), S::ld(tsc + yo));
 }
 
 template <class S>
-__device__ __forceinline__ typename S::T init_sc(const Ctx &c, const SInfo &sv, int v, int idx) {
-    if (sv.flags & SF_ENDSC) return S::add(S::ld(c.el_sca + idx), S::ldg(c.p->endsc + v));
+__device__ __forceinline__ typename S::T init_sc(const K &k, const SInfo &sv, int v, int idx) {
+    if (sv.flags & SF_ENDSC) return S::add(S::ld(k.s.el + idx), S::ld(k.s.endsc + v));
     return S::zero();
 }
 
+__device__ __forceinline__ int resid(const Lane &L, int x, int rmask) { return L.ring[x & rmask]; }
+
 // One warp-wide chunk of an ordinary state (not B, not IL).
 template <class S>
-__device__ __forceinline__ void do_chunk(const Ctx &c, int v, int d0, int lane) {
+__device__ __forceinline__ void do_chunk(const K &k, const Lane &L, int v, const SInfo &sv, int d0, int lane) {
     typedef typename S::T T;
-    const ScanParams &p = *c.p;
-    SInfo sv = load_info(p.states, v);
-    int d = d0 + lane;
-    int dx = min(c.jrow, (int)sv.dxcap);
+    const int d = d0 + lane;
+    const int dx = min(L.jrow, sv.dxcap);
     if (d > dx) return;
-    int t = sv.type;
-    int sd = state_delta(t);
-    bool rem = right_em(t);
-    int slot_y = rem ? c.prv : c.cur;
-    int idx = d - sd;
+    const int t = sv.type;
     T terms[6];
-    child_terms<S>(c, sv, v, idx, slot_y, terms, 0);
+    child_terms<S>(k, v, sv.cnum, L.deck, L.par, d, terms, 0);
+    const int idx = d - sv.sd;
     T sc;
     if (sv.flags & SF_BEGL) {
         // BEGL_S folds its children in natural order (src/cm_nohmm.rs:601-611)
-        sc = init_sc<S>(c, sv, v, idx);
-        for (int yo = 0; yo < sv.cnum; yo++) sc = S::comb(sc, terms[yo], c.tbl, p.ilog_nz);
+        sc = init_sc<S>(k, sv, v, idx);
+#pragma unroll
+        for (int yo = 0; yo < 6; yo++)
+            if (yo < sv.cnum) sc = S::comb(sc, terms[yo], k.s.tbl, k.nz);
     } else {
-        sc = reduce_c<S>(sv.cnum, terms, init_sc<S>(c, sv, v, idx), c.tbl, p.ilog_nz);
+        sc = reduce_c<S>(sv.cnum, terms, init_sc<S>(k, sv, v, idx), k.s.tbl, k.nz);
     }
-    int esc_off = v * 324;
     if (t == 2 || t == 4) {  // ML, IL: residue i = j-d+1
-        sc = S::add(sc, S::ldg(p.esc + esc_off + res(c.frame, c.j - d + 1)));
+        sc = S::add(sc, esc1<S>(k, v, sv.escoff, resid(L, L.j - d + 1, k.rmask)));
     } else if (t == 3 || t == 5) {  // MR, IR: residue j
-        sc = S::add(sc, S::ldg(p.esc + esc_off + res(c.frame, c.j)));
+        sc = S::add(sc, esc1<S>(k, v, sv.escoff, resid(L, L.j, k.rmask)));
     } else if (t == 1) {  // MP
-        sc = S::add(sc, S::ldg(p.esc + esc_off + res(c.frame, c.j - d + 1) * 18 + res(c.frame, c.j)));
+        sc = S::add(sc, esc2<S>(k, v, sv.escoff, resid(L, L.j - d + 1, k.rmask), resid(L, L.j, k.rmask)));
     }
-    int so;
-    if (sv.flags & SF_BEGL)
-        so = c.jm * sv.width;
-    else if (sv.flags & SF_TWO_SLOT)
-        so = c.cur * sv.width;
-    else
-        so = 0;
-    S::st(c.deck + sv.base + so + d, sc);
+    const int wbase = (sv.flags & SF_BEGL) ? k.s.wb[v * 2] + L.jm * sv.span : k.s.wb[v * 2 + L.par];
+    S::st(L.deck + wbase + d, sc);
 }
 
 // Bifurcation chunk: alpha[v][d] = init (+) over k ascending of
 // BEGL(j-k, d-k) + BEGR(j, k) (src/cm_nohmm.rs:578-600).
 template <class S>
-__device__ __forceinline__ void do_bif_chunk(const Ctx &c, int v, int d0, int lane) {
+__device__ __forceinline__ void do_bif_chunk(const K &k, const Lane &L, int v, const SInfo &sv, int d0, int lane) {
     typedef typename S::T T;
-    const ScanParams &p = *c.p;
-    SInfo sv = load_info(p.states, v);
-    int d = d0 + lane;
-    int dx = min(c.jrow, (int)sv.dxcap);
+    const int d = d0 + lane;
+    const int dx = min(L.jrow, sv.dxcap);
     if (d > dx) return;
-    int4 q2 = __ldg(reinterpret_cast<const int4 *>(p.states + v) + 1);
-    int kdn_y = (int16_t)(q2.x & 0xffff), kdx_y = (int16_t)((uint32_t)q2.x >> 16);
-    int kdn_w = (int16_t)(q2.y & 0xffff), kdx_w = (int16_t)((uint32_t)q2.y >> 16);
-    int wl = sv.cfirst, y = sv.cnum;
-    SInfo sw = load_info(p.states, wl);
-    SInfo sy = load_info(p.states, y);
-    int kmin = max(0, max(kdn_y, d - kdx_w));
-    int kmax = min(kdx_y, d - kdn_w);
-    T sc = init_sc<S>(c, sv, v, d);
-    const int W1 = p.W + 1;
-    int col = c.jm - kmin;
+    const int32_t *c = k.s.cb + v * 12;
+    const int begl = c[0], begr = c[2], kdn_y = c[4], kdx_y = c[5], kdn_w = c[6], kdx_w = c[7], span_w = c[8];
+    const int kmin = max(0, max(kdn_y, d - kdx_w));
+    const int kmax = min(kdx_y, d - kdn_w);
+    T sc = init_sc<S>(k, sv, v, d);
+    const int W1 = k.p->W + 1;
+    int col = L.jm - kmin;
     if (col < 0) col += W1;
+    const uint32_t *left = L.deck + begl + d;
+    const uint32_t *right = L.deck + begr;
     for (int kk = kmin; kk <= kmax; kk++) {
-        T left = rd<S>(sw, c.deck, col, d - kk, p.init0, wl);
-        T right = rd<S>(sy, c.deck, c.cur, kk, p.init0, y);
-        sc = S::comb(sc, S::add(left, right), c.tbl, p.ilog_nz);
+        T lv = S::ld(left + col * span_w - kk);
+        T rv = S::ld(right + kk);
+        sc = S::comb(sc, S::add(lv, rv), k.s.tbl, k.nz);
         col = col == 0 ? W1 - 1 : col - 1;
     }
-    int so = (sv.flags & SF_TWO_SLOT) ? c.cur * sv.width : 0;
-    S::st(c.deck + sv.base + so + d, sc);
+    S::st(L.deck + k.s.wb[v * 2 + L.par] + d, sc);
+}
+
+// IL relaxation with up to KC cells per lane held in registers.
+template <class S, int KC>
+__device__ __forceinline__ void il_relax(const K &k, const Lane &L, int v, const SInfo &sv, int dn, int dx, int kk,
+                                         int lane) {
+    typedef typename S::T T;
+    const T t0 = S::ld(k.s.tsc + v * 6);
+    uint32_t *dst = L.deck + k.s.wb[v * 2];  // IL is single-slot
+    T cv[KC], ev[KC], xv[KC];
+    const int dbeg = dn + lane * kk;
+    const bool has = dbeg <= dx;
+#pragma unroll
+    for (int q = 0; q < KC; q++) {
+        int d = dbeg + q;
+        cv[q] = S::zero();
+        ev[q] = S::zero();
+        xv[q] = S::zero();
+        if (q < kk && d <= dx) {
+            T terms[6];
+            child_terms<S>(k, v, sv.cnum, L.deck, L.par, d, terms, 1);
+            cv[q] = reduce_c_noself<S>(sv.cnum, terms, init_sc<S>(k, sv, v, d - 1), k.s.tbl, k.nz);
+            ev[q] = esc1<S>(k, v, sv.escoff, resid(L, L.j - d + 1, k.rmask));
+        }
+    }
+    // x at d = dn-1 is an unwritten cell of the emitter: zero.
+    T xin = S::zero(), xin_prev = S::zero();
+    for (int it = 0; it < 34; it++) {
+        T x = xin;
+#pragma unroll
+        for (int q = 0; q < KC; q++) {
+            if (q < kk && dbeg + q <= dx) {
+                x = S::add(S::comb(cv[q], S::add(x, t0), k.s.tbl, k.nz), ev[q]);
+                xv[q] = x;
+            }
+        }
+        // a lane without cells passes nothing on
+        T xlast = has ? x : S::zero();
+        bool same = !has || S::u(xin) == S::u(xin_prev);
+        if (it > 0 && __all_sync(0xffffffffu, same)) break;
+        xin_prev = xin;
+        T up = __shfl_up_sync(0xffffffffu, xlast, 1);
+        xin = lane == 0 ? S::zero() : up;
+    }
+#pragma unroll
+    for (int q = 0; q < KC; q++) {
+        int d = dbeg + q;
+        if (q < kk && d <= dx) S::st(dst + d, xv[q]);
+    }
 }
 
 // IL state: whole band by one warp (see the file comment).
 template <class S>
-__device__ __forceinline__ void do_il(const Ctx &c, int v, int lane) {
+__device__ __forceinline__ void do_il(const K &k, const Lane &L, int v, const SInfo &sv, int lane) {
     typedef typename S::T T;
-    const ScanParams &p = *c.p;
-    SInfo sv = load_info(p.states, v);
     const int dn = sv.dn;
-    const int dx = min(c.jrow, (int)sv.dxcap);
+    const int dx = min(L.jrow, sv.dxcap);
     const int n = dx - dn + 1;
     if (n <= 0) return;
-    const T t0 = S::ldg(p.tsc + v * 6);
-    const int esc_off = v * 324;
-    uint32_t *dst = c.deck + sv.base;  // IL is single-slot
-    const int k = (n + 31) >> 5;
-    if (k <= IL_KMAX) {
-        T cv[IL_KMAX], ev[IL_KMAX], xv[IL_KMAX];
-        const int dbeg = dn + lane * k;
-#pragma unroll
-        for (int q = 0; q < IL_KMAX; q++) {
-            int d = dbeg + q;
-            cv[q] = S::zero();
-            ev[q] = S::zero();
-            xv[q] = S::zero();
-            if (q < k && d <= dx) {
-                int idx = d - 1;
-                T terms[6];
-                child_terms<S>(c, sv, v, idx, c.cur, terms, 1);
-                cv[q] = reduce_c_noself<S>(sv.cnum, terms, init_sc<S>(c, sv, v, idx), c.tbl, p.ilog_nz);
-                ev[q] = S::ldg(p.esc + esc_off + res(c.frame, c.j - d + 1));
-            }
-        }
-        // x at d = dn-1 is an unwritten cell of the emitter: zero.
-        T xin = S::zero(), xin_prev = S::zero(), xlast = S::zero();
-        for (int it = 0; it < 34; it++) {
-            T x = xin;
-#pragma unroll
-            for (int q = 0; q < IL_KMAX; q++) {
-                if (q < k && dbeg + q <= dx) {
-                    x = S::add(S::comb(cv[q], S::add(x, t0), c.tbl, p.ilog_nz), ev[q]);
-                    xv[q] = x;
-                }
-            }
-            xlast = x;
-            bool same = S::u(xin) == S::u(xin_prev);
-            if (it > 0 && __all_sync(0xffffffffu, same)) break;
-            xin_prev = xin;
-            T up = __shfl_up_sync(0xffffffffu, xlast, 1);
-            xin = lane == 0 ? S::zero() : up;
-        }
-#pragma unroll
-        for (int q = 0; q < IL_KMAX; q++) {
-            int d = dbeg + q;
-            if (q < k && d <= dx) S::st(dst + d, xv[q]);
-        }
+    const int kk = (n + 31) >> 5;
+    if (kk == 1) {
+        il_relax<S, 1>(k, L, v, sv, dn, dx, kk, lane);
+    } else if (kk == 2) {
+        il_relax<S, 2>(k, L, v, sv, dn, dx, kk, lane);
+    } else if (kk <= 4) {
+        il_relax<S, 4>(k, L, v, sv, dn, dx, kk, lane);
+    } else if (kk <= IL_KMAX) {
+        il_relax<S, IL_KMAX>(k, L, v, sv, dn, dx, kk, lane);
     } else {
-        // wide band: compute c in parallel into the deck, then one lane walks d
+        // wide band: c in parallel into the deck, then one lane walks d
+        const T t0 = S::ld(k.s.tsc + v * 6);
+        uint32_t *dst = L.deck + k.s.wb[v * 2];
         for (int d = dn + lane; d <= dx; d += 32) {
-            int idx = d - 1;
             T terms[6];
-            child_terms<S>(c, sv, v, idx, c.cur, terms, 1);
-            S::st(dst + d, reduce_c_noself<S>(sv.cnum, terms, init_sc<S>(c, sv, v, idx), c.tbl, p.ilog_nz));
+            child_terms<S>(k, v, sv.cnum, L.deck, L.par, d, terms, 1);
+            S::st(dst + d, reduce_c_noself<S>(sv.cnum, terms, init_sc<S>(k, sv, v, d - 1), k.s.tbl, k.nz));
         }
         __syncwarp();
         if (lane == 0) {
             T x = S::zero();
             for (int d = dn; d <= dx; d++) {
-                T e = S::ldg(p.esc + esc_off + res(c.frame, c.j - d + 1));
-                x = S::add(S::comb(S::ld(dst + d), S::add(x, t0), c.tbl, p.ilog_nz), e);
+                T e = esc1<S>(k, v, sv.escoff, resid(L, L.j - d + 1, k.rmask));
+                x = S::add(S::comb(S::ld(dst + d), S::add(x, t0), k.s.tbl, k.nz), e);
                 S::st(dst + d, x);
             }
         }
@@ -379,102 +383,231 @@ __device__ __forceinline__ void do_il(const Ctx &c, int v, int lane) {
     }
 }
 
+// lane-state fields in shared memory
+enum { LS_ITEM = 0, LS_JB, LS_JSTART, LS_JEND, LS_JREPORT, LS_OFFLO, LS_OFFHI, LS_JM };
+constexpr int LS_W = 8;
+
 template <bool INS, bool DECK_SMEM>
-__global__ void __launch_bounds__(512) qdb_scan_kernel(ScanParams p) {
+__global__ void __launch_bounds__(512, 1) qdb_scan_kernel(ScanParams p) {
     typedef Sem<INS> S;
     typedef typename S::T T;
     extern __shared__ __align__(16) uint32_t smem[];
-    uint32_t *s_el = smem;                                     // W+1
-    uint16_t *s_tbl = reinterpret_cast<uint16_t *>(smem + (p.W + 1));
-    const int tbl_words = INS ? (p.ilog_nz + 1) / 2 : 0;
-    uint32_t *s_deck = smem + (p.W + 1) + tbl_words;
-    __shared__ int s_item;
+    __shared__ int s_fresh[MAX_LANES];
+    __shared__ int s_any;
+    const SmemLayout &ly = p.lay;
+    K k;
+    k.p = &p;
+    k.nz = p.ilog_nz;
+    k.s.el = smem + ly.el;
+    k.s.tbl = reinterpret_cast<const uint16_t *>(smem + ly.tbl);
+    k.s.info = reinterpret_cast<const int4 *>(smem + ly.info);
+    k.s.wb = reinterpret_cast<const int32_t *>(smem + ly.wb);
+    k.s.cb = reinterpret_cast<const int32_t *>(smem + ly.cb);
+    k.s.tsc = smem + ly.tsc;
+    k.s.endsc = smem + ly.endsc;
+    k.s.escc = smem + ly.escc;
+    k.s.chunks = reinterpret_cast<const int2 *>(smem + ly.chunks);
+    k.s.lvl = reinterpret_cast<const int32_t *>(smem + ly.lvl);
+    k.s.begin = reinterpret_cast<const int4 *>(smem + ly.begin);
+    k.s.beginsc = smem + ly.beginsc;
+    k.s.ring = reinterpret_cast<uint8_t *>(smem + ly.ring);
+    k.s.lane = reinterpret_cast<int32_t *>(smem + ly.lane);
+    k.rmask = ly.ring_len - 1;
 
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
-    for (int k = tid; k <= p.W; k += blockDim.x) s_el[k] = __ldg(p.el_sca + k);
-    if (INS)
-        for (int k = tid; k < p.ilog_nz; k += blockDim.x) s_tbl[k] = __ldg(p.ilog + k);
-
-    Ctx c;
-    c.p = &p;
-    c.deck = DECK_SMEM ? s_deck : p.deck_global + (size_t)blockIdx.x * (size_t)p.deck_stride;
-    c.el_sca = s_el;
-    c.tbl = s_tbl;
-    const T ZERO = S::zero();
+    const int tid = threadIdx.x, wl = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    const int bs = blockDim.x;
+    const int lanes = p.lanes;
     const int W1 = p.W + 1;
+    const T ZERO = S::zero();
+
+    // ---- model metadata into shared memory ----
+    {
+        auto copy32 = [&](int dst, const void *src, int n) {
+            const uint32_t *g = reinterpret_cast<const uint32_t *>(src);
+            for (int x = tid; x < n; x += bs) smem[dst + x] = __ldg(g + x);
+        };
+        copy32(ly.el, p.el_sca, p.W + 1);
+        if (INS) copy32(ly.tbl, p.ilog, (p.ilog_nz + 1) / 2);
+        copy32(ly.info, p.states, p.M * 4);
+        copy32(ly.wb, p.wb, p.M * 2);
+        copy32(ly.cb, p.cb, p.M * 12);
+        copy32(ly.tsc, p.tsc, p.M * 6);
+        copy32(ly.endsc, p.endsc, p.M);
+        copy32(ly.escc, p.esc_c, p.n_esc_c);
+        copy32(ly.chunks, p.chunks, p.nchunks * 2);
+        copy32(ly.lvl, p.level_start, p.nlev + 1);
+        copy32(ly.begin, p.begins, p.nbegin * 4);
+        copy32(ly.beginsc, p.beginsc, p.nbegin);
+        if (tid < MAX_LANES * LS_W) k.s.lane[tid] = tid % LS_W == LS_ITEM ? -1 : 0;
+    }
+    uint32_t *deck_base = DECK_SMEM ? smem + ly.deck
+                                    : p.deck_global + (size_t)blockIdx.x * (size_t)lanes * (size_t)p.deck_stride;
+    const int64_t deck_stride = DECK_SMEM ? p.deck_elems : p.deck_stride;
+    const int rw = max(0, p.root_dxcap - p.root_dn + 1);
+    // per-warp walk over units (ci, l): start (u_c0, u_l0), stride (u_dc, u_dl)
+    const int u_l0 = warp % lanes, u_c0 = warp / lanes;
+    const int u_dl = nwarps % lanes, u_dc = nwarps / lanes;
+    // per-thread walk over root cells (l, d): start (r_l0, r_d0), stride (r_dl, r_dd)
+    const int r_l0 = rw > 0 ? tid / rw : 0, r_d0 = rw > 0 ? tid % rw : 0;
+    const int r_dl = rw > 0 ? bs / rw : 0, r_dd = rw > 0 ? bs % rw : 0;
 
     for (;;) {
         __syncthreads();
-        if (tid == 0) s_item = atomicAdd(p.next_item, 1);
+        // ---- refill lanes whose item ended ----
+        if (tid == 0) {
+            int any = 0;
+            for (int l = 0; l < lanes; l++) {
+                int32_t *ls = k.s.lane + l * LS_W;
+                s_fresh[l] = 0;
+                if (ls[LS_ITEM] == -1 || (ls[LS_ITEM] >= 0 && ls[LS_JB] > ls[LS_JEND])) {
+                    int it = atomicAdd(p.next_item, 1);
+                    if (it < p.nitems) {
+                        WorkItem wi = p.items[it];
+                        ls[LS_ITEM] = it;
+                        ls[LS_JB] = wi.jstart;
+                        ls[LS_JSTART] = wi.jstart;
+                        ls[LS_JEND] = wi.jend;
+                        ls[LS_JREPORT] = wi.jreport;
+                        ls[LS_OFFLO] = (int32_t)(uint32_t)((uint64_t)wi.dsq_off & 0xffffffffu);
+                        ls[LS_OFFHI] = (int32_t)(uint32_t)((uint64_t)wi.dsq_off >> 32);
+                        ls[LS_JM] = wi.jstart % W1;
+                        s_fresh[l] = 1;
+                    } else {
+                        ls[LS_ITEM] = -2;
+                    }
+                }
+                if (ls[LS_ITEM] >= 0) any = 1;
+            }
+            s_any = any;
+        }
         __syncthreads();
-        const int it = s_item;
-        if (it >= p.nitems) break;
-        const WorkItem wi = p.items[it];
-        for (int64_t k = tid; k < p.deck_elems; k += blockDim.x) S::st(c.deck + k, ZERO);
+        if (!s_any) break;
+        // ---- fresh decks: fill, then the d = 0 base cells ----
+        bool any_fresh = false;
+        for (int l = 0; l < lanes; l++) {
+            if (!s_fresh[l]) continue;
+            any_fresh = true;
+            uint32_t *dk = deck_base + (size_t)l * deck_stride;
+            for (int64_t x = tid; x < p.deck_elems; x += bs) S::st(dk + x, ZERO);
+        }
+        if (any_fresh) {
+            __syncthreads();
+            for (int l = 0; l < lanes; l++) {
+                if (!s_fresh[l]) continue;
+                uint32_t *dk = deck_base + (size_t)l * deck_stride;
+                for (int x = tid; x < p.ninit; x += bs) dk[__ldg(p.init_off + x)] = __ldg(p.init_val + x);
+            }
+        }
+        // ---- residues of this block into the lane rings ----
+        for (int t = tid; t < lanes * COL_BLOCK; t += bs) {
+            int l = t / COL_BLOCK, q = t % COL_BLOCK;
+            const int32_t *ls = k.s.lane + l * LS_W;
+            int x = ls[LS_JB] + q;
+            if (ls[LS_ITEM] >= 0 && x <= ls[LS_JEND]) {
+                uint64_t off = (uint64_t)(uint32_t)ls[LS_OFFLO] | ((uint64_t)(uint32_t)ls[LS_OFFHI] << 32);
+                int c = __ldg(p.dsq + off + x);
+                k.s.ring[l * ly.ring_len + (x & k.rmask)] = (uint8_t)(c > 17 ? 17 : c);
+            }
+        }
         __syncthreads();
-        c.frame = p.dsq + wi.dsq_off;
-        int jm = wi.jstart % W1;
-        for (int j = wi.jstart; j <= wi.jend; j++) {
-            c.j = j;
-            c.cur = j & 1;
-            c.prv = c.cur ^ 1;
-            c.jm = jm;
-            c.jrow = min(j - wi.jstart + 1, p.W);
-            for (int l = 0; l < p.nlev; l++) {
-                const int c0 = __ldg(p.level_start + l), c1 = __ldg(p.level_start + l + 1);
-                for (int ci = c0 + warp; ci < c1; ci += nwarps) {
-                    ChunkDev ch = p.chunks[ci];
-                    int t = p.states[ch.v].type;
-                    if (ch.d0 < 0)
-                        do_il<S>(c, ch.v, lane);
-                    else if (t == 8)
-                        do_bif_chunk<S>(c, ch.v, ch.d0, lane);
+
+        for (int step = 0; step < COL_BLOCK; step++) {
+            // ---- levels ----
+            for (int lev = 0; lev < p.nlev; lev++) {
+                const int c0 = k.s.lvl[lev], nch = k.s.lvl[lev + 1] - c0;
+                // unit u = ci * lanes + l, walked without divisions
+                int l = u_l0, ci = u_c0;
+                for (; ci < nch; l += u_dl, ci += u_dc) {
+                    if (l >= lanes) {
+                        l -= lanes;
+                        ci++;
+                        if (ci >= nch) break;
+                    }
+                    const int32_t *ls = k.s.lane + l * LS_W;
+                    const int j = ls[LS_JB] + step;
+                    if (ls[LS_ITEM] < 0 || j > ls[LS_JEND]) continue;
+                    Lane L;
+                    L.deck = deck_base + (size_t)l * deck_stride;
+                    L.ring = k.s.ring + l * ly.ring_len;
+                    L.j = j;
+                    L.par = j & 1;
+                    int jm = ls[LS_JM] + step;
+                    while (jm >= W1) jm -= W1;
+                    L.jm = jm;
+                    L.jrow = min(j - ls[LS_JSTART] + 1, p.W);
+                    const int2 ch = k.s.chunks[c0 + ci];
+                    const SInfo sv = unpack(k.s.info[ch.x]);
+                    if (ch.y < 0)
+                        do_il<S>(k, L, ch.x, sv, wl);
+                    else if (sv.type == 8)
+                        do_bif_chunk<S>(k, L, ch.x, sv, ch.y, wl);
                     else
-                        do_chunk<S>(c, ch.v, ch.d0, lane);
+                        do_chunk<S>(k, L, ch.x, sv, ch.y, wl);
                 }
                 __syncthreads();
             }
-            // ROOT_S, local begins, candidates
-            const int dx0 = min(c.jrow, p.root_dxcap);
-            const bool report = j >= wi.jreport;
-            for (int dbase = p.root_dn; dbase <= dx0; dbase += blockDim.x) {
-                const int d = dbase + tid;
+            // ---- ROOT_S, local begins, candidates ----
+            int rl = r_l0, rd0 = r_d0;
+            for (int tb = 0; tb < lanes * rw; tb += bs, rl += r_dl, rd0 += r_dd) {
+                if (rd0 >= rw) {
+                    rd0 -= rw;
+                    rl++;
+                }
                 bool hit = false;
                 T a = ZERO;
-                if (d <= dx0) {
-                    for (int yo = 0; yo < p.root_cnum; yo++) {
-                        int y = p.root_cfirst + yo;
-                        SInfo sy = load_info(p.states, y);
-                        T term = S::add(rd<S>(sy, c.deck, c.cur, d, p.init0, y), S::ldg(p.tsc + yo));
-                        a = yo == 0 ? S::comb(ZERO, term, c.tbl, p.ilog_nz) : S::comb(a, term, c.tbl, p.ilog_nz);
-                    }
-                    if (p.local) {
-                        for (int b = 0; b < p.nbegin; b++) {
-                            int y = __ldg(p.begin_states + b);
-                            SInfo sy = load_info(p.states, y);
-                            int hi = min(dx0, (int)sy.dxcap);
-                            if (d < sy.dn || d > hi) continue;
-                            T val = rd<S>(sy, c.deck, (sy.flags & SF_BEGL) ? jm : c.cur, d, p.init0, y);
-                            T cand = S::add(val, S::ldg(p.beginsc + y));
-                            if (a < cand) a = cand;
+                int l = rl, d = p.root_dn + rd0, j = 0;
+                if (rl < lanes) {
+                    const int32_t *ls = k.s.lane + l * LS_W;
+                    j = ls[LS_JB] + step;
+                    if (ls[LS_ITEM] >= 0 && j <= ls[LS_JEND]) {
+                        const int jrow = min(j - ls[LS_JSTART] + 1, p.W);
+                        const int dx0 = min(jrow, p.root_dxcap);
+                        if (d <= dx0) {
+                            const uint32_t *deck = deck_base + (size_t)l * deck_stride;
+                            const int par = j & 1;
+                            int jm = ls[LS_JM] + step;
+                            while (jm >= W1) jm -= W1;
+#pragma unroll
+                            for (int yo = 0; yo < 6; yo++) {
+                                if (yo < p.root_cnum) {
+                                    T term = S::add(S::ld(deck + k.s.cb[2 * yo + par] + d), S::ld(k.s.tsc + yo));
+                                    a = yo == 0 ? S::comb(ZERO, term, k.s.tbl, k.nz) : S::comb(a, term, k.s.tbl, k.nz);
+                                }
+                            }
+                            if (p.local) {
+                                for (int b = 0; b < p.nbegin; b++) {
+                                    const int4 bd = k.s.begin[b];
+                                    const int dn = (int16_t)(bd.w & 0xffff), dxc = (int16_t)((uint32_t)bd.w >> 16);
+                                    if (d < dn || d > dxc) continue;
+                                    int rb;
+                                    if (bd.y == bd.z) {  // single slot, or a BEGL ring
+                                        const SInfo sy = unpack(k.s.info[bd.x]);
+                                        rb = (sy.flags & SF_BEGL) ? bd.y + jm * sy.span : bd.y;
+                                    } else {
+                                        rb = par ? bd.z : bd.y;
+                                    }
+                                    T cand = S::add(S::ld(deck + rb + d), S::ld(k.s.beginsc + b));
+                                    if (a < cand) a = cand;
+                                }
+                            }
+                            if (j >= ls[LS_JREPORT]) {
+                                float sc = S::bits(a);
+                                hit = sc >= p.cutoff && sc > IMPOSSIBLE_D + 1.0f;
+                            }
                         }
-                    }
-                    if (report) {
-                        float sc = S::bits(a);
-                        hit = sc >= p.cutoff && sc > IMPOSSIBLE_D + 1.0f;
                     }
                 }
                 unsigned m = __ballot_sync(0xffffffffu, hit);
                 if (m) {
                     int leader = __ffs(m) - 1;
                     int base = 0;
-                    if (lane == leader) base = atomicAdd(p.cand_count, __popc(m));
+                    if (wl == leader) base = atomicAdd(p.cand_count, __popc(m));
                     base = __shfl_sync(0xffffffffu, base, leader);
                     if (hit) {
-                        int pos = base + __popc(m & ((1u << lane) - 1));
+                        int pos = base + __popc(m & ((1u << wl) - 1));
                         if (pos < p.cand_cap) {
                             Cand cd;
-                            cd.item = p.item_base + it;
+                            cd.item = p.item_base + k.s.lane[l * LS_W + LS_ITEM];
                             cd.j = j;
                             cd.d = d;
                             cd.raw = S::u(a);
@@ -483,14 +616,23 @@ __global__ void __launch_bounds__(512) qdb_scan_kernel(ScanParams p) {
                     }
                 }
             }
-            jm = jm + 1 == W1 ? 0 : jm + 1;
+        }
+        // advance every live lane by one block
+        __syncthreads();
+        if (tid < lanes) {
+            int32_t *ls = k.s.lane + tid * LS_W;
+            if (ls[LS_ITEM] >= 0) {
+                ls[LS_JB] += COL_BLOCK;
+                ls[LS_JM] = (ls[LS_JM] + COL_BLOCK) % W1;
+            }
         }
     }
 }
 
 template <bool INS, bool DS>
-static cudaError_t launch_t(const ScanParams &p, int ctas, int threads, size_t smem, cudaStream_t s) {
+static cudaError_t launch_t(const ScanParams &p, int ctas, int threads, cudaStream_t s) {
     auto kern = qdb_scan_kernel<INS, DS>;
+    size_t smem = (size_t)p.lay.words * 4;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     kern<<<ctas, threads, smem, s>>>(p);
@@ -498,9 +640,10 @@ static cudaError_t launch_t(const ScanParams &p, int ctas, int threads, size_t s
 }
 
 template <bool INS, bool DS>
-static int occupancy_t(int threads, size_t smem) {
+static int occupancy_t(const ScanParams &p, int threads) {
     int n = 0;
     auto kern = qdb_scan_kernel<INS, DS>;
+    size_t smem = (size_t)p.lay.words * 4;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, threads, smem) != cudaSuccess) return 0;
     return n;
@@ -508,27 +651,48 @@ static int occupancy_t(int threads, size_t smem) {
 
 }  // namespace dev
 
-size_t scan_smem_bytes(const ScanParams &p, bool deck_smem) {
-    size_t b = (size_t)(p.W + 1) * 4;
-    if (p.inside) b += (size_t)((p.ilog_nz + 1) / 2) * 4;
-    if (deck_smem) b += (size_t)p.deck_elems * 4;
-    return b;
+SmemLayout scan_layout(const ScanParams &p, int lanes, bool deck_smem) {
+    SmemLayout L{};
+    int64_t w = 0;
+    auto take = [&](int64_t n) {
+        int64_t o = w;
+        w += (n + 3) & ~(int64_t)3;  // keep 16-byte alignment
+        return (int)o;
+    };
+    L.el = take(p.W + 1);
+    L.tbl = take(p.inside ? (p.ilog_nz + 1) / 2 : 0);
+    L.info = take((int64_t)p.M * 4);
+    L.wb = take((int64_t)p.M * 2);
+    L.cb = take((int64_t)p.M * 12);
+    L.tsc = take((int64_t)p.M * 6);
+    L.endsc = take(p.M);
+    L.escc = take(p.n_esc_c);
+    L.chunks = take((int64_t)p.nchunks * 2);
+    L.lvl = take(p.nlev + 1);
+    L.begin = take((int64_t)p.nbegin * 4);
+    L.beginsc = take(p.nbegin);
+    int r = 1;
+    while (r < p.W + 64) r <<= 1;
+    L.ring_len = r;
+    L.ring = take((int64_t)lanes * r / 4);
+    L.lane = take((int64_t)MAX_LANES * 8);
+    L.deck = take(deck_smem ? (int64_t)lanes * p.deck_elems : 0);
+    L.words = w;
+    return L;
 }
 
-int scan_occupancy(const ScanParams &p, bool deck_smem, int threads) {
-    size_t smem = scan_smem_bytes(p, deck_smem);
+int scan_occupancy(const ScanParams &p, int threads) {
     if (p.inside)
-        return deck_smem ? dev::occupancy_t<true, true>(threads, smem) : dev::occupancy_t<true, false>(threads, smem);
-    return deck_smem ? dev::occupancy_t<false, true>(threads, smem) : dev::occupancy_t<false, false>(threads, smem);
+        return p.deck_smem ? dev::occupancy_t<true, true>(p, threads) : dev::occupancy_t<true, false>(p, threads);
+    return p.deck_smem ? dev::occupancy_t<false, true>(p, threads) : dev::occupancy_t<false, false>(p, threads);
 }
 
-cudaError_t scan_launch(const ScanParams &p, bool deck_smem, int ctas, int threads, cudaStream_t s) {
-    size_t smem = scan_smem_bytes(p, deck_smem);
+cudaError_t scan_launch(const ScanParams &p, int ctas, int threads, cudaStream_t s) {
     if (p.inside)
-        return deck_smem ? dev::launch_t<true, true>(p, ctas, threads, smem, s)
-                         : dev::launch_t<true, false>(p, ctas, threads, smem, s);
-    return deck_smem ? dev::launch_t<false, true>(p, ctas, threads, smem, s)
-                     : dev::launch_t<false, false>(p, ctas, threads, smem, s);
+        return p.deck_smem ? dev::launch_t<true, true>(p, ctas, threads, s)
+                           : dev::launch_t<true, false>(p, ctas, threads, s);
+    return p.deck_smem ? dev::launch_t<false, true>(p, ctas, threads, s)
+                       : dev::launch_t<false, false>(p, ctas, threads, s);
 }
 
 }  // namespace cmx

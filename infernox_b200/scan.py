@@ -68,8 +68,8 @@ class Scanner:
         except Exception:
             pass
 
-    def set_shape(self, ctas_per_sm: int = 0, threads: int = 0, chunk: int = 0) -> None:
-        N.check(N.lib().cmgpu_workspace_set_shape(self._ws, ctas_per_sm, threads, chunk))
+    def set_shape(self, ctas_per_sm: int = 0, threads: int = 0, chunk: int = 0, lanes: int = 0) -> None:
+        N.check(N.lib().cmgpu_workspace_set_shape(self._ws, ctas_per_sm, threads, chunk, lanes))
 
     def stats(self) -> dict:
         s = N.Stats()

@@ -55,14 +55,17 @@ def test_generic_scan_matches_oracle(case):
     assert hits_equal(got, ref), (got[:5], ref[:5])
 
 
-@pytest.mark.parametrize("chunk", [0, 200, 1000])
-def test_subchunked_windows_match(chunk):
-    """Forced small work items: warm-up restarts must not change any hit."""
+@pytest.mark.parametrize("shape", [(0, 0, 0, 0), (0, 0, 200, 1), (0, 256, 200, 3), (2, 128, 1000, 2),
+                                   (1, 512, 300, 8)])
+def test_subchunked_windows_match(shape):
+    """Forced small work items, several items per CTA: warm-up restarts and
+    lane refills must not change any hit."""
+    ctas, threads, chunk, lanes = shape
     cm, g, l = models("trna")
     n = 6000
     dsq = frame(planted_seq(cm, n, 0.45, 6, seed=7))
     s = scan.Scanner(l)
-    s.set_shape(chunk=chunk)
+    s.set_shape(ctas_per_sm=ctas, threads=threads, chunk=chunk, lanes=lanes)
     for sr, band in ((CYK_F32, QDB1), (INSIDE_I32, QDB2)):
         ref, _, _, _ = oracle.qdb_scan(l, sr, band, dsq, 1, n, -3.0, True)
         got = s.generic_scan(sr, band, dsq, 1, n, -3.0, True)
