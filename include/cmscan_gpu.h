@@ -180,6 +180,26 @@ int cmgpu_qdb_scan(const cmgpu_model *m, cmgpu_workspace *ws, int semiring,
                    int32_t j0, float cutoff, int do_null3, cmgpu_hit *hits,
                    int32_t cap, int32_t *n_out);
 
+/* Window scan that allocates no device memory.  It has no counterpart in the
+ * reference; it exists for callers that cannot call cudaMalloc during a scan:
+ * code running while a stream is captured into a CUDA graph, services whose
+ * device memory belongs to a framework's pool or budget, and latency-bound
+ * loops that cannot afford an allocation and the synchronisation it implies.
+ * Same arguments and results as cmgpu_qdb_scan, minus the workspace; stream
+ * is a cudaStream_t (NULL: the default stream) and the call returns after the
+ * scan has finished on it.  Its scratch -- a copy of the scan plan, the
+ * residues, work items, counters, reportable cells and, when they do not fit
+ * in shared memory, the decks -- lives in one 16 MiB `static __device__` array
+ * that every GPU loading the library holds until the process exits.  Requests
+ * that do not fit return CMGPU_ENOSPACE.  The first call on a device looks up
+ * the array's address (set-up), so make it before any stream capture.  All
+ * calls on a device share the array: calls that overlap on the GPU race, so
+ * serialise them.  The model must already be uploaded (cmgpu_model_upload). */
+int cmgpu_qdb_scan_noalloc(const cmgpu_model *m, void *stream, int semiring, int qdbidx,
+                           const uint8_t *dsq, int32_t n, int32_t i0, int32_t j0,
+                           float cutoff, int do_null3, cmgpu_hit *hits, int32_t cap,
+                           int32_t *n_out);
+
 /* Test hook, the analogue of the reference's DUMP_* value dumps: every
  * reportable cell (j, d) of a generic_scan of [i0, j0] with bestsc >= cutoff,
  * sorted by (j, d), with its bit score, before null3 and greedy reporting. */

@@ -122,6 +122,8 @@ def lib() -> C.CDLL:
     L.cmgpu_workspace_set_shape.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int]
     L.cmgpu_qdb_scan.argtypes = [vp, vp, C.c_int, C.c_int, P(C.c_uint8), C.c_int32, C.c_int32,
                                  C.c_int32, C.c_float, C.c_int, vp, C.c_int32, P(C.c_int32)]
+    L.cmgpu_qdb_scan_noalloc.argtypes = [vp, vp, C.c_int, C.c_int, P(C.c_uint8), C.c_int32, C.c_int32,
+                                         C.c_int32, C.c_float, C.c_int, vp, C.c_int32, P(C.c_int32)]
     L.cmgpu_qdb_scan_cells.argtypes = [vp, vp, C.c_int, C.c_int, P(C.c_uint8), C.c_int32, C.c_int32,
                                        C.c_int32, C.c_float, vp, vp, vp, C.c_int32, P(C.c_int32)]
     L.cmgpu_cyk_seq_filter.argtypes = [vp, vp, P(C.c_uint8), C.c_int32, C.c_float, C.c_int, vp,
@@ -150,6 +152,6 @@ EXPORTED = [
     "cmgpu_last_error", "cmgpu_version", "cmgpu_prep_configure", "cmgpu_ilogsum_table",
     "cmgpu_flogsum_table", "cmgpu_model_upload", "cmgpu_model_free", "cmgpu_workspace_create",
     "cmgpu_workspace_free", "cmgpu_workspace_stats", "cmgpu_workspace_set_shape",
-    "cmgpu_qdb_scan", "cmgpu_qdb_scan_cells", "cmgpu_cyk_seq_filter", "cmgpu_final_stage_inside_opt",
+    "cmgpu_qdb_scan", "cmgpu_qdb_scan_noalloc", "cmgpu_qdb_scan_cells", "cmgpu_cyk_seq_filter", "cmgpu_final_stage_inside_opt",
     "cmgpu_scan_batch", "cmgpu_scan_batch_device", "cmgpu_scan_plain", "cmgpu_count_work",
 ]

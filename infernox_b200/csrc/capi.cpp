@@ -24,6 +24,7 @@
 
 #include "../../include/cmscan_gpu.h"
 #include "cm_internal.h"
+#include "model_internal.h"
 #include "qdb_kernel.h"
 #include "qdb_plan.h"
 
@@ -44,102 +45,6 @@ void count_column_public(const cmgpu_cm *cm, const Plan &p, int qdbidx, int jrow
         }                                                                                       \
     } while (0)
 
-// ---------------------------------------------------------------------------
-// host copy of a configured CM
-// ---------------------------------------------------------------------------
-struct HostCM {
-    cmgpu_cm view{};
-    std::vector<int8_t> sttype, stid;
-    std::vector<int32_t> cfirst, cnum, itsc, ioesc, iendsc, ibeginsc, dmin1, dmax1, dmin2, dmax2;
-    std::vector<float> tsc, oesc, endsc, beginsc;
-
-    bool load(const cmgpu_cm *c) {
-        const int M = c->M;
-        if (M < 2 || c->W < 1 || !c->sttype || !c->stid || !c->cfirst || !c->cnum || !c->tsc || !c->oesc ||
-            !c->endsc || !c->beginsc || !c->itsc || !c->ioesc || !c->iendsc || !c->ibeginsc || !c->dmin1 ||
-            !c->dmax1 || !c->dmin2 || !c->dmax2)
-            return false;
-        sttype.assign(c->sttype, c->sttype + M);
-        stid.assign(c->stid, c->stid + M);
-        cfirst.assign(c->cfirst, c->cfirst + M);
-        cnum.assign(c->cnum, c->cnum + M);
-        tsc.assign(c->tsc, c->tsc + (size_t)M * MAXC);
-        oesc.assign(c->oesc, c->oesc + (size_t)M * ESC);
-        endsc.assign(c->endsc, c->endsc + M);
-        beginsc.assign(c->beginsc, c->beginsc + M);
-        itsc.assign(c->itsc, c->itsc + (size_t)M * MAXC);
-        ioesc.assign(c->ioesc, c->ioesc + (size_t)M * ESC);
-        iendsc.assign(c->iendsc, c->iendsc + M);
-        ibeginsc.assign(c->ibeginsc, c->ibeginsc + M);
-        dmin1.assign(c->dmin1, c->dmin1 + M);
-        dmax1.assign(c->dmax1, c->dmax1 + M);
-        dmin2.assign(c->dmin2, c->dmin2 + M);
-        dmax2.assign(c->dmax2, c->dmax2 + M);
-        view = *c;
-        view.sttype = sttype.data();
-        view.stid = stid.data();
-        view.cfirst = cfirst.data();
-        view.cnum = cnum.data();
-        view.tsc = tsc.data();
-        view.oesc = oesc.data();
-        view.endsc = endsc.data();
-        view.beginsc = beginsc.data();
-        view.itsc = itsc.data();
-        view.ioesc = ioesc.data();
-        view.iendsc = iendsc.data();
-        view.ibeginsc = ibeginsc.data();
-        view.dmin1 = dmin1.data();
-        view.dmax1 = dmax1.data();
-        view.dmin2 = dmin2.data();
-        view.dmax2 = dmax2.data();
-        // structural sanity: children inside [0, M), B children valid
-        for (int v = 0; v < M; v++) {
-            int st = sttype[v];
-            if (st < 0 || st > 8) return false;
-            if (st == E_ST) continue;
-            if (st == B_ST) {
-                if (cfirst[v] <= v || cfirst[v] >= M || cnum[v] <= v || cnum[v] >= M) return false;
-                if (stid[cfirst[v]] != BEGL_S) return false;
-            } else {
-                if (cnum[v] < 1 || cnum[v] > MAXC || cfirst[v] < v || cfirst[v] + cnum[v] > M) return false;
-                for (int yo = 0; yo < cnum[v]; yo++) {
-                    int y = cfirst[v] + yo;
-                    if (y == v && st != IL_ST && st != IR_ST) return false;
-                }
-            }
-        }
-        return true;
-    }
-};
-
-struct DevPlan {
-    Plan host;
-    StateDev *states = nullptr;
-    ChunkDev *chunks = nullptr;
-    BeginDev *begins = nullptr;
-    int32_t *level_start = nullptr, *wb = nullptr, *cb = nullptr, *init_off = nullptr;
-    uint32_t *tsc = nullptr, *endsc = nullptr, *beginsc = nullptr, *esc = nullptr, *el_sca = nullptr,
-             *esc_c = nullptr, *init_val = nullptr;
-    std::vector<double> cells_prefix, terms_prefix;  // per jrow, prefix over jrow = 1..W
-    double cells_full = 0, terms_full = 0;
-    ~DevPlan() {
-        cudaFree(states);
-        cudaFree(chunks);
-        cudaFree(begins);
-        cudaFree(level_start);
-        cudaFree(wb);
-        cudaFree(cb);
-        cudaFree(init_off);
-        cudaFree(tsc);
-        cudaFree(endsc);
-        cudaFree(beginsc);
-        cudaFree(esc);
-        cudaFree(el_sca);
-        cudaFree(esc_c);
-        cudaFree(init_val);
-    }
-};
-
 template <class T>
 static int upload_vec(T **dst, const std::vector<T> &v) {
     size_t n = std::max<size_t>(v.size(), 1);
@@ -151,17 +56,6 @@ static int upload_vec(T **dst, const std::vector<T> &v) {
 }  // namespace cmx
 
 using namespace cmx;
-
-struct cmgpu_model {
-    int device = 0;
-    HostCM cm;
-    std::mutex mu;
-    std::map<int, std::unique_ptr<DevPlan>> plans;  // key semiring*8 + qdbidx
-    uint16_t *ilog = nullptr;
-    int ilog_nz = 0;
-    std::vector<float> flog;  // host FLogsum table for null3
-    ~cmgpu_model() { cudaFree(ilog); }
-};
 
 struct cmgpu_workspace {
     int device = 0;
@@ -340,7 +234,7 @@ static void remove_overlaps(std::vector<cmgpu_hit> &h) {
 
 // Replays report_hits_greedily for one window from its candidate cells
 // (sorted by j, d).  frame = window frame (host), needed for null3.
-static void report_window(const cmgpu_model *m, int semiring, const Cand *c, size_t n, const uint8_t *frame,
+void report_window(const cmgpu_model *m, int semiring, const Cand *c, size_t n, const uint8_t *frame,
                           int32_t i0, float cutoff, int do_null3, std::vector<cmgpu_hit> &out) {
     std::vector<cmgpu_hit> tmp;
     // prefix counts of canonical residues over the candidates' span
