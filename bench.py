@@ -241,6 +241,7 @@ def main():
     def step_e2e():
         return sc.scan_batch(sr, band, buf, wins, CUTOFF_BITS, True)
 
+    tune = sc.autotune(sr, band, buf, wins, CUTOFF_BITS, device_buf=d_buf.data_ptr())
     for _ in range(args.warmup):
         hits = step_device()
     ref_hits = hits
@@ -356,6 +357,8 @@ def main():
             "batched_over_plain": (value / plain["value"]) if plain else None,
             "cpu_baseline": cb,
             "clocks": clk,
+            "launch_shape": {"lanes": tune["best"]["lanes"], "threads": tune["best"]["threads"],
+                             "tuned_over": [(t["lanes"], round(t["kernel_ms"], 1)) for t in tune["trials"]]},
             "hits_per_step": int(len(ref_hits)),
         }
         print(json.dumps(line))

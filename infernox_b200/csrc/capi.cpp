@@ -407,8 +407,10 @@ static int run_scan(cmgpu_model *m, cmgpu_workspace *ws, int semiring, int qdbid
     const int W = pl.W;
     int64_t chunk = ws->chunk;
     if (chunk <= 0) {
+        // about four items per lane slot, but no piece shorter than 2W (the
+        // W-1 warm-up columns are overhead) and none longer than 32768
         chunk = total_cols / std::max<int64_t>(1, (int64_t)max_ctas * best_l * 4);
-        chunk = std::max<int64_t>(chunk, 4 * (int64_t)W);
+        chunk = std::max<int64_t>(chunk, 2 * (int64_t)W);
         chunk = std::min<int64_t>(chunk, 32768);
     }
     for (size_t wi = 0; wi < wins.size(); wi++) {

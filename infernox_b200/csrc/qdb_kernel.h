@@ -11,7 +11,7 @@ namespace cmx {
 
 constexpr int IL_KMAX = 8;     // IL cells per lane kept in registers (W <= 255)
 constexpr int COL_BLOCK = 32;  // columns a lane advances between refills
-constexpr int MAX_LANES = 8;   // work items one CTA scans side by side
+constexpr int MAX_LANES = 16;  // work items one CTA scans side by side
 
 // A piece of one window: columns jstart..jend are scanned, candidates are
 // emitted for columns >= jreport (the first W-1 are warm-up).

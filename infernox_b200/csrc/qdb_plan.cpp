@@ -317,7 +317,7 @@ bool build_plan(const cmgpu_cm *cm, int semiring, int qdbidx, Plan &p) {
             if (st == IL_ST) {
                 lc.push_back({1e9 + width[v], ChunkDev{v, -1}});
             } else {
-                for (int d0 = s.dn; d0 <= s.dxcap; d0 += 32) {
+                for (int d0 = s.dn; d0 <= s.dxcap; d0 += 64) {
                     double cost = st == B_ST ? 1e6 + d0 : (double)s.cnum;
                     lc.push_back({cost, ChunkDev{v, d0}});
                 }

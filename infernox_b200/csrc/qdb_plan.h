@@ -33,7 +33,8 @@ struct StateDev {
 };
 static_assert(sizeof(StateDev) == 16, "StateDev layout");
 
-// A unit of work inside one level: state v, cells d0..d0+31 (warp-wide).
+// A unit of work inside one level: state v, cells d0..d0+63 (a warp, two
+// cells per lane).
 // For IL states d0 = -1: one warp resolves the whole band.
 struct ChunkDev {
     int32_t v;

@@ -52,6 +52,7 @@ struct Sem;
 template <>
 struct Sem<false> {  // CYK: f32, ESL_MAX
     typedef float T;
+    static constexpr bool ORDERED = false;
     __device__ static __forceinline__ T zero() { return IMPOSSIBLE_D; }
     __device__ static __forceinline__ T add(T a, T b) { return __fadd_rn(a, b); }
     __device__ static __forceinline__ T comb(T a, T b, const uint16_t *, int) { return a >= b ? a : b; }
@@ -65,6 +66,7 @@ struct Sem<false> {  // CYK: f32, ESL_MAX
 template <>
 struct Sem<true> {  // Inside: i32 wrapping adds, ILogsum
     typedef int32_t T;
+    static constexpr bool ORDERED = true;
     __device__ static __forceinline__ T zero() { return -INFTY_D; }
     __device__ static __forceinline__ T add(T a, T b) { return (int32_t)((uint32_t)a + (uint32_t)b); }
     // ILogsum (src/cp9.rs:65-75): max + tbl[max-min]; the table is stored up
@@ -150,6 +152,15 @@ __device__ __forceinline__ typename S::T reduce_c(int cnum, const typename S::T 
                                                   const uint16_t *tb, int nz) {
     typedef typename S::T T;
     T s;
+    if (!S::ORDERED) {
+        // CYK: max selects one operand exactly, so any bracketing returns the
+        // same value; a tree shortens the dependency chain.
+        T a = init, b = cnum > 0 ? t[0] : init, c = cnum > 1 ? t[1] : init;
+        T d = cnum > 2 ? t[2] : init, e = cnum > 3 ? t[3] : init, f = cnum > 4 ? t[4] : init;
+        T g = cnum > 5 ? t[5] : init;
+        T ab = S::comb(a, b, tb, nz), cd = S::comb(c, d, tb, nz), ef = S::comb(e, f, tb, nz);
+        return S::comb(S::comb(ab, cd, tb, nz), S::comb(ef, g, tb, nz), tb, nz);
+    }
     switch (cnum) {
     case 1: s = S::comb(init, t[0], tb, nz); break;
     case 2: s = S::comb(S::comb(t[1], init, tb, nz), t[0], tb, nz); break;
@@ -236,13 +247,10 @@ __device__ __forceinline__ typename S::T init_sc(const K &k, const SInfo &sv, in
 
 __device__ __forceinline__ int resid(const Lane &L, int x, int rmask) { return L.ring[x & rmask]; }
 
-// One warp-wide chunk of an ordinary state (not B, not IL).
+// Value of cell d of an ordinary state (not B, not IL), before the store.
 template <class S>
-__device__ __forceinline__ void do_chunk(const K &k, const Lane &L, int v, const SInfo &sv, int d0, int lane) {
+__device__ __forceinline__ typename S::T cell_value(const K &k, const Lane &L, int v, const SInfo &sv, int d) {
     typedef typename S::T T;
-    const int d = d0 + lane;
-    const int dx = min(L.jrow, sv.dxcap);
-    if (d > dx) return;
     const int t = sv.type;
     T terms[6];
     child_terms<S>(k, v, sv.cnum, L.deck, L.par, d, terms, 0);
@@ -264,18 +272,31 @@ __device__ __forceinline__ void do_chunk(const K &k, const Lane &L, int v, const
     } else if (t == 1) {  // MP
         sc = S::add(sc, esc2<S>(k, v, sv.escoff, resid(L, L.j - d + 1, k.rmask), resid(L, L.j, k.rmask)));
     }
-    const int wbase = (sv.flags & SF_BEGL) ? k.s.wb[v * 2] + L.jm * sv.span : k.s.wb[v * 2 + L.par];
-    S::st(L.deck + wbase + d, sc);
+    return sc;
 }
 
-// Bifurcation chunk: alpha[v][d] = init (+) over k ascending of
+// One warp-wide chunk of an ordinary state (not B, not IL): 64 cells, two per
+// lane (d0+lane and d0+32+lane).  Both values are computed before either is
+// stored, so the two dependency chains overlap.
+template <class S>
+__device__ __forceinline__ void do_chunk(const K &k, const Lane &L, int v, const SInfo &sv, int d0, int lane) {
+    typedef typename S::T T;
+    const int dx = min(L.jrow, sv.dxcap);
+    const int da = d0 + lane, db = da + 32;
+    if (da > dx) return;
+    const bool has_b = db <= dx;
+    T va = cell_value<S>(k, L, v, sv, da);
+    T vb = has_b ? cell_value<S>(k, L, v, sv, db) : va;
+    const int wbase = (sv.flags & SF_BEGL) ? k.s.wb[v * 2] + L.jm * sv.span : k.s.wb[v * 2 + L.par];
+    S::st(L.deck + wbase + da, va);
+    if (has_b) S::st(L.deck + wbase + db, vb);
+}
+
+// Bifurcation cell: alpha[v][d] = init (+) over k ascending of
 // BEGL(j-k, d-k) + BEGR(j, k) (src/cm_nohmm.rs:578-600).
 template <class S>
-__device__ __forceinline__ void do_bif_chunk(const K &k, const Lane &L, int v, const SInfo &sv, int d0, int lane) {
+__device__ __forceinline__ typename S::T bif_value(const K &k, const Lane &L, int v, const SInfo &sv, int d) {
     typedef typename S::T T;
-    const int d = d0 + lane;
-    const int dx = min(L.jrow, sv.dxcap);
-    if (d > dx) return;
     const int32_t *c = k.s.cb + v * 12;
     const int begl = c[0], begr = c[2], kdn_y = c[4], kdx_y = c[5], kdn_w = c[6], kdx_w = c[7], span_w = c[8];
     const int kmin = max(0, max(kdn_y, d - kdx_w));
@@ -292,7 +313,22 @@ __device__ __forceinline__ void do_bif_chunk(const K &k, const Lane &L, int v, c
         sc = S::comb(sc, S::add(lv, rv), k.s.tbl, k.nz);
         col = col == 0 ? W1 - 1 : col - 1;
     }
-    S::st(L.deck + k.s.wb[v * 2 + L.par] + d, sc);
+    return sc;
+}
+
+// Bifurcation chunk: 64 cells, two per lane, computed before the stores.
+template <class S>
+__device__ __forceinline__ void do_bif_chunk(const K &k, const Lane &L, int v, const SInfo &sv, int d0, int lane) {
+    typedef typename S::T T;
+    const int dx = min(L.jrow, sv.dxcap);
+    const int da = d0 + lane, db = da + 32;
+    if (da > dx) return;
+    const bool has_b = db <= dx;
+    T va = bif_value<S>(k, L, v, sv, da);
+    T vb = has_b ? bif_value<S>(k, L, v, sv, db) : va;
+    const int wb = k.s.wb[v * 2 + L.par];
+    S::st(L.deck + wb + da, va);
+    if (has_b) S::st(L.deck + wb + db, vb);
 }
 
 // IL relaxation with up to KC cells per lane held in registers.
