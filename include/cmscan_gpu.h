@@ -249,6 +249,34 @@ int cmgpu_scan_plain(const cmgpu_model *m, cmgpu_workspace *ws, int semiring,
                      int do_null3, cmgpu_batch_hit *hits, int32_t cap,
                      int32_t *n_out);
 
+/* ---- P7 Viterbi filter (F2) ---------------------------------------------
+ * A p7 filter profile as the reference's P7Profile holds it
+ * (src/p7_hmm.rs:62-92): mat[k*4+x] match emissions for k = 1..M (row 0
+ * unused), trans[k*7+t] transitions MM,MI,MD,IM,II,DM,DD for k = 0..M. */
+typedef struct cmgpu_p7_profile {
+    int32_t M;
+    const float *mat;
+    const float *trans;
+} cmgpu_p7_profile;
+
+typedef struct cmgpu_vit_filter cmgpu_vit_filter;
+
+/* build_vit_filter (src/p7_vitfilter.rs:121-278): quantised int16 tables,
+ * uploaded to `device` (device < 0: host tables only, for inspection). */
+int cmgpu_vit_filter_build(const cmgpu_p7_profile *p, int device, cmgpu_vit_filter **out);
+void cmgpu_vit_filter_free(cmgpu_vit_filter *f);
+/* The filter's tables, [(M+1)][26]: emissions of the 18 codes, then local
+ * entry, MM, IM, DM (row k-1 feeds position k), MI, II, MD, DD; specials =
+ * {base_w, E move, E loop}.  For tests and inspection. */
+int cmgpu_vit_filter_tables(const cmgpu_vit_filter *f, int16_t *tab, int32_t cap, int32_t *n_out,
+                            int16_t *specials);
+/* vit_score (src/p7_vitfilter.rs:292): the filter score in bits of residues
+ * i0..j0 of every window; scored[w] = 0 where the reference returns None
+ * (16-bit overflow, score NaN).  stream: cudaStream_t or NULL. */
+int cmgpu_vit_score_batch(const cmgpu_vit_filter *f, void *stream, const uint8_t *dsq_all,
+                          int64_t dsq_len, const cmgpu_window *wins, int32_t nwin, float *scores,
+                          uint8_t *scored);
+
 /* Exact counts of cells and terms the reference scanner evaluates for a
  * window of length L (host only; used for Gcells/s). */
 int cmgpu_count_work(const cmgpu_cm *cm, int semiring, int qdbidx, int32_t L,

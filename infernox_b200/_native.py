@@ -64,6 +64,10 @@ class CmScores(C.Structure):
     ]
 
 
+class P7Profile(C.Structure):
+    _fields_ = [("M", C.c_int32), ("mat", P(C.c_float)), ("trans", P(C.c_float))]
+
+
 class Hit(C.Structure):
     _fields_ = [("i", C.c_int32), ("j", C.c_int32), ("score", C.c_float), ("bias", C.c_float)]
 
@@ -136,6 +140,11 @@ def lib() -> C.CDLL:
                                      C.c_int32, C.c_float, C.c_int, vp, C.c_int32, P(C.c_int32)]
     L.cmgpu_scan_batch_device.argtypes = [vp, vp, C.c_int, C.c_int, vp, C.c_int64, vp, C.c_int32,
                                           C.c_float, C.c_int, vp, C.c_int32, P(C.c_int32)]
+    L.cmgpu_vit_filter_build.argtypes = [vp, C.c_int, P(vp)]
+    L.cmgpu_vit_filter_free.argtypes = [vp]
+    L.cmgpu_vit_filter_free.restype = None
+    L.cmgpu_vit_filter_tables.argtypes = [vp, vp, C.c_int32, P(C.c_int32), vp]
+    L.cmgpu_vit_score_batch.argtypes = [vp, vp, vp, C.c_int64, vp, C.c_int32, vp, vp]
     L.cmgpu_count_work.argtypes = [P(Cm), C.c_int, C.c_int, C.c_int32, P(C.c_double),
                                    P(C.c_double)]
     _lib = L
@@ -154,4 +163,5 @@ EXPORTED = [
     "cmgpu_workspace_free", "cmgpu_workspace_stats", "cmgpu_workspace_set_shape",
     "cmgpu_qdb_scan", "cmgpu_qdb_scan_noalloc", "cmgpu_qdb_scan_cells", "cmgpu_cyk_seq_filter", "cmgpu_final_stage_inside_opt",
     "cmgpu_scan_batch", "cmgpu_scan_batch_device", "cmgpu_scan_plain", "cmgpu_count_work",
+    "cmgpu_vit_filter_build", "cmgpu_vit_filter_free", "cmgpu_vit_filter_tables", "cmgpu_vit_score_batch",
 ]

@@ -29,8 +29,8 @@ def build() -> str:
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(
-                os.path.join(HERE, "qdb_oracle.c")):
+        srcs = [os.path.join(HERE, f) for f in ("qdb_oracle.c", "p7_oracle.c")]
+        if not os.path.exists(LIB_PATH) or any(os.path.getmtime(LIB_PATH) < os.path.getmtime(f) for f in srcs):
             build()
         L = C.CDLL(LIB_PATH)
         vp = C.c_void_p
@@ -42,6 +42,8 @@ def lib():
                                             C.c_int32, P(C.c_int32)]
         L.oracle_final_stage_inside_opt.argtypes = [vp, P(C.c_uint8), vp, C.c_int32, C.c_float,
                                                     C.c_int, C.c_int, vp, C.c_int32, P(C.c_int32)]
+        L.oracle_vit_score_batch.argtypes = [C.c_int, vp, vp, vp, vp, vp, C.c_int32, vp, vp]
+        L.oracle_vit_tables.argtypes = [C.c_int, vp, vp, vp, vp]
         L.oracle_ilogsum_table.argtypes = [P(C.c_int32), C.c_int]
         L.oracle_ilogsum.argtypes = [C.c_int32, C.c_int32]
         L.oracle_ilogsum.restype = C.c_int32
@@ -122,3 +124,26 @@ def ilogsum_table(n=23000):
 
 def ilogsum(a, b):
     return int(lib().oracle_ilogsum(a, b))
+
+
+def vit_score_batch(M, mat, trans, buf, offs, lens):
+    """vit_score_scalar on each sequence: (scores f32, scored u8; 0 = overflow)."""
+    mat = np.ascontiguousarray(mat, np.float32)
+    trans = np.ascontiguousarray(trans, np.float32)
+    buf = np.ascontiguousarray(buf, np.uint8)
+    offs = np.ascontiguousarray(offs, np.int64)
+    lens = np.ascontiguousarray(lens, np.int32)
+    sc = np.zeros(len(lens), np.float32)
+    ok = np.zeros(len(lens), np.uint8)
+    lib().oracle_vit_score_batch(int(M), mat.ctypes.data, trans.ctypes.data, buf.ctypes.data, offs.ctypes.data,
+                                 lens.ctypes.data, len(lens), sc.ctypes.data, ok.ctypes.data)
+    return sc, ok
+
+
+def vit_tables(M, mat, trans):
+    mat = np.ascontiguousarray(mat, np.float32)
+    trans = np.ascontiguousarray(trans, np.float32)
+    tab = np.zeros((M + 1) * 26, np.int16)
+    sp = np.zeros(3, np.int16)
+    lib().oracle_vit_tables(int(M), mat.ctypes.data, trans.ctypes.data, tab.ctypes.data, sp.ctypes.data)
+    return tab, sp
