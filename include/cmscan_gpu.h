@@ -277,6 +277,60 @@ int cmgpu_vit_score_batch(const cmgpu_vit_filter *f, void *stream, const uint8_t
                           int64_t dsq_len, const cmgpu_window *wins, int32_t nwin, float *scores,
                           uint8_t *scored);
 
+/* ---- P7 MSV / SSV filter (F1) ------------------------------------------ */
+typedef struct cmgpu_msv_filter cmgpu_msv_filter;
+
+/* A candidate window of f1_msv_windows: residues start..end (1-based, in the
+ * chunk's own coordinates) of chunk `chunk`, with the SSV diagonal score of
+ * its first diagonal (src/cm_pipeline.rs:466-471). */
+typedef struct cmgpu_f1_window {
+    int64_t start, end;
+    float score;
+    int32_t chunk;
+} cmgpu_f1_window;
+
+/* One SSV diagonal as ssv_diagonals returns it (src/cm_pipeline.rs:455-462):
+ * target start n, model length, model end k, score. */
+typedef struct cmgpu_ssv_diagonal {
+    int64_t n, length, k;
+    float score;
+    int32_t chunk;
+} cmgpu_ssv_diagonal;
+
+/* build_msv_filter (src/cm_pipeline.rs:201-340) with max_length = the
+ * pipeline's maxW; lmmu / lmlambda are the profile's local MSV Gumbel
+ * parameters (P7Profile.evparam).  device < 0: host tables only. */
+int cmgpu_msv_filter_build(const cmgpu_p7_profile *p, int32_t max_length, double lmmu, double lmlambda,
+                           int device, cmgpu_msv_filter **out);
+void cmgpu_msv_filter_free(cmgpu_msv_filter *f);
+/* The filter's tables: emission costs rbv[(M+1)*18], bytes5 = {base_b, bias_b,
+ * tbm_b, tec_b, tjb_b}, prefix/suffix lengths [M+1], scale_b.  For tests. */
+int cmgpu_msv_filter_tables(const cmgpu_msv_filter *f, uint8_t *rbv, int32_t cap, int32_t *n_out,
+                            uint8_t *bytes5, float *prefix, float *suffix, float *scale_b);
+/* The SSV trigger threshold sc_thresh of ssv_diagonals for F1 = f1. */
+int cmgpu_ssv_threshold(const cmgpu_msv_filter *f, double f1, int32_t *thresh);
+/* msv_score (src/cm_pipeline.rs:402, wlen == NULL) or msv_score_reconfig
+ * (:410, length model of wlen[w] residues) of residues i0..j0 of every
+ * window; scored[w] = 0 where the reference returns None (8-bit overflow). */
+int cmgpu_msv_score_batch(const cmgpu_msv_filter *f, void *stream, const uint8_t *dsq_all, int64_t dsq_len,
+                          const cmgpu_window *wins, int32_t nwin, const int32_t *wlen, float *scores,
+                          uint8_t *scored);
+/* f1_msv_windows (src/cm_pipeline.rs:842) on every chunk in one call: the
+ * chunk's residues are i0..j0 of its window (local position 1 = i0).
+ * Windows come back grouped by chunk, each chunk's in the reference's order.
+ * CMGPU_EOVERFLOW with the needed count in *n_out when cap is too small. */
+int cmgpu_f1_msv_windows(const cmgpu_msv_filter *f, void *stream, const uint8_t *dsq_all, int64_t dsq_len,
+                         const cmgpu_window *chunks, int32_t nchunk, double f1, int64_t cmw,
+                         cmgpu_f1_window *out, int32_t cap, int32_t *n_out);
+/* ssv_diagonals (src/cm_pipeline.rs:521) on every chunk: the raw diagonals
+ * before extension and merging (the reference's DUMP_SSV lines). */
+int cmgpu_ssv_diagonals(const cmgpu_msv_filter *f, void *stream, const uint8_t *dsq_all, int64_t dsq_len,
+                        const cmgpu_window *chunks, int32_t nchunk, double f1, cmgpu_ssv_diagonal *out,
+                        int32_t cap, int32_t *n_out);
+/* Device time, cells (rows x M, warm-up rows included) and kernel launches
+ * of the last scoring or scanning call on this filter. */
+int cmgpu_msv_filter_stats(const cmgpu_msv_filter *f, double *kernel_ms, int64_t *cells, int32_t *launches);
+
 /* Exact counts of cells and terms the reference scanner evaluates for a
  * window of length L (host only; used for Gcells/s). */
 int cmgpu_count_work(const cmgpu_cm *cm, int semiring, int qdbidx, int32_t L,

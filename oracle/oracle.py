@@ -1,4 +1,5 @@
-"""TEST INFRASTRUCTURE ONLY: ctypes binding of the oracle (qdb_oracle.c).
+"""TEST INFRASTRUCTURE ONLY: ctypes binding of the oracle (qdb_oracle.c,
+p7_oracle.c, msv_oracle.c).
 
 Used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as
 the checker of the GPU scanner.  The product package never imports it.
@@ -29,7 +30,7 @@ def build() -> str:
 def lib():
     global _lib
     if _lib is None:
-        srcs = [os.path.join(HERE, f) for f in ("qdb_oracle.c", "p7_oracle.c")]
+        srcs = [os.path.join(HERE, f) for f in ("qdb_oracle.c", "p7_oracle.c", "msv_oracle.c")]
         if not os.path.exists(LIB_PATH) or any(os.path.getmtime(LIB_PATH) < os.path.getmtime(f) for f in srcs):
             build()
         L = C.CDLL(LIB_PATH)
@@ -44,6 +45,14 @@ def lib():
                                                     C.c_int, C.c_int, vp, C.c_int32, P(C.c_int32)]
         L.oracle_vit_score_batch.argtypes = [C.c_int, vp, vp, vp, vp, vp, C.c_int32, vp, vp]
         L.oracle_vit_tables.argtypes = [C.c_int, vp, vp, vp, vp]
+        L.oracle_msv_tables.argtypes = [C.c_int, vp, vp, C.c_int, vp, vp, vp, vp, vp]
+        L.oracle_msv_score_batch.argtypes = [C.c_int, vp, vp, C.c_int, vp, vp, vp, vp, C.c_int32, vp, vp]
+        L.oracle_f1_msv_windows.argtypes = [C.c_int, vp, vp, C.c_int, C.c_double, C.c_double, vp, vp, vp,
+                                            C.c_int32, C.c_double, C.c_int64, vp, vp, C.c_int64, vp, vp,
+                                            C.c_int64, P(C.c_int64)]
+        L.oracle_f1_msv_windows.restype = C.c_int64
+        L.oracle_ssv_threshold.argtypes = [C.c_int, vp, vp, C.c_int, C.c_double, C.c_double, C.c_double]
+        L.oracle_ssv_threshold.restype = C.c_int
         L.oracle_ilogsum_table.argtypes = [P(C.c_int32), C.c_int]
         L.oracle_ilogsum.argtypes = [C.c_int32, C.c_int32]
         L.oracle_ilogsum.restype = C.c_int32
@@ -147,3 +156,64 @@ def vit_tables(M, mat, trans):
     sp = np.zeros(3, np.int16)
     lib().oracle_vit_tables(int(M), mat.ctypes.data, trans.ctypes.data, tab.ctypes.data, sp.ctypes.data)
     return tab, sp
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, np.float32)
+
+
+def msv_tables(M, mat, trans, max_length):
+    """build_msv_filter restated: (rbv [(M+1)*18] u8, [base, bias, tbm, tec, tjb], prefix, suffix, scale_b)."""
+    mat, trans = _f32(mat), _f32(trans)
+    rbv = np.zeros((M + 1) * 18, np.uint8)
+    b6 = np.zeros(6, np.uint8)
+    pre = np.zeros(M + 1, np.float32)
+    suf = np.zeros(M + 1, np.float32)
+    sc = np.zeros(1, np.float32)
+    lib().oracle_msv_tables(int(M), mat.ctypes.data, trans.ctypes.data, int(max_length), rbv.ctypes.data,
+                            b6.ctypes.data, pre.ctypes.data, suf.ctypes.data, sc.ctypes.data)
+    return rbv, b6[:5], pre, suf, sc[0]
+
+
+def msv_score_batch(M, mat, trans, max_length, buf, offs, lens, wlen=None):
+    """msv_score (wlen None) / msv_score_reconfig per frame: (scores f32, scored u8; 0 = overflow)."""
+    mat, trans = _f32(mat), _f32(trans)
+    buf = np.ascontiguousarray(buf, np.uint8)
+    offs = np.ascontiguousarray(offs, np.int64)
+    lens = np.ascontiguousarray(lens, np.int32)
+    wl = None if wlen is None else np.ascontiguousarray(wlen, np.int32)
+    sc = np.zeros(len(lens), np.float32)
+    ok = np.zeros(len(lens), np.uint8)
+    lib().oracle_msv_score_batch(int(M), mat.ctypes.data, trans.ctypes.data, int(max_length), buf.ctypes.data,
+                                 offs.ctypes.data, lens.ctypes.data, None if wl is None else wl.ctypes.data,
+                                 len(lens), sc.ctypes.data, ok.ctypes.data)
+    return sc, ok
+
+
+def f1_msv_windows(M, mat, trans, max_length, mmu, mlambda, buf, offs, lens, f1, cmw):
+    """f1_msv_windows restated on each chunk: (windows [(chunk, start, end)], scores, raws [(chunk, n, length, k)],
+    raw scores)."""
+    mat, trans = _f32(mat), _f32(trans)
+    buf = np.ascontiguousarray(buf, np.uint8)
+    offs = np.ascontiguousarray(offs, np.int64)
+    lens = np.ascontiguousarray(lens, np.int32)
+    cap = 1024
+    while True:
+        out = np.zeros((cap, 3), np.int64)
+        osc = np.zeros(cap, np.float32)
+        raw = np.zeros((cap, 4), np.int64)
+        rsc = np.zeros(cap, np.float32)
+        nr = C.c_int64()
+        n = lib().oracle_f1_msv_windows(int(M), mat.ctypes.data, trans.ctypes.data, int(max_length), float(mmu),
+                                        float(mlambda), buf.ctypes.data, offs.ctypes.data, lens.ctypes.data,
+                                        len(lens), float(f1), int(cmw), out.ctypes.data, osc.ctypes.data, cap,
+                                        raw.ctypes.data, rsc.ctypes.data, cap, C.byref(nr))
+        if n <= cap and nr.value <= cap:
+            return out[:n], osc[:n], raw[: nr.value], rsc[: nr.value]
+        cap = max(n, nr.value) + 16
+
+
+def ssv_threshold(M, mat, trans, max_length, mmu, mlambda, f1):
+    mat, trans = _f32(mat), _f32(trans)
+    return int(lib().oracle_ssv_threshold(int(M), mat.ctypes.data, trans.ctypes.data, int(max_length), float(mmu),
+                                          float(mlambda), float(f1)))

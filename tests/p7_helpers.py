@@ -61,3 +61,45 @@ def reference_grid(reps=8):
             seqs = [random_dsq(rng, l) for l in LS]
             out.append((p, seqs))
     return out
+
+
+def peaked_profile(seed: int, m: int, peak: float = 0.85):
+    """A profile with one strong residue per match position (so SSV/MSV
+    diagonals along planted consensus runs score high) and its consensus."""
+    r = np.random.default_rng(seed)
+    mat = np.zeros((m + 1, 4), np.float32)
+    cons = r.integers(0, 4, m + 1)
+    for k in range(1, m + 1):
+        v = r.uniform(0.02, 0.1, 4)
+        v[cons[k]] = 0.0
+        v = v / v.sum() * (1.0 - peak)
+        v[cons[k]] = peak
+        mat[k] = v.astype(np.float32)
+    trans = np.zeros((m + 1, 7), np.float32)
+    for k in range(m + 1):
+        mi, md = r.uniform(0.01, 0.08, 2)
+        ii = r.uniform(0.2, 0.6)
+        dd = r.uniform(0.1, 0.5)
+        trans[k] = [1 - mi - md, mi, md, 1 - ii, ii, 1 - dd, dd]
+    return P7Profile(m, mat, trans), cons
+
+
+def planted_frame(seed: int, l: int, cons, nplant: int, mut: float = 0.1, iupac: float = 0.002):
+    """[255, residues..., 255] of i.i.d. codes with nplant consensus runs."""
+    r = np.random.default_rng(seed)
+    d = np.full(l + 2, 255, np.uint8)
+    d[1:-1] = r.integers(0, 4, l)
+    ambig = r.random(l) < iupac
+    d[1:-1][ambig] = r.integers(4, 16, int(ambig.sum()))
+    m = len(cons) - 1
+    for _ in range(nplant):
+        k0 = int(r.integers(1, max(2, m // 2)))
+        k1 = int(min(m, k0 + r.integers(max(2, m // 4), m + 1)))
+        run = np.array(cons[k0:k1 + 1], np.uint8)
+        flip = r.random(len(run)) < mut
+        run[flip] = r.integers(0, 4, int(flip.sum()))
+        if len(run) >= l:
+            continue
+        p = int(r.integers(1, l - len(run) + 1))
+        d[p:p + len(run)] = run
+    return d
