@@ -48,6 +48,7 @@ extern "C" {
  * `generic_scan::<i32>`, src/cm_nohmm.rs:406). */
 #define CMGPU_CYK_F32 0
 #define CMGPU_INSIDE_I32 1
+#define CMGPU_INSIDE_F32 2    /* float Inside (FLogsum): HMM-banded scans only */
 
 /* Band sets (src/cm_nohmm.rs:261-262 SMX_QDB1_TIGHT / SMX_QDB2_LOOSE; 0 = the
  * `nonbanded` full d-range of the --max path, src/cm_nohmm.rs:431-437). */
@@ -248,6 +249,61 @@ int cmgpu_scan_plain(const cmgpu_model *m, cmgpu_workspace *ws, int semiring,
                      const cmgpu_window *wins, int32_t nwin, float cutoff,
                      int do_null3, cmgpu_batch_hit *hits, int32_t cap,
                      int32_t *n_out);
+
+/* ---- HMM-banded (CP9-banded) scanners ------------------------------------
+ * Bands of one envelope as CP9Bands holds them (src/cp9.rs:1450-1495): for
+ * each CM state v, rows j = jmin[v]..jmax[v] (none when jmax < jmin), and for
+ * row jp = j - jmin[v] the d-band hdmin..hdmax (empty when hdmax < hdmin),
+ * stored at hdmin[hd_off[v] + jp] / hdmax[hd_off[v] + jp].  Every cell must
+ * lie inside the envelope (i = j-d+1 >= i0, j <= j0, d >= 0); rows of
+ * emitting states start at d >= 1 and END rows are non-empty, as
+ * ij2d_bands (src/cp9.rs:3815) and the reference's wide-band test fixture
+ * build them. */
+typedef struct cmgpu_hb_bands {
+    const int32_t *jmin, *jmax;   /* [M] */
+    const int32_t *hd_off;        /* [M] */
+    const int32_t *hdmin, *hdmax; /* rows */
+} cmgpu_hb_bands;
+
+/* One envelope of a batched HMM-banded scan: residues i0..j0 of the buffer
+ * at dsq_offset (dsq_offset + x is residue x), its bands and cutoffs. */
+typedef struct cmgpu_hb_task {
+    int64_t dsq_offset;
+    int32_t i0, j0;
+    float env_cutoff, cutoff;
+    cmgpu_hb_bands bands;
+} cmgpu_hb_task;
+
+/* Per-envelope result: vsc_root, the envelope of ROOT cells >= env_cutoff
+ * (-1 when none), and the envelope's hits in hits[hit_first .. +nhits). */
+typedef struct cmgpu_hb_result {
+    float vsc_root;
+    int32_t nhits;
+    int64_t envi, envj;
+    int64_t hit_first;
+} cmgpu_hb_result;
+
+/* fast_cyk_scan_hb (src/cp9.rs:4682): HMM-banded CYK filter scan of dsq's
+ * residues i0..j0 (dsq = [255, codes.., 255] frame of n residues). */
+int cmgpu_fast_cyk_scan_hb(const cmgpu_model *m, const cmgpu_hb_bands *bands, const uint8_t *dsq,
+                           int32_t n, int32_t i0, int32_t j0, float env_cutoff, float *vsc_root,
+                           int64_t *envi, int64_t *envj);
+/* fast_fcyk_scan_hb (:4704, semiring CMGPU_CYK_F32) and fast_finside_scan_hb
+ * (:5465, CMGPU_INSIDE_F32): the same plus the greedily reported hits (with
+ * null3 when do_null3), before overlap removal, as the reference returns
+ * them.  CMGPU_EOVERFLOW with the needed count in *n_out if cap is short. */
+int cmgpu_hb_scan_hits(const cmgpu_model *m, int semiring, const cmgpu_hb_bands *bands,
+                       const uint8_t *dsq, int32_t n, int32_t i0, int32_t j0, float env_cutoff,
+                       float cutoff, int do_null3, float *vsc_root, int64_t *envi, int64_t *envj,
+                       cmgpu_hit *hits, int32_t cap, int32_t *n_out);
+/* Many envelopes (each with its own bands) in one call, one CTA per
+ * envelope.  report_hits = 0 gives the filter form (no hits). */
+int cmgpu_hb_scan_batch(const cmgpu_model *m, void *stream, int semiring, int report_hits, int do_null3,
+                        const uint8_t *dsq_all, int64_t dsq_len, const cmgpu_hb_task *tasks,
+                        int32_t ntask, cmgpu_hb_result *results, cmgpu_hit *hits, int64_t cap,
+                        int64_t *n_out);
+/* Device time and cells of the last HMM-banded call on this model. */
+int cmgpu_hb_stats(const cmgpu_model *m, double *kernel_ms, int64_t *cells, int32_t *launches);
 
 /* ---- P7 Viterbi filter (F2) ---------------------------------------------
  * A p7 filter profile as the reference's P7Profile holds it

@@ -16,7 +16,7 @@ LIB_PATH = os.path.join(_HERE, "_lib", "libcmscan_gpu.so")
 
 CMGPU_OK = 0
 CMGPU_EOVERFLOW = -4
-CYK_F32, INSIDE_I32 = 0, 1
+CYK_F32, INSIDE_I32, INSIDE_F32 = 0, 1, 2
 NOQDB, QDB1, QDB2 = 0, 1, 2
 
 P = C.POINTER
@@ -77,6 +77,21 @@ BATCH_HIT_DTYPE = np.dtype([("win", np.int32), ("i", np.int32), ("j", np.int32),
                             ("score", np.float32), ("bias", np.float32)])
 ENV_DTYPE = np.dtype([("start", np.int32), ("end", np.int32)])
 WINDOW_DTYPE = np.dtype([("dsq_offset", np.int64), ("i0", np.int32), ("j0", np.int32)])
+
+
+class HbBands(C.Structure):
+    _fields_ = [("jmin", P(C.c_int32)), ("jmax", P(C.c_int32)), ("hd_off", P(C.c_int32)),
+                ("hdmin", P(C.c_int32)), ("hdmax", P(C.c_int32))]
+
+
+class HbTask(C.Structure):
+    _fields_ = [("dsq_offset", C.c_int64), ("i0", C.c_int32), ("j0", C.c_int32), ("env_cutoff", C.c_float),
+                ("cutoff", C.c_float), ("bands", HbBands)]
+
+
+class HbResult(C.Structure):
+    _fields_ = [("vsc_root", C.c_float), ("nhits", C.c_int32), ("envi", C.c_int64), ("envj", C.c_int64),
+                ("hit_first", C.c_int64)]
 
 
 class Stats(C.Structure):
@@ -156,6 +171,14 @@ def lib() -> C.CDLL:
     L.cmgpu_ssv_diagonals.argtypes = [vp, vp, vp, C.c_int64, vp, C.c_int32, C.c_double, vp, C.c_int32,
                                       P(C.c_int32)]
     L.cmgpu_msv_filter_stats.argtypes = [vp, P(C.c_double), P(C.c_int64), P(C.c_int32)]
+    L.cmgpu_fast_cyk_scan_hb.argtypes = [vp, P(HbBands), vp, C.c_int32, C.c_int32, C.c_int32, C.c_float,
+                                         P(C.c_float), P(C.c_int64), P(C.c_int64)]
+    L.cmgpu_hb_scan_hits.argtypes = [vp, C.c_int, P(HbBands), vp, C.c_int32, C.c_int32, C.c_int32, C.c_float,
+                                     C.c_float, C.c_int, P(C.c_float), P(C.c_int64), P(C.c_int64), vp, C.c_int32,
+                                     P(C.c_int32)]
+    L.cmgpu_hb_scan_batch.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, vp, C.c_int64, vp, C.c_int32, vp, vp,
+                                      C.c_int64, P(C.c_int64)]
+    L.cmgpu_hb_stats.argtypes = [vp, P(C.c_double), P(C.c_int64), P(C.c_int32)]
     L.cmgpu_count_work.argtypes = [P(Cm), C.c_int, C.c_int, C.c_int32, P(C.c_double),
                                    P(C.c_double)]
     _lib = L
@@ -177,4 +200,5 @@ EXPORTED = [
     "cmgpu_vit_filter_build", "cmgpu_vit_filter_free", "cmgpu_vit_filter_tables", "cmgpu_vit_score_batch",
     "cmgpu_msv_filter_build", "cmgpu_msv_filter_free", "cmgpu_msv_filter_tables", "cmgpu_ssv_threshold",
     "cmgpu_msv_score_batch", "cmgpu_f1_msv_windows", "cmgpu_ssv_diagonals", "cmgpu_msv_filter_stats",
+    "cmgpu_fast_cyk_scan_hb", "cmgpu_hb_scan_hits", "cmgpu_hb_scan_batch", "cmgpu_hb_stats",
 ]

@@ -202,6 +202,8 @@ static float null3_correction(const cmgpu_model *m, const float *comp, int len) 
     return flogsum_host(m->flog, 0.0f, score);
 }
 
+float null3_corr(const cmgpu_model *m, const float *comp, int len) { return null3_correction(m, comp, len); }
+
 static inline float raw_bits(int semiring, uint32_t raw) {
     if (semiring == CMGPU_INSIDE_I32) {
         int32_t s = (int32_t)raw;

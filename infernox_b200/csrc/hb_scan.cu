@@ -1,0 +1,759 @@
+// HMM-banded (CP9-banded) CYK and float-Inside scans of envelopes
+// (fast_cyk_scan_hb_core, src/cp9.rs:4717-5379; fast_finside_scan_hb,
+// :5465-6014), many envelopes per launch, one CTA per envelope.
+//
+// Each envelope keeps the reference's banded matrix: state v, row jp = j -
+// jmin[v], cells d = hdmin..hdmax stored contiguously from the row offset
+// (in HBM; an envelope's working set stays in L2 while its states are
+// computed).  The states are grouped in dependency levels on the host (a
+// state's level is one more than its children's, END states are level 0), so
+// every state of a level depends only on finished levels and itself.  A level
+// is one phase of the CTA: its tasks are spread round-robin over the threads,
+// a task being
+//   * one band row (v, jp) for every state except IR -- its cells d run in
+//     order in one thread, which is exactly what IL's self-transition (cell
+//     d-1 of the same row) needs;
+//   * one diagonal i = j-d+1 for IR states -- IR's self-transition reads
+//     cell (j-1, d-1), the previous cell of the same diagonal, so the thread
+//     walks the diagonal's rows in order.
+// Every cell folds its children in the reference's order (children in
+// ascending offset, bifurcation splits k ascending) starting from the local
+// end value, then adds its emission and clamps at IMPOSSIBLE, so the float
+// results are the reference's bit for bit (FLogsum is order-sensitive; MAX
+// is taken with the reference's strict comparison).  After the last level a
+// root pass applies the local begins (MAX in both semirings), finds vsc_root
+// (first maximum in (j, d) order), the envelope of cells >= env_cutoff and the
+// reportable cells; the host replays the greedy report with null3.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "model_internal.h"
+
+namespace cmx {
+
+struct HbDev {
+    int M = 0, nlev = 0, nbeg = 0;
+    int8_t *sttype = nullptr;
+    int32_t *cfirst = nullptr, *cnum = nullptr, *lev_start = nullptr, *lev_states = nullptr, *begins = nullptr;
+    float *tsc = nullptr, *oesc = nullptr, *endsc = nullptr, *beginsc = nullptr, *flog = nullptr;
+    double last_ms = 0;
+    int64_t last_cells = 0;
+    int32_t last_launches = 0;
+};
+
+void hb_free(HbDev *h) {
+    if (!h) return;
+    cudaFree(h->sttype);
+    cudaFree(h->cfirst);
+    cudaFree(h->cnum);
+    cudaFree(h->lev_start);
+    cudaFree(h->lev_states);
+    cudaFree(h->begins);
+    cudaFree(h->tsc);
+    cudaFree(h->oesc);
+    cudaFree(h->endsc);
+    cudaFree(h->beginsc);
+    cudaFree(h->flog);
+    delete h;
+}
+
+namespace hb {
+
+struct Env {
+    int64_t alpha_off;  // first cell of this envelope's matrix
+    int64_t dsq_off;    // buffer index of residue 0
+    int32_t i0, j0;
+    float env_cutoff, cutoff;
+    int32_t st_off;     // first State of this envelope
+    int32_t cand_cap;
+};
+
+struct State {
+    int32_t jmin, jmax, row0, ntask;
+    int32_t ilo, hmn_min, hmx_max, pad;  // IR: first diagonal, band extremes
+};
+
+struct Row {
+    int32_t roff, hmn, hmx, pad;
+};
+
+struct Cand {
+    int32_t env, j, d;
+    float sc;
+};
+
+struct Out {
+    float vsc;
+    int32_t envi, envj, ncand;
+};
+
+struct Tables {
+    const int8_t *sttype;
+    const int32_t *cfirst, *cnum, *lev_start, *lev_states, *begins;
+    const float *tsc, *oesc, *endsc, *beginsc, *flog;
+    float el_selfsc;
+    int nlev, nbeg, local_begin;
+};
+
+__device__ __forceinline__ int sdelta(int st) {
+    return st == MP_ST ? 2 : (st == ML_ST || st == MR_ST || st == IL_ST || st == IR_ST) ? 1 : 0;
+}
+__device__ __forceinline__ int srdelta(int st) { return st == MP_ST || st == MR_ST || st == IR_ST; }
+
+// FLogsum (src/cp9.rs:5405-5413)
+__device__ __forceinline__ float flogsum(const float *tbl, float a, float b) {
+    const float mx = fmaxf(a, b), mn = fminf(a, b);
+    const float diff = __fsub_rn(mx, mn);
+    if (mn == -INFINITY || diff >= 23.0f) return mx;
+    return __fadd_rn(mx, __ldg(tbl + (int)__fmul_rn(diff, 1000.0f)));
+}
+
+template <bool INS>
+__device__ __forceinline__ float comb(const float *tbl, float cur, float cand) {
+    if (INS) return flogsum(tbl, cur, cand);
+    return cand > cur ? cand : cur;
+}
+
+// Cells dlo..dhi of row jp of a non-bifurcation state v.
+template <bool INS>
+__device__ void row_cells(const Tables &t, const State *st, const Row *rows, float *alpha, const uint8_t *dsq,
+                          int v, int stt, int jp, int dlo, int dhi) {
+    const State sv = st[v];
+    const int j = sv.jmin + jp;
+    const Row rv = rows[sv.row0 + jp];
+    const int av = rv.roff - rv.hmn;  // alpha[av + d] = cell d of this row
+    const int sd = sdelta(stt), sdr = srdelta(stt);
+    const float endsc = t.endsc[v];
+    const bool has_end = endsc > -9.999e35f;
+    if (stt == E_ST) {
+        for (int d = dlo; d <= dhi; d++) {
+            const float cur =
+                has_end ? __fadd_rn(__fmul_rn(t.el_selfsc, (float)max(d - sd, 0)), endsc) : IMPOSSIBLE;
+            alpha[av + d] = d == rv.hmn ? 0.0f : cur;
+        }
+        return;
+    }
+    const int ny = t.cnum[v], y0 = t.cfirst[v];
+    int cx[MAXC], clo[MAXC], chi[MAXC];
+    float ct[MAXC];
+#pragma unroll
+    for (int yo = 0; yo < MAXC; yo++) {
+        clo[yo] = 1;
+        chi[yo] = 0;
+        cx[yo] = 0;
+        ct[yo] = 0.0f;
+        if (yo < ny) {
+            const int y = y0 + yo, jy = j - sdr;
+            const State sy = st[y];
+            ct[yo] = t.tsc[v * MAXC + yo];
+            if (jy >= sy.jmin && jy <= sy.jmax) {
+                const Row ry = rows[sy.row0 + jy - sy.jmin];
+                cx[yo] = ry.roff - ry.hmn - sd;  // alpha[cx + d] = child cell d - sd of row jy
+                clo[yo] = ry.hmn + sd;
+                chi[yo] = ry.hmx + sd;
+            }
+        }
+    }
+    const float *oesc = t.oesc + (size_t)v * ESC;
+    const int xj = dsq[j];
+    for (int d = dlo; d <= dhi; d++) {
+        float cur = has_end ? __fadd_rn(__fmul_rn(t.el_selfsc, (float)max(d - sd, 0)), endsc) : IMPOSSIBLE;
+#pragma unroll
+        for (int yo = 0; yo < MAXC; yo++)
+            if (d >= clo[yo] && d <= chi[yo]) cur = comb<INS>(t.flog, cur, __fadd_rn(alpha[cx[yo] + d], ct[yo]));
+        if (stt == ML_ST || stt == IL_ST)
+            cur = __fadd_rn(cur, oesc[dsq[j - d + 1]]);
+        else if (stt == MR_ST || stt == IR_ST)
+            cur = __fadd_rn(cur, oesc[xj]);
+        else if (stt == MP_ST)
+            cur = __fadd_rn(cur, oesc[dsq[j - d + 1] * KP + xj]);
+        if (cur < IMPOSSIBLE) cur = IMPOSSIBLE;
+        alpha[av + d] = cur;
+    }
+}
+
+// Row jp of a bifurcation state v: split k over the right child z's row j.
+template <bool INS>
+__device__ void bif_row(const Tables &t, const State *st, const Row *rows, float *alpha, int v, int jp) {
+    const State sv = st[v];
+    const int j = sv.jmin + jp;
+    const Row rv = rows[sv.row0 + jp];
+    const int av = rv.roff - rv.hmn;
+    const float endsc = t.endsc[v];
+    const bool has_end = endsc > -9.999e35f;
+    const int y = t.cfirst[v], z = t.cnum[v];
+    const State sy = st[y], sz = st[z];
+    const bool inz = j >= sz.jmin && j <= sz.jmax;
+    Row rz{0, 1, 0, 0};
+    if (inz) rz = rows[sz.row0 + j - sz.jmin];
+    const int jpy = j - sy.jmin;
+    const int kn = max(max(j - sy.jmax, rz.hmn), 0), kx = min(jpy, rz.hmx);
+    const int zx = rz.roff - rz.hmn;  // alpha[zx + k] = right child cell k
+    for (int d = rv.hmn; d <= rv.hmx; d++) {
+        float cur = has_end ? __fadd_rn(__fmul_rn(t.el_selfsc, (float)d), endsc) : IMPOSSIBLE;
+        if (inz)
+            for (int k = kn; k <= kx; k++) {
+                const Row ry = rows[sy.row0 + jpy - k];
+                if (k >= d - ry.hmx && k <= d - ry.hmn)
+                    cur = comb<INS>(t.flog, cur, __fadd_rn(alpha[ry.roff + (d - ry.hmn - k)], alpha[zx + k]));
+            }
+        alpha[av + d] = cur;
+    }
+}
+
+// IR state v, diagonal i: cells (j, j-i+1) in row order.
+template <bool INS>
+__device__ void ir_diag(const Tables &t, const State *st, const Row *rows, float *alpha, const uint8_t *dsq, int v,
+                        int i) {
+    const State sv = st[v];
+    const int jlo = max(sv.jmin, i + sv.hmn_min - 1), jhi = min(sv.jmax, i + sv.hmx_max - 1);
+    for (int j = jlo; j <= jhi; j++) {
+        const int jp = j - sv.jmin, d = j - i + 1;
+        const Row rv = rows[sv.row0 + jp];
+        if (d >= rv.hmn && d <= rv.hmx) row_cells<INS>(t, st, rows, alpha, dsq, v, IR_ST, jp, d, d);
+    }
+}
+
+template <bool INS>
+__global__ void __launch_bounds__(256, 2) hb_kernel(Tables t, const Env *__restrict__ envs, int nenv,
+                                                 const State *__restrict__ states, const Row *__restrict__ rows,
+                                                 float *alpha_all, const uint8_t *__restrict__ dsq_all, int report,
+                                                 Cand *cands, int64_t cand_cap, unsigned long long *ncand, Out *out) {
+    __shared__ float s_v[256];
+    __shared__ int s_j[256];
+    __shared__ int s_envi, s_envj, s_nc;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int e = blockIdx.x; e < nenv; e += gridDim.x) {
+        const Env env = envs[e];
+        const State *st = states + env.st_off;
+        float *alpha = alpha_all + env.alpha_off;
+        const uint8_t *dsq = dsq_all + env.dsq_off;
+        for (int lev = 0; lev < t.nlev; lev++) {
+            int base = 0;
+            for (int q = t.lev_start[lev]; q < t.lev_start[lev + 1]; q++) {
+                const int v = t.lev_states[q];
+                const int n = st[v].ntask, stt = t.sttype[v];
+                // this thread's tasks: base + task = tid (mod nt)
+                for (int task = ((tid - base) % nt + nt) % nt; task < n; task += nt) {
+                    if (stt == IR_ST)
+                        ir_diag<INS>(t, st, rows, alpha, dsq, v, st[v].ilo + task);
+                    else if (stt == B_ST)
+                        bif_row<INS>(t, st, rows, alpha, v, task);
+                    else {
+                        const Row r = rows[st[v].row0 + task];
+                        if (r.hmn <= r.hmx) row_cells<INS>(t, st, rows, alpha, dsq, v, stt, task, r.hmn, r.hmx);
+                    }
+                }
+                base += n;
+            }
+            __syncthreads();
+        }
+        // root pass: local begins, vsc_root, envelope, reportable cells
+        if (tid == 0) {
+            s_envi = INT_MAX;
+            s_envj = INT_MIN;
+            s_nc = 0;
+        }
+        __syncthreads();
+        // vsc_root is the first maximum in (j, d) order: per row the first
+        // strict maximum, per thread (rows ascending) a later row wins only
+        // on a strictly larger value, across threads the smallest j wins ties
+        float best = IMPOSSIBLE;
+        int bestj = INT_MAX;
+        const State s0 = st[0];
+        for (int jp = tid; jp <= s0.jmax - s0.jmin; jp += nt) {
+            const int j = s0.jmin + jp;
+            const Row r0 = rows[s0.row0 + jp];
+            const int av = r0.roff - r0.hmn;
+            if (t.local_begin)
+                for (int b = 0; b < t.nbeg; b++) {
+                    const int y = t.begins[b];
+                    const State sy = st[y];
+                    if (j < sy.jmin || j > sy.jmax) continue;
+                    const Row ry = rows[sy.row0 + j - sy.jmin];
+                    const int dn = max(r0.hmn, ry.hmn), dx = min(r0.hmx, ry.hmx);
+                    const float bsc = t.beginsc[y];
+                    for (int d = dn; d <= dx; d++) {
+                        const float sc = __fadd_rn(alpha[ry.roff + d - ry.hmn], bsc);
+                        if (sc > alpha[av + d]) alpha[av + d] = sc;
+                    }
+                }
+            float rb = IMPOSSIBLE;
+            for (int d = r0.hmn; d <= r0.hmx; d++) {
+                const float sc = alpha[av + d];
+                if (sc > rb) rb = sc;
+                if (sc >= env.env_cutoff) {
+                    atomicMin(&s_envi, j - d + 1);
+                    atomicMax(&s_envj, j);
+                }
+                if (report && d >= 1 && sc >= env.cutoff && sc > -9.999e35f) {
+                    const unsigned long long slot = atomicAdd(ncand, 1ull);
+                    atomicAdd(&s_nc, 1);
+                    if ((int64_t)slot < cand_cap) cands[slot] = Cand{e, j, d, sc};
+                }
+            }
+            if (rb > best) {
+                best = rb;
+                bestj = j;
+            }
+        }
+        s_v[tid] = best;
+        s_j[tid] = bestj;
+        __syncthreads();
+        if (tid == 0) {
+            float bv = IMPOSSIBLE;
+            int bj = INT_MAX;
+            for (int q = 0; q < nt; q++)
+                if (s_v[q] > bv || (s_v[q] == bv && s_j[q] < bj)) {
+                    bv = s_v[q];
+                    bj = s_j[q];
+                }
+            out[e] = Out{bv, s_envi == INT_MAX ? -1 : s_envi, s_envj == INT_MIN ? -1 : s_envj, s_nc};
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace hb
+
+namespace {
+
+template <class T>
+int upload(T **dst, const T *src, size_t n) {
+    if (cudaMalloc((void **)dst, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) return CMGPU_ENOMEM;
+    if (n && cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess) return CMGPU_EDEVICE;
+    return CMGPU_OK;
+}
+
+// model tables and the level schedule, built once per model
+int hb_prepare(cmgpu_model *m, HbDev **out) {
+    std::lock_guard<std::mutex> g(m->mu);
+    if (m->hb) {
+        *out = m->hb;
+        return CMGPU_OK;
+    }
+    const HostCM &c = m->cm;
+    const int M = c.view.M;
+    std::vector<int> level(M, 0);
+    int nlev = 0;
+    for (int v = M - 1; v >= 0; v--) {
+        const int st = c.sttype[v];
+        int l = 0;
+        if (st == B_ST)
+            l = 1 + std::max(level[c.cfirst[v]], level[c.cnum[v]]);
+        else if (st != E_ST)
+            for (int yo = 0; yo < c.cnum[v]; yo++) {
+                const int y = c.cfirst[v] + yo;
+                if (y != v) l = std::max(l, 1 + level[y]);
+            }
+        level[v] = l;
+        nlev = std::max(nlev, l + 1);
+    }
+    std::vector<int32_t> lev_start(nlev + 1, 0), lev_states(M);
+    for (int v = 0; v < M; v++) lev_start[level[v] + 1]++;
+    for (int l = 0; l < nlev; l++) lev_start[l + 1] += lev_start[l];
+    std::vector<int32_t> fill(lev_start.begin(), lev_start.end() - 1);
+    for (int v = M - 1; v >= 0; v--) lev_states[fill[level[v]]++] = v;
+    std::vector<int32_t> begins;
+    for (int y = 1; y < M; y++)
+        if (c.beginsc[y] > -9.999e35f) begins.push_back(y);
+    HbDev *h = new HbDev();
+    h->M = M;
+    h->nlev = nlev;
+    h->nbeg = (int)begins.size();
+    int rc = CMGPU_OK;
+    if (cudaSetDevice(m->device) != cudaSuccess) rc = CMGPU_EDEVICE;
+    if (!rc) rc = upload(&h->sttype, c.sttype.data(), M);
+    if (!rc) rc = upload(&h->cfirst, c.cfirst.data(), M);
+    if (!rc) rc = upload(&h->cnum, c.cnum.data(), M);
+    if (!rc) rc = upload(&h->lev_start, lev_start.data(), lev_start.size());
+    if (!rc) rc = upload(&h->lev_states, lev_states.data(), lev_states.size());
+    if (!rc) rc = upload(&h->begins, begins.data(), begins.size());
+    if (!rc) rc = upload(&h->tsc, c.tsc.data(), c.tsc.size());
+    if (!rc) rc = upload(&h->oesc, c.oesc.data(), c.oesc.size());
+    if (!rc) rc = upload(&h->endsc, c.endsc.data(), c.endsc.size());
+    if (!rc) rc = upload(&h->beginsc, c.beginsc.data(), c.beginsc.size());
+    if (!rc) rc = upload(&h->flog, m->flog.data(), m->flog.size());
+    if (rc) {
+        hb_free(h);
+        set_error("HMM-banded scan: uploading the model tables failed");
+        return rc;
+    }
+    m->hb = h;
+    *out = h;
+    return CMGPU_OK;
+}
+
+int sdelta_h(int st) { return st == MP_ST ? 2 : (st == ML_ST || st == MR_ST || st == IL_ST || st == IR_ST) ? 1 : 0; }
+
+// validates one envelope's bands and appends its State / Row tables;
+// returns the envelope's cell count or -1 (error set)
+int64_t add_envelope(const HostCM &c, const cmgpu_hb_task &tk, int64_t dsq_len, const uint8_t *dsq_all,
+                     std::vector<hb::State> &states, std::vector<hb::Row> &rows) {
+    const int M = c.view.M;
+    const cmgpu_hb_bands &b = tk.bands;
+    if (!b.jmin || !b.jmax || !b.hd_off || !b.hdmin || !b.hdmax) {
+        set_error("HMM-banded scan: missing band arrays");
+        return -1;
+    }
+    if (tk.i0 < 1 || tk.j0 < tk.i0 - 1 || tk.dsq_offset < 0 || tk.dsq_offset + (int64_t)tk.j0 + 1 > dsq_len) {
+        set_error("HMM-banded scan: envelope outside the residue buffer");
+        return -1;
+    }
+    for (int32_t x = tk.i0; x <= tk.j0; x++)
+        if (dsq_all[tk.dsq_offset + x] > 17) {
+            set_error("HMM-banded scan: residue code > 17");
+            return -1;
+        }
+    int64_t ncells = 0;
+    for (int v = 0; v < M; v++) {
+        const int st = c.sttype[v], sd = sdelta_h(st);
+        hb::State s{b.jmin[v], b.jmax[v], (int32_t)rows.size(), 0, 0, INT_MAX, INT_MIN, 0};
+        const int nj = b.jmax[v] >= b.jmin[v] ? b.jmax[v] - b.jmin[v] + 1 : 0;
+        int ilo = INT_MAX, ihi = INT_MIN;
+        for (int jp = 0; jp < nj; jp++) {
+            const int j = b.jmin[v] + jp;
+            const int hmn = b.hdmin[b.hd_off[v] + jp], hmx = b.hdmax[b.hd_off[v] + jp];
+            if (hmx >= hmn) {
+                // every cell inside the envelope; emitting states need d >= 1
+                // so that the residue(s) they emit lie inside it
+                if (hmn < (sd > 0 ? 1 : 0) || j > tk.j0 || j - hmx + 1 < tk.i0) {
+                    set_error("HMM-banded scan: band cell outside the envelope (state " + std::to_string(v) +
+                              ", j " + std::to_string(j) + ")");
+                    return -1;
+                }
+                ilo = std::min(ilo, j - hmx + 1);
+                ihi = std::max(ihi, j - hmn + 1);
+                s.hmn_min = std::min(s.hmn_min, hmn);
+                s.hmx_max = std::max(s.hmx_max, hmx);
+            } else if (st == E_ST) {
+                set_error("HMM-banded scan: empty END state row");
+                return -1;
+            }
+            rows.push_back(hb::Row{(int32_t)ncells, hmn, hmx, 0});
+            if (hmx >= hmn) ncells += hmx - hmn + 1;
+            if (ncells > INT32_MAX) {
+                set_error("HMM-banded scan: more than 2^31 band cells in one envelope");
+                return -1;
+            }
+        }
+        if (st == IR_ST) {
+            s.ilo = ilo;
+            s.ntask = ihi >= ilo ? ihi - ilo + 1 : 0;
+        } else {
+            s.ntask = nj;
+        }
+        states.push_back(s);
+    }
+    if (b.jmax[0] < b.jmin[0]) {
+        // no ROOT rows: nothing to report; keep the tables consistent
+    }
+    return ncells;
+}
+
+// greedy report of one envelope from its reportable cells (sorted by j, d)
+void hb_report(const cmgpu_model *m, const hb::Cand *c, size_t n, const uint8_t *dsq, int32_t i0, float cutoff,
+               int do_null3, std::vector<cmgpu_hit> &out) {
+    if (!n) return;
+    std::vector<int32_t> pre;
+    int32_t lo = i0 - 1, hi = c[n - 1].j;
+    if (do_null3) {
+        pre.assign((size_t)(hi - lo + 1) * 4, 0);
+        for (int32_t p = lo + 1; p <= hi; p++) {
+            for (int a = 0; a < 4; a++) pre[(size_t)(p - lo) * 4 + a] = pre[(size_t)(p - 1 - lo) * 4 + a];
+            if (dsq[p] < 4) pre[(size_t)(p - lo) * 4 + dsq[p]]++;
+        }
+    }
+    size_t k = 0;
+    while (k < n) {
+        const int32_t j = c[k].j;
+        float max_rep = IMPOSSIBLE;
+        for (; k < n && c[k].j == j; k++) {
+            const int32_t d = c[k].d, i = j - d + 1;
+            float hit_sc = c[k].sc, bias = 0.0f;
+            if (!(hit_sc > max_rep && hit_sc >= cutoff && hit_sc > -9.999e35f)) continue;
+            bool rep = true;
+            if (do_null3) {
+                float comp[4];
+                for (int a = 0; a < 4; a++)
+                    comp[a] = (float)(double)(pre[(size_t)(j - lo) * 4 + a] - pre[(size_t)(i - 1 - lo) * 4 + a]);
+                // esl_vec_fnorm with a compensated sum (src/cp9.rs:464)
+                float sum = 0.0f, cc = 0.0f;
+                for (int a = 0; a < 4; a++) {
+                    const float y = comp[a] - cc, t = sum + y;
+                    cc = (t - sum) - y;
+                    sum = t;
+                }
+                for (int a = 0; a < 4; a++) comp[a] = sum != 0.0f ? comp[a] / sum : 0.25f;
+                const float corr = null3_corr(m, comp, d);
+                hit_sc -= corr;
+                bias = corr;
+                rep = hit_sc > max_rep && hit_sc >= cutoff;
+            }
+            if (rep) {
+                out.push_back(cmgpu_hit{i, j, hit_sc, bias});
+                max_rep = hit_sc;
+            }
+        }
+    }
+}
+
+#define HB_TRY(call)                                                                            \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess) {                                                                \
+            set_error(std::string("HMM-banded scan: ") + #call + ": " + cudaGetErrorString(e_)); \
+            return CMGPU_EDEVICE;                                                               \
+        }                                                                                       \
+    } while (0)
+
+struct DevBufs {
+    std::vector<void *> p;
+    ~DevBufs() {
+        for (void *q : p) cudaFree(q);
+    }
+    template <class T>
+    bool get(T **out, size_t bytes) {
+        void *q = nullptr;
+        if (cudaMalloc(&q, std::max<size_t>(bytes, 16)) != cudaSuccess) return false;
+        p.push_back(q);
+        *out = (T *)q;
+        return true;
+    }
+};
+
+// one launch over envelopes [e0, e1) (their tables already built)
+int hb_launch(cmgpu_model *m, HbDev *h, cudaStream_t st, int semiring, int report, int do_null3,
+              const uint8_t *dsq_all, int64_t dsq_len, const cmgpu_hb_task *tasks, int32_t e0, int32_t e1,
+              const std::vector<hb::State> &states, const std::vector<hb::Row> &rows,
+              const std::vector<int64_t> &alpha_off, const std::vector<int32_t> &st_off,
+              const std::vector<int64_t> &row_base, cmgpu_hb_result *results, std::vector<cmgpu_hit> &hits,
+              double &ms_total, int &launches) {
+    const int n = e1 - e0;
+    const int M = m->cm.view.M;
+    // rows of these envelopes are contiguous from row_base[e0]
+    const int64_t r0 = row_base[e0], r1 = row_base[e1];
+    const int64_t s0 = (int64_t)st_off[e0], s1 = (int64_t)e1 * M;
+    std::vector<hb::State> lst(states.begin() + s0, states.begin() + s1);
+    for (auto &s : lst) s.row0 -= (int32_t)r0;
+    std::vector<hb::Env> envs(n);
+    int64_t cells = alpha_off[e1] - alpha_off[e0];
+    for (int e = 0; e < n; e++) {
+        const cmgpu_hb_task &tk = tasks[e0 + e];
+        envs[e] = hb::Env{alpha_off[e0 + e] - alpha_off[e0], tk.dsq_offset, tk.i0, tk.j0, tk.env_cutoff, tk.cutoff,
+                          (int32_t)(st_off[e0 + e] - s0), 0};
+    }
+    DevBufs bufs;
+    hb::Env *d_env;
+    hb::State *d_st;
+    hb::Row *d_rows;
+    float *d_alpha;
+    uint8_t *d_dsq;
+    hb::Out *d_out;
+    unsigned long long *d_nc;
+    if (!bufs.get(&d_env, sizeof(hb::Env) * n) || !bufs.get(&d_st, sizeof(hb::State) * lst.size()) ||
+        !bufs.get(&d_rows, sizeof(hb::Row) * (size_t)(r1 - r0)) || !bufs.get(&d_alpha, sizeof(float) * (size_t)cells) ||
+        !bufs.get(&d_dsq, (size_t)dsq_len) || !bufs.get(&d_out, sizeof(hb::Out) * n) ||
+        !bufs.get(&d_nc, sizeof(unsigned long long))) {
+        set_error("HMM-banded scan: device allocation failed");
+        return CMGPU_ENOMEM;
+    }
+    HB_TRY(cudaMemcpyAsync(d_env, envs.data(), sizeof(hb::Env) * n, cudaMemcpyHostToDevice, st));
+    HB_TRY(cudaMemcpyAsync(d_st, lst.data(), sizeof(hb::State) * lst.size(), cudaMemcpyHostToDevice, st));
+    HB_TRY(cudaMemcpyAsync(d_rows, rows.data() + r0, sizeof(hb::Row) * (size_t)(r1 - r0), cudaMemcpyHostToDevice, st));
+    HB_TRY(cudaMemcpyAsync(d_dsq, dsq_all, (size_t)dsq_len, cudaMemcpyHostToDevice, st));
+    hb::Tables t{h->sttype, h->cfirst, h->cnum, h->lev_start, h->lev_states, h->begins, h->tsc, h->oesc,
+                 h->endsc, h->beginsc, h->flog, m->cm.view.el_selfsc, h->nlev, h->nbeg,
+                 (int)((m->cm.view.flags >> 10) & 1u)};
+    int64_t cap = report ? 4096 + 4 * (int64_t)n : 0;
+    cudaEvent_t ev0, ev1;
+    HB_TRY(cudaEventCreate(&ev0));
+    HB_TRY(cudaEventCreate(&ev1));
+    for (int attempt = 0; attempt < 2; attempt++) {
+        DevBufs cb;
+        hb::Cand *d_c = nullptr;
+        if (!cb.get(&d_c, sizeof(hb::Cand) * (size_t)std::max<int64_t>(cap, 1))) {
+            cudaEventDestroy(ev0);
+            cudaEventDestroy(ev1);
+            set_error("HMM-banded scan: device allocation failed");
+            return CMGPU_ENOMEM;
+        }
+        HB_TRY(cudaMemsetAsync(d_nc, 0, sizeof(unsigned long long), st));
+        HB_TRY(cudaEventRecord(ev0, st));
+        if (semiring == CMGPU_INSIDE_F32)
+            hb::hb_kernel<true><<<n, 256, 0, st>>>(t, d_env, n, d_st, d_rows, d_alpha, d_dsq, report, d_c, cap, d_nc,
+                                                   d_out);
+        else
+            hb::hb_kernel<false><<<n, 256, 0, st>>>(t, d_env, n, d_st, d_rows, d_alpha, d_dsq, report, d_c, cap, d_nc,
+                                                    d_out);
+        HB_TRY(cudaGetLastError());
+        HB_TRY(cudaEventRecord(ev1, st));
+        unsigned long long nc = 0;
+        std::vector<hb::Out> outv(n);
+        HB_TRY(cudaMemcpyAsync(&nc, d_nc, sizeof(nc), cudaMemcpyDeviceToHost, st));
+        HB_TRY(cudaMemcpyAsync(outv.data(), d_out, sizeof(hb::Out) * n, cudaMemcpyDeviceToHost, st));
+        HB_TRY(cudaStreamSynchronize(st));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ev0, ev1);
+        ms_total += ms;
+        launches++;
+        if ((int64_t)nc > cap) {
+            cap = (int64_t)nc;
+            continue;
+        }
+        std::vector<hb::Cand> hc((size_t)nc);
+        if (nc) {
+            HB_TRY(cudaMemcpyAsync(hc.data(), d_c, sizeof(hb::Cand) * (size_t)nc, cudaMemcpyDeviceToHost, st));
+            HB_TRY(cudaStreamSynchronize(st));
+        }
+        std::sort(hc.begin(), hc.end(), [](const hb::Cand &a, const hb::Cand &b) {
+            if (a.env != b.env) return a.env < b.env;
+            if (a.j != b.j) return a.j < b.j;
+            return a.d < b.d;
+        });
+        size_t q = 0;
+        for (int e = 0; e < n; e++) {
+            const cmgpu_hb_task &tk = tasks[e0 + e];
+            cmgpu_hb_result &r = results[e0 + e];
+            r.vsc_root = outv[e].vsc;
+            r.envi = outv[e].envi;
+            r.envj = outv[e].envj;
+            r.hit_first = (int64_t)hits.size();
+            size_t q1 = q;
+            while (q1 < hc.size() && hc[q1].env == e) q1++;
+            if (report) hb_report(m, hc.data() + q, q1 - q, dsq_all + tk.dsq_offset, tk.i0, tk.cutoff, do_null3, hits);
+            r.nhits = (int32_t)((int64_t)hits.size() - r.hit_first);
+            q = q1;
+        }
+        break;
+    }
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+    h->last_cells += cells;
+    return CMGPU_OK;
+}
+
+int hb_batch(const cmgpu_model *mc, cudaStream_t st, int semiring, int report, int do_null3, const uint8_t *dsq_all,
+             int64_t dsq_len, const cmgpu_hb_task *tasks, int32_t ntask, cmgpu_hb_result *results,
+             std::vector<cmgpu_hit> &hits) {
+    cmgpu_model *m = const_cast<cmgpu_model *>(mc);
+    if (semiring != CMGPU_CYK_F32 && semiring != CMGPU_INSIDE_F32) {
+        set_error("HMM-banded scan: semiring must be CMGPU_CYK_F32 or CMGPU_INSIDE_F32");
+        return CMGPU_EINVAL;
+    }
+    HbDev *h = nullptr;
+    int rc = hb_prepare(m, &h);
+    if (rc) return rc;
+    HB_TRY(cudaSetDevice(m->device));
+    std::vector<hb::State> states;
+    std::vector<hb::Row> rows;
+    std::vector<int64_t> alpha_off(ntask + 1, 0), row_base(ntask + 1, 0);
+    std::vector<int32_t> st_off(ntask + 1, 0);
+    for (int32_t e = 0; e < ntask; e++) {
+        st_off[e] = (int32_t)states.size();
+        row_base[e] = (int64_t)rows.size();
+        const int64_t nc = add_envelope(m->cm, tasks[e], dsq_len, dsq_all, states, rows);
+        if (nc < 0) return CMGPU_EINVAL;
+        alpha_off[e + 1] = alpha_off[e] + nc;
+    }
+    st_off[ntask] = (int32_t)states.size();
+    row_base[ntask] = (int64_t)rows.size();
+    h->last_ms = 0;
+    h->last_cells = 0;
+    h->last_launches = 0;
+    // launches of at most ~1 Gi cells of matrix (4 GiB) each
+    const int64_t budget = (int64_t)1 << 30;
+    int launches = 0;
+    double ms = 0;
+    int32_t e0 = 0;
+    while (e0 < ntask) {
+        int32_t e1 = e0 + 1;
+        while (e1 < ntask && alpha_off[e1 + 1] - alpha_off[e0] <= budget) e1++;
+        rc = hb_launch(m, h, st, semiring, report, do_null3, dsq_all, dsq_len, tasks, e0, e1, states, rows, alpha_off,
+                       st_off, row_base, results, hits, ms, launches);
+        if (rc) return rc;
+        e0 = e1;
+    }
+    h->last_ms = ms;
+    h->last_launches = launches;
+    return CMGPU_OK;
+}
+
+}  // namespace
+}  // namespace cmx
+
+using namespace cmx;
+
+extern "C" int cmgpu_hb_scan_batch(const cmgpu_model *m, void *stream, int semiring, int report_hits, int do_null3,
+                                   const uint8_t *dsq_all, int64_t dsq_len, const cmgpu_hb_task *tasks,
+                                   int32_t ntask, cmgpu_hb_result *results, cmgpu_hit *hits, int64_t cap,
+                                   int64_t *n_out) {
+    if (!m || !dsq_all || ntask < 0 || (ntask > 0 && (!tasks || !results)) || !n_out) return CMGPU_EINVAL;
+    *n_out = 0;
+    if (ntask == 0) return CMGPU_OK;
+    std::vector<cmgpu_hit> all;
+    int rc = hb_batch(m, (cudaStream_t)stream, semiring, report_hits, do_null3, dsq_all, dsq_len, tasks, ntask,
+                      results, all);
+    if (rc) return rc;
+    *n_out = (int64_t)all.size();
+    if ((int64_t)all.size() > cap) {
+        set_error("cmgpu_hb_scan_batch: hit capacity too small");
+        return CMGPU_EOVERFLOW;
+    }
+    if (hits) std::copy(all.begin(), all.end(), hits);
+    return CMGPU_OK;
+}
+
+extern "C" int cmgpu_fast_cyk_scan_hb(const cmgpu_model *m, const cmgpu_hb_bands *bands, const uint8_t *dsq,
+                                      int32_t n, int32_t i0, int32_t j0, float env_cutoff, float *vsc_root,
+                                      int64_t *envi, int64_t *envj) {
+    if (!m || !bands || !dsq || n < 0 || !vsc_root || !envi || !envj) return CMGPU_EINVAL;
+    cmgpu_hb_task tk{0, i0, j0, env_cutoff, 0.0f, *bands};
+    cmgpu_hb_result r{};
+    std::vector<cmgpu_hit> hits;
+    int rc = hb_batch(m, nullptr, CMGPU_CYK_F32, 0, 0, dsq, (int64_t)n + 2, &tk, 1, &r, hits);
+    if (rc) return rc;
+    *vsc_root = r.vsc_root;
+    *envi = r.envi;
+    *envj = r.envj;
+    return CMGPU_OK;
+}
+
+extern "C" int cmgpu_hb_scan_hits(const cmgpu_model *m, int semiring, const cmgpu_hb_bands *bands,
+                                  const uint8_t *dsq, int32_t n, int32_t i0, int32_t j0, float env_cutoff,
+                                  float cutoff, int do_null3, float *vsc_root, int64_t *envi, int64_t *envj,
+                                  cmgpu_hit *hits, int32_t cap, int32_t *n_out) {
+    if (!m || !bands || !dsq || n < 0 || !vsc_root || !envi || !envj || !n_out) return CMGPU_EINVAL;
+    *n_out = 0;
+    cmgpu_hb_task tk{0, i0, j0, env_cutoff, cutoff, *bands};
+    cmgpu_hb_result r{};
+    std::vector<cmgpu_hit> all;
+    int rc = hb_batch(m, nullptr, semiring, 1, do_null3, dsq, (int64_t)n + 2, &tk, 1, &r, all);
+    if (rc) return rc;
+    *vsc_root = r.vsc_root;
+    *envi = r.envi;
+    *envj = r.envj;
+    *n_out = (int32_t)all.size();
+    if ((int64_t)all.size() > cap) {
+        set_error("cmgpu_hb_scan_hits: hit capacity too small");
+        return CMGPU_EOVERFLOW;
+    }
+    if (hits) std::copy(all.begin(), all.end(), hits);
+    return CMGPU_OK;
+}
+
+extern "C" int cmgpu_hb_stats(const cmgpu_model *m, double *kernel_ms, int64_t *cells, int32_t *launches) {
+    if (!m) return CMGPU_EINVAL;
+    const HbDev *h = m->hb;
+    if (kernel_ms) *kernel_ms = h ? h->last_ms : 0.0;
+    if (cells) *cells = h ? h->last_cells : 0;
+    if (launches) *launches = h ? h->last_launches : 0;
+    return CMGPU_OK;
+}

@@ -18,6 +18,8 @@
 namespace cmx {
 
 void set_error(const std::string &msg);
+struct HbDev;  // device tables of the HMM-banded scanner (hb_scan.cu)
+void hb_free(HbDev *h);
 bool build_plan(const cmgpu_cm *cm, int semiring, int qdbidx, Plan &p);
 
 // ---------------------------------------------------------------------------
@@ -128,11 +130,17 @@ struct cmgpu_model {
     uint16_t *ilog = nullptr;
     int ilog_nz = 0;
     std::vector<float> flog;  // host FLogsum table for null3
-    ~cmgpu_model() { cudaFree(ilog); }
+    cmx::HbDev *hb = nullptr;  // built on the first HMM-banded scan
+    ~cmgpu_model() {
+        cudaFree(ilog);
+        cmx::hb_free(hb);
+    }
 };
 
 
 namespace cmx {
+// score_correction_null3 (src/cp9.rs:6516-6528) with the model's null and omega
+float null3_corr(const cmgpu_model *m, const float *comp, int len);
 // Replays the reference's greedy report for one window from its reportable
 // cells (sorted by j, d) and removes overlaps; appends to `out`.
 void report_window(const cmgpu_model *m, int semiring, const Cand *c, size_t n, const uint8_t *frame,

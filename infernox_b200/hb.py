@@ -1,0 +1,125 @@
+"""HMM-banded (CP9-banded) scanners on the GPU.
+
+Mirrors the reference's functions over `&CM` and `&CP9Bands`
+(src/cp9.rs):
+
+    fast_cyk_scan_hb(cm, cp9b, dsq, i0, j0, env_cutoff) -> (vsc_root, envi, envj)       :4682
+    fast_fcyk_scan_hb(cm, cp9b, dsq, i0, j0, env_cutoff, cutoff, do_null3)
+        -> (vsc_root, envi, envj, hits)                                                 :4704
+    fast_finside_scan_hb(cm, cp9b, dsq, i0, j0, env_cutoff, cutoff, do_null3)
+        -> (vsc_root, envi, envj, hits)                                                 :5465
+
+`Bands` holds what the scanners read from CP9Bands: jmin/jmax per state and
+the per-row d-bands hdmin/hdmax.  `hb_scan_batch` scans many envelopes, each
+with its own bands, in one call.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native as N
+from .scan import Scanner, _frame, _scanner
+
+
+@dataclass
+class Bands:
+    """jmin/jmax [M]; hdmin/hdmax rows of state v at hd_off[v] + (j - jmin[v])."""
+    jmin: np.ndarray
+    jmax: np.ndarray
+    hd_off: np.ndarray
+    hdmin: np.ndarray
+    hdmax: np.ndarray
+
+    @staticmethod
+    def from_rows(jmin, jmax, rows_min, rows_max) -> "Bands":
+        """Build from per-state row lists (hdmin[v][jp], hdmax[v][jp]) as CP9Bands stores them."""
+        off, acc = [], 0
+        for r in rows_min:
+            off.append(acc)
+            acc += len(r)
+        cat = lambda rs: np.ascontiguousarray(np.concatenate([np.asarray(r, np.int32) for r in rs] or [np.zeros(0)]),
+                                              np.int32)
+        return Bands(np.ascontiguousarray(jmin, np.int32), np.ascontiguousarray(jmax, np.int32),
+                     np.asarray(off, np.int32), cat(rows_min), cat(rows_max))
+
+    def struct(self) -> N.HbBands:
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))
+        self._keep = [np.ascontiguousarray(a, np.int32) for a in (self.jmin, self.jmax, self.hd_off, self.hdmin,
+                                                                    self.hdmax)]
+        return N.HbBands(*[ip(a) for a in self._keep])
+
+
+def _hits(arr, n):
+    return [(int(h["i"]), int(h["j"]), float(h["score"]), float(h["bias"])) for h in arr[:n]]
+
+
+def _hb_hits(sc: Scanner, semiring, bands: Bands, dsq, i0, j0, env_cutoff, cutoff, do_null3):
+    a = _frame(dsq)
+    b = bands.struct()
+    vsc, ei, ej = C.c_float(), C.c_int64(), C.c_int64()
+    cap = 256
+    while True:
+        out = np.zeros(cap, N.HIT_DTYPE)
+        n = C.c_int32()
+        rc = N.lib().cmgpu_hb_scan_hits(sc._model, semiring, C.byref(b), a.ctypes.data, a.size - 2, i0, j0,
+                                        float(env_cutoff), float(cutoff), int(bool(do_null3)), C.byref(vsc),
+                                        C.byref(ei), C.byref(ej), out.ctypes.data, cap, C.byref(n))
+        if rc == N.CMGPU_EOVERFLOW and n.value > cap:
+            cap = n.value
+            continue
+        N.check(rc)
+        return vsc.value, ei.value, ej.value, _hits(out, n.value)
+
+
+def fast_cyk_scan_hb(cm, bands: Bands, dsq, i0: int, j0: int, env_cutoff: float):
+    """src/cp9.rs:4682 -- (vsc_root, envi, envj); envi/envj -1 when no cell reaches env_cutoff."""
+    sc = cm if isinstance(cm, Scanner) else _scanner(cm)
+    a = _frame(dsq)
+    b = bands.struct()
+    vsc, ei, ej = C.c_float(), C.c_int64(), C.c_int64()
+    N.check(N.lib().cmgpu_fast_cyk_scan_hb(sc._model, C.byref(b), a.ctypes.data, a.size - 2, i0, j0,
+                                           float(env_cutoff), C.byref(vsc), C.byref(ei), C.byref(ej)))
+    return vsc.value, ei.value, ej.value
+
+
+def fast_fcyk_scan_hb(cm, bands: Bands, dsq, i0: int, j0: int, env_cutoff: float, cutoff: float, do_null3: bool):
+    """src/cp9.rs:4704 -- (vsc_root, envi, envj, hits (i, j, score, bias) before overlap removal)."""
+    sc = cm if isinstance(cm, Scanner) else _scanner(cm)
+    return _hb_hits(sc, N.CYK_F32, bands, dsq, i0, j0, env_cutoff, cutoff, do_null3)
+
+
+def fast_finside_scan_hb(cm, bands: Bands, dsq, i0: int, j0: int, env_cutoff: float, cutoff: float,
+                         do_null3: bool):
+    """src/cp9.rs:5465 -- float Inside (FLogsum); same returns as fast_fcyk_scan_hb."""
+    sc = cm if isinstance(cm, Scanner) else _scanner(cm)
+    return _hb_hits(sc, N.INSIDE_F32, bands, dsq, i0, j0, env_cutoff, cutoff, do_null3)
+
+
+def hb_scan_batch(sc: Scanner, semiring: int, report_hits: bool, do_null3: bool, buf: np.ndarray, tasks):
+    """tasks: [(dsq_offset, i0, j0, env_cutoff, cutoff, Bands)] -> [(vsc, envi, envj, hits)] per task."""
+    b = np.ascontiguousarray(buf, np.uint8)
+    tk = (N.HbTask * len(tasks))()
+    for q, (off, i0, j0, ec, cut, bands) in enumerate(tasks):
+        tk[q] = N.HbTask(off, i0, j0, ec, cut, bands.struct())
+    res = (N.HbResult * len(tasks))()
+    cap = 1024
+    while True:
+        out = np.zeros(cap, N.HIT_DTYPE)
+        n = C.c_int64()
+        rc = N.lib().cmgpu_hb_scan_batch(sc._model, None, semiring, int(bool(report_hits)), int(bool(do_null3)),
+                                         b.ctypes.data, b.size, tk, len(tasks), res, out.ctypes.data, cap,
+                                         C.byref(n))
+        if rc == N.CMGPU_EOVERFLOW and n.value > cap:
+            cap = n.value
+            continue
+        N.check(rc)
+        return [(r.vsc_root, r.envi, r.envj, _hits(out[r.hit_first:], r.nhits)) for r in res]
+
+
+def hb_stats(sc: Scanner):
+    ms, cells, launches = C.c_double(), C.c_int64(), C.c_int32()
+    N.check(N.lib().cmgpu_hb_stats(sc._model, C.byref(ms), C.byref(cells), C.byref(launches)))
+    return ms.value, cells.value, launches.value

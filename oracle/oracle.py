@@ -1,5 +1,5 @@
 """TEST INFRASTRUCTURE ONLY: ctypes binding of the oracle (qdb_oracle.c,
-p7_oracle.c, msv_oracle.c).
+hb_oracle.c, p7_oracle.c, msv_oracle.c).
 
 Used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as
 the checker of the GPU scanner.  The product package never imports it.
@@ -30,7 +30,7 @@ def build() -> str:
 def lib():
     global _lib
     if _lib is None:
-        srcs = [os.path.join(HERE, f) for f in ("qdb_oracle.c", "p7_oracle.c", "msv_oracle.c")]
+        srcs = [os.path.join(HERE, f) for f in ("qdb_oracle.c", "hb_oracle.c", "p7_oracle.c", "msv_oracle.c")]
         if not os.path.exists(LIB_PATH) or any(os.path.getmtime(LIB_PATH) < os.path.getmtime(f) for f in srcs):
             build()
         L = C.CDLL(LIB_PATH)
@@ -53,6 +53,9 @@ def lib():
         L.oracle_f1_msv_windows.restype = C.c_int64
         L.oracle_ssv_threshold.argtypes = [C.c_int, vp, vp, C.c_int, C.c_double, C.c_double, C.c_double]
         L.oracle_ssv_threshold.restype = C.c_int
+        L.oracle_hb_scan.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp, vp, C.c_int32, C.c_int32, C.c_float,
+                                     C.c_int, C.c_float, C.c_int, P(C.c_float), P(C.c_int64), P(C.c_int64), vp,
+                                     C.c_int32]
         L.oracle_ilogsum_table.argtypes = [P(C.c_int32), C.c_int]
         L.oracle_ilogsum.argtypes = [C.c_int32, C.c_int32]
         L.oracle_ilogsum.restype = C.c_int32
@@ -217,3 +220,21 @@ def ssv_threshold(M, mat, trans, max_length, mmu, mlambda, f1):
     mat, trans = _f32(mat), _f32(trans)
     return int(lib().oracle_ssv_threshold(int(M), mat.ctypes.data, trans.ctypes.data, int(max_length), float(mmu),
                                           float(mlambda), float(f1)))
+
+
+def hb_scan(cm, inside, bands, dsq, i0, j0, env_cutoff, report, cutoff, do_null3):
+    """fast_cyk_scan_hb_core / fast_finside_scan_hb restated: (vsc_root, envi, envj, hits).
+    bands: (jmin, jmax, hd_off, hdmin, hdmax) int32 arrays."""
+    a, _ = _u8(dsq)
+    bs = [np.ascontiguousarray(x, np.int32) for x in bands]
+    vsc, ei, ej = C.c_float(), C.c_int64(), C.c_int64()
+    cap = 256
+    while True:
+        hits = np.zeros(cap, HIT_DTYPE)
+        n = lib().oracle_hb_scan(C.byref(cm.as_struct()), int(bool(inside)), *[b.ctypes.data for b in bs],
+                                 a.ctypes.data, i0, j0, float(env_cutoff), int(bool(report)), float(cutoff),
+                                 int(bool(do_null3)), C.byref(vsc), C.byref(ei), C.byref(ej), hits.ctypes.data, cap)
+        if n <= cap:
+            out = [(int(h["i"]), int(h["j"]), float(h["score"]), float(h["bias"])) for h in hits[:n]]
+            return vsc.value, ei.value, ej.value, out
+        cap = n

@@ -667,3 +667,14 @@ int oracle_final_stage_inside_opt(const cmgpu_cm *cm, const uint8_t *dsq, const 
     free(out.v);
     return rc;
 }
+
+/* shared with hb_oracle.c */
+float oracle_flogsum(float a, float b) {
+    init_tables();
+    return flogsum(a, b);
+}
+
+float oracle_null3(const float *null0, const float *comp, int len, float omega) {
+    init_tables();
+    return null3_correction(null0, comp, len, omega);
+}
