@@ -1,5 +1,12 @@
 """Benchmark of the batched QDB/Inside window scan (one JSON line on rank 0).
 
+Other workloads (--workload): "nohmm-cyk-filter" (QDB1 CYK over 100 kb
+chunks), and the filter/banded stages of the default pipeline --
+"f1-ssv" (SSV windows over 100 kb chunks, both strands, of a 4.6 Mb
+sequence, F1 = 0.35), "f2-vit" (Viterbi filter over F1-sized windows),
+"hb-cyk" / "hb-inside" (HMM-banded CYK / float Inside over envelopes with
+CP9-shaped bands) -- each with the oracle timed on the host cores beside it.
+
 Workload (default "batched-uneven-max"): the batched uneven-window Inside scan
 of the --max path.  One 120-consensus-column CM with 3 bifurcations (seeded
 synthetic, local configuration), sequences with log-normal lengths clipped to
@@ -40,6 +47,7 @@ WORKLOADS = {
     "nohmm-cyk-filter": dict(clen=72, paired=None, nbif=2, sseed=0, pseed=11, semiring=0, band=1,
                              median=100000, sigma=0.0, lo=100000, hi=100000, gc=0.50),
 }
+FILTER_WORKLOADS = ("f1-ssv", "f2-vit", "hb-cyk", "hb-inside")
 OPS_PER_TERM = {0: 2.0, 1: 7.0}   # CYK: FADD + select; Inside: 6 INT + 1 LDS
 OPS_PER_CELL = 2.0                # emission add + store
 CUTOFF_BITS = 15.0                # stands in for the E-value threshold
@@ -186,12 +194,15 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batched-uneven-max", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="batched-uneven-max",
+                    choices=sorted(WORKLOADS) + list(FILTER_WORKLOADS))
     ap.add_argument("--batch", type=int, default=300, help="sequences per step per rank")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--plain-windows", type=int, default=16)
     args = ap.parse_args()
+    if args.workload in FILTER_WORKLOADS:
+        return filter_main(args)
     w = WORKLOADS[args.workload]
     rank, world, local_rank = env_rank()
     cm = make_model(w)
@@ -365,6 +376,202 @@ def main():
     sc.close()
     if dist:
         dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# filter and HMM-banded stages
+# ---------------------------------------------------------------------------
+# lane-ops per algorithmic cell, for the issue roofline of each kernel:
+# SSV: max(dp, xB), +bias (saturating), -cost (floored), row max;
+# Viterbi: M 4 adds + 3 max + emission, I 2 adds + max, D 2 adds + max;
+# HB: per child relaxation 2 (CYK) or 9 (FLogsum), about 3 children per
+# cell, plus emission add and clamp.
+FILTER_OPS_PER_CELL = {"f1-ssv": 4.0, "f2-vit": 14.0, "hb-cyk": 8.0, "hb-inside": 29.0}
+
+
+def _chunks(total, chunk, rng, cons, nplant, gc):
+    """Both strands of a total-residue sequence with planted consensus runs,
+    cut into chunk frames."""
+    from infernox_b200 import p7, synth
+    frames, wins, off = [], [], 0
+    top = p7.planted_residues(total, cons, nplant, int(rng.integers(1 << 30)), gc=gc)
+    for s in (top, synth.revcomp(top)):
+        for a in range(0, total, chunk):
+            piece = s[a:a + chunk]
+            f = np.concatenate([[255], piece, [255]]).astype(np.uint8)
+            frames.append(f)
+            wins.append((off, 1, len(piece)))
+            off += len(f)
+    W = np.array(wins, dtype=[("dsq_offset", np.int64), ("i0", np.int32), ("j0", np.int32)])
+    return np.concatenate(frames), W
+
+
+def _same(out, ref):
+    if isinstance(out, np.ndarray):
+        return np.array_equal(out.view(np.uint8), ref.view(np.uint8))
+    if isinstance(out, tuple):  # bits: overflowed windows score NaN
+        return all(np.array_equal(np.ascontiguousarray(a).view(np.uint8), np.ascontiguousarray(b).view(np.uint8))
+                   for a, b in zip(out, ref))
+    return out == ref
+
+
+def filter_main(args):
+    """One JSON line for the F1 / F2 / HB workloads (rank 0 prints)."""
+    from concurrent.futures import ThreadPoolExecutor
+    rank, world, local_rank = env_rank()
+    kind = args.workload
+    rng = np.random.default_rng(4242 + rank)
+    from infernox_b200 import hb, model, p7, synth
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    config = {"workload": kind, "parallelism": f"dp{world}", "l2": "flushed (256 MB write) before each timed step"}
+    if kind in ("f1-ssv", "f2-vit"):
+        M = 120
+        prof, cons = p7.synthetic_profile(M, 77, 0.6)
+        maxl = int(1.25 * M)
+        mmu, mlam, f1 = -8.0, 0.693, 0.35
+        if kind == "f1-ssv":
+            buf, wins = _chunks(4_600_000, 100_000, rng, cons, 40, 0.508)
+            config.update({"model": f"synthetic p7 profile M={M} (peak 0.6)",
+                           "sequence": "4.6 Mb, both strands, 100 kb chunks, 40 planted consensus runs",
+                           "f1": f1, "lmmu": mmu, "lmlambda": mlam, "max_length": maxl})
+        else:
+            buf, wins = _chunks(2_000_000, 2 * maxl, rng, cons, 40, 0.508)
+            config.update({"model": f"synthetic p7 profile M={M} (peak 0.6)",
+                           "windows": f"{len(wins)} windows of {2 * maxl} residues (2 Mb, both strands)"})
+        cells_step = int((wins["j0"] - wins["i0"] + 1).sum()) * M
+    else:
+        cmw = WORKLOADS["batched-uneven-max"]
+        cm_s = synth.synth_cm(synth.structure(cmw["clen"], cmw["paired"], cmw["nbif"], cmw["sseed"]), cmw["pseed"],
+                              name="bench")
+        cfg = model.configure(cm_s, local=True)
+        frames, tasks, off = [], [], 0
+        nenv = 2000
+        for q in range(nenv):
+            h = synth.emit(cm_s, rng)
+            n = cfg.W + 40
+            seq = synth.random_dsq(n, 0.45, rng)
+            p = int(rng.integers(10, max(11, n - len(h) - 10)))
+            seq[p - 1:p - 1 + len(h)] = h[: n - p + 1]
+            f = np.concatenate([[255], seq, [255]]).astype(np.uint8)
+            i0, j0 = 5, 5 + cfg.W - 1
+            im, ix, jm, jx = synth.hb_band_rects(cm_s.st, p, i0, j0, 20, rng)
+            tasks.append((off, i0, j0, 0.0, 0.0, hb.ij2d_bands(cfg.sttype, im, ix, jm, jx)))
+            frames.append(f)
+            off += len(f)
+        buf = np.concatenate(frames)
+        cells_step = sum(int(np.maximum(t[5].hdmax - t[5].hdmin + 1, 0).sum()) for t in tasks)
+        config.update({"model": f"synthetic CM clen={cfg.clen} M={cfg.M} W={cfg.W} (local)",
+                       "envelopes": f"{nenv} envelopes of W residues, one sampled homolog each, CP9-shaped bands "
+                                    "(per-state i/j rectangles of +-20 around the homolog's consensus coordinates)",
+                       "band_cells_per_step": cells_step})
+    import torch
+    torch.cuda.set_device(local_rank)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device="cuda")
+    pinned = torch.from_numpy(buf).pin_memory()  # e2e copies come from pinned host memory
+    buf = pinned.numpy()
+    if kind == "f1-ssv":
+        f = p7.MsvFilter(prof, maxl, mmu, mlam, device=local_rank)
+        call = lambda: f.f1_windows_batch(buf, wins, f1, maxl)
+        stats = f.stats
+        h2d = buf.nbytes + len(wins) * 16
+    elif kind == "f2-vit":
+        f = p7.VitFilter(prof, device=local_rank)
+        call = lambda: f.score_batch(buf, wins)
+        stats = lambda: p7.vit_stats(f)
+        h2d = buf.nbytes + len(wins) * 24
+    else:
+        from infernox_b200.scan import Scanner
+        sc = Scanner(cfg, device=local_rank)
+        sr = 0 if kind == "hb-cyk" else 2
+        call = lambda: hb.hb_scan_batch(sc, sr, True, True, buf, tasks)
+        stats = lambda: hb.hb_stats(sc)
+        h2d = buf.nbytes + sum(t[5].hdmin.nbytes + t[5].hdmax.nbytes + 3 * t[5].jmin.nbytes for t in tasks)
+    for _ in range(args.warmup):
+        ref = call()
+    clocks = ClockSampler(local_rank)
+    torch.cuda.synchronize()
+    clocks.start()
+    times, kms, launches = [], [], 0
+    for _ in range(args.steps):
+        flush.fill_(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = call()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+        ms, _, nl = stats()
+        kms.append(ms)
+        launches += nl
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    if not _same(out, ref):
+        raise RuntimeError("results differ between steps")
+    kernel_ms = sum(kms) / len(kms)
+    value = cells_step / (kernel_ms / 1e3) / 1e9
+    e2e = cells_step / (statistics.mean(times) / 1e3) / 1e9
+    sm_mhz = clk["sm_mhz"] or 1965.0
+    nsm = torch.cuda.get_device_properties(local_rank).multi_processor_count
+    peak = nsm * 128 * sm_mhz * 1e6 / 1e9
+    achieved = FILTER_OPS_PER_CELL[kind] * cells_step / (kernel_ms / 1e3) / 1e9
+    # CPU: the oracle on all host cores over a bounded sample of the same inputs
+    import oracle
+    oracle.lib()
+    cores = os.cpu_count() or 1
+    if kind == "f1-ssv":
+        units = [(int(o), int(j)) for o, _, j in wins]
+        one = lambda u: oracle.f1_msv_windows(M, prof.mat, prof.trans, maxl, mmu, mlam, buf, [u[0]], [u[1]], f1,
+                                              maxl) and u[1] * M
+    elif kind == "f2-vit":
+        units = [(int(o), int(j)) for o, _, j in wins]
+        one = lambda u: oracle.vit_score_batch(M, prof.mat, prof.trans, buf, [u[0]], [u[1]]) and u[1] * M
+    else:
+        units = list(range(len(tasks)))
+
+        def one(q):
+            o, i0, j0, ec, cut, b = tasks[q]
+            oracle.hb_scan(cfg, kind == "hb-inside", (b.jmin, b.jmax, b.hd_off, b.hdmin, b.hdmax),
+                           buf[o:o + j0 + 2], i0, j0, ec, True, cut, True)
+            return int(np.maximum(b.hdmax - b.hdmin + 1, 0).sum())
+    order = [units[int(k)] for k in np.random.default_rng(7).permutation(len(units))]
+    lock = threading.Lock()
+    st = {"next": 0, "cells": 0}
+    deadline = time.perf_counter() + args.cpu_seconds
+
+    def worker():
+        while time.perf_counter() < deadline:
+            with lock:
+                if st["next"] >= len(order):
+                    return
+                u = order[st["next"]]
+                st["next"] += 1
+            c = one(u)
+            with lock:
+                st["cells"] += c
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(cores) as ex:
+        for _ in range(cores):
+            ex.submit(worker)
+    dt = time.perf_counter() - t0
+    cb = {"value": st["cells"] / dt / 1e9, "unit": "Gcells/s", "cores": cores, "kind": "port",
+          "sample": f"{st['next']} of {len(units)} units of one step's inputs, {dt:.1f} s on {cores} threads"}
+    metric = {"f1-ssv": "F1 SSV window scan Gcells/s", "f2-vit": "F2 Viterbi filter Gcells/s",
+              "hb-cyk": "HMM-banded CYK Gcells/s", "hb-inside": "HMM-banded Inside Gcells/s"}[kind]
+    line = {"metric": metric, "value": value, "unit": "Gcells/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": statistics.mean(times), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": {"f1-ssv": "u8 (packed s16x2)", "f2-vit": "i16", "hb-cyk": "f32", "hb-inside": "f32"}[kind],
+            "data": "synthetic", "config": config,
+            "e2e": {"value": e2e, "unit": "Gcells/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": None},
+            "gpu_launches": launches,
+            "roofline": {"bound": "issue", "achieved": achieved, "peak": peak, "unit": "Gop/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "note": f"{FILTER_OPS_PER_CELL[kind]:.0f} lane-ops per cell; {nsm} SMs x 128 lanes x "
+                                 f"{sm_mhz:.0f} MHz"},
+            "cpu_baseline": cb, "clocks": clk}
+    if rank == 0:
+        print(json.dumps(line))
 
 
 if __name__ == "__main__":

@@ -333,6 +333,10 @@ int cmgpu_vit_score_batch(const cmgpu_vit_filter *f, void *stream, const uint8_t
                           int64_t dsq_len, const cmgpu_window *wins, int32_t nwin, float *scores,
                           uint8_t *scored);
 
+/* Device time, cells (residues x M) and launches of the last
+ * cmgpu_vit_score_batch call on this filter. */
+int cmgpu_vit_filter_stats(const cmgpu_vit_filter *f, double *kernel_ms, int64_t *cells, int32_t *launches);
+
 /* ---- P7 MSV / SSV filter (F1) ------------------------------------------ */
 typedef struct cmgpu_msv_filter cmgpu_msv_filter;
 

@@ -160,6 +160,7 @@ def lib() -> C.CDLL:
     L.cmgpu_vit_filter_free.restype = None
     L.cmgpu_vit_filter_tables.argtypes = [vp, vp, C.c_int32, P(C.c_int32), vp]
     L.cmgpu_vit_score_batch.argtypes = [vp, vp, vp, C.c_int64, vp, C.c_int32, vp, vp]
+    L.cmgpu_vit_filter_stats.argtypes = [vp, P(C.c_double), P(C.c_int64), P(C.c_int32)]
     L.cmgpu_msv_filter_build.argtypes = [vp, C.c_int32, C.c_double, C.c_double, C.c_int, P(vp)]
     L.cmgpu_msv_filter_free.argtypes = [vp]
     L.cmgpu_msv_filter_free.restype = None
@@ -198,7 +199,7 @@ EXPORTED = [
     "cmgpu_qdb_scan", "cmgpu_qdb_scan_noalloc", "cmgpu_qdb_scan_cells", "cmgpu_cyk_seq_filter", "cmgpu_final_stage_inside_opt",
     "cmgpu_scan_batch", "cmgpu_scan_batch_device", "cmgpu_scan_plain", "cmgpu_count_work",
     "cmgpu_vit_filter_build", "cmgpu_vit_filter_free", "cmgpu_vit_filter_tables", "cmgpu_vit_score_batch",
-    "cmgpu_msv_filter_build", "cmgpu_msv_filter_free", "cmgpu_msv_filter_tables", "cmgpu_ssv_threshold",
+    "cmgpu_vit_filter_stats", "cmgpu_msv_filter_build", "cmgpu_msv_filter_free", "cmgpu_msv_filter_tables", "cmgpu_ssv_threshold",
     "cmgpu_msv_score_batch", "cmgpu_f1_msv_windows", "cmgpu_ssv_diagonals", "cmgpu_msv_filter_stats",
     "cmgpu_fast_cyk_scan_hb", "cmgpu_hb_scan_hits", "cmgpu_hb_scan_batch", "cmgpu_hb_stats",
 ]

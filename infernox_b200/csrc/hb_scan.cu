@@ -32,8 +32,10 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
+#include "devbuf.h"
 #include "model_internal.h"
 
 namespace cmx {
@@ -46,10 +48,16 @@ struct HbDev {
     double last_ms = 0;
     int64_t last_cells = 0;
     int32_t last_launches = 0;
+    DevArena arena;          // per-call device buffers (tables, matrix, results), reused
+    PinnedBuf st_pin, row_pin;  // per-call host band tables, staged in pinned memory
+    int64_t cand_hint = 0;   // reportable cells the last call needed
 };
 
 void hb_free(HbDev *h) {
     if (!h) return;
+    h->arena.release();
+    h->st_pin.release();
+    h->row_pin.release();
     cudaFree(h->sttype);
     cudaFree(h->cfirst);
     cudaFree(h->cnum);
@@ -69,14 +77,15 @@ namespace hb {
 struct Env {
     int64_t alpha_off;  // first cell of this envelope's matrix
     int64_t dsq_off;    // buffer index of residue 0
+    int64_t row_off;    // first Row of this envelope
     int32_t i0, j0;
     float env_cutoff, cutoff;
     int32_t st_off;     // first State of this envelope
-    int32_t cand_cap;
+    int32_t pad;
 };
 
 struct State {
-    int32_t jmin, jmax, row0, ntask;
+    int32_t jmin, jmax, row0, ntask;  // row0: first Row of state v within its envelope
     int32_t ilo, hmn_min, hmx_max, pad;  // IR: first diagonal, band extremes
 };
 
@@ -222,17 +231,18 @@ __device__ void ir_diag(const Tables &t, const State *st, const Row *rows, float
 }
 
 template <bool INS>
-__global__ void __launch_bounds__(256, 2) hb_kernel(Tables t, const Env *__restrict__ envs, int nenv,
-                                                 const State *__restrict__ states, const Row *__restrict__ rows,
+__global__ void __launch_bounds__(128, 4) hb_kernel(Tables t, const Env *__restrict__ envs, int nenv,
+                                                 const State *__restrict__ states, const Row *__restrict__ rows_all,
                                                  float *alpha_all, const uint8_t *__restrict__ dsq_all, int report,
                                                  Cand *cands, int64_t cand_cap, unsigned long long *ncand, Out *out) {
-    __shared__ float s_v[256];
-    __shared__ int s_j[256];
+    __shared__ float s_v[128];
+    __shared__ int s_j[128];
     __shared__ int s_envi, s_envj, s_nc;
     const int tid = threadIdx.x, nt = blockDim.x;
     for (int e = blockIdx.x; e < nenv; e += gridDim.x) {
         const Env env = envs[e];
         const State *st = states + env.st_off;
+        const Row *rows = rows_all + env.row_off;
         float *alpha = alpha_all + env.alpha_off;
         const uint8_t *dsq = dsq_all + env.dsq_off;
         for (int lev = 0; lev < t.nlev; lev++) {
@@ -393,40 +403,44 @@ int hb_prepare(cmgpu_model *m, HbDev **out) {
 
 int sdelta_h(int st) { return st == MP_ST ? 2 : (st == ML_ST || st == MR_ST || st == IL_ST || st == IR_ST) ? 1 : 0; }
 
-// validates one envelope's bands and appends its State / Row tables;
-// returns the envelope's cell count or -1 (error set)
-int64_t add_envelope(const HostCM &c, const cmgpu_hb_task &tk, int64_t dsq_len, const uint8_t *dsq_all,
-                     std::vector<hb::State> &states, std::vector<hb::Row> &rows) {
+// rows of one envelope's bands (the sum of its states' j-ranges)
+int64_t count_rows(int M, const cmgpu_hb_bands &b) {
+    int64_t n = 0;
+    for (int v = 0; v < M; v++) n += b.jmax[v] >= b.jmin[v] ? (int64_t)b.jmax[v] - b.jmin[v] + 1 : 0;
+    return n;
+}
+
+// Validates one envelope's bands and fills its M States and its Rows (row
+// indices and cell offsets relative to the envelope); returns the envelope's
+// cell count, or -1 with err set.
+int64_t fill_envelope(const HostCM &c, const cmgpu_hb_task &tk, int64_t dsq_len, const uint8_t *dsq_all,
+                      hb::State *states, hb::Row *rows, std::string &err) {
     const int M = c.view.M;
     const cmgpu_hb_bands &b = tk.bands;
-    if (!b.jmin || !b.jmax || !b.hd_off || !b.hdmin || !b.hdmax) {
-        set_error("HMM-banded scan: missing band arrays");
-        return -1;
-    }
     if (tk.i0 < 1 || tk.j0 < tk.i0 - 1 || tk.dsq_offset < 0 || tk.dsq_offset + (int64_t)tk.j0 + 1 > dsq_len) {
-        set_error("HMM-banded scan: envelope outside the residue buffer");
+        err = "HMM-banded scan: envelope outside the residue buffer";
         return -1;
     }
-    for (int32_t x = tk.i0; x <= tk.j0; x++)
-        if (dsq_all[tk.dsq_offset + x] > 17) {
-            set_error("HMM-banded scan: residue code > 17");
-            return -1;
-        }
+    if (tk.j0 >= tk.i0 && any_code_above_17(dsq_all + tk.dsq_offset + tk.i0, (int64_t)tk.j0 - tk.i0 + 1)) {
+        err = "HMM-banded scan: residue code > 17";
+        return -1;
+    }
     int64_t ncells = 0;
+    int32_t nrow = 0;
     for (int v = 0; v < M; v++) {
         const int st = c.sttype[v], sd = sdelta_h(st);
-        hb::State s{b.jmin[v], b.jmax[v], (int32_t)rows.size(), 0, 0, INT_MAX, INT_MIN, 0};
+        hb::State s{b.jmin[v], b.jmax[v], nrow, 0, 0, INT_MAX, INT_MIN, 0};
         const int nj = b.jmax[v] >= b.jmin[v] ? b.jmax[v] - b.jmin[v] + 1 : 0;
+        const int32_t *hmn_v = b.hdmin + b.hd_off[v], *hmx_v = b.hdmax + b.hd_off[v];
         int ilo = INT_MAX, ihi = INT_MIN;
         for (int jp = 0; jp < nj; jp++) {
-            const int j = b.jmin[v] + jp;
-            const int hmn = b.hdmin[b.hd_off[v] + jp], hmx = b.hdmax[b.hd_off[v] + jp];
+            const int j = b.jmin[v] + jp, hmn = hmn_v[jp], hmx = hmx_v[jp];
             if (hmx >= hmn) {
                 // every cell inside the envelope; emitting states need d >= 1
                 // so that the residue(s) they emit lie inside it
                 if (hmn < (sd > 0 ? 1 : 0) || j > tk.j0 || j - hmx + 1 < tk.i0) {
-                    set_error("HMM-banded scan: band cell outside the envelope (state " + std::to_string(v) +
-                              ", j " + std::to_string(j) + ")");
+                    err = "HMM-banded scan: band cell outside the envelope (state " + std::to_string(v) + ", j " +
+                          std::to_string(j) + ")";
                     return -1;
                 }
                 ilo = std::min(ilo, j - hmx + 1);
@@ -434,15 +448,15 @@ int64_t add_envelope(const HostCM &c, const cmgpu_hb_task &tk, int64_t dsq_len, 
                 s.hmn_min = std::min(s.hmn_min, hmn);
                 s.hmx_max = std::max(s.hmx_max, hmx);
             } else if (st == E_ST) {
-                set_error("HMM-banded scan: empty END state row");
+                err = "HMM-banded scan: empty END state row";
                 return -1;
             }
-            rows.push_back(hb::Row{(int32_t)ncells, hmn, hmx, 0});
+            rows[nrow++] = hb::Row{(int32_t)ncells, hmn, hmx, 0};
             if (hmx >= hmn) ncells += hmx - hmn + 1;
-            if (ncells > INT32_MAX) {
-                set_error("HMM-banded scan: more than 2^31 band cells in one envelope");
-                return -1;
-            }
+        }
+        if (ncells > INT32_MAX) {
+            err = "HMM-banded scan: more than 2^31 band cells in one envelope";
+            return -1;
         }
         if (st == IR_ST) {
             s.ilo = ilo;
@@ -450,10 +464,7 @@ int64_t add_envelope(const HostCM &c, const cmgpu_hb_task &tk, int64_t dsq_len, 
         } else {
             s.ntask = nj;
         }
-        states.push_back(s);
-    }
-    if (b.jmax[0] < b.jmin[0]) {
-        // no ROOT rows: nothing to report; keep the tables consistent
+        states[v] = s;
     }
     return ncells;
 }
@@ -514,43 +525,23 @@ void hb_report(const cmgpu_model *m, const hb::Cand *c, size_t n, const uint8_t 
         }                                                                                       \
     } while (0)
 
-struct DevBufs {
-    std::vector<void *> p;
-    ~DevBufs() {
-        for (void *q : p) cudaFree(q);
-    }
-    template <class T>
-    bool get(T **out, size_t bytes) {
-        void *q = nullptr;
-        if (cudaMalloc(&q, std::max<size_t>(bytes, 16)) != cudaSuccess) return false;
-        p.push_back(q);
-        *out = (T *)q;
-        return true;
-    }
-};
-
-// one launch over envelopes [e0, e1) (their tables already built)
+// one launch over envelopes [e0, e1), whose State and Row tables are staged
+// in pinned memory (states: M per envelope; rows from row_base[e])
 int hb_launch(cmgpu_model *m, HbDev *h, cudaStream_t st, int semiring, int report, int do_null3,
               const uint8_t *dsq_all, int64_t dsq_len, const cmgpu_hb_task *tasks, int32_t e0, int32_t e1,
-              const std::vector<hb::State> &states, const std::vector<hb::Row> &rows,
-              const std::vector<int64_t> &alpha_off, const std::vector<int32_t> &st_off,
-              const std::vector<int64_t> &row_base, cmgpu_hb_result *results, std::vector<cmgpu_hit> &hits,
+              const hb::State *st_pin, const hb::Row *row_pin, const std::vector<int64_t> &row_base,
+              const std::vector<int64_t> &alpha_off, cmgpu_hb_result *results, std::vector<cmgpu_hit> &hits,
               double &ms_total, int &launches) {
     const int n = e1 - e0;
     const int M = m->cm.view.M;
-    // rows of these envelopes are contiguous from row_base[e0]
-    const int64_t r0 = row_base[e0], r1 = row_base[e1];
-    const int64_t s0 = (int64_t)st_off[e0], s1 = (int64_t)e1 * M;
-    std::vector<hb::State> lst(states.begin() + s0, states.begin() + s1);
-    for (auto &s : lst) s.row0 -= (int32_t)r0;
+    const int64_t r0 = row_base[e0], nrows = row_base[e1] - r0;
+    const int64_t cells = alpha_off[e1] - alpha_off[e0];
     std::vector<hb::Env> envs(n);
-    int64_t cells = alpha_off[e1] - alpha_off[e0];
     for (int e = 0; e < n; e++) {
         const cmgpu_hb_task &tk = tasks[e0 + e];
-        envs[e] = hb::Env{alpha_off[e0 + e] - alpha_off[e0], tk.dsq_offset, tk.i0, tk.j0, tk.env_cutoff, tk.cutoff,
-                          (int32_t)(st_off[e0 + e] - s0), 0};
+        envs[e] = hb::Env{alpha_off[e0 + e] - alpha_off[e0], tk.dsq_offset, row_base[e0 + e] - r0, tk.i0, tk.j0,
+                          tk.env_cutoff, tk.cutoff, e * M, 0};
     }
-    DevBufs bufs;
     hb::Env *d_env;
     hb::State *d_st;
     hb::Row *d_rows;
@@ -558,28 +549,29 @@ int hb_launch(cmgpu_model *m, HbDev *h, cudaStream_t st, int semiring, int repor
     uint8_t *d_dsq;
     hb::Out *d_out;
     unsigned long long *d_nc;
-    if (!bufs.get(&d_env, sizeof(hb::Env) * n) || !bufs.get(&d_st, sizeof(hb::State) * lst.size()) ||
-        !bufs.get(&d_rows, sizeof(hb::Row) * (size_t)(r1 - r0)) || !bufs.get(&d_alpha, sizeof(float) * (size_t)cells) ||
-        !bufs.get(&d_dsq, (size_t)dsq_len) || !bufs.get(&d_out, sizeof(hb::Out) * n) ||
-        !bufs.get(&d_nc, sizeof(unsigned long long))) {
+    DevArena &ar = h->arena;
+    if (ar.get(0, &d_env, sizeof(hb::Env) * n) || ar.get(1, &d_st, sizeof(hb::State) * (size_t)n * M) ||
+        ar.get(2, &d_rows, sizeof(hb::Row) * (size_t)nrows) || ar.get(3, &d_alpha, sizeof(float) * (size_t)cells) ||
+        ar.get(4, &d_dsq, (size_t)dsq_len) || ar.get(5, &d_out, sizeof(hb::Out) * n) ||
+        ar.get(6, &d_nc, sizeof(unsigned long long))) {
         set_error("HMM-banded scan: device allocation failed");
         return CMGPU_ENOMEM;
     }
     HB_TRY(cudaMemcpyAsync(d_env, envs.data(), sizeof(hb::Env) * n, cudaMemcpyHostToDevice, st));
-    HB_TRY(cudaMemcpyAsync(d_st, lst.data(), sizeof(hb::State) * lst.size(), cudaMemcpyHostToDevice, st));
-    HB_TRY(cudaMemcpyAsync(d_rows, rows.data() + r0, sizeof(hb::Row) * (size_t)(r1 - r0), cudaMemcpyHostToDevice, st));
+    HB_TRY(cudaMemcpyAsync(d_st, st_pin + (size_t)e0 * M, sizeof(hb::State) * (size_t)n * M, cudaMemcpyHostToDevice,
+                           st));
+    HB_TRY(cudaMemcpyAsync(d_rows, row_pin + r0, sizeof(hb::Row) * (size_t)nrows, cudaMemcpyHostToDevice, st));
     HB_TRY(cudaMemcpyAsync(d_dsq, dsq_all, (size_t)dsq_len, cudaMemcpyHostToDevice, st));
     hb::Tables t{h->sttype, h->cfirst, h->cnum, h->lev_start, h->lev_states, h->begins, h->tsc, h->oesc,
                  h->endsc, h->beginsc, h->flog, m->cm.view.el_selfsc, h->nlev, h->nbeg,
                  (int)((m->cm.view.flags >> 10) & 1u)};
-    int64_t cap = report ? 4096 + 4 * (int64_t)n : 0;
+    int64_t cap = report ? std::max<int64_t>(4096 + 16 * (int64_t)n, h->cand_hint) : 0;
     cudaEvent_t ev0, ev1;
     HB_TRY(cudaEventCreate(&ev0));
     HB_TRY(cudaEventCreate(&ev1));
     for (int attempt = 0; attempt < 2; attempt++) {
-        DevBufs cb;
         hb::Cand *d_c = nullptr;
-        if (!cb.get(&d_c, sizeof(hb::Cand) * (size_t)std::max<int64_t>(cap, 1))) {
+        if (ar.get(7, &d_c, sizeof(hb::Cand) * (size_t)std::max<int64_t>(cap, 1))) {
             cudaEventDestroy(ev0);
             cudaEventDestroy(ev1);
             set_error("HMM-banded scan: device allocation failed");
@@ -588,10 +580,10 @@ int hb_launch(cmgpu_model *m, HbDev *h, cudaStream_t st, int semiring, int repor
         HB_TRY(cudaMemsetAsync(d_nc, 0, sizeof(unsigned long long), st));
         HB_TRY(cudaEventRecord(ev0, st));
         if (semiring == CMGPU_INSIDE_F32)
-            hb::hb_kernel<true><<<n, 256, 0, st>>>(t, d_env, n, d_st, d_rows, d_alpha, d_dsq, report, d_c, cap, d_nc,
+            hb::hb_kernel<true><<<n, 128, 0, st>>>(t, d_env, n, d_st, d_rows, d_alpha, d_dsq, report, d_c, cap, d_nc,
                                                    d_out);
         else
-            hb::hb_kernel<false><<<n, 256, 0, st>>>(t, d_env, n, d_st, d_rows, d_alpha, d_dsq, report, d_c, cap, d_nc,
+            hb::hb_kernel<false><<<n, 128, 0, st>>>(t, d_env, n, d_st, d_rows, d_alpha, d_dsq, report, d_c, cap, d_nc,
                                                     d_out);
         HB_TRY(cudaGetLastError());
         HB_TRY(cudaEventRecord(ev1, st));
@@ -605,7 +597,8 @@ int hb_launch(cmgpu_model *m, HbDev *h, cudaStream_t st, int semiring, int repor
         ms_total += ms;
         launches++;
         if ((int64_t)nc > cap) {
-            cap = (int64_t)nc;
+            cap = (int64_t)nc + (int64_t)nc / 4;
+            h->cand_hint = cap;
             continue;
         }
         std::vector<hb::Cand> hc((size_t)nc);
@@ -648,23 +641,50 @@ int hb_batch(const cmgpu_model *mc, cudaStream_t st, int semiring, int report, i
         set_error("HMM-banded scan: semiring must be CMGPU_CYK_F32 or CMGPU_INSIDE_F32");
         return CMGPU_EINVAL;
     }
+    for (int32_t e = 0; e < ntask; e++) {
+        const cmgpu_hb_bands &b = tasks[e].bands;
+        if (!b.jmin || !b.jmax || !b.hd_off || !b.hdmin || !b.hdmax) {
+            set_error("HMM-banded scan: missing band arrays");
+            return CMGPU_EINVAL;
+        }
+    }
     HbDev *h = nullptr;
     int rc = hb_prepare(m, &h);
     if (rc) return rc;
     HB_TRY(cudaSetDevice(m->device));
-    std::vector<hb::State> states;
-    std::vector<hb::Row> rows;
-    std::vector<int64_t> alpha_off(ntask + 1, 0), row_base(ntask + 1, 0);
-    std::vector<int32_t> st_off(ntask + 1, 0);
-    for (int32_t e = 0; e < ntask; e++) {
-        st_off[e] = (int32_t)states.size();
-        row_base[e] = (int64_t)rows.size();
-        const int64_t nc = add_envelope(m->cm, tasks[e], dsq_len, dsq_all, states, rows);
-        if (nc < 0) return CMGPU_EINVAL;
-        alpha_off[e + 1] = alpha_off[e] + nc;
+    const int M = m->cm.view.M;
+    // band tables: count, then fill in parallel straight into pinned staging
+    std::vector<int64_t> row_base(ntask + 1, 0), alpha_off(ntask + 1, 0), ncells(ntask, 0);
+    for (int32_t e = 0; e < ntask; e++) row_base[e + 1] = row_base[e] + count_rows(M, tasks[e].bands);
+    hb::State *st_pin = h->st_pin.get<hb::State>((size_t)ntask * M);
+    hb::Row *row_pin = h->row_pin.get<hb::Row>((size_t)std::max<int64_t>(row_base[ntask], 1));
+    if (!st_pin || !row_pin) {
+        set_error("HMM-banded scan: pinned host allocation failed");
+        return CMGPU_ENOMEM;
     }
-    st_off[ntask] = (int32_t)states.size();
-    row_base[ntask] = (int64_t)rows.size();
+    std::vector<std::string> errs(ntask);
+    const int nthr = (int)std::max<int64_t>(1, std::min<int64_t>({(int64_t)std::thread::hardware_concurrency(), 32,
+                                                                   (int64_t)ntask / 16 + 1}));
+    auto work = [&](int32_t a, int32_t b) {
+        for (int32_t e = a; e < b; e++)
+            ncells[e] = fill_envelope(m->cm, tasks[e], dsq_len, dsq_all, st_pin + (size_t)e * M,
+                                      row_pin + row_base[e], errs[e]);
+    };
+    if (nthr == 1) {
+        work(0, ntask);
+    } else {
+        std::vector<std::thread> pool;
+        for (int k = 0; k < nthr; k++)
+            pool.emplace_back(work, (int32_t)((int64_t)ntask * k / nthr), (int32_t)((int64_t)ntask * (k + 1) / nthr));
+        for (auto &t : pool) t.join();
+    }
+    for (int32_t e = 0; e < ntask; e++) {
+        if (ncells[e] < 0) {
+            set_error(errs[e]);
+            return CMGPU_EINVAL;
+        }
+        alpha_off[e + 1] = alpha_off[e] + ncells[e];
+    }
     h->last_ms = 0;
     h->last_cells = 0;
     h->last_launches = 0;
@@ -676,8 +696,8 @@ int hb_batch(const cmgpu_model *mc, cudaStream_t st, int semiring, int report, i
     while (e0 < ntask) {
         int32_t e1 = e0 + 1;
         while (e1 < ntask && alpha_off[e1 + 1] - alpha_off[e0] <= budget) e1++;
-        rc = hb_launch(m, h, st, semiring, report, do_null3, dsq_all, dsq_len, tasks, e0, e1, states, rows, alpha_off,
-                       st_off, row_base, results, hits, ms, launches);
+        rc = hb_launch(m, h, st, semiring, report, do_null3, dsq_all, dsq_len, tasks, e0, e1, st_pin, row_pin,
+                       row_base, alpha_off, results, hits, ms, launches);
         if (rc) return rc;
         e0 = e1;
     }

@@ -43,6 +43,7 @@
 #include <vector>
 
 #include "../../include/cmscan_gpu.h"
+#include "devbuf.h"
 
 namespace cmx {
 void set_error(const std::string &msg);
@@ -166,7 +167,10 @@ struct cmgpu_msv_filter {
     mutable double last_ms = 0;
     mutable int64_t last_cells = 0;
     mutable int32_t last_launches = 0;
+    mutable cmx::DevArena arena;  // per-call buffers, reused
+    mutable int cap_hint = 64;    // candidate slots per segment the last scan needed
     ~cmgpu_msv_filter() {
+        arena.release();
         cudaFree(d_negc);
         cudaFree(d_rbv);
     }
@@ -457,25 +461,9 @@ namespace {
         }                                                                                       \
     } while (0)
 
-// device buffers of one call, freed on every return path
-struct Bufs {
-    std::vector<void *> p;
-    ~Bufs() {
-        for (void *q : p) cudaFree(q);
-    }
-    template <class T>
-    cudaError_t get(T **out, size_t bytes) {
-        void *q = nullptr;
-        cudaError_t e = cudaMalloc(&q, std::max<size_t>(bytes, 16));
-        if (e == cudaSuccess) p.push_back(q);
-        *out = (T *)q;
-        return e;
-    }
-};
-
-#define MSV_ALLOC(ptr, bytes)                                                                   \
+#define MSV_ALLOC(slot, ptr, bytes)                                                             \
     do {                                                                                        \
-        cudaError_t e_ = bufs.get(&(ptr), (bytes));                                             \
+        cudaError_t e_ = f->arena.get((slot), &(ptr), (bytes));                                 \
         if (e_ != cudaSuccess) {                                                                \
             set_error(std::string("msv: device allocation: ") + cudaGetErrorString(e_));        \
             return CMGPU_ENOMEM;                                                                \
@@ -489,11 +477,10 @@ int check_windows(const char *who, const uint8_t *dsq_all, int64_t dsq_len, cons
             set_error(std::string(who) + ": window outside the residue buffer");
             return CMGPU_EINVAL;
         }
-        for (int32_t x = w.i0; x <= w.j0; x++)
-            if (dsq_all[w.dsq_offset + x] > 17) {
-                set_error(std::string(who) + ": residue code > 17");
-                return CMGPU_EINVAL;
-            }
+        if (w.j0 >= w.i0 && any_code_above_17(dsq_all + w.dsq_offset + w.i0, (int64_t)w.j0 - w.i0 + 1)) {
+            set_error(std::string(who) + ": residue code > 17");
+            return CMGPU_EINVAL;
+        }
     }
     return CMGPU_OK;
 }
@@ -616,33 +603,31 @@ int ssv_run(const cmgpu_msv_filter *f, cudaStream_t st, const uint8_t *dsq_all, 
     }
     const int nseg = (int)segs.size();
     if (nseg == 0) return CMGPU_OK;
-    Bufs bufs;
     uint8_t *d_dsq;
     dev::SsvSeg *d_segs;
     dev::SsvChunk *d_ch;
     int *d_counts, *d_nraw, *d_need;
-    MSV_ALLOC(d_dsq, (size_t)dsq_len);
-    MSV_ALLOC(d_segs, sizeof(dev::SsvSeg) * nseg);
-    MSV_ALLOC(d_ch, sizeof(dev::SsvChunk) * nch);
-    MSV_ALLOC(d_counts, sizeof(int) * nseg);
-    MSV_ALLOC(d_nraw, sizeof(int) * nch);
-    MSV_ALLOC(d_need, sizeof(int));
+    MSV_ALLOC(0, d_dsq, (size_t)dsq_len);
+    MSV_ALLOC(1, d_segs, sizeof(dev::SsvSeg) * nseg);
+    MSV_ALLOC(2, d_ch, sizeof(dev::SsvChunk) * nch);
+    MSV_ALLOC(3, d_counts, sizeof(int) * nseg);
+    MSV_ALLOC(4, d_nraw, sizeof(int) * nch);
+    MSV_ALLOC(5, d_need, sizeof(int));
     MSV_TRY(cudaMemcpyAsync(d_dsq, dsq_all, (size_t)dsq_len, cudaMemcpyHostToDevice, st));
     MSV_TRY(cudaMemcpyAsync(d_segs, segs.data(), sizeof(dev::SsvSeg) * nseg, cudaMemcpyHostToDevice, st));
     MSV_TRY(cudaMemcpyAsync(d_ch, ch.data(), sizeof(dev::SsvChunk) * nch, cudaMemcpyHostToDevice, st));
     cudaEvent_t e0, e1;
     MSV_TRY(cudaEventCreate(&e0));
     MSV_TRY(cudaEventCreate(&e1));
-    int cap = 32;
+    int cap = f->cap_hint;
     double ms_total = 0;
     int launches = 0;
     for (int attempt = 0; attempt < 2; attempt++) {
-        Bufs cb;
         dev::SsvCand *d_cands;
         dev::SsvRaw *d_raws;
         cudaError_t e;
-        if ((e = cb.get(&d_cands, sizeof(dev::SsvCand) * (size_t)nseg * cap)) != cudaSuccess ||
-            (e = cb.get(&d_raws, sizeof(dev::SsvRaw) * (size_t)nseg * cap)) != cudaSuccess) {
+        if ((e = f->arena.get(6, &d_cands, sizeof(dev::SsvCand) * (size_t)nseg * cap)) != cudaSuccess ||
+            (e = f->arena.get(7, &d_raws, sizeof(dev::SsvRaw) * (size_t)nseg * cap)) != cudaSuccess) {
             cudaEventDestroy(e0);
             cudaEventDestroy(e1);
             set_error(std::string("msv: device allocation: ") + cudaGetErrorString(e));
@@ -666,7 +651,8 @@ int ssv_run(const cmgpu_msv_filter *f, cudaStream_t st, const uint8_t *dsq_all, 
         ms_total += ms;
         launches += 2;
         if (need > cap) {
-            cap = need;
+            cap = need + need / 4;
+            f->cap_hint = cap;
             continue;
         }
         std::vector<dev::SsvRaw> hr((size_t)nseg * cap);
@@ -785,13 +771,12 @@ extern "C" int cmgpu_msv_score_batch(const cmgpu_msv_filter *f, void *stream_ptr
     }
     cudaStream_t st = (cudaStream_t)stream_ptr;
     MSV_TRY(cudaSetDevice(f->device));
-    Bufs bufs;
     uint8_t *d_dsq;
     dev::MsvWin *d_w;
     int *d_out;
-    MSV_ALLOC(d_dsq, (size_t)dsq_len);
-    MSV_ALLOC(d_w, sizeof(dev::MsvWin) * nwin);
-    MSV_ALLOC(d_out, sizeof(int) * nwin);
+    MSV_ALLOC(0, d_dsq, (size_t)dsq_len);
+    MSV_ALLOC(8, d_w, sizeof(dev::MsvWin) * nwin);
+    MSV_ALLOC(9, d_out, sizeof(int) * nwin);
     MSV_TRY(cudaMemcpyAsync(d_dsq, dsq_all, (size_t)dsq_len, cudaMemcpyHostToDevice, st));
     MSV_TRY(cudaMemcpyAsync(d_w, vw.data(), sizeof(dev::MsvWin) * nwin, cudaMemcpyHostToDevice, st));
     cudaEvent_t e0, e1;

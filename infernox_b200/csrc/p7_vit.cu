@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "../../include/cmscan_gpu.h"
+#include "devbuf.h"
 
 namespace cmx {
 void set_error(const std::string &msg);
@@ -120,7 +121,13 @@ struct cmgpu_vit_filter {
     int device = 0;
     VitHost host;
     int16_t *d_tab = nullptr;
-    ~cmgpu_vit_filter() { cudaFree(d_tab); }
+    double last_ms = 0;
+    int64_t last_cells = 0;
+    cmx::DevArena arena;  // per-call buffers, reused
+    ~cmgpu_vit_filter() {
+        arena.release();
+        cudaFree(d_tab);
+    }
 };
 
 namespace cmx {
@@ -309,11 +316,10 @@ extern "C" int cmgpu_vit_score_batch(const cmgpu_vit_filter *f, void *stream_ptr
             set_error("cmgpu_vit_score_batch: window outside the residue buffer");
             return CMGPU_EINVAL;
         }
-        for (int32_t x = w.i0; x <= w.j0; x++)
-            if (dsq_all[w.dsq_offset + x] > 17) {
-                set_error("cmgpu_vit_score_batch: residue code > 17");
-                return CMGPU_EINVAL;
-            }
+        if (w.j0 >= w.i0 && cmx::any_code_above_17(dsq_all + w.dsq_offset + w.i0, (int64_t)w.j0 - w.i0 + 1)) {
+            set_error("cmgpu_vit_score_batch: residue code > 17");
+            return CMGPU_EINVAL;
+        }
         vw[k].off = w.dsq_offset;
         vw[k].i0 = w.i0;
         vw[k].j0 = w.j0;
@@ -326,17 +332,13 @@ extern "C" int cmgpu_vit_score_batch(const cmgpu_vit_filter *f, void *stream_ptr
     dev::VitWin *d_w = nullptr;
     int *d_out = nullptr;
     uint8_t *d_st = nullptr;
-    auto cleanup = [&]() {
-        cudaFree(d_dsq);
-        cudaFree(d_w);
-        cudaFree(d_out);
-        cudaFree(d_st);
-    };
+    cmgpu_vit_filter *mf = const_cast<cmgpu_vit_filter *>(f);
+    auto cleanup = [&]() {};
     cudaError_t e = cudaSuccess;
-    if ((e = cudaMalloc((void **)&d_dsq, (size_t)dsq_len)) != cudaSuccess ||
-        (e = cudaMalloc((void **)&d_w, sizeof(dev::VitWin) * nwin)) != cudaSuccess ||
-        (e = cudaMalloc((void **)&d_out, sizeof(int) * nwin)) != cudaSuccess ||
-        (e = cudaMalloc((void **)&d_st, (size_t)nwin)) != cudaSuccess) {
+    if ((e = mf->arena.get(0, &d_dsq, (size_t)dsq_len)) != cudaSuccess ||
+        (e = mf->arena.get(1, &d_w, sizeof(dev::VitWin) * nwin)) != cudaSuccess ||
+        (e = mf->arena.get(2, &d_out, sizeof(int) * nwin)) != cudaSuccess ||
+        (e = mf->arena.get(3, &d_st, (size_t)nwin)) != cudaSuccess) {
         cleanup();
         set_error(std::string("cmgpu_vit_score_batch: ") + cudaGetErrorString(e));
         return CMGPU_ENOMEM;
@@ -369,17 +371,33 @@ extern "C" int cmgpu_vit_score_batch(const cmgpu_vit_filter *f, void *stream_ptr
         set_error(std::string("cmgpu_vit_score_batch: ") + cudaGetErrorString(e));
         return CMGPU_EDEVICE;
     }
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEventCreate(&ev0);
+    cudaEventCreate(&ev1);
+    cudaEventRecord(ev0, st);
     dev::vit_kernel<<<grid, warps * 32, smem, st>>>(f->d_tab, M, f->host.base_w, f->host.e_move, f->host.e_loop,
                                                   d_dsq, d_w, nwin, d_out, d_st);
+    cudaEventRecord(ev1, st);
     if ((e = cudaGetLastError()) != cudaSuccess ||
         (e = cudaMemcpyAsync(out.data(), d_out, sizeof(int) * nwin, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
         (e = cudaMemcpyAsync(stv.data(), d_st, (size_t)nwin, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
         (e = cudaStreamSynchronize(st)) != cudaSuccess) {
         cleanup();
+        cudaEventDestroy(ev0);
+        cudaEventDestroy(ev1);
         set_error(std::string("cmgpu_vit_score_batch: ") + cudaGetErrorString(e));
         return CMGPU_EDEVICE;
     }
     cleanup();
+    {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ev0, ev1);
+        cudaEventDestroy(ev0);
+        cudaEventDestroy(ev1);
+        mf->last_ms = ms;
+        mf->last_cells = 0;
+        for (int32_t k = 0; k < nwin; k++) mf->last_cells += (int64_t)(wins[k].j0 - wins[k].i0 + 1) * M;
+    }
     // C->T (src/p7_vitfilter.rs:376-384), in f32 as the reference
     for (int32_t k = 0; k < nwin; k++) {
         scored[k] = stv[k];
@@ -396,5 +414,14 @@ extern "C" int cmgpu_vit_score_batch(const cmgpu_vit_filter *f, void *stream_ptr
             scores[k] = -INFINITY;
         }
     }
+    return CMGPU_OK;
+}
+
+extern "C" int cmgpu_vit_filter_stats(const cmgpu_vit_filter *f, double *kernel_ms, int64_t *cells,
+                                      int32_t *launches) {
+    if (!f) return CMGPU_EINVAL;
+    if (kernel_ms) *kernel_ms = f->last_ms;
+    if (cells) *cells = f->last_cells;
+    if (launches) *launches = f->last_ms > 0 ? 1 : 0;
     return CMGPU_OK;
 }

@@ -52,6 +52,34 @@ class Bands:
         return N.HbBands(*[ip(a) for a in self._keep])
 
 
+_E_ST = 7
+
+
+def _sdelta(st: int) -> int:
+    return 2 if st == 1 else (1 if st in (2, 3, 4, 5) else 0)
+
+
+def ij2d_bands(sttype, imin, imax, jmin, jmax) -> Bands:
+    """ij2d_bands (src/cp9.rs:3815-3850, non-truncated): per-state i/j bands
+    to d-bands.  END rows are 0..0; other rows hdmin = max(j - imax + 1, sd),
+    hdmax = j - imin + 1, empty (-1/-2) when hdmax < sd."""
+    mins, maxs = [], []
+    for v, st in enumerate(np.asarray(sttype)):
+        st = int(st)
+        n = max(0, int(jmax[v]) - int(jmin[v]) + 1)
+        j = np.arange(int(jmin[v]), int(jmin[v]) + n, dtype=np.int64)
+        if st == _E_ST:
+            mins.append(np.zeros(n, np.int32))
+            maxs.append(np.zeros(n, np.int32))
+            continue
+        dn = _sdelta(st)
+        hdn = j - int(imax[v]) + 1
+        hdx = j - int(imin[v]) + 1
+        mins.append(np.where(hdx < dn, -1, np.maximum(hdn, dn)).astype(np.int32))
+        maxs.append(np.where(hdx < dn, -2, hdx).astype(np.int32))
+    return Bands.from_rows(jmin, jmax, mins, maxs)
+
+
 def _hits(arr, n):
     return [(int(h["i"]), int(h["j"]), float(h["score"]), float(h["bias"])) for h in arr[:n]]
 
@@ -105,7 +133,7 @@ def hb_scan_batch(sc: Scanner, semiring: int, report_hits: bool, do_null3: bool,
     for q, (off, i0, j0, ec, cut, bands) in enumerate(tasks):
         tk[q] = N.HbTask(off, i0, j0, ec, cut, bands.struct())
     res = (N.HbResult * len(tasks))()
-    cap = 1024
+    cap = 1024 + 16 * len(tasks)
     while True:
         out = np.zeros(cap, N.HIT_DTYPE)
         n = C.c_int64()

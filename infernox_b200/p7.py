@@ -68,6 +68,13 @@ class VitFilter:
         return sc, ok
 
 
+def vit_stats(f: VitFilter):
+    """(kernel ms, cells, launches) of the last score_batch call."""
+    ms, cells, launches = C.c_double(), C.c_int64(), C.c_int32()
+    N.check(N.lib().cmgpu_vit_filter_stats(f._h, C.byref(ms), C.byref(cells), C.byref(launches)))
+    return ms.value, cells.value, launches.value
+
+
 def vit_score(f: VitFilter, dsq, l: int):
     """src/p7_vitfilter.rs:292 -- Some(score) or None."""
     a = np.ascontiguousarray(dsq, np.uint8)
@@ -142,8 +149,7 @@ class MsvFilter:
                                               ok.ctypes.data))
         return sc, ok
 
-    def _grow(self, fn, dtype, *args):
-        cap = 256
+    def _grow(self, fn, dtype, *args, cap=256):
         while True:
             out = np.zeros(cap, dtype)
             n = C.c_int32()
@@ -159,13 +165,13 @@ class MsvFilter:
         b = np.ascontiguousarray(buf, np.uint8)
         c = np.ascontiguousarray(chunks, N.WINDOW_DTYPE)
         return self._grow(N.lib().cmgpu_f1_msv_windows, F1_WINDOW_DTYPE, self._h, None, b.ctypes.data, b.size,
-                          c.ctypes.data, len(c), float(f1), int(cmw))
+                          c.ctypes.data, len(c), float(f1), int(cmw), cap=4096 + b.size // 64)
 
     def ssv_diagonals_batch(self, buf: np.ndarray, chunks: np.ndarray, f1: float) -> np.ndarray:
         b = np.ascontiguousarray(buf, np.uint8)
         c = np.ascontiguousarray(chunks, N.WINDOW_DTYPE)
         return self._grow(N.lib().cmgpu_ssv_diagonals, SSV_DIAG_DTYPE, self._h, None, b.ctypes.data, b.size,
-                          c.ctypes.data, len(c), float(f1))
+                          c.ctypes.data, len(c), float(f1), cap=4096 + b.size // 64)
 
 
 def msv_score(f: MsvFilter, dsq, l: int):
@@ -184,3 +190,40 @@ def f1_msv_windows(f: MsvFilter, dsq, l: int, f1: float, cmw: int):
     """src/cm_pipeline.rs:842 -- [(start, end, score)] of one chunk frame."""
     w = f.f1_windows_batch(np.ascontiguousarray(dsq, np.uint8), np.array([(0, 1, l)], N.WINDOW_DTYPE), f1, cmw)
     return [(int(r["start"]), int(r["end"]), float(r["score"])) for r in w]
+
+
+def synthetic_profile(m: int, seed: int, peak: float = 0.6):
+    """A seeded p7 filter profile: one preferred residue per match state with
+    probability `peak`, insert/delete transitions of a few percent.  Returns
+    the profile and its consensus residues (index k = 1..M)."""
+    r = np.random.default_rng(seed)
+    mat = np.zeros((m + 1, 4), np.float32)
+    cons = r.integers(0, 4, m + 1)
+    for k in range(1, m + 1):
+        v = r.uniform(0.5, 1.5, 4)
+        v[cons[k]] = 0.0
+        v = v / v.sum() * (1.0 - peak)
+        v[cons[k]] = peak
+        mat[k] = v.astype(np.float32)
+    trans = np.zeros((m + 1, 7), np.float32)
+    for k in range(m + 1):
+        mi, md = r.uniform(0.01, 0.05, 2)
+        ii, dd = r.uniform(0.2, 0.5), r.uniform(0.2, 0.5)
+        trans[k] = [1 - mi - md, mi, md, 1 - ii, ii, 1 - dd, dd]
+    return P7Profile(m, mat, trans), cons
+
+
+def planted_residues(n: int, cons, nplant: int, seed: int, mut: float = 0.25, gc: float = 0.5) -> np.ndarray:
+    """n i.i.d. residue codes (0..3) with nplant mutated consensus runs."""
+    r = np.random.default_rng(seed)
+    p = np.array([(1 - gc) / 2, gc / 2, gc / 2, (1 - gc) / 2])
+    seq = r.choice(4, n, p=p).astype(np.uint8)
+    m = len(cons) - 1
+    for _ in range(nplant):
+        run = np.array(cons[1:], np.uint8)
+        flip = r.random(m) < mut
+        run[flip] = r.integers(0, 4, int(flip.sum()))
+        if m < n:
+            q = int(r.integers(0, n - m))
+            seq[q:q + m] = run
+    return seq

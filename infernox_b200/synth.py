@@ -547,3 +547,31 @@ def revcomp(dsq: np.ndarray) -> np.ndarray:
     m = r < 4
     r[m] = 3 - r[m]
     return r
+
+
+def hb_band_rects(st: CMStructure, p: int, i0: int, j0: int, slack: int, rng):
+    """Per-state (i, j) rectangles of HMM-band shape for a homolog whose
+    consensus column 1 sits at sequence position p: state v of node n spans
+    i near p + lpos(n) - 1 and j near p + rpos(n) - 1, widened by a seeded
+    0..slack on each side and clipped to the envelope [i0, j0]; END states
+    sit one residue left of their i (empty subsequences).  Returns imin,
+    imax, jmin, jmax, ready for hb.ij2d_bands."""
+    lpos, rpos = emit_map(st)
+    M = st.M
+    node = np.asarray(st.ndidx, np.int64)
+    ic = p + lpos[node] - 1
+    jc = p + rpos[node] - 1
+    emits_left = np.isin(np.asarray(st.sttype), (1, 2, 4))  # MP, ML, IL: i is their own column
+    ic = np.where(emits_left, ic, ic + 1)
+    jc = np.maximum(jc, ic - 1)
+    s = lambda: rng.integers(0, slack + 1, M)
+    imin = np.clip(ic - s(), i0, j0)
+    imax = np.clip(ic + s(), i0, j0)
+    jmin = np.clip(jc - s(), i0, j0)
+    jmax = np.clip(jc + s(), i0, j0)
+    is_end = np.asarray(st.sttype) == 7
+    jmin = np.where(is_end, np.clip(ic - 1 - slack, i0 - 1, j0), jmin)
+    jmax = np.where(is_end, np.clip(ic - 1 + slack, i0 - 1, j0), jmax)
+    imin = np.minimum(imin, imax)
+    jmax = np.maximum(jmax, jmin)
+    return imin.astype(np.int32), imax.astype(np.int32), jmin.astype(np.int32), jmax.astype(np.int32)
