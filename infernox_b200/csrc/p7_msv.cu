@@ -251,6 +251,28 @@ __device__ __forceinline__ int leftmost_k(const uint32_t (&w)[R], int lane, int 
     return warp_min(kk);
 }
 
+__device__ __forceinline__ int warp_incl_sum(int v, int lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(FULL, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+__device__ __forceinline__ int warp_incl_max(int v, int lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(FULL, v, o);
+        if (lane >= o) v = max(v, t);
+    }
+    return v;
+}
+// emission cost of residue code `code` at model position k (255 for codes
+// past the alphabet, as the reference's sentinel rule)
+__device__ __forceinline__ int cost_of(const uint8_t *rbv_s, int k, int code) {
+    return code < KP ? rbv_s[k * KP + code] : 255;
+}
+
 struct MsvWin {
     int64_t off;  // buffer index of local residue 1 minus 1
     int32_t l;
@@ -362,6 +384,9 @@ __global__ void __launch_bounds__(128) ssv_replay_kernel(const uint32_t *__restr
                                                          const SsvCand *__restrict__ cands,
                                                          const int *__restrict__ counts, SsvRaw *raws, int *nraw,
                                                          int *need) {
+    extern __shared__ uint8_t rbv_s[];  // emission costs [(M+1) * 18]
+    for (int q = threadIdx.x; q < (M + 1) * KP; q += blockDim.x) rbv_s[q] = rbv[q];
+    __syncthreads();
     const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const uint32_t bias2 = pack2(bias), xbb2 = pack2(xbb);
     for (int c = blockIdx.x * nw + (threadIdx.x >> 5); c < nchunk; c += gridDim.x * nw) {
@@ -404,38 +429,65 @@ __global__ void __launch_bounds__(128) ssv_replay_kernel(const uint32_t *__restr
                     ek = leftmost_k<R>(w, lane, xe);
                 }
                 // trigger at row r: recover the diagonal and extend it
-                // (src/cm_pipeline.rs:637-705)
-                int max_end = 0;
-                if (lane == 0) {
-                    auto cost = [&](int k, int code) -> int { return code < KP ? rbv[k * KP + code] : 255; };
+                // (src/cm_pipeline.rs:637-705), 32 steps at a time
+                int start, tstart, max_sc = xe, max_end = r;
+                {
+                    // backward: step s reads (ek - s, r - s) while rem > baseline
                     const int baseline = base - tjb - tbm;
-                    int start = ek, tstart = r, rem = xe;
-                    while (rem > baseline && start >= 1 && tstart >= 1) {
-                        rem -= bias - cost(start, frame[tstart]);
-                        start--;
-                        tstart--;
-                    }
-                    start++;
-                    tstart++;
-                    int sc2 = xe, max_sc = xe, since = 0, k = ek + 1, n = r + 1;
-                    max_end = r;
-                    while (k < M && n <= ch.l) {
-                        sc2 += bias - cost(k, frame[n]);
-                        if (sc2 >= max_sc) {
-                            max_sc = sc2;
-                            max_end = n;
-                            since = 0;
-                        } else if (++since == 5) {
+                    int taken = 0, rem = xe;
+                    for (;;) {
+                        const int kk = ek - taken - lane, tt = r - taken - lane;
+                        const bool valid = kk >= 1 && tt >= 1;
+                        const int delta = valid ? bias - cost_of(rbv_s, kk, frame[tt]) : 0;
+                        const int incl = warp_incl_sum(delta, lane);
+                        const bool cont = valid && rem - (incl - delta) > baseline;
+                        const unsigned stop = __ballot_sync(FULL, !cont);
+                        if (stop) {
+                            taken += __ffs(stop) - 1;
                             break;
                         }
-                        k++;
-                        n++;
+                        taken += 32;
+                        rem -= __shfl_sync(FULL, incl, 31);
                     }
+                    start = ek - taken + 1;
+                    tstart = r - taken + 1;
+                    // forward: running score, new maxima reset the miss count,
+                    // the fifth miss in a row (or the model / chunk end) stops
+                    int t0 = 0, base_sc = xe, runmax = xe, since = 0;
+                    for (;;) {
+                        const int k = ek + 1 + t0 + lane, n = r + 1 + t0 + lane;
+                        const bool valid = k < M && n <= ch.l;
+                        const int delta = valid ? bias - cost_of(rbv_s, k, frame[n]) : 0;
+                        const int sc = base_sc + warp_incl_sum(delta, lane);
+                        int pm = warp_incl_max(sc, lane);
+                        int before = __shfl_up_sync(FULL, pm, 1);
+                        before = lane == 0 ? runmax : max(runmax, before);
+                        const bool imp = valid && sc >= before;
+                        const unsigned impm = __ballot_sync(FULL, imp);
+                        const unsigned upto = lane == 31 ? 0xffffffffu : ((1u << (lane + 1)) - 1u);
+                        const unsigned mine = impm & upto;
+                        const int since_t = mine ? lane - (31 - __clz(mine)) : since + lane + 1;
+                        const bool halt = !valid || (!imp && since_t == 5);
+                        const unsigned hm = __ballot_sync(FULL, halt);
+                        const int q = hm ? __ffs(hm) - 1 : 32;          // first lane that ends the walk
+                        const unsigned before_q = q == 32 ? impm : (impm & ((1u << q) - 1u));
+                        if (before_q) {
+                            const int pl = 31 - __clz(before_q);      // last new maximum before the end
+                            max_sc = __shfl_sync(FULL, sc, pl);
+                            max_end = r + 1 + t0 + pl;
+                        }
+                        if (hm) break;
+                        since = impm ? 31 - (31 - __clz(impm)) : since + 32;
+                        runmax = max(runmax, __shfl_sync(FULL, pm, 31));
+                        base_sc = __shfl_sync(FULL, sc, 31);
+                        t0 += 32;
+                    }
+                }
+                if (lane == 0) {
                     const int end_model = ek + (max_end - r);
                     const float sc = (__fsub_rn((float)(max_sc - tjb), (float)base) / scale_b) - 3.0f;
                     out[nr] = SsvRaw{tstart, end_model - start + 1, end_model, sc};
                 }
-                max_end = __shfl_sync(FULL, max_end, 0);
                 nr++;
                 z = max_end + 1;
                 i = max_end + 1;
@@ -504,7 +556,9 @@ void launch_ssv(const cmgpu_msv_filter *f, cudaStream_t st, int xbb, int thr, co
     const MsvHost &h = f->host;
     dev::ssv_scan_kernel<R><<<(nseg + 7) / 8, 256, smem, st>>>(f->d_negc, h.bias_b, xbb, thr, d_dsq, d_segs, nseg, cap,
                                                               d_cands, d_counts);
-    dev::ssv_replay_kernel<R><<<(nch + 3) / 4, 128, 0, st>>>(f->d_negc, f->d_rbv, h.M, h.bias_b, xbb, thr, h.base_b,
+    const size_t rsm = (size_t)(h.M + 1) * KP;
+    cudaFuncSetAttribute(dev::ssv_replay_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsm);
+    dev::ssv_replay_kernel<R><<<(nch + 3) / 4, 128, rsm, st>>>(f->d_negc, f->d_rbv, h.M, h.bias_b, xbb, thr, h.base_b,
                                                             h.tjb_b, h.tbm_b, h.scale_b, d_dsq, d_ch, nch, cap, d_cands,
                                                             d_counts, d_raws, d_nraw, d_need);
 }
