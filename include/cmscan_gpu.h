@@ -302,6 +302,63 @@ int cmgpu_hb_scan_batch(const cmgpu_model *m, void *stream, int semiring, int re
                         const uint8_t *dsq_all, int64_t dsq_len, const cmgpu_hb_task *tasks,
                         int32_t ntask, cmgpu_hb_result *results, cmgpu_hit *hits, int64_t cap,
                         int64_t *n_out);
+/* ---- truncated HMM-banded scanners (tr_cyk_scan_hb / ftr_inside_scan_hb) --
+ * The per-pass inputs the reference's truncated scanner selects internally
+ * (src/cm_dpsearch_trunc.rs:264-300): marginal emissions (CM.lmesc/rmesc,
+ * src/cp9.rs:4441), the truncated-begin penalties of the pass and
+ * configuration (TrPenalties l/g[pty_idx_for_pass(pass)], IMPOSSIBLE where
+ * none), and the node span allow_truncation reads for each state (lpos of
+ * the state's node, +1 unless MATP/MATL; rpos, -1 unless MATP/MATR). */
+typedef struct cmgpu_tr_tables {
+    const float *lmesc, *rmesc;   /* [M*18] */
+    const float *pty;             /* [M] */
+    const int32_t *lpos, *rpos;   /* [M] */
+    int32_t clen;
+    int32_t local;                /* truncation rules of local configurations */
+} cmgpu_tr_tables;
+
+/* TrHit (src/cm_dpsearch_trunc.rs:131-139): mode 3 J, 2 L, 1 R, 0 T;
+ * root = the entry (truncated-begin) state. */
+typedef struct cmgpu_tr_hit {
+    int32_t i, j;
+    float score, bias;
+    int32_t mode, root;
+} cmgpu_tr_hit;
+
+/* One envelope of a batched truncated scan: as cmgpu_hb_task plus the
+ * per-state J/L/R/T validity of its bands (CP9Bands jvalid..tvalid). */
+typedef struct cmgpu_tr_task {
+    int64_t dsq_offset;
+    int32_t i0, j0;
+    float env_cutoff, cutoff;
+    cmgpu_hb_bands bands;
+    const uint8_t *jvalid, *lvalid, *rvalid, *tvalid;  /* [M] */
+} cmgpu_tr_task;
+
+typedef struct cmgpu_tr_result {
+    float vsc_root;
+    int32_t vmode;
+    int64_t envi, envj;
+    int64_t hit_first;
+    int32_t nhits, pad;
+} cmgpu_tr_result;
+
+/* tr_cyk_scan_hb (CMGPU_CYK_F32, src/cm_dpsearch_trunc.rs:264) and
+ * ftr_inside_scan_hb (CMGPU_INSIDE_F32, :1055) of residues i0..j0 of dsq
+ * in pass pass_idx (PLI_PASS_*: 2 5'-only, 3 3'-only, 4/5 5'-and-3'):
+ * vsc_root and its mode, the envelope (-1 when none) and the hits after
+ * overlap removal, as the reference returns them. */
+int cmgpu_tr_scan_hb(const cmgpu_model *m, int semiring, const cmgpu_tr_tables *tt, const cmgpu_hb_bands *bands,
+                     const uint8_t *jvalid, const uint8_t *lvalid, const uint8_t *rvalid, const uint8_t *tvalid,
+                     const uint8_t *dsq, int32_t n, int32_t i0, int32_t j0, float cutoff, int do_null3,
+                     int pass_idx, float env_cutoff, float *vsc_root, int32_t *vmode, int64_t *envi,
+                     int64_t *envj, cmgpu_tr_hit *hits, int32_t cap, int32_t *n_out);
+/* Many envelopes in one call, one CTA per envelope. */
+int cmgpu_tr_scan_hb_batch(const cmgpu_model *m, void *stream, int semiring, const cmgpu_tr_tables *tt,
+                           int pass_idx, int do_null3, const uint8_t *dsq_all, int64_t dsq_len,
+                           const cmgpu_tr_task *tasks, int32_t ntask, cmgpu_tr_result *results,
+                           cmgpu_tr_hit *hits, int64_t cap, int64_t *n_out);
+
 /* Device time and cells of the last HMM-banded call on this model. */
 int cmgpu_hb_stats(const cmgpu_model *m, double *kernel_ms, int64_t *cells, int32_t *launches);
 

@@ -89,6 +89,26 @@ class HbTask(C.Structure):
                 ("cutoff", C.c_float), ("bands", HbBands)]
 
 
+class TrTables(C.Structure):
+    _fields_ = [("lmesc", P(C.c_float)), ("rmesc", P(C.c_float)), ("pty", P(C.c_float)),
+                ("lpos", P(C.c_int32)), ("rpos", P(C.c_int32)), ("clen", C.c_int32), ("local", C.c_int32)]
+
+
+class TrTask(C.Structure):
+    _fields_ = [("dsq_offset", C.c_int64), ("i0", C.c_int32), ("j0", C.c_int32), ("env_cutoff", C.c_float),
+                ("cutoff", C.c_float), ("bands", HbBands), ("jvalid", P(C.c_uint8)), ("lvalid", P(C.c_uint8)),
+                ("rvalid", P(C.c_uint8)), ("tvalid", P(C.c_uint8))]
+
+
+class TrResult(C.Structure):
+    _fields_ = [("vsc_root", C.c_float), ("vmode", C.c_int32), ("envi", C.c_int64), ("envj", C.c_int64),
+                ("hit_first", C.c_int64), ("nhits", C.c_int32), ("pad", C.c_int32)]
+
+
+TR_HIT_DTYPE = np.dtype([("i", np.int32), ("j", np.int32), ("score", np.float32), ("bias", np.float32),
+                         ("mode", np.int32), ("root", np.int32)])
+
+
 class HbResult(C.Structure):
     _fields_ = [("vsc_root", C.c_float), ("nhits", C.c_int32), ("envi", C.c_int64), ("envj", C.c_int64),
                 ("hit_first", C.c_int64)]
@@ -179,6 +199,11 @@ def lib() -> C.CDLL:
                                      P(C.c_int32)]
     L.cmgpu_hb_scan_batch.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, vp, C.c_int64, vp, C.c_int32, vp, vp,
                                       C.c_int64, P(C.c_int64)]
+    L.cmgpu_tr_scan_hb.argtypes = [vp, C.c_int, P(TrTables), P(HbBands), vp, vp, vp, vp, vp, C.c_int32, C.c_int32,
+                                   C.c_int32, C.c_float, C.c_int, C.c_int, C.c_float, P(C.c_float), P(C.c_int32),
+                                   P(C.c_int64), P(C.c_int64), vp, C.c_int32, P(C.c_int32)]
+    L.cmgpu_tr_scan_hb_batch.argtypes = [vp, vp, C.c_int, P(TrTables), C.c_int, C.c_int, vp, C.c_int64, vp,
+                                         C.c_int32, vp, vp, C.c_int64, P(C.c_int64)]
     L.cmgpu_hb_stats.argtypes = [vp, P(C.c_double), P(C.c_int64), P(C.c_int32)]
     L.cmgpu_count_work.argtypes = [P(Cm), C.c_int, C.c_int, C.c_int32, P(C.c_double),
                                    P(C.c_double)]
@@ -202,4 +227,5 @@ EXPORTED = [
     "cmgpu_vit_filter_stats", "cmgpu_msv_filter_build", "cmgpu_msv_filter_free", "cmgpu_msv_filter_tables", "cmgpu_ssv_threshold",
     "cmgpu_msv_score_batch", "cmgpu_f1_msv_windows", "cmgpu_ssv_diagonals", "cmgpu_msv_filter_stats",
     "cmgpu_fast_cyk_scan_hb", "cmgpu_hb_scan_hits", "cmgpu_hb_scan_batch", "cmgpu_hb_stats",
+    "cmgpu_tr_scan_hb", "cmgpu_tr_scan_hb_batch",
 ]

@@ -9,9 +9,17 @@ Mirrors the reference's functions over `&CM` and `&CP9Bands`
     fast_finside_scan_hb(cm, cp9b, dsq, i0, j0, env_cutoff, cutoff, do_null3)
         -> (vsc_root, envi, envj, hits)                                                 :5465
 
+and the truncated scanners (src/cm_dpsearch_trunc.rs):
+
+    tr_cyk_scan_hb(cm, trp, cp9b, dsq, i0, j0, cutoff, do_null3, pass_idx, env_cutoff, local)
+        -> (hits, vsc_root, vmode_root, envi, envj)                                     :264
+    ftr_inside_scan_hb(...) (same)                                                      :1055
+
 `Bands` holds what the scanners read from CP9Bands: jmin/jmax per state and
-the per-row d-bands hdmin/hdmax.  `hb_scan_batch` scans many envelopes, each
-with its own bands, in one call.
+the per-row d-bands hdmin/hdmax (and, for the truncated scans, the per-state
+J/L/R/T validity).  `TrInputs` holds what the truncated scanners select from
+the CM and TrPenalties for one pass.  The batch functions scan many
+envelopes, each with its own bands, in one call.
 """
 from __future__ import annotations
 
@@ -151,3 +159,98 @@ def hb_stats(sc: Scanner):
     ms, cells, launches = C.c_double(), C.c_int64(), C.c_int32()
     N.check(N.lib().cmgpu_hb_stats(sc._model, C.byref(ms), C.byref(cells), C.byref(launches)))
     return ms.value, cells.value, launches.value
+
+
+@dataclass
+class TrInputs:
+    """Per-pass inputs of the truncated scanners: lmesc/rmesc [M*18], the
+    pass's truncated-begin penalties pty [M], the node spans lpos/rpos [M]
+    that allow_truncation reads, clen, and whether local rules apply."""
+    lmesc: np.ndarray
+    rmesc: np.ndarray
+    pty: np.ndarray
+    lpos: np.ndarray
+    rpos: np.ndarray
+    clen: int
+    local: bool
+
+    def struct(self) -> N.TrTables:
+        self._keep = [np.ascontiguousarray(self.lmesc, np.float32), np.ascontiguousarray(self.rmesc, np.float32),
+                      np.ascontiguousarray(self.pty, np.float32), np.ascontiguousarray(self.lpos, np.int32),
+                      np.ascontiguousarray(self.rpos, np.int32)]
+        fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))
+        k = self._keep
+        return N.TrTables(fp(k[0]), fp(k[1]), fp(k[2]), ip(k[3]), ip(k[4]), int(self.clen), int(bool(self.local)))
+
+
+def _tr_hits(arr, n):
+    return [(int(h["i"]), int(h["j"]), float(h["score"]), float(h["bias"]), int(h["mode"]), int(h["root"]))
+            for h in arr[:n]]
+
+
+def _u8p(a):
+    return a.ctypes.data_as(C.POINTER(C.c_uint8))
+
+
+def _tr_scan(sc, semiring, tri: TrInputs, bands: Bands, valid, dsq, i0, j0, cutoff, do_null3, pass_idx, env_cutoff):
+    a = _frame(dsq)
+    b = bands.struct()
+    tt = tri.struct()
+    vs = [np.ascontiguousarray(x, np.uint8) for x in valid]
+    vsc, vmode, ei, ej = C.c_float(), C.c_int32(), C.c_int64(), C.c_int64()
+    cap = 256
+    while True:
+        out = np.zeros(cap, N.TR_HIT_DTYPE)
+        n = C.c_int32()
+        rc = N.lib().cmgpu_tr_scan_hb(sc._model, semiring, C.byref(tt), C.byref(b), *[v.ctypes.data for v in vs],
+                                      a.ctypes.data, a.size - 2, i0, j0, float(cutoff), int(bool(do_null3)),
+                                      int(pass_idx), float(env_cutoff), C.byref(vsc), C.byref(vmode), C.byref(ei),
+                                      C.byref(ej), out.ctypes.data, cap, C.byref(n))
+        if rc == N.CMGPU_EOVERFLOW and n.value > cap:
+            cap = n.value
+            continue
+        N.check(rc)
+        return _tr_hits(out, n.value), vsc.value, vmode.value, ei.value, ej.value
+
+
+def tr_cyk_scan_hb(cm, tri: TrInputs, bands: Bands, valid, dsq, i0: int, j0: int, cutoff: float, do_null3: bool,
+                   pass_idx: int, env_cutoff: float):
+    """src/cm_dpsearch_trunc.rs:264 -- (hits (i, j, score, bias, mode, root), vsc_root, vmode, envi, envj);
+    valid = (jvalid, lvalid, rvalid, tvalid) per state."""
+    sc = cm if isinstance(cm, Scanner) else _scanner(cm)
+    return _tr_scan(sc, N.CYK_F32, tri, bands, valid, dsq, i0, j0, cutoff, do_null3, pass_idx, env_cutoff)
+
+
+def ftr_inside_scan_hb(cm, tri: TrInputs, bands: Bands, valid, dsq, i0: int, j0: int, cutoff: float,
+                       do_null3: bool, pass_idx: int, env_cutoff: float):
+    """src/cm_dpsearch_trunc.rs:1055 -- the float Inside sibling of tr_cyk_scan_hb."""
+    sc = cm if isinstance(cm, Scanner) else _scanner(cm)
+    return _tr_scan(sc, N.INSIDE_F32, tri, bands, valid, dsq, i0, j0, cutoff, do_null3, pass_idx, env_cutoff)
+
+
+def tr_scan_hb_batch(sc: Scanner, semiring: int, tri: TrInputs, pass_idx: int, do_null3: bool, buf: np.ndarray,
+                     tasks):
+    """tasks: [(dsq_offset, i0, j0, env_cutoff, cutoff, Bands, (jvalid, lvalid, rvalid, tvalid))]
+    -> [(hits, vsc, vmode, envi, envj)] per task."""
+    b = np.ascontiguousarray(buf, np.uint8)
+    tk = (N.TrTask * len(tasks))()
+    keep = []
+    for q, (off, i0, j0, ec, cut, bands, valid) in enumerate(tasks):
+        vs = [np.ascontiguousarray(x, np.uint8) for x in valid]
+        keep.append(vs)
+        tk[q] = N.TrTask(off, i0, j0, ec, cut, bands.struct(), *[_u8p(v) for v in vs])
+    tt = tri.struct()
+    res = (N.TrResult * len(tasks))()
+    cap = 1024 + 16 * len(tasks)
+    while True:
+        out = np.zeros(cap, N.TR_HIT_DTYPE)
+        n = C.c_int64()
+        rc = N.lib().cmgpu_tr_scan_hb_batch(sc._model, None, semiring, C.byref(tt), int(pass_idx),
+                                            int(bool(do_null3)), b.ctypes.data, b.size, tk, len(tasks), res,
+                                            out.ctypes.data, cap, C.byref(n))
+        if rc == N.CMGPU_EOVERFLOW and n.value > cap:
+            cap = n.value
+            continue
+        N.check(rc)
+        return [(_tr_hits(out[r.hit_first:], r.nhits), r.vsc_root, r.vmode, r.envi, r.envj) for r in res]

@@ -1,5 +1,5 @@
 """TEST INFRASTRUCTURE ONLY: ctypes binding of the oracle (qdb_oracle.c,
-hb_oracle.c, p7_oracle.c, msv_oracle.c).
+hb_oracle.c, tr_oracle.c, p7_oracle.c, msv_oracle.c).
 
 Used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as
 the checker of the GPU scanner.  The product package never imports it.
@@ -30,7 +30,7 @@ def build() -> str:
 def lib():
     global _lib
     if _lib is None:
-        srcs = [os.path.join(HERE, f) for f in ("qdb_oracle.c", "hb_oracle.c", "p7_oracle.c", "msv_oracle.c")]
+        srcs = [os.path.join(HERE, f) for f in ("qdb_oracle.c", "hb_oracle.c", "tr_oracle.c", "p7_oracle.c", "msv_oracle.c")]
         if not os.path.exists(LIB_PATH) or any(os.path.getmtime(LIB_PATH) < os.path.getmtime(f) for f in srcs):
             build()
         L = C.CDLL(LIB_PATH)
@@ -56,6 +56,9 @@ def lib():
         L.oracle_hb_scan.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp, vp, C.c_int32, C.c_int32, C.c_float,
                                      C.c_int, C.c_float, C.c_int, P(C.c_float), P(C.c_int64), P(C.c_int64), vp,
                                      C.c_int32]
+        L.oracle_tr_hb_scan.argtypes = [vp, C.c_int] + [vp] * 5 + [C.c_int32] + [vp] * 4 + [vp] * 5 + [
+            vp, C.c_int32, C.c_int32, C.c_float, C.c_int, C.c_int, C.c_float, C.c_int, P(C.c_float), P(C.c_int32),
+            P(C.c_int64), P(C.c_int64), vp, C.c_int32]
         L.oracle_ilogsum_table.argtypes = [P(C.c_int32), C.c_int]
         L.oracle_ilogsum.argtypes = [C.c_int32, C.c_int32]
         L.oracle_ilogsum.restype = C.c_int32
@@ -237,4 +240,36 @@ def hb_scan(cm, inside, bands, dsq, i0, j0, env_cutoff, report, cutoff, do_null3
         if n <= cap:
             out = [(int(h["i"]), int(h["j"]), float(h["score"]), float(h["bias"])) for h in hits[:n]]
             return vsc.value, ei.value, ej.value, out
+        cap = n
+
+
+TR_HIT_DTYPE = np.dtype([("i", np.int32), ("j", np.int32), ("score", np.float32), ("bias", np.float32),
+                         ("mode", np.int32), ("root", np.int32)])
+
+
+def tr_hb_scan(cm, inside, tt, valid, bands, dsq, i0, j0, cutoff, do_null3, pass_idx, env_cutoff, local):
+    """tr_cyk_scan_hb / ftr_inside_scan_hb restated: (hits, vsc_root, vmode, envi, envj).
+    tt: dict lmesc [M*18], rmesc, pty [M], lpos, rpos [M], clen; valid: (j, l, r, t) uint8 [M];
+    bands: (jmin, jmax, hd_off, hdmin, hdmax)."""
+    a, _ = _u8(dsq)
+    f32 = lambda x: np.ascontiguousarray(x, np.float32)
+    i32 = lambda x: np.ascontiguousarray(x, np.int32)
+    lm, rm, pty = f32(tt["lmesc"]), f32(tt["rmesc"]), f32(tt["pty"])
+    lp, rp = i32(tt["lpos"]), i32(tt["rpos"])
+    vs = [np.ascontiguousarray(x, np.uint8) for x in valid]
+    bs = [i32(x) for x in bands]
+    vsc, vmode, ei, ej = C.c_float(), C.c_int32(), C.c_int64(), C.c_int64()
+    cap = 256
+    while True:
+        hits = np.zeros(cap, TR_HIT_DTYPE)
+        n = lib().oracle_tr_hb_scan(C.byref(cm.as_struct()), int(bool(inside)), lm.ctypes.data, rm.ctypes.data,
+                                    pty.ctypes.data, lp.ctypes.data, rp.ctypes.data, int(tt["clen"]),
+                                    *[v.ctypes.data for v in vs], *[b.ctypes.data for b in bs], a.ctypes.data,
+                                    i0, j0, float(cutoff), int(bool(do_null3)), int(pass_idx), float(env_cutoff),
+                                    int(bool(local)), C.byref(vsc), C.byref(vmode), C.byref(ei), C.byref(ej),
+                                    hits.ctypes.data, cap)
+        if n <= cap:
+            out = [(int(h["i"]), int(h["j"]), float(h["score"]), float(h["bias"]), int(h["mode"]), int(h["root"]))
+                   for h in hits[:n]]
+            return out, vsc.value, vmode.value, ei.value, ej.value
         cap = n
