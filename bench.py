@@ -5,7 +5,8 @@ chunks), and the filter/banded stages of the default pipeline --
 "f1-ssv" (SSV windows over 100 kb chunks, both strands, of a 4.6 Mb
 sequence, F1 = 0.35), "f2-vit" (Viterbi filter over F1-sized windows),
 "hb-cyk" / "hb-inside" (HMM-banded CYK / float Inside over envelopes with
-CP9-shaped bands) -- each with the oracle timed on the host cores beside it.
+CP9-shaped bands), "hb-trcyk" (truncated HMM-banded CYK, 5'-and-3' pass, all
+four planes) -- each with the oracle timed on the host cores beside it.
 
 Workload (default "batched-uneven-max"): the batched uneven-window Inside scan
 of the --max path.  One 120-consensus-column CM with 3 bifurcations (seeded
@@ -47,7 +48,7 @@ WORKLOADS = {
     "nohmm-cyk-filter": dict(clen=72, paired=None, nbif=2, sseed=0, pseed=11, semiring=0, band=1,
                              median=100000, sigma=0.0, lo=100000, hi=100000, gc=0.50),
 }
-FILTER_WORKLOADS = ("f1-ssv", "f2-vit", "hb-cyk", "hb-inside")
+FILTER_WORKLOADS = ("f1-ssv", "f2-vit", "hb-cyk", "hb-inside", "hb-trcyk")
 OPS_PER_TERM = {0: 2.0, 1: 7.0}   # CYK: FADD + select; Inside: 6 INT + 1 LDS
 OPS_PER_CELL = 2.0                # emission add + store
 CUTOFF_BITS = 15.0                # stands in for the E-value threshold
@@ -385,8 +386,9 @@ def main():
 # SSV: max(dp, xB), +bias (saturating), -cost (floored), row max;
 # Viterbi: M 4 adds + 3 max + emission, I 2 adds + max, D 2 adds + max;
 # HB: per child relaxation 2 (CYK) or 9 (FLogsum), about 3 children per
-# cell, plus emission add and clamp.
-FILTER_OPS_PER_CELL = {"f1-ssv": 4.0, "f2-vit": 14.0, "hb-cyk": 8.0, "hb-inside": 29.0}
+# cell, plus emission add and clamp; truncated CYK: the same over the J, L
+# and R planes (T only at bifurcations).
+FILTER_OPS_PER_CELL = {"f1-ssv": 4.0, "f2-vit": 14.0, "hb-cyk": 8.0, "hb-inside": 29.0, "hb-trcyk": 24.0}
 
 
 def _chunks(total, chunk, rng, cons, nplant, gc):
@@ -480,6 +482,18 @@ def filter_main(args):
         call = lambda: f.score_batch(buf, wins)
         stats = lambda: p7.vit_stats(f)
         h2d = buf.nbytes + len(wins) * 24
+    elif kind == "hb-trcyk":
+        from infernox_b200.scan import Scanner
+        sc = Scanner(cfg, device=local_rank)
+        tri = hb.synthetic_tr_inputs(cm_s, cfg, True)
+        ones = np.ones(cfg.M, np.uint8)
+        valid = (ones, ones, ones, ones)
+        ttasks = [t + (valid,) for t in tasks]
+        config.update({"pass": "5'-and-3' (PLI_PASS_5P_AND_3P_FORCE), J/L/R/T planes", "planes": 4})
+        call = lambda: hb.tr_scan_hb_batch(sc, 0, tri, 4, True, buf, ttasks)
+        stats = lambda: hb.hb_stats(sc)
+        h2d = buf.nbytes + sum(t[5].hdmin.nbytes + t[5].hdmax.nbytes + 3 * t[5].jmin.nbytes + 4 * cfg.M
+                               for t in tasks)
     else:
         from infernox_b200.scan import Scanner
         sc = Scanner(cfg, device=local_rank)
@@ -526,6 +540,16 @@ def filter_main(args):
     elif kind == "f2-vit":
         units = [(int(o), int(j)) for o, _, j in wins]
         one = lambda u: oracle.vit_score_batch(M, prof.mat, prof.trans, buf, [u[0]], [u[1]]) and u[1] * M
+    elif kind == "hb-trcyk":
+        units = list(range(len(tasks)))
+        ttab = {"lmesc": tri.lmesc, "rmesc": tri.rmesc, "pty": tri.pty, "lpos": tri.lpos, "rpos": tri.rpos,
+                "clen": tri.clen}
+
+        def one(q):
+            o, i0, j0, ec, cut, b = tasks[q]
+            oracle.tr_hb_scan(cfg, False, ttab, valid, (b.jmin, b.jmax, b.hd_off, b.hdmin, b.hdmax),
+                              buf[o:o + j0 + 2], i0, j0, cut, True, 4, ec, True)
+            return int(np.maximum(b.hdmax - b.hdmin + 1, 0).sum())
     else:
         units = list(range(len(tasks)))
 
@@ -557,11 +581,13 @@ def filter_main(args):
     cb = {"value": st["cells"] / dt / 1e9, "unit": "Gcells/s", "cores": cores, "kind": "port",
           "sample": f"{st['next']} of {len(units)} units of one step's inputs, {dt:.1f} s on {cores} threads"}
     metric = {"f1-ssv": "F1 SSV window scan Gcells/s", "f2-vit": "F2 Viterbi filter Gcells/s",
-              "hb-cyk": "HMM-banded CYK Gcells/s", "hb-inside": "HMM-banded Inside Gcells/s"}[kind]
+              "hb-cyk": "HMM-banded CYK Gcells/s", "hb-inside": "HMM-banded Inside Gcells/s",
+              "hb-trcyk": "truncated HMM-banded CYK Gcells/s (band cells, 4 planes each)"}[kind]
     line = {"metric": metric, "value": value, "unit": "Gcells/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": statistics.mean(times), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": {"f1-ssv": "u8 (packed s16x2)", "f2-vit": "i16", "hb-cyk": "f32", "hb-inside": "f32"}[kind],
+            "dtype": {"f1-ssv": "u8 (packed s16x2)", "f2-vit": "i16", "hb-cyk": "f32", "hb-inside": "f32",
+                      "hb-trcyk": "f32"}[kind],
             "data": "synthetic", "config": config,
             "e2e": {"value": e2e, "unit": "Gcells/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": None},
             "gpu_launches": launches,

@@ -254,3 +254,55 @@ def tr_scan_hb_batch(sc: Scanner, semiring: int, tri: TrInputs, pass_idx: int, d
             continue
         N.check(rc)
         return [(_tr_hits(out[r.hit_first:], r.nhits), r.vsc_root, r.vmode, r.envi, r.envj) for r in res]
+
+
+# canonical residues (bit a = residue a) of each RNA code 0..17
+_DEGEN_BITS = [0x1, 0x2, 0x4, 0x8, 0x0, 0x5, 0xA, 0x3, 0xC, 0x6, 0x9, 0xB, 0xE, 0x7, 0xD, 0xF, 0x0, 0x0]
+
+
+def synthetic_tr_inputs(cm_s, cfg, local: bool) -> TrInputs:
+    """Truncated-scan inputs for a synthetic CM (synth.SynthCM + its
+    configuration): marginal emissions laid out as fill_marginal_emissions
+    lays them out (src/cp9.rs:4441 -- MP rows the log-odds of the summed
+    left/right pair marginals, degenerate codes the mean over their residues;
+    ML/IL their own emissions on the left and 0 on the right, MR/IR the
+    reverse; gap / non-residue / missing codes IMPOSSIBLE), the node spans
+    allow_truncation reads, and a stand-in for the pass's truncation
+    penalties: log2(2 / (clen (clen + 1))) on the states the reference
+    penalises (MATP_MP, MATL_ML, MATR_MR, BIF_B and insert states), which is
+    the global 5'-and-3' penalty with every such state weighted equally."""
+    from . import synth
+    st = cm_s.st
+    M = cfg.M
+    imp = np.float32(-1e36)
+    lm = np.zeros((M, 18), np.float32)
+    rm = np.zeros((M, 18), np.float32)
+    for v in range(M):
+        lm[v, [4, 16, 17]] = imp
+        rm[v, [4, 16, 17]] = imp
+        t = int(cfg.sttype[v])
+        if t == 1:
+            e = np.asarray(cm_s.e[v][:16], np.float64).reshape(4, 4)
+            for x in range(4):
+                lm[v, x] = np.float32(np.log2(e[x].sum() / float(cfg.null[x])))
+                rm[v, x] = np.float32(np.log2(e[:, x].sum() / float(cfg.null[x])))
+            for code in range(5, 16):
+                bset = [b for b in range(4) if _DEGEN_BITS[code] >> b & 1]
+                lm[v, code] = np.float32(np.mean([lm[v, b] for b in bset]))
+                rm[v, code] = np.float32(np.mean([rm[v, b] for b in bset]))
+        elif t in (2, 4):
+            lm[v] = cfg.oesc[v, :18]
+        elif t in (3, 5):
+            rm[v] = cfg.oesc[v, :18]
+    lpos_n, rpos_n = synth.emit_map(st)
+    nd = np.asarray(st.ndidx)
+    ndt = np.asarray(st.ndtype)[nd]
+    lpos = np.where(np.isin(ndt, (synth.MATP_ND, synth.MATL_ND)), lpos_n[nd], lpos_n[nd] + 1).astype(np.int32)
+    rpos = np.where(np.isin(ndt, (synth.MATP_ND, synth.MATR_ND)), rpos_n[nd], rpos_n[nd] - 1).astype(np.int32)
+    clen = int(cfg.clen)
+    pen = np.float32(np.log2(2.0 / (clen * (clen + 1))))
+    qual = np.isin(np.asarray(cfg.stid), (synth.MATP_MP, synth.MATL_ML, synth.MATR_MR, synth.BIF_B)) | \
+        np.isin(np.asarray(cfg.sttype), (4, 5))
+    pty = np.where(qual, pen, imp).astype(np.float32)
+    pty[0] = imp
+    return TrInputs(lm.ravel(), rm.ravel(), pty, lpos, rpos, clen, bool(local))

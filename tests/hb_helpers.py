@@ -149,61 +149,11 @@ def ragged_bands(cm, i0, j0, seed, trim=4):
 
 
 # ---- truncated-scan inputs ----------------------------------------------
-MATP_ND, MATL_ND, MATR_ND, BIF_ND, END_ND = 1, 2, 3, 0, 7
-
-
 def tr_tables(cm_s, cfg, pass_idx, local):
-    """Per-pass inputs of the truncated scanners for a synthetic CM:
-    marginal emissions as fill_marginal_emissions lays them out
-    (src/cp9.rs:4441: MP rows the summed left/right marginals, ML/IL and
-    MR/IR their own emissions on one side and 0 on the other, gap / non-
-    residue / missing codes IMPOSSIBLE), the node spans allow_truncation
-    reads (src/cm_dpsearch_trunc.rs:2376), and a seeded stand-in for the
-    pass's truncation penalties (log2 of 2/(clen(clen+1)) on the states the
-    reference gives penalties to: MP, ML, MR, B and attached inserts)."""
-    from infernox_b200 import synth
-    st = cm_s.st
-    M = cfg.M
-    imp = np.float32(-1e36)
-    lm = np.zeros((M, 18), np.float32)
-    rm = np.zeros((M, 18), np.float32)
-    for v in range(M):
-        lm[v, [4, 16, 17]] = imp
-        rm[v, [4, 16, 17]] = imp
-        t = int(cfg.sttype[v])
-        if t == 1:  # MP: marginals of the pair probabilities
-            e = np.asarray(cm_s.e[v][:16], np.float64).reshape(4, 4)
-            for x in range(4):
-                lm[v, x] = np.float32(np.log2(e[x].sum() / float(cfg.null[x])))
-                rm[v, x] = np.float32(np.log2(e[:, x].sum() / float(cfg.null[x])))
-            for code in range(5, 16):
-                bits = [b for b in range(4) if synth_degen(code) >> b & 1]
-                lm[v, code] = np.float32(np.mean([lm[v, b] for b in bits]))
-                rm[v, code] = np.float32(np.mean([rm[v, b] for b in bits]))
-        elif t in (2, 4):
-            lm[v] = cfg.oesc[v, :18]
-        elif t in (3, 5):
-            rm[v] = cfg.oesc[v, :18]
-    lpos_n, rpos_n = synth.emit_map(st)
-    nd = np.asarray(st.ndidx)
-    ndt = np.asarray(st.ndtype)[nd]
-    lpos = np.where(np.isin(ndt, (MATP_ND, MATL_ND)), lpos_n[nd], lpos_n[nd] + 1).astype(np.int32)
-    rpos = np.where(np.isin(ndt, (MATP_ND, MATR_ND)), rpos_n[nd], rpos_n[nd] - 1).astype(np.int32)
-    clen = int(cfg.clen)
-    pen = np.float32(np.log2(2.0 / (clen * (clen + 1))))
-    stid = np.asarray(cfg.stid)
-    qual = np.isin(stid, (6, 12, 15, 18)) | np.isin(np.asarray(cfg.sttype), (4, 5))  # MATP_MP, MATL_ML, MATR_MR, BIF_B
-    pty = np.where(qual, pen, imp).astype(np.float32)
-    pty[0] = imp
-    return {"lmesc": lm.ravel(), "rmesc": rm.ravel(), "pty": pty, "lpos": lpos, "rpos": rpos, "clen": clen}
-
-
-# canonical residues (bit a = residue a) of each RNA code 0..17
-DEGEN_BITS = [0x1, 0x2, 0x4, 0x8, 0x0, 0x5, 0xA, 0x3, 0xC, 0x6, 0x9, 0xB, 0xE, 0x7, 0xD, 0xF, 0x0, 0x0]
-
-
-def synth_degen(code):
-    return DEGEN_BITS[code]
+    """Per-pass truncated-scan inputs as a dict (see hb.synthetic_tr_inputs)."""
+    from infernox_b200.hb import synthetic_tr_inputs
+    t = synthetic_tr_inputs(cm_s, cfg, local)
+    return {"lmesc": t.lmesc, "rmesc": t.rmesc, "pty": t.pty, "lpos": t.lpos, "rpos": t.rpos, "clen": t.clen}
 
 
 def tr_valid(M, seed, pass_idx, dense=True):
