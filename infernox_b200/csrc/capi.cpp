@@ -123,6 +123,7 @@ static int get_plan(cmgpu_model *m, int semiring, int qdbidx, DevPlan **out) {
     if ((rc = upload_vec(&dp->tsc, p.tsc))) return rc;
     if ((rc = upload_vec(&dp->endsc, p.endsc))) return rc;
     if ((rc = upload_vec(&dp->beginsc, p.beginsc))) return rc;
+    if ((rc = upload_vec(&dp->beginsc_all, p.beginsc_all))) return rc;
     if ((rc = upload_vec(&dp->esc, p.esc))) return rc;
     if ((rc = upload_vec(&dp->el_sca, p.el_sca))) return rc;
     if ((rc = upload_vec(&dp->esc_c, p.esc_c))) return rc;
@@ -348,6 +349,18 @@ static int run_scan(cmgpu_model *m, cmgpu_workspace *ws, int semiring, int qdbid
     sp.root_cnum = pl.root_cnum;
     sp.local = pl.local ? 1 : 0;
     sp.inside = semiring == CMGPU_INSIDE_I32;
+    // integer Inside with local begins: begin states post their cells to a
+    // per-lane ROOT row (an atomic max) instead of ROOT scanning every begin
+    // state per cell; only when the rows are small and no insert state is a
+    // begin state (inserts are relaxed outside the chunk path)
+    {
+        bool ok = sp.inside && sp.local && (size_t)MAX_LANES * (pl.root_dxcap + 1) * 4 <= 64 * 1024;
+        for (size_t v = 0; ok && v < pl.states.size(); v++)
+            if ((pl.states[v].flags & SF_BEGIN) && (pl.states[v].type == IL_ST || pl.states[v].type == IR_ST))
+                ok = false;
+        sp.fuse_begin = ok ? 1 : 0;
+        sp.beginsc_all = dp->beginsc_all;
+    }
     sp.deck_elems = pl.deck_elems;
     sp.ilog = m->ilog;
     sp.ilog_nz = m->ilog_nz;

@@ -97,7 +97,7 @@ struct DevPlan {
     BeginDev *begins = nullptr;
     int32_t *level_start = nullptr, *wb = nullptr, *cb = nullptr, *init_off = nullptr;
     uint32_t *tsc = nullptr, *endsc = nullptr, *beginsc = nullptr, *esc = nullptr, *el_sca = nullptr,
-             *esc_c = nullptr, *init_val = nullptr;
+             *esc_c = nullptr, *init_val = nullptr, *beginsc_all = nullptr;
     std::vector<double> cells_prefix, terms_prefix;  // per jrow, prefix over jrow = 1..W
     double cells_full = 0, terms_full = 0;
     ~DevPlan() {
@@ -115,6 +115,7 @@ struct DevPlan {
         cudaFree(el_sca);
         cudaFree(esc_c);
         cudaFree(init_val);
+        cudaFree(beginsc_all);
     }
 };
 

@@ -30,6 +30,7 @@ struct Cand {
 // dynamic shared memory.  Computed once on the host (scan_layout).
 struct SmemLayout {
     int el, tbl, info, wb, cb, tsc, endsc, escc, chunks, lvl, begin, beginsc, ring, lane, deck;
+    int bsv, bmax;     // fused local begins: per-state begin score, per-lane ROOT row
     int ring_len;      // residues per lane ring (power of two >= W + 64)
     int64_t words;     // total
 };
@@ -46,6 +47,10 @@ struct ScanParams {
     const BeginDev *begins;
     const uint32_t *beginsc;
     int nbegin;
+    // fused local begins (integer Inside): every begin state's cells post
+    // cell + beginsc to a per-lane ROOT row with an atomic max
+    int fuse_begin;
+    const uint32_t *beginsc_all;  // [M], -INFTY where no local begin
     const int32_t *init_off;
     const uint32_t *init_val;
     int ninit;

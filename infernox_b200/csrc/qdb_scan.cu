@@ -113,6 +113,9 @@ struct Smem {
     const int4 *info;
     const int32_t *wb, *cb;
     const uint32_t *tsc, *endsc, *escc, *beginsc;
+    const uint32_t *bsv;  // [M] begin score per state (fused begins)
+    int32_t *bmax;        // [lanes][bstride] ROOT-row begin maxima (fused begins)
+    int bstride;
     const int32_t *lvl;
     const int4 *begin;
     const int2 *chunks;
@@ -125,6 +128,7 @@ struct Lane {
     uint32_t *deck;
     const uint8_t *ring;  // residue at position x: ring[x & rmask]
     int j, par, jm, jrow;
+    int l;                // lane (work item slot) index
 };
 
 struct K {
@@ -275,6 +279,19 @@ __device__ __forceinline__ typename S::T cell_value(const K &k, const Lane &L, i
     return sc;
 }
 
+// Fused local begins (integer Inside): ROOT cell d takes the maximum of
+// cell(v, d) + beginsc[v] over the begin states v, and a maximum needs no
+// order, so each begin state posts its cells as it computes them.
+template <class S>
+__device__ __forceinline__ void post_begin(const K &k, const Lane &L, const SInfo &sv, int v, int d,
+                                           typename S::T x) {
+    if (S::ORDERED && k.p->fuse_begin && (sv.flags & SF_BEGIN) && d >= k.p->root_dn &&
+        d <= min(L.jrow, k.p->root_dxcap)) {
+        const int32_t c = (int32_t)((uint32_t)S::u(x) + k.s.bsv[v]);
+        atomicMax(k.s.bmax + L.l * k.s.bstride + d, c);
+    }
+}
+
 // One warp-wide chunk of an ordinary state (not B, not IL): 64 cells, two per
 // lane (d0+lane and d0+32+lane).  Both values are computed before either is
 // stored, so the two dependency chains overlap.
@@ -290,6 +307,8 @@ __device__ __forceinline__ void do_chunk(const K &k, const Lane &L, int v, const
     const int wbase = (sv.flags & SF_BEGL) ? k.s.wb[v * 2] + L.jm * sv.span : k.s.wb[v * 2 + L.par];
     S::st(L.deck + wbase + da, va);
     if (has_b) S::st(L.deck + wbase + db, vb);
+    post_begin<S>(k, L, sv, v, da, va);
+    if (has_b) post_begin<S>(k, L, sv, v, db, vb);
 }
 
 // Bifurcation cell: alpha[v][d] = init (+) over k ascending of
@@ -329,6 +348,8 @@ __device__ __forceinline__ void do_bif_chunk(const K &k, const Lane &L, int v, c
     const int wb = k.s.wb[v * 2 + L.par];
     S::st(L.deck + wb + da, va);
     if (has_b) S::st(L.deck + wb + db, vb);
+    post_begin<S>(k, L, sv, v, da, va);
+    if (has_b) post_begin<S>(k, L, sv, v, db, vb);
 }
 
 // IL relaxation with up to KC cells per lane held in registers.
@@ -448,6 +469,9 @@ __global__ void __launch_bounds__(512, 1) qdb_scan_kernel(ScanParams p) {
     k.s.beginsc = smem + ly.beginsc;
     k.s.ring = reinterpret_cast<uint8_t *>(smem + ly.ring);
     k.s.lane = reinterpret_cast<int32_t *>(smem + ly.lane);
+    k.s.bsv = smem + ly.bsv;
+    k.s.bmax = reinterpret_cast<int32_t *>(smem + ly.bmax);
+    k.s.bstride = p.root_dxcap + 1;
     k.rmask = ly.ring_len - 1;
 
     const int tid = threadIdx.x, wl = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
@@ -474,6 +498,10 @@ __global__ void __launch_bounds__(512, 1) qdb_scan_kernel(ScanParams p) {
         copy32(ly.lvl, p.level_start, p.nlev + 1);
         copy32(ly.begin, p.begins, p.nbegin * 4);
         copy32(ly.beginsc, p.beginsc, p.nbegin);
+        if (INS && p.fuse_begin) {
+            copy32(ly.bsv, p.beginsc_all, p.M);
+            for (int x = tid; x < lanes * (p.root_dxcap + 1); x += bs) k.s.bmax[x] = -INFTY_D;
+        }
         if (tid < MAX_LANES * LS_W) k.s.lane[tid] = tid % LS_W == LS_ITEM ? -1 : 0;
     }
     uint32_t *deck_base = DECK_SMEM ? smem + ly.deck
@@ -563,6 +591,7 @@ __global__ void __launch_bounds__(512, 1) qdb_scan_kernel(ScanParams p) {
                     const int j = ls[LS_JB] + step;
                     if (ls[LS_ITEM] < 0 || j > ls[LS_JEND]) continue;
                     Lane L;
+                    L.l = l;
                     L.deck = deck_base + (size_t)l * deck_stride;
                     L.ring = k.s.ring + l * ly.ring_len;
                     L.j = j;
@@ -610,7 +639,12 @@ __global__ void __launch_bounds__(512, 1) qdb_scan_kernel(ScanParams p) {
                                     a = yo == 0 ? S::comb(ZERO, term, k.s.tbl, k.nz) : S::comb(a, term, k.s.tbl, k.nz);
                                 }
                             }
-                            if (p.local) {
+                            if (INS && p.fuse_begin) {
+                                int32_t *bm = k.s.bmax + l * k.s.bstride + d;
+                                const T cand = (T)*bm;
+                                *bm = -INFTY_D;
+                                if (a < cand) a = cand;
+                            } else if (p.local) {
                                 for (int b = 0; b < p.nbegin; b++) {
                                     const int4 bd = k.s.begin[b];
                                     const int dn = (int16_t)(bd.w & 0xffff), dxc = (int16_t)((uint32_t)bd.w >> 16);
@@ -652,6 +686,7 @@ __global__ void __launch_bounds__(512, 1) qdb_scan_kernel(ScanParams p) {
                     }
                 }
             }
+            if (INS && p.fuse_begin) __syncthreads();  // ROOT-row resets before the next column's posts
         }
         // advance every live lane by one block
         __syncthreads();
@@ -712,6 +747,8 @@ SmemLayout scan_layout(const ScanParams &p, int lanes, bool deck_smem) {
     L.ring_len = r;
     L.ring = take((int64_t)lanes * r / 4);
     L.lane = take((int64_t)MAX_LANES * 8);
+    L.bsv = take(p.fuse_begin ? p.M : 0);
+    L.bmax = take(p.fuse_begin ? (int64_t)lanes * (p.root_dxcap + 1) : 0);
     L.deck = take(deck_smem ? (int64_t)lanes * p.deck_elems : 0);
     L.words = w;
     return L;
