@@ -201,6 +201,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--plain-windows", type=int, default=16)
+    ap.add_argument("--envelopes", type=int, default=2000, help="envelopes per step (HB workloads)")
     args = ap.parse_args()
     if args.workload in FILTER_WORKLOADS:
         return filter_main(args)
@@ -447,7 +448,7 @@ def filter_main(args):
                               name="bench")
         cfg = model.configure(cm_s, local=True)
         frames, tasks, off = [], [], 0
-        nenv = 2000
+        nenv = args.envelopes
         for q in range(nenv):
             h = synth.emit(cm_s, rng)
             n = cfg.W + 40
