@@ -146,7 +146,9 @@ struct VitWin {
 };
 
 // One warp per window.  out[w] = final xC (int16 in an int32), status[w] =
-// 1 scored, 0 overflow (xE reached 32767).
+// 1 scored, 0 overflow (xE reached 32767).  The score table is staged in
+// shared memory transposed, tabT[c][k] (c = 0..25, k = 0..M), so the lanes
+// of a warp read neighbouring positions of one entry.
 __global__ void __launch_bounds__(256) vit_kernel(const int16_t *__restrict__ tab, int M, int base_w, int e_move,
                                                   int e_loop, const uint8_t *__restrict__ dsq,
                                                   const VitWin *__restrict__ wins, int nwin, int *out,
@@ -156,6 +158,14 @@ __global__ void __launch_bounds__(256) vit_kernel(const int16_t *__restrict__ ta
     const int B = (M + 31) / 32;
     const int stride = (B % 2 == 0) ? B + 1 : B + 2;  // odd stride: lanes hit distinct banks
     const int rowlen = 32 * stride;
+    const int tstride = M + 2;                          // entries per table column (k = 0..M, padded)
+    int16_t *tabT = reinterpret_cast<int16_t *>(vsm + (size_t)nw * 6 * rowlen);
+    for (int q = threadIdx.x; q < (M + 1) * 26; q += blockDim.x) {
+        const int k = q / 26, c = q - k * 26;
+        tabT[c * tstride + k] = tab[q];
+    }
+    __syncthreads();
+    auto T = [&](int c, int k) -> int { return tabT[c * tstride + k]; };
     int *base = vsm + (size_t)warp * 6 * rowlen;
     int *mp = base, *ip = base + rowlen, *dp = base + 2 * rowlen;
     int *mc = base + 3 * rowlen, *ic = base + 4 * rowlen, *dc = base + 5 * rowlen;
@@ -184,14 +194,13 @@ __global__ void __launch_bounds__(256) vit_kernel(const int16_t *__restrict__ ta
                 const int k = k0 + b;
                 int vm = -32768, vi = -32768;
                 if (k <= M) {
-                    const int16_t *tk = tab + (size_t)k * 26, *tk1 = tab + (size_t)(k - 1) * 26;
-                    int sc = adds16(xb, tk[18]);
-                    sc = max(sc, adds16(pm, tk1[19]));
-                    sc = max(sc, adds16(pi, tk1[20]));
-                    sc = max(sc, adds16(pd, tk1[21]));
-                    vm = adds16(sc, tk[x]);
+                    int sc = adds16(xb, T(18, k));
+                    sc = max(sc, adds16(pm, T(19, k - 1)));
+                    sc = max(sc, adds16(pi, T(20, k - 1)));
+                    sc = max(sc, adds16(pd, T(21, k - 1)));
+                    vm = adds16(sc, T(x, k));
                     const int cm = mp[lane * stride + b], ci = ip[lane * stride + b];
-                    vi = max(adds16(cm, tk[22]), adds16(ci, tk[23]));
+                    vi = max(adds16(cm, T(22, k)), adds16(ci, T(23, k)));
                     xe = max(xe, vm);
                 }
                 pm = mp[lane * stride + b];
@@ -211,10 +220,7 @@ __global__ void __launch_bounds__(256) vit_kernel(const int16_t *__restrict__ ta
                 for (int b = 0; b < B; b++) {
                     const int k = k0 + b;
                     int v = -32768;
-                    if (k <= M) {
-                        const int16_t *tk1 = tab + (size_t)(k - 1) * 26;
-                        v = max(adds16(mprev, tk1[24]), adds16(d, tk1[25]));
-                    }
+                    if (k <= M) v = max(adds16(mprev, T(24, k - 1)), adds16(d, T(25, k - 1)));
                     dc[lane * stride + b] = v;
                     d = v;
                     mprev = mc[lane * stride + b];
@@ -346,11 +352,12 @@ extern "C" int cmgpu_vit_score_batch(const cmgpu_vit_filter *f, void *stream_ptr
     const int M = f->host.M;
     const int B = (M + 31) / 32;
     const int stride = (B % 2 == 0) ? B + 1 : B + 2;
+    const size_t tab_bytes = ((size_t)26 * (M + 2) * sizeof(int16_t) + 15) & ~(size_t)15;
     int warps = 8;
-    size_t smem = (size_t)warps * 6 * 32 * stride * sizeof(int);
+    size_t smem = (size_t)warps * 6 * 32 * stride * sizeof(int) + tab_bytes;
     while (smem > 200 * 1024 && warps > 1) {
         warps /= 2;
-        smem = (size_t)warps * 6 * 32 * stride * sizeof(int);
+        smem = (size_t)warps * 6 * 32 * stride * sizeof(int) + tab_bytes;
     }
     if (smem > 227 * 1024) {
         cleanup();
