@@ -75,6 +75,10 @@ void hb_free(HbDev *h) {
 
 namespace hb {
 
+// threads per envelope CTA: a dependency level rarely holds more than a few
+// dozen band rows, and small CTAs let more envelopes share an SM
+constexpr int HB_THREADS = 64;
+
 struct Env {
     int64_t alpha_off;  // first cell of this envelope's matrix
     int64_t dsq_off;    // buffer index of residue 0
@@ -232,12 +236,12 @@ __device__ void ir_diag(const Tables &t, const State *st, const Row *rows, float
 }
 
 template <bool INS>
-__global__ void __launch_bounds__(128, 4) hb_kernel(Tables t, const Env *__restrict__ envs, int nenv,
+__global__ void __launch_bounds__(HB_THREADS, 8) hb_kernel(Tables t, const Env *__restrict__ envs, int nenv,
                                                  const State *__restrict__ states, const Row *__restrict__ rows_all,
                                                  float *alpha_all, const uint8_t *__restrict__ dsq_all, int report,
                                                  Cand *cands, int64_t cand_cap, unsigned long long *ncand, Out *out) {
-    __shared__ float s_v[128];
-    __shared__ int s_j[128];
+    __shared__ float s_v[HB_THREADS];
+    __shared__ int s_j[HB_THREADS];
     __shared__ int s_envi, s_envj, s_nc;
     const int tid = threadIdx.x, nt = blockDim.x;
     for (int e = blockIdx.x; e < nenv; e += gridDim.x) {
@@ -609,13 +613,13 @@ __device__ void tr_bif_row(const Tables &t, const TrTab &tr, const State *st, co
 }
 
 template <bool INS>
-__global__ void __launch_bounds__(128, 4) tr_kernel(Tables t, TrTab tr, const Env *__restrict__ envs, int nenv,
+__global__ void __launch_bounds__(HB_THREADS, 8) tr_kernel(Tables t, TrTab tr, const Env *__restrict__ envs, int nenv,
                                                  const State *__restrict__ states, const Row *__restrict__ rows_all,
                                                  float *planes, int64_t plane_stride, const uint8_t *__restrict__ dsq_all,
                                                  int report, TrCand *cands, int64_t cand_cap,
                                                  unsigned long long *ncand, TrOut *out) {
-    __shared__ float s_v[4];
-    __shared__ int s_m[4], s_j[4];
+    __shared__ float s_v[HB_THREADS / 32];
+    __shared__ int s_m[HB_THREADS / 32], s_j[HB_THREADS / 32];
     __shared__ int s_envi, s_envj;
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
     for (int e = blockIdx.x; e < nenv; e += gridDim.x) {
@@ -1010,10 +1014,10 @@ int hb_launch(cmgpu_model *m, HbDev *h, cudaStream_t st, int semiring, int repor
         HB_TRY(cudaMemsetAsync(d_nc, 0, sizeof(unsigned long long), st));
         HB_TRY(cudaEventRecord(ev0, st));
         if (semiring == CMGPU_INSIDE_F32)
-            hb::hb_kernel<true><<<n, 128, 0, st>>>(t, d_env, n, d_st, d_rows, d_alpha, d_dsq, report, d_c, cap, d_nc,
+            hb::hb_kernel<true><<<n, hb::HB_THREADS, 0, st>>>(t, d_env, n, d_st, d_rows, d_alpha, d_dsq, report, d_c, cap, d_nc,
                                                    d_out);
         else
-            hb::hb_kernel<false><<<n, 128, 0, st>>>(t, d_env, n, d_st, d_rows, d_alpha, d_dsq, report, d_c, cap, d_nc,
+            hb::hb_kernel<false><<<n, hb::HB_THREADS, 0, st>>>(t, d_env, n, d_st, d_rows, d_alpha, d_dsq, report, d_c, cap, d_nc,
                                                     d_out);
         HB_TRY(cudaGetLastError());
         HB_TRY(cudaEventRecord(ev1, st));
@@ -1271,10 +1275,10 @@ int tr_launch(cmgpu_model *m, HbDev *h, cudaStream_t st, int semiring, const hb:
         HB_TRY(cudaMemsetAsync(d_nc, 0, sizeof(unsigned long long), st));
         HB_TRY(cudaEventRecord(ev0, st));
         if (semiring == CMGPU_INSIDE_F32)
-            hb::tr_kernel<true><<<n, 128, 0, st>>>(t, trt, d_env, n, d_st, d_rows, d_planes, cells, d_dsq, report, d_c,
+            hb::tr_kernel<true><<<n, hb::HB_THREADS, 0, st>>>(t, trt, d_env, n, d_st, d_rows, d_planes, cells, d_dsq, report, d_c,
                                                    cap, d_nc, d_out);
         else
-            hb::tr_kernel<false><<<n, 128, 0, st>>>(t, trt, d_env, n, d_st, d_rows, d_planes, cells, d_dsq, report,
+            hb::tr_kernel<false><<<n, hb::HB_THREADS, 0, st>>>(t, trt, d_env, n, d_st, d_rows, d_planes, cells, d_dsq, report,
                                                     d_c, cap, d_nc, d_out);
         HB_TRY(cudaGetLastError());
         HB_TRY(cudaEventRecord(ev1, st));
