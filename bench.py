@@ -59,6 +59,21 @@ def env_rank():
             int(os.environ.get("LOCAL_RANK", 0)))
 
 
+def aggregate_ranks(dist, total_ms, e2e_ms, cells, device="cuda"):
+    """Whole-job figures over the ranks (weak scaling, no data exchange): the
+    slowest rank's device times (max) and the cells of all ranks (sum).
+    dist is torch.distributed after init_process_group, or None for one rank."""
+    if dist is None:
+        return total_ms, e2e_ms, cells
+    import torch
+    t = torch.tensor([total_ms, e2e_ms, cells], dtype=torch.float64, device=device)
+    tmax = t.clone()
+    dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    tsum = t.clone()
+    dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+    return tmax[0].item(), tmax[1].item(), tsum[2].item()
+
+
 def make_model(w):
     from infernox_b200 import model, synth
     if w["paired"] is None:
@@ -299,15 +314,7 @@ def main():
         raise RuntimeError("e2e hits differ from the device-resident path")
     e2e_ms = sum(etimes)
 
-    t = torch.tensor([total_ms, e2e_ms, cells, float(sum(kms))], dtype=torch.float64, device="cuda")
-    if dist:
-        tmax = t.clone()
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        tsum = t.clone()
-        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
-        total_ms_all, e2e_ms_all, cells_all = tmax[0].item(), tmax[1].item(), tsum[2].item()
-    else:
-        total_ms_all, e2e_ms_all, cells_all = total_ms, e2e_ms, cells
+    total_ms_all, e2e_ms_all, cells_all = aggregate_ranks(dist, total_ms, e2e_ms, cells)
 
     plain = None
     cb = None
