@@ -165,7 +165,8 @@ def hb_stats(sc: Scanner):
 class TrInputs:
     """Per-pass inputs of the truncated scanners: lmesc/rmesc [M*18], the
     pass's truncated-begin penalties pty [M], the node spans lpos/rpos [M]
-    that allow_truncation reads, clen, and whether local rules apply."""
+    that allow_truncation reads, clen, and whether local rules apply; the
+    integer tables ilmesc/irmesc/ipty for the integer Inside scan."""
     lmesc: np.ndarray
     rmesc: np.ndarray
     pty: np.ndarray
@@ -173,6 +174,9 @@ class TrInputs:
     rpos: np.ndarray
     clen: int
     local: bool
+    ilmesc: np.ndarray = None
+    irmesc: np.ndarray = None
+    ipty: np.ndarray = None
 
     def struct(self) -> N.TrTables:
         self._keep = [np.ascontiguousarray(self.lmesc, np.float32), np.ascontiguousarray(self.rmesc, np.float32),
@@ -305,4 +309,23 @@ def synthetic_tr_inputs(cm_s, cfg, local: bool) -> TrInputs:
         np.isin(np.asarray(cfg.sttype), (4, 5))
     pty = np.where(qual, pen, imp).astype(np.float32)
     pty[0] = imp
-    return TrInputs(lm.ravel(), rm.ravel(), pty, lpos, rpos, clen, bool(local))
+    # integer tables: the states' own integer emissions on their side, the
+    # MP marginals and the penalty scaled as Prob2Score scales (x1000, rounded)
+    ninf = -987654321
+    ilm = np.zeros((M, 18), np.int32)
+    irm = np.zeros((M, 18), np.int32)
+    for v in range(M):
+        t = int(cfg.sttype[v])
+        if t in (2, 4):
+            ilm[v] = cfg.ioesc[v, :18]
+        elif t in (3, 5):
+            irm[v] = cfg.ioesc[v, :18]
+        else:
+            for src, dst in ((lm[v], ilm[v]), (rm[v], irm[v])):
+                x = np.floor(0.5 + 1000.0 * src.astype(np.float64))
+                dst[:] = np.where(src <= -1e35, ninf, np.clip(x, ninf, 1e9)).astype(np.int64)
+        ilm[v, [4, 16, 17]] = ninf
+        irm[v, [4, 16, 17]] = ninf
+    ipty = np.where(qual, int(np.floor(0.5 + 1000.0 * float(pen))), ninf).astype(np.int32)
+    ipty[0] = ninf
+    return TrInputs(lm.ravel(), rm.ravel(), pty, lpos, rpos, clen, bool(local), ilm.ravel(), irm.ravel(), ipty)

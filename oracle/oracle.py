@@ -1,5 +1,5 @@
 """TEST INFRASTRUCTURE ONLY: ctypes binding of the oracle (qdb_oracle.c,
-hb_oracle.c, tr_oracle.c, p7_oracle.c, msv_oracle.c).
+hb_oracle.c, tr_oracle.c, trq_oracle.c, p7_oracle.c, msv_oracle.c).
 
 Used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as
 the checker of the GPU scanner.  The product package never imports it.
@@ -30,7 +30,7 @@ def build() -> str:
 def lib():
     global _lib
     if _lib is None:
-        srcs = [os.path.join(HERE, f) for f in ("qdb_oracle.c", "hb_oracle.c", "tr_oracle.c", "p7_oracle.c", "msv_oracle.c")]
+        srcs = [os.path.join(HERE, f) for f in ("qdb_oracle.c", "hb_oracle.c", "tr_oracle.c", "trq_oracle.c", "p7_oracle.c", "msv_oracle.c")]
         if not os.path.exists(LIB_PATH) or any(os.path.getmtime(LIB_PATH) < os.path.getmtime(f) for f in srcs):
             build()
         L = C.CDLL(LIB_PATH)
@@ -59,6 +59,9 @@ def lib():
         L.oracle_tr_hb_scan.argtypes = [vp, C.c_int] + [vp] * 5 + [C.c_int32] + [vp] * 4 + [vp] * 5 + [
             vp, C.c_int32, C.c_int32, C.c_float, C.c_int, C.c_int, C.c_float, C.c_int, P(C.c_float), P(C.c_int32),
             P(C.c_int64), P(C.c_int64), vp, C.c_int32]
+        L.oracle_trq_scan.argtypes = [vp, C.c_int] + [vp] * 8 + [C.c_int32, vp, C.c_int32, C.c_int32, C.c_float,
+                                     C.c_int, C.c_int, C.c_int, C.c_int, P(C.c_float), P(C.c_int32),
+                                     P(C.c_float), vp, C.c_int32]
         L.oracle_ilogsum_table.argtypes = [P(C.c_int32), C.c_int]
         L.oracle_ilogsum.argtypes = [C.c_int32, C.c_int32]
         L.oracle_ilogsum.restype = C.c_int32
@@ -272,4 +275,27 @@ def tr_hb_scan(cm, inside, tt, valid, bands, dsq, i0, j0, cutoff, do_null3, pass
             out = [(int(h["i"]), int(h["j"]), float(h["score"]), float(h["bias"]), int(h["mode"]), int(h["root"]))
                    for h in hits[:n]]
             return out, vsc.value, vmode.value, ei.value, ej.value
+        cap = n
+
+
+def trq_scan(cm, inside, tt, dsq, i0, j0, cutoff, do_null3, qdbidx, pass_idx, local):
+    """generic_tr_scan restated (ref_tr_cyk_scan / ref_itr_inside_scan): (hits, vsc_root, vmode, bsc_full).
+    tt: dict with lmesc, rmesc, pty (float), ilmesc, irmesc, ipty (int), lpos, rpos, clen."""
+    a, _ = _u8(dsq)
+    f32 = lambda x: np.ascontiguousarray(x, np.float32)
+    i32 = lambda x: np.ascontiguousarray(x, np.int32)
+    arrs = [f32(tt["lmesc"]), f32(tt["rmesc"]), f32(tt["pty"]), i32(tt["ilmesc"]), i32(tt["irmesc"]),
+            i32(tt["ipty"]), i32(tt["lpos"]), i32(tt["rpos"])]
+    vsc, vmode, bfull = C.c_float(), C.c_int32(), C.c_float()
+    cap = 256
+    while True:
+        hits = np.zeros(cap, TR_HIT_DTYPE)
+        n = lib().oracle_trq_scan(C.byref(cm.as_struct()), int(bool(inside)), *[x.ctypes.data for x in arrs],
+                                  int(tt["clen"]), a.ctypes.data, i0, j0, float(cutoff), int(bool(do_null3)),
+                                  int(qdbidx), int(pass_idx), int(bool(local)), C.byref(vsc), C.byref(vmode),
+                                  C.byref(bfull), hits.ctypes.data, cap)
+        if n <= cap:
+            out = [(int(h["i"]), int(h["j"]), float(h["score"]), float(h["bias"]), int(h["mode"]), int(h["root"]))
+                   for h in hits[:n]]
+            return out, vsc.value, vmode.value, bfull.value
         cap = n

@@ -153,7 +153,8 @@ def tr_tables(cm_s, cfg, pass_idx, local):
     """Per-pass truncated-scan inputs as a dict (see hb.synthetic_tr_inputs)."""
     from infernox_b200.hb import synthetic_tr_inputs
     t = synthetic_tr_inputs(cm_s, cfg, local)
-    return {"lmesc": t.lmesc, "rmesc": t.rmesc, "pty": t.pty, "lpos": t.lpos, "rpos": t.rpos, "clen": t.clen}
+    return {"lmesc": t.lmesc, "rmesc": t.rmesc, "pty": t.pty, "lpos": t.lpos, "rpos": t.rpos, "clen": t.clen,
+            "ilmesc": t.ilmesc, "irmesc": t.irmesc, "ipty": t.ipty}
 
 
 def tr_valid(M, seed, pass_idx, dense=True):
