@@ -315,6 +315,9 @@ typedef struct cmgpu_tr_tables {
     const int32_t *lpos, *rpos;   /* [M] */
     int32_t clen;
     int32_t local;                /* truncation rules of local configurations */
+    /* integer versions (CM.ilmesc/irmesc, TrPenalties il/ig), read only by
+     * the integer Inside truncated QDB scan; may be NULL otherwise */
+    const int32_t *ilmesc, *irmesc, *ipty;
 } cmgpu_tr_tables;
 
 /* TrHit (src/cm_dpsearch_trunc.rs:131-139): mode 3 J, 2 L, 1 R, 0 T;
@@ -358,6 +361,34 @@ int cmgpu_tr_scan_hb_batch(const cmgpu_model *m, void *stream, int semiring, con
                            int pass_idx, int do_null3, const uint8_t *dsq_all, int64_t dsq_len,
                            const cmgpu_tr_task *tasks, int32_t ntask, cmgpu_tr_result *results,
                            cmgpu_tr_hit *hits, int64_t cap, int64_t *n_out);
+
+/* ---- truncated QDB / non-banded scanner (generic_tr_scan) ---------------
+ * ref_tr_cyk_scan (CMGPU_CYK_F32, src/cm_dpsearch_trunc.rs:207) and
+ * ref_itr_inside_scan (CMGPU_INSIDE_I32, :226) of residues i0..j0 with the
+ * QDB bands qdbidx (CMGPU_NOQDB / QDB1 / QDB2) in pass pass_idx: the hits
+ * after overlap removal, vsc_root and its mode, and the best score spanning
+ * the full window as the reference computes it (bsc_full).  The scan runs
+ * the columns of a window in order on one CTA: its ROOT row carries over
+ * from column to column as in the reference, so windows are not split. */
+typedef struct cmgpu_trq_result {
+    float vsc_root;
+    int32_t vmode;
+    float bsc_full;
+    int32_t nhits;
+    int64_t hit_first;
+} cmgpu_trq_result;
+
+int cmgpu_tr_qdb_scan(const cmgpu_model *m, int semiring, int qdbidx, const cmgpu_tr_tables *tt,
+                      const uint8_t *dsq, int32_t n, int32_t i0, int32_t j0, float cutoff, int do_null3,
+                      int pass_idx, float *vsc_root, int32_t *vmode, float *bsc_full, cmgpu_tr_hit *hits,
+                      int32_t cap, int32_t *n_out);
+/* Many windows in one call, one CTA per window. */
+int cmgpu_tr_qdb_scan_batch(const cmgpu_model *m, void *stream, int semiring, int qdbidx,
+                            const cmgpu_tr_tables *tt, int pass_idx, int do_null3, const uint8_t *dsq_all,
+                            int64_t dsq_len, const cmgpu_window *wins, int32_t nwin, float cutoff,
+                            cmgpu_trq_result *results, cmgpu_tr_hit *hits, int64_t cap, int64_t *n_out);
+/* Device time, J-plane cells and launches of the last truncated QDB call. */
+int cmgpu_tr_qdb_stats(const cmgpu_model *m, double *kernel_ms, int64_t *cells, int32_t *launches);
 
 /* Device time and cells of the last HMM-banded call on this model. */
 int cmgpu_hb_stats(const cmgpu_model *m, double *kernel_ms, int64_t *cells, int32_t *launches);

@@ -91,7 +91,13 @@ class HbTask(C.Structure):
 
 class TrTables(C.Structure):
     _fields_ = [("lmesc", P(C.c_float)), ("rmesc", P(C.c_float)), ("pty", P(C.c_float)),
-                ("lpos", P(C.c_int32)), ("rpos", P(C.c_int32)), ("clen", C.c_int32), ("local", C.c_int32)]
+                ("lpos", P(C.c_int32)), ("rpos", P(C.c_int32)), ("clen", C.c_int32), ("local", C.c_int32),
+                ("ilmesc", P(C.c_int32)), ("irmesc", P(C.c_int32)), ("ipty", P(C.c_int32))]
+
+
+class TrqResult(C.Structure):
+    _fields_ = [("vsc_root", C.c_float), ("vmode", C.c_int32), ("bsc_full", C.c_float), ("nhits", C.c_int32),
+                ("hit_first", C.c_int64)]
 
 
 class TrTask(C.Structure):
@@ -205,6 +211,12 @@ def lib() -> C.CDLL:
     L.cmgpu_tr_scan_hb_batch.argtypes = [vp, vp, C.c_int, P(TrTables), C.c_int, C.c_int, vp, C.c_int64, vp,
                                          C.c_int32, vp, vp, C.c_int64, P(C.c_int64)]
     L.cmgpu_hb_stats.argtypes = [vp, P(C.c_double), P(C.c_int64), P(C.c_int32)]
+    L.cmgpu_tr_qdb_scan.argtypes = [vp, C.c_int, C.c_int, P(TrTables), vp, C.c_int32, C.c_int32, C.c_int32,
+                                    C.c_float, C.c_int, C.c_int, P(C.c_float), P(C.c_int32), P(C.c_float), vp,
+                                    C.c_int32, P(C.c_int32)]
+    L.cmgpu_tr_qdb_scan_batch.argtypes = [vp, vp, C.c_int, C.c_int, P(TrTables), C.c_int, C.c_int, vp, C.c_int64,
+                                          vp, C.c_int32, C.c_float, vp, vp, C.c_int64, P(C.c_int64)]
+    L.cmgpu_tr_qdb_stats.argtypes = [vp, P(C.c_double), P(C.c_int64), P(C.c_int32)]
     L.cmgpu_count_work.argtypes = [P(Cm), C.c_int, C.c_int, C.c_int32, P(C.c_double),
                                    P(C.c_double)]
     _lib = L
@@ -227,5 +239,6 @@ EXPORTED = [
     "cmgpu_vit_filter_stats", "cmgpu_msv_filter_build", "cmgpu_msv_filter_free", "cmgpu_msv_filter_tables", "cmgpu_ssv_threshold",
     "cmgpu_msv_score_batch", "cmgpu_f1_msv_windows", "cmgpu_ssv_diagonals", "cmgpu_msv_filter_stats",
     "cmgpu_fast_cyk_scan_hb", "cmgpu_hb_scan_hits", "cmgpu_hb_scan_batch", "cmgpu_hb_stats",
-    "cmgpu_tr_scan_hb", "cmgpu_tr_scan_hb_batch",
+    "cmgpu_tr_scan_hb", "cmgpu_tr_scan_hb_batch", "cmgpu_tr_qdb_scan", "cmgpu_tr_qdb_scan_batch",
+    "cmgpu_tr_qdb_stats",
 ]

@@ -37,6 +37,7 @@
 
 #include "devbuf.h"
 #include "model_internal.h"
+#include "trunc_report.h"
 
 namespace cmx {
 
@@ -348,18 +349,10 @@ __global__ void __launch_bounds__(HB_THREADS, 8) hb_kernel(Tables t, const Env *
 // inherits.  ROOT is left out of the levels: its cells are the truncated
 // begins, applied in the root pass.
 // ---------------------------------------------------------------------------
-enum { TRM_T = 0, TRM_R = 1, TRM_L = 2, TRM_J = 3, TRM_UNKNOWN = 4 };
-
 struct TrTab {
     const float *lmesc, *rmesc, *pty;  // [M*18], [M*18], [M]
     const int32_t *pbeg;               // states y >= 1 with a truncated-begin penalty, ascending
     int npbeg, fill_l, fill_r, fill_t;
-};
-
-struct TrCand {
-    int32_t env, j, d;
-    float sc;
-    int32_t mode, root;
 };
 
 struct TrOut {
@@ -767,6 +760,79 @@ __global__ void __launch_bounds__(HB_THREADS, 8) tr_kernel(Tables t, TrTab tr, c
 
 }  // namespace hb
 
+// ---------------------------------------------------------------------------
+// truncated scans: host side
+// ---------------------------------------------------------------------------
+bool allow_trunc(const TrCtx &c, int64_t start, int64_t stop, int64_t i0, int64_t j0, int mode, int b) {
+    if (c.pass_idx == 1 || c.pass_idx == 5) return true;  // STD_ANY, 5P_AND_3P_ANY
+    if (start == i0 && stop == j0) return true;
+    const int lp = c.tt->lpos[b], rp = c.tt->rpos[b];
+    if (c.local) {
+        if (mode == hb::TRM_J) return true;
+        if (mode == hb::TRM_L) return stop == j0;
+        if (mode == hb::TRM_R) return start == i0;
+        return false;
+    }
+    if (mode == hb::TRM_J) return lp == 1 && rp == c.tt->clen;
+    if (mode == hb::TRM_L) return stop == j0 && lp == 1;
+    if (mode == hb::TRM_R) return start == i0 && rp == c.tt->clen;
+    return false;
+}
+
+void tr_report(const cmgpu_model *m, const TrCtx &cx, const hb::TrCand *c, size_t n, const uint8_t *dsq, int32_t i0,
+               int32_t j0, float cutoff, int do_null3, std::vector<cmgpu_tr_hit> &out) {
+    std::vector<cmgpu_tr_hit> tmp;
+    std::vector<int32_t> pre;
+    const int32_t lo = i0 - 1;
+    if (do_null3 && n) {
+        const int32_t hi = c[n - 1].j;
+        pre.assign((size_t)(hi - lo + 1) * 4, 0);
+        for (int32_t p = lo + 1; p <= hi; p++) {
+            for (int a = 0; a < 4; a++) pre[(size_t)(p - lo) * 4 + a] = pre[(size_t)(p - 1 - lo) * 4 + a];
+            if (dsq[p] < 4) pre[(size_t)(p - lo) * 4 + dsq[p]]++;
+        }
+    }
+    size_t k = 0;
+    while (k < n) {
+        const int32_t j = c[k].j;
+        float max_rep = IMPOSSIBLE;
+        for (; k < n && c[k].j == j; k++) {
+            const int32_t d = c[k].d, i = j - d + 1;
+            float sc = c[k].sc, bias = 0.0f;
+            if (!(sc > max_rep && sc >= cutoff && sc > IMPOSSIBLE + 1.0f)) continue;
+            bool rep = allow_trunc(cx, i, j, i0, j0, c[k].mode, c[k].root);
+            if (rep && do_null3) {
+                float comp[4], sum = 0.0f;
+                for (int a = 0; a < 4; a++) {
+                    comp[a] = (float)(double)(pre[(size_t)(j - lo) * 4 + a] - pre[(size_t)(i - 1 - lo) * 4 + a]);
+                    sum += comp[a];
+                }
+                for (int a = 0; a < 4; a++) comp[a] = sum > 0.0f ? comp[a] / sum : 0.25f;
+                const float corr = null3_corr(m, comp, d);
+                sc -= corr;
+                bias = corr;
+                rep = sc > max_rep && sc >= cutoff;
+            }
+            if (rep) {
+                tmp.push_back(cmgpu_tr_hit{i, j, sc, bias, c[k].mode, c[k].root});
+                max_rep = sc;
+            }
+        }
+    }
+    std::stable_sort(tmp.begin(), tmp.end(), [](const cmgpu_tr_hit &a, const cmgpu_tr_hit &b) {
+        if (a.score != b.score) return a.score > b.score;
+        return a.i < b.i;
+    });
+    std::vector<char> removed(tmp.size(), 0);
+    for (size_t a = 0; a < tmp.size(); a++) {
+        if (removed[a]) continue;
+        for (size_t b = a + 1; b < tmp.size(); b++)
+            if (!removed[b] && !(tmp[b].j < tmp[a].i) && !(tmp[a].j < tmp[b].i)) removed[b] = 1;
+    }
+    for (size_t a = 0; a < tmp.size(); a++)
+        if (!removed[a]) out.push_back(tmp[a]);
+}
+
 namespace {
 
 template <class T>
@@ -1140,87 +1206,6 @@ int hb_batch(const cmgpu_model *mc, cudaStream_t st, int semiring, int report, i
     return CMGPU_OK;
 }
 
-
-// ---------------------------------------------------------------------------
-// truncated scans: host side
-// ---------------------------------------------------------------------------
-struct TrCtx {
-    const cmgpu_tr_tables *tt;
-    int pass_idx, local;
-};
-
-// allow_truncation (src/cm_dpsearch_trunc.rs:2376-2440)
-bool allow_trunc(const TrCtx &c, int64_t start, int64_t stop, int64_t i0, int64_t j0, int mode, int b) {
-    if (c.pass_idx == 1 || c.pass_idx == 5) return true;  // STD_ANY, 5P_AND_3P_ANY
-    if (start == i0 && stop == j0) return true;
-    const int lp = c.tt->lpos[b], rp = c.tt->rpos[b];
-    if (c.local) {
-        if (mode == hb::TRM_J) return true;
-        if (mode == hb::TRM_L) return stop == j0;
-        if (mode == hb::TRM_R) return start == i0;
-        return false;
-    }
-    if (mode == hb::TRM_J) return lp == 1 && rp == c.tt->clen;
-    if (mode == hb::TRM_L) return stop == j0 && lp == 1;
-    if (mode == hb::TRM_R) return start == i0 && rp == c.tt->clen;
-    return false;
-}
-
-// greedy report (src/cm_dpsearch_trunc.rs:2322-2374) from the reportable
-// cells of one envelope (sorted by j, d), then overlap removal (:2470)
-void tr_report(const cmgpu_model *m, const TrCtx &cx, const hb::TrCand *c, size_t n, const uint8_t *dsq, int32_t i0,
-               int32_t j0, float cutoff, int do_null3, std::vector<cmgpu_tr_hit> &out) {
-    std::vector<cmgpu_tr_hit> tmp;
-    std::vector<int32_t> pre;
-    const int32_t lo = i0 - 1;
-    if (do_null3 && n) {
-        const int32_t hi = c[n - 1].j;
-        pre.assign((size_t)(hi - lo + 1) * 4, 0);
-        for (int32_t p = lo + 1; p <= hi; p++) {
-            for (int a = 0; a < 4; a++) pre[(size_t)(p - lo) * 4 + a] = pre[(size_t)(p - 1 - lo) * 4 + a];
-            if (dsq[p] < 4) pre[(size_t)(p - lo) * 4 + dsq[p]]++;
-        }
-    }
-    size_t k = 0;
-    while (k < n) {
-        const int32_t j = c[k].j;
-        float max_rep = IMPOSSIBLE;
-        for (; k < n && c[k].j == j; k++) {
-            const int32_t d = c[k].d, i = j - d + 1;
-            float sc = c[k].sc, bias = 0.0f;
-            if (!(sc > max_rep && sc >= cutoff && sc > IMPOSSIBLE + 1.0f)) continue;
-            bool rep = allow_trunc(cx, i, j, i0, j0, c[k].mode, c[k].root);
-            if (rep && do_null3) {
-                float comp[4], sum = 0.0f;
-                for (int a = 0; a < 4; a++) {
-                    comp[a] = (float)(double)(pre[(size_t)(j - lo) * 4 + a] - pre[(size_t)(i - 1 - lo) * 4 + a]);
-                    sum += comp[a];
-                }
-                for (int a = 0; a < 4; a++) comp[a] = sum > 0.0f ? comp[a] / sum : 0.25f;
-                const float corr = null3_corr(m, comp, d);
-                sc -= corr;
-                bias = corr;
-                rep = sc > max_rep && sc >= cutoff;
-            }
-            if (rep) {
-                tmp.push_back(cmgpu_tr_hit{i, j, sc, bias, c[k].mode, c[k].root});
-                max_rep = sc;
-            }
-        }
-    }
-    std::stable_sort(tmp.begin(), tmp.end(), [](const cmgpu_tr_hit &a, const cmgpu_tr_hit &b) {
-        if (a.score != b.score) return a.score > b.score;
-        return a.i < b.i;
-    });
-    std::vector<char> removed(tmp.size(), 0);
-    for (size_t a = 0; a < tmp.size(); a++) {
-        if (removed[a]) continue;
-        for (size_t b = a + 1; b < tmp.size(); b++)
-            if (!removed[b] && !(tmp[b].j < tmp[a].i) && !(tmp[a].j < tmp[b].i)) removed[b] = 1;
-    }
-    for (size_t a = 0; a < tmp.size(); a++)
-        if (!removed[a]) out.push_back(tmp[a]);
-}
 
 int tr_launch(cmgpu_model *m, HbDev *h, cudaStream_t st, int semiring, const hb::TrTab &trt, const TrCtx &cx,
               int report, int do_null3, const uint8_t *dsq_all, int64_t dsq_len, const cmgpu_tr_task *tasks,

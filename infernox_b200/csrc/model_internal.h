@@ -20,6 +20,8 @@ namespace cmx {
 void set_error(const std::string &msg);
 struct HbDev;  // device tables of the HMM-banded scanner (hb_scan.cu)
 void hb_free(HbDev *h);
+struct TrqDev;  // device tables of the truncated QDB / non-banded scanner (trq_scan.cu)
+void trq_free(TrqDev *t);
 bool build_plan(const cmgpu_cm *cm, int semiring, int qdbidx, Plan &p);
 
 // ---------------------------------------------------------------------------
@@ -132,9 +134,11 @@ struct cmgpu_model {
     int ilog_nz = 0;
     std::vector<float> flog;  // host FLogsum table for null3
     cmx::HbDev *hb = nullptr;  // built on the first HMM-banded scan
+    cmx::TrqDev *trq = nullptr;  // built on the first truncated QDB / non-banded scan
     ~cmgpu_model() {
         cudaFree(ilog);
         cmx::hb_free(hb);
+        cmx::trq_free(trq);
     }
 };
 

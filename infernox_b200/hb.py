@@ -185,7 +185,11 @@ class TrInputs:
         fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
         ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))
         k = self._keep
-        return N.TrTables(fp(k[0]), fp(k[1]), fp(k[2]), ip(k[3]), ip(k[4]), int(self.clen), int(bool(self.local)))
+        ints = [None if x is None else np.ascontiguousarray(x, np.int32) for x in (self.ilmesc, self.irmesc, self.ipty)]
+        k.extend(ints)
+        ipn = lambda a: None if a is None else ip(a)
+        return N.TrTables(fp(k[0]), fp(k[1]), fp(k[2]), ip(k[3]), ip(k[4]), int(self.clen), int(bool(self.local)),
+                          ipn(ints[0]), ipn(ints[1]), ipn(ints[2]))
 
 
 def _tr_hits(arr, n):
@@ -258,6 +262,69 @@ def tr_scan_hb_batch(sc: Scanner, semiring: int, tri: TrInputs, pass_idx: int, d
             continue
         N.check(rc)
         return [(_tr_hits(out[r.hit_first:], r.nhits), r.vsc_root, r.vmode, r.envi, r.envj) for r in res]
+
+
+def _trq_scan(sc, semiring, qdbidx, tri: TrInputs, dsq, i0, j0, cutoff, do_null3, pass_idx):
+    a = _frame(dsq)
+    tt = tri.struct()
+    vsc, vmode, bfull = C.c_float(), C.c_int32(), C.c_float()
+    cap = 256
+    while True:
+        out = np.zeros(cap, N.TR_HIT_DTYPE)
+        n = C.c_int32()
+        rc = N.lib().cmgpu_tr_qdb_scan(sc._model, semiring, int(qdbidx), C.byref(tt), a.ctypes.data, a.size - 2, i0,
+                                       j0, float(cutoff), int(bool(do_null3)), int(pass_idx), C.byref(vsc),
+                                       C.byref(vmode), C.byref(bfull), out.ctypes.data, cap, C.byref(n))
+        if rc == N.CMGPU_EOVERFLOW and n.value > cap:
+            cap = n.value
+            continue
+        N.check(rc)
+        return _tr_hits(out, n.value), vsc.value, vmode.value, bfull.value
+
+
+def ref_tr_cyk_scan(cm, tri: TrInputs, dsq, i0: int, j0: int, cutoff: float, qdbidx: int, do_null3: bool,
+                    pass_idx: int):
+    """src/cm_dpsearch_trunc.rs:207 (generic_tr_scan, TrCYK) -- (hits (i, j, score, bias, mode, root),
+    vsc_root, vmode, bsc_full); qdbidx N.NOQDB / N.QDB1 / N.QDB2."""
+    sc = cm if isinstance(cm, Scanner) else _scanner(cm)
+    return _trq_scan(sc, N.CYK_F32, qdbidx, tri, dsq, i0, j0, cutoff, do_null3, pass_idx)
+
+
+def ref_itr_inside_scan(cm, tri: TrInputs, dsq, i0: int, j0: int, cutoff: float, qdbidx: int, do_null3: bool,
+                        pass_idx: int):
+    """src/cm_dpsearch_trunc.rs:226 (generic_tr_scan, integer TrInside) -- same results as ref_tr_cyk_scan;
+    reads the integer tables tri.ilmesc / irmesc / ipty."""
+    sc = cm if isinstance(cm, Scanner) else _scanner(cm)
+    return _trq_scan(sc, N.INSIDE_I32, qdbidx, tri, dsq, i0, j0, cutoff, do_null3, pass_idx)
+
+
+def tr_qdb_scan_batch(sc: Scanner, semiring: int, qdbidx: int, tri: TrInputs, pass_idx: int, do_null3: bool,
+                      buf: np.ndarray, windows, cutoff: float):
+    """Many windows in one call: windows is N.WINDOW_DTYPE (dsq_offset, i0, j0) into buf ->
+    [(hits, vsc_root, vmode, bsc_full)] per window."""
+    b = np.ascontiguousarray(buf, np.uint8)
+    w = np.ascontiguousarray(windows, N.WINDOW_DTYPE)
+    tt = tri.struct()
+    res = (N.TrqResult * max(len(w), 1))()
+    cap = 1024 + 16 * len(w)
+    while True:
+        out = np.zeros(cap, N.TR_HIT_DTYPE)
+        n = C.c_int64()
+        rc = N.lib().cmgpu_tr_qdb_scan_batch(sc._model, None, semiring, int(qdbidx), C.byref(tt), int(pass_idx),
+                                             int(bool(do_null3)), b.ctypes.data, b.size, w.ctypes.data, len(w),
+                                             float(cutoff), res, out.ctypes.data, cap, C.byref(n))
+        if rc == N.CMGPU_EOVERFLOW and n.value > cap:
+            cap = n.value
+            continue
+        N.check(rc)
+        return [(_tr_hits(out[r.hit_first:], r.nhits), r.vsc_root, r.vmode, r.bsc_full) for r in res[:len(w)]]
+
+
+def tr_qdb_stats(sc: Scanner):
+    """(kernel ms, J-plane cells, launches) of the last truncated QDB call on this model."""
+    ms, cells, launches = C.c_double(), C.c_int64(), C.c_int32()
+    N.check(N.lib().cmgpu_tr_qdb_stats(sc._model, C.byref(ms), C.byref(cells), C.byref(launches)))
+    return ms.value, cells.value, launches.value
 
 
 # canonical residues (bit a = residue a) of each RNA code 0..17

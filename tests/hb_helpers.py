@@ -12,7 +12,10 @@
 """
 import numpy as np
 
+from infernox_b200 import synth
 from infernox_b200.hb import Bands
+
+from helpers import frame
 
 E_ST, B_ST = 7, 8
 EMIT = (1, 2, 3, 4, 5)  # MP, ML, MR, IL, IR
@@ -165,3 +168,26 @@ def tr_valid(M, seed, pass_idx, dense=True):
         return j, np.ones(M, np.uint8), np.ones(M, np.uint8), np.ones(M, np.uint8)
     return j, (r.random(M) < 0.7).astype(np.uint8), (r.random(M) < 0.7).astype(np.uint8), \
         (r.random(M) < 0.5).astype(np.uint8)
+
+
+def truncated_window(cm, cfg, pass_idx, seed, max_len=None, flank=30):
+    """A sequence holding one sampled homolog and an envelope [i0, j0] that
+    cuts it at the 5' end (pass 2), the 3' end (pass 3) or both (4, 5), with
+    `flank` residues of background on an uncut side; at most max_len
+    (default W) residues long."""
+    rng = np.random.default_rng(seed)
+    h = synth.emit(cm, rng)
+    while len(h) < 20:
+        h = synth.emit(cm, rng)
+    n = len(h) + 2 * max(60, flank + 1)
+    seq = synth.random_dsq(n, 0.5, rng)
+    p = max(60, flank + 1)
+    seq[p:p + len(h)] = h
+    cut = max(3, len(h) // 4)
+    i0, j0 = p + 1 - flank, p + len(h) + flank
+    if pass_idx in (2, 4, 5):
+        i0 = p + 1 + cut
+    if pass_idx in (3, 4, 5):
+        j0 = p + len(h) - cut
+    j0 = min(j0, i0 + (max_len or cfg.W) - 1)
+    return frame(seq), i0, j0

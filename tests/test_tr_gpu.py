@@ -18,7 +18,7 @@ from infernox_b200 import synth
 from infernox_b200.hb import TrInputs, ftr_inside_scan_hb, tr_cyk_scan_hb, tr_scan_hb_batch
 from infernox_b200.scan import Scanner
 
-from hb_helpers import as_tuple, qdb_bands, ragged_bands, tr_tables, tr_valid, wide_bands
+from hb_helpers import as_tuple, qdb_bands, ragged_bands, tr_tables, tr_valid, truncated_window, wide_bands
 from helpers import frame, models
 
 pytestmark = pytest.mark.gpu
@@ -34,27 +34,6 @@ def bits(x):
 
 def hb(hits):
     return [(i, j, bits(s), bits(b), m, r) for i, j, s, b, m, r in hits]
-
-
-def truncated_window(cm, cfg, pass_idx, seed):
-    """A sequence holding one sampled homolog and an envelope [i0, j0] that
-    cuts it at the 5' end (pass 2), the 3' end (pass 3) or both (4, 5)."""
-    rng = np.random.default_rng(seed)
-    h = synth.emit(cm, rng)
-    while len(h) < 20:
-        h = synth.emit(cm, rng)
-    n = len(h) + 120
-    seq = synth.random_dsq(n, 0.5, rng)
-    p = 60
-    seq[p:p + len(h)] = h
-    cut = max(3, len(h) // 4)
-    i0, j0 = p + 1 - 30, p + len(h) + 30
-    if pass_idx in (2, 4, 5):
-        i0 = p + 1 + cut
-    if pass_idx in (3, 4, 5):
-        j0 = p + len(h) - cut
-    j0 = min(j0, i0 + cfg.W - 1)
-    return frame(seq), i0, j0
 
 
 CASES = [(m, loc, p, kind, dense) for m in ("trna", "small2", "mb3") for loc in (False, True)
