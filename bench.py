@@ -6,7 +6,10 @@ chunks), and the filter/banded stages of the default pipeline --
 sequence, F1 = 0.35), "f2-vit" (Viterbi filter over F1-sized windows),
 "hb-cyk" / "hb-inside" (HMM-banded CYK / float Inside over envelopes with
 CP9-shaped bands), "hb-trcyk" (truncated HMM-banded CYK, 5'-and-3' pass, all
-four planes) -- each with the oracle timed on the host cores beside it.
+four planes), "trq-inside" / "trq-cyk" (the truncated non-banded integer
+TrInside / QDB1 TrCYK window scan, 5'-and-3' pass, over short sequences that
+hold a homolog cut at both ends) -- each with the oracle timed on the host
+cores beside it.
 
 Workload (default "batched-uneven-max"): the batched uneven-window Inside scan
 of the --max path.  One 120-consensus-column CM with 3 bifurcations (seeded
@@ -48,7 +51,7 @@ WORKLOADS = {
     "nohmm-cyk-filter": dict(clen=72, paired=None, nbif=2, sseed=0, pseed=11, semiring=0, band=1,
                              median=100000, sigma=0.0, lo=100000, hi=100000, gc=0.50),
 }
-FILTER_WORKLOADS = ("f1-ssv", "f2-vit", "hb-cyk", "hb-inside", "hb-trcyk")
+FILTER_WORKLOADS = ("f1-ssv", "f2-vit", "hb-cyk", "hb-inside", "hb-trcyk", "trq-inside", "trq-cyk")
 OPS_PER_TERM = {0: 2.0, 1: 7.0}   # CYK: FADD + select; Inside: 6 INT + 1 LDS
 OPS_PER_CELL = 2.0                # emission add + store
 CUTOFF_BITS = 15.0                # stands in for the E-value threshold
@@ -399,6 +402,37 @@ def main():
 FILTER_OPS_PER_CELL = {"f1-ssv": 4.0, "f2-vit": 14.0, "hb-cyk": 8.0, "hb-inside": 29.0, "hb-trcyk": 24.0}
 
 
+def trq_work(cfg, qdb, L, fill_t=True):
+    """(J-plane cells, child relaxations) of the truncated QDB scan of one
+    window of L residues, counted from generic_tr_scan's loops: cnum per cell
+    for each non-bifurcation state and the k-splits of B states, on the J, L
+    and R planes (and the T plane's splits of B states)."""
+    M, W = cfg.M, cfg.W
+    w = min(W, L)
+    dmax = {0: np.full(M, W), 1: np.asarray(cfg.dmax1), 2: np.asarray(cfg.dmax2)}[qdb]
+    dxcap = np.minimum(dmax, W)
+    st, stid = np.asarray(cfg.sttype), np.asarray(cfg.stid)
+    cnum, cfirst = np.asarray(cfg.cnum), np.asarray(cfg.cfirst)
+    live = np.array([v > 0 and st[v] != 7 and not (st[v] in (2, 3, 4, 5) and v + 1 < M and stid[v + 1] == 19)
+                     for v in range(M)])
+    lv = np.nonzero(live)[0]
+    nb, bb = lv[st[lv] != 8], lv[st[lv] == 8]
+    cells = terms = 0.0
+    for jrow in range(1, w + 1):
+        ncol = 1 if jrow < w else L - w + 1
+        c = np.minimum(jrow, dxcap[nb])
+        cells += ncol * float(c.sum())
+        terms += ncol * 3.0 * float((c * cnum[nb]).sum())
+        for v in bb:
+            cb = min(jrow, int(dxcap[v]))
+            y, wl = int(cnum[v]), int(cfirst[v])
+            d = np.arange(1, cb + 1)
+            k = d + 1 if qdb == 0 else np.maximum(np.minimum(dxcap[y], d) - np.maximum(d - dxcap[wl], 0) + 1, 0)
+            cells += ncol * cb
+            terms += ncol * float(k.sum()) * (4 if fill_t else 3)
+    return cells, terms
+
+
 def _chunks(total, chunk, rng, cons, nplant, gc):
     """Both strands of a total-residue sequence with planted consensus runs,
     cut into chunk frames."""
@@ -449,6 +483,32 @@ def filter_main(args):
             config.update({"model": f"synthetic p7 profile M={M} (peak 0.6)",
                            "windows": f"{len(wins)} windows of {2 * maxl} residues (2 Mb, both strands)"})
         cells_step = int((wins["j0"] - wins["i0"] + 1).sum()) * M
+    elif kind in ("trq-inside", "trq-cyk"):
+        cmw = WORKLOADS["batched-uneven-max"]
+        cm_s = synth.synth_cm(synth.structure(cmw["clen"], cmw["paired"], cmw["nbif"], cmw["sseed"]), cmw["pseed"],
+                              name="bench")
+        cfg = model.configure(cm_s, local=True)
+        frames, wl, off = [], [], 0
+        for q in range(args.envelopes):
+            h = synth.emit(cm_s, rng)
+            c5, c3 = len(h) // 4, len(h) // 5
+            seq = np.concatenate([synth.random_dsq(20, 0.45, rng), h[c5:len(h) - c3],
+                                  synth.random_dsq(20, 0.45, rng)]).astype(np.uint8)
+            f = np.concatenate([[255], seq, [255]]).astype(np.uint8)
+            frames.append(f)
+            wl.append((off, 1, len(seq)))
+            off += len(f)
+        buf = np.concatenate(frames)
+        wins = np.array(wl, dtype=[("dsq_offset", np.int64), ("i0", np.int32), ("j0", np.int32)])
+        trq_qdb = 0 if kind == "trq-inside" else 1
+        lens = wins["j0"] - wins["i0"] + 1
+        config.update({"model": f"synthetic CM clen={cfg.clen} M={cfg.M} W={cfg.W} (local)",
+                       "windows": f"{len(wins)} whole sequences, each a sampled homolog cut by 1/4 at the 5' end "
+                                  f"and 1/5 at the 3' end between 20-nt random flanks (median "
+                                  f"{int(np.median(lens))} nt)",
+                       "pass": "5'-and-3' (PLI_PASS_5P_AND_3P_FORCE), J/L/R/T planes",
+                       "bands": "non-banded" if trq_qdb == 0 else "QDB1 (beta1)"})
+        cells_step = None  # counted by the library (J-plane cells)
     else:
         cmw = WORKLOADS["batched-uneven-max"]
         cm_s = synth.synth_cm(synth.structure(cmw["clen"], cmw["paired"], cmw["nbif"], cmw["sseed"]), cmw["pseed"],
@@ -490,6 +550,24 @@ def filter_main(args):
         call = lambda: f.score_batch(buf, wins)
         stats = lambda: p7.vit_stats(f)
         h2d = buf.nbytes + len(wins) * 24
+    elif kind in ("trq-inside", "trq-cyk"):
+        from infernox_b200 import _native as N
+        from infernox_b200.scan import Scanner
+        sc = Scanner(cfg, device=local_rank)
+        tri = hb.synthetic_tr_inputs(cm_s, cfg, True)
+        sr = N.INSIDE_I32 if kind == "trq-inside" else N.CYK_F32
+        call = lambda: hb.tr_qdb_scan_batch(sc, sr, trq_qdb, tri, 4, True, buf, wins, 0.0)
+        stats = lambda: hb.tr_qdb_stats(sc)
+        call()
+        cells_step = stats()[1]
+        per = {}
+        for L in lens:
+            if int(L) not in per:
+                per[int(L)] = trq_work(cfg, trq_qdb, int(L))
+        tpc = sum(per[int(L)][1] for L in lens) / max(sum(per[int(L)][0] for L in lens), 1.0)
+        FILTER_OPS_PER_CELL[kind] = tpc * (7.0 if kind == "trq-inside" else 2.0) + 2.0
+        config.update({"cells_per_step": int(cells_step), "child_terms_per_cell": round(tpc, 2)})
+        h2d = buf.nbytes + len(wins) * 16 + cfg.M * (2 * 18 + 1) * 4
     elif kind == "hb-trcyk":
         from infernox_b200.scan import Scanner
         sc = Scanner(cfg, device=local_rank)
@@ -548,6 +626,14 @@ def filter_main(args):
     elif kind == "f2-vit":
         units = [(int(o), int(j)) for o, _, j in wins]
         one = lambda u: oracle.vit_score_batch(M, prof.mat, prof.trans, buf, [u[0]], [u[1]]) and u[1] * M
+    elif kind in ("trq-inside", "trq-cyk"):
+        units = list(range(len(wins)))
+        ttab = {"lmesc": tri.lmesc, "rmesc": tri.rmesc, "pty": tri.pty, "ilmesc": tri.ilmesc, "irmesc": tri.irmesc,
+                "ipty": tri.ipty, "lpos": tri.lpos, "rpos": tri.rpos, "clen": tri.clen}
+        def one(q):
+            o, i0, j0 = (int(x) for x in wins[q])
+            oracle.trq_scan(cfg, kind == "trq-inside", ttab, buf[o:o + j0 + 2], i0, j0, 0.0, True, trq_qdb, 4, True)
+            return int(per[j0 - i0 + 1][0])
     elif kind == "hb-trcyk":
         units = list(range(len(tasks)))
         ttab = {"lmesc": tri.lmesc, "rmesc": tri.rmesc, "pty": tri.pty, "lpos": tri.lpos, "rpos": tri.rpos,
@@ -590,12 +676,14 @@ def filter_main(args):
           "sample": f"{st['next']} of {len(units)} units of one step's inputs, {dt:.1f} s on {cores} threads"}
     metric = {"f1-ssv": "F1 SSV window scan Gcells/s", "f2-vit": "F2 Viterbi filter Gcells/s",
               "hb-cyk": "HMM-banded CYK Gcells/s", "hb-inside": "HMM-banded Inside Gcells/s",
-              "hb-trcyk": "truncated HMM-banded CYK Gcells/s (band cells, 4 planes each)"}[kind]
+              "hb-trcyk": "truncated HMM-banded CYK Gcells/s (band cells, 4 planes each)",
+              "trq-inside": "truncated non-banded TrInside Gcells/s (J-plane cells, 4 planes each)",
+              "trq-cyk": "truncated QDB TrCYK Gcells/s (J-plane cells, 4 planes each)"}[kind]
     line = {"metric": metric, "value": value, "unit": "Gcells/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": statistics.mean(times), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
             "dtype": {"f1-ssv": "u8 (packed s16x2)", "f2-vit": "i16", "hb-cyk": "f32", "hb-inside": "f32",
-                      "hb-trcyk": "f32"}[kind],
+                      "hb-trcyk": "f32", "trq-inside": "i32", "trq-cyk": "f32"}[kind],
             "data": "synthetic", "config": config,
             "e2e": {"value": e2e, "unit": "Gcells/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": None},
             "gpu_launches": launches,

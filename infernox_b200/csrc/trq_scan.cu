@@ -9,23 +9,40 @@
 // BEGL decks are a ring over the last w+1 columns.  So one CTA runs one
 // window, column by column, on exactly the reference's layout in HBM:
 //   J/L/R/T planes [2][M][w+1] and BEGL decks J/L/R [w+1][nbegl][w+1],
-// with the d = 0 cells set once when the window starts.  Within a column the
-// states run in dependency levels (one more than the deepest child; END
-// states are level 0): a level's states read only finished levels, the
-// previous column, or -- IL only -- their own cell d-1.  A level is cut into
-// units of 32 cells of one state, one unit per warp, lane = d; an IL state is
-// one unit whose warp walks d in order and passes the self-transition value
-// lane to lane, because the reference folds it second (after the local end
-// value) and before the other children, an order Inside's rounding depends
-// on.  Every cell folds its children in the reference's order with its comb
-// (>= max for CYK, ILogsum for Inside), max2 (>= max) and wrapping i32 adds,
-// so the results are the reference's bit for bit.  After the levels, one
-// thread per d applies the truncated begins -- states ascending, planes J, L,
-// R, then T for B states, the reference's order for one d -- to the
-// persistent ROOT row, keeps the column's best begin and emits the reportable
-// cells; the host replays the greedy report with null3.  vsc_root is the
-// first strict maximum in (j, d) order: each d keeps its best and the first
-// column that reached it, reduced when the window ends.
+// with the d = 0 cells set once when the window starts.  The states are
+// grouped in dependency levels (one more than the deepest child; END states
+// are level 0).  Every read of a cell (v, d) of the current column is of a
+// lower level at d' <= d or of v's own cell d-1 (IL's self-loop); every read
+// of an earlier column is of a lower level, or of v itself (IR), at d' <= d.
+// So a column runs as a wavefront over (level, 8-cell chunk) -- unit (l, c)
+// in step l + c, the truncated begins (ROOT) as the last level -- and
+// column j+1 may run its step s as soon as column j has finished step s.
+// A CTA's warps each run one column at a time (column jj on warp jj mod 8),
+// step after step, waiting (on a shared-memory progress counter, with a
+// bounded spin) only for the previous column's same step: no CTA-wide
+// barriers, up to 8 columns of a window in flight.  The decks keep
+// P = 9 column planes and a BEGL ring of w + 9 columns instead of the
+// reference's 2 and w + 1; a warp starts column jj only after column jj-1
+// began, hence after column jj-9 (the last one on that plane) and every
+// reader of the ring slot it reuses have finished.  The values are the
+// same: a state's band [1, dxcap] only grows with jrow, so a cell the
+// reference reads from two columns back (its rolling matrices) was written
+// in the previous column or never, and reads the same in any ring; the ROOT
+// row, which the reference does carry across columns of the same parity,
+// keeps two parities of its own.
+// Plain cells take one lane each; an IL chunk of 8 cells is walked by one
+// lane in d order, the self-transition value carried in a register,
+// because the reference folds it second (after the local end value) and
+// before the other children, an order Inside's rounding depends on.  Every
+// cell folds its children in the reference's order with its comb (>= max
+// for CYK, ILogsum for Inside), max2 (>= max) and wrapping i32 adds, so the
+// results are the reference's bit for bit.  A ROOT cell d applies the
+// truncated begins -- states ascending, planes J, L, R, then T for B
+// states, the reference's order for one d -- to the persistent ROOT row,
+// keeps the column's best begin and emits it if reportable; the host
+// replays the greedy report with null3.  vsc_root is the first strict
+// maximum in (j, d) order: each d keeps its best and the first column that
+// reached it, reduced when the window ends.
 //
 // The CTAs are persistent: each owns one deck region and takes windows from
 // a queue ordered longest first, so device memory is bounded by the resident
@@ -79,7 +96,9 @@ void trq_free(TrqDev *t) {
 namespace trq {
 
 constexpr int THREADS = 256;
-constexpr int NWARP = THREADS / 32;
+constexpr int NW = THREADS / 32;  // warps, columns in flight per window
+constexpr int CH = 8;             // cells per wavefront unit
+constexpr long long SPIN_LIMIT = 1ll << 24;  // polls of a wait (about a second) before it gives up
 constexpr int END_E = 19;  // unique state id of END states (src/constants.rs)
 
 // what a state does in the column loop
@@ -99,11 +118,13 @@ struct Res {
 
 struct Tab {
     const int8_t *sttype, *kind;
-    const int32_t *cfirst, *cnum, *dxcap, *begl_idx, *lev_start, *pbeg;
-    const int2 *units;  // (state, first d) per unit; d = 0 marks an IL chain
+    const int32_t *cfirst, *cnum, *dxcap, *begl_idx, *pbeg;
+    const int32_t *cu_off, *il_off;  // [step][chunk 0..nc]: first unit of the step's chunk
+    const int2 *units, *il_units;    // (state, first d) of 8-cell units, by (step, chunk)
     const uint32_t *tsc, *esc, *lm, *rm, *pty, *init_sc, *base;  // semiring words
     const uint16_t *ilog;
-    int ilog_nz, M, W, nbegl, nlev, npbeg, nonbanded, fill_l, fill_r, fill_t;
+    int ilog_nz, M, W, nbegl, npbeg, nonbanded, fill_l, fill_r, fill_t;
+    int nl, nc, nstep;  // levels, chunks, steps per column
 };
 
 template <bool INS>
@@ -151,18 +172,22 @@ __device__ __forceinline__ T max2(T a, T b) {
 
 // one window's decks
 struct Deck {
-    uint32_t *J, *L, *R, *T, *BJ, *BL, *BR;
-    int W1, M, nbegl;
+    uint32_t *J, *L, *R, *T, *BJ, *BL, *BR, *root;
+    int W1, M, nbegl, RG;  // RG: BEGL ring length
     __device__ __forceinline__ uint32_t *c(uint32_t *P, int a, int v, int d) const {
         return P + ((size_t)(a * M + v) * W1 + d);
     }
     __device__ __forceinline__ uint32_t *b(uint32_t *P, int slot, int bi, int d) const {
         return P + ((size_t)(slot * nbegl + bi) * W1 + d);
     }
+    // ROOT row of plane pl (J, L, R, T) for columns of parity par
+    __device__ __forceinline__ uint32_t *rt(int pl, int par, int d) const {
+        return root + ((size_t)(pl * 2 + par) * W1 + d);
+    }
 };
 
 struct Col {
-    int j, cur, prv, jrow, slot0;  // slot0 = j mod (w+1), the BEGL ring slot of column j
+    int j, cur, prv, jrow, slot0;  // planes of columns j and j-1; slot0: BEGL ring slot of column j
     const uint8_t *dsq;
 };
 
@@ -188,21 +213,32 @@ __device__ __forceinline__ void cell(const Tab &t, const Deck &k, const Col &c, 
         }
         const T a = S::tab(isv + d);
         T jsc = a, lsc = FL ? a : Z, rsc = FR ? a : Z, tsc2 = FT ? a : Z;
-        for (int q = kmin; q <= kmax; q++) {
-            int s = c.slot0 - q;
-            if (s < 0) s += k.W1;
-            const T lft = S::ld(k.b(k.BJ, s, bi, d - q));
-            const T yj = S::ld(k.c(k.J, cur, y, q));
-            jsc = S::comb(jsc, S::add(lft, yj), lt, nz);
-            if (FL) lsc = S::comb(lsc, S::add(lft, S::ld(k.c(k.L, cur, y, q))), lt, nz);
-            if (FR) rsc = S::comb(rsc, S::add(S::ld(k.b(k.BR, s, bi, d - q)), yj), lt, nz);
-        }
-        if (FT) {
-            const int kn = max(kmin, 1), kx = min(d - 1, kmax);
-            for (int q = kn; q <= kx; q++) {
+        // splits k ascending, BU at a time with their loads issued together;
+        // the T plane (fill_t implies fill_l and fill_r) folds the same
+        // loaded values over k = max(kmin,1)..min(d-1,kmax) in its own chain,
+        // in the same ascending order as the reference's separate loop
+        constexpr int BU = 8;
+        for (int q0 = kmin; q0 <= kmax; q0 += BU) {
+            T lj[BU], yj[BU], yl[BU], rb[BU];
+#pragma unroll
+            for (int u = 0; u < BU; u++) {
+                const int q = min(q0 + u, kmax);
                 int s = c.slot0 - q;
-                if (s < 0) s += k.W1;
-                tsc2 = S::comb(tsc2, S::add(S::ld(k.b(k.BR, s, bi, d - q)), S::ld(k.c(k.L, cur, y, q))), lt, nz);
+                if (s < 0) s += k.RG;
+                lj[u] = S::ld(k.b(k.BJ, s, bi, d - q));
+                yj[u] = S::ld(k.c(k.J, cur, y, q));
+                yl[u] = FL ? S::ld(k.c(k.L, cur, y, q)) : Z;
+                rb[u] = FR ? S::ld(k.b(k.BR, s, bi, d - q)) : Z;
+            }
+#pragma unroll
+            for (int u = 0; u < BU; u++) {
+                const int q = q0 + u;
+                if (q <= kmax) {
+                    jsc = S::comb(jsc, S::add(lj[u], yj[u]), lt, nz);
+                    if (FL) lsc = S::comb(lsc, S::add(lj[u], yl[u]), lt, nz);
+                    if (FR) rsc = S::comb(rsc, S::add(rb[u], yj[u]), lt, nz);
+                    if (FT && q >= 1 && q <= d - 1) tsc2 = S::comb(tsc2, S::add(rb[u], yl[u]), lt, nz);
+                }
             }
         }
         S::st(k.c(k.J, cur, v, d), jsc);
@@ -317,13 +353,12 @@ __device__ __forceinline__ void cell(const Tab &t, const Deck &k, const Col &c, 
     }
 }
 
-// IL state v, cells 1..dx in order: one warp, lane = d within 32-cell
-// chunks; the other children and the R plane are read / computed by every
-// lane at once, the J and L chains through the self-transition one lane
-// after the other.
+// Cells d0..d1 of IL state v, in d order, by one lane: the self-transition
+// value of cell d-1 is carried in a register (cell d0-1 comes from the
+// previous step); the R plane reads only other children.
 template <bool INS>
-__device__ __forceinline__ void il_chain(const Tab &t, const Deck &k, const Col &c, const uint16_t *lt, int v,
-                                         int dx, int lane) {
+__device__ __forceinline__ void il_chunk(const Tab &t, const Deck &k, const Col &c, const uint16_t *lt, int v,
+                                         int d0, int d1) {
     using S = Sr<INS>;
     using T = typename S::T;
     const int nz = t.ilog_nz;
@@ -336,69 +371,159 @@ __device__ __forceinline__ void il_chain(const Tab &t, const Deck &k, const Col 
     T tv[MAXC];
 #pragma unroll
     for (int yo = 0; yo < MAXC; yo++) tv[yo] = yo < cn ? S::tab(ts + yo) : Z;
-    T carryJ = S::ld(k.c(k.J, cur, v, 0)), carryL = FL ? S::ld(k.c(k.L, cur, v, 0)) : Z;
-    for (int d0 = 1; d0 <= dx; d0 += 32) {
-        const int d = d0 + lane;
-        const bool act = d <= dx;
-        T cj[MAXC], cl[MAXC], a = Z, e = Z;
+    T carryJ = S::ld(k.c(k.J, cur, v, d0 - 1)), carryL = FL ? S::ld(k.c(k.L, cur, v, d0 - 1)) : Z;
+#pragma unroll 1
+    for (int d = d0; d <= d1; d++) {
+        const T a = S::tab(isv + d - 1), e = S::tab(esc + c.dsq[c.j - d + 1]);
+        T cj[MAXC], cl[MAXC];
 #pragma unroll
         for (int yo = 0; yo < MAXC; yo++) {
-            cj[yo] = Z;
-            cl[yo] = Z;
+            const bool other = yo < cn && y + yo != v;
+            cj[yo] = other ? S::ld(k.c(k.J, cur, y + yo, d - 1)) : Z;
+            cl[yo] = other && FL ? S::ld(k.c(k.L, cur, y + yo, d - 1)) : Z;
         }
-        if (act) {
-            a = S::tab(isv + d - 1);
-            e = S::tab(esc + c.dsq[c.j - d + 1]);
+        T jsc = a, lsc = FL ? a : Z;
 #pragma unroll
-            for (int yo = 0; yo < MAXC; yo++)
-                if (yo < cn && y + yo != v) {
-                    cj[yo] = S::ld(k.c(k.J, cur, y + yo, d - 1));
-                    if (FL) cl[yo] = S::ld(k.c(k.L, cur, y + yo, d - 1));
-                }
-            if (FR) {
-                T rsc = S::tab(isv + d);
-#pragma unroll
-                for (int yo = 1; yo < MAXC; yo++)
-                    if (yo < cn)
-                        rsc = S::comb(rsc,
-                                      max2(S::add(S::ld(k.c(k.J, cur, y + yo, d)), tv[yo]),
-                                           S::add(S::ld(k.c(k.R, cur, y + yo, d)), tv[yo])),
-                                      lt, nz);
-                S::st(k.c(k.R, cur, v, d), rsc);
+        for (int yo = 0; yo < MAXC; yo++)
+            if (yo < cn) {
+                const bool self = y + yo == v;
+                jsc = S::comb(jsc, S::add(self ? carryJ : cj[yo], tv[yo]), lt, nz);
+                if (FL) lsc = S::comb(lsc, S::add(self ? carryL : cl[yo], tv[yo]), lt, nz);
             }
+        carryJ = S::add(jsc, e);
+        S::st(k.c(k.J, cur, v, d), carryJ);
+        if (FL) {
+            carryL = d >= 2 ? S::add(lsc, e) : e;
+            S::st(k.c(k.L, cur, v, d), carryL);
         }
-        T rj = Z, rl = Z;
-        const int n = min(32, dx - d0 + 1);
-        for (int s = 0; s < n; s++) {
-            if (lane == s) {
-                T jsc = a, lsc = FL ? a : Z;
+        if (FR) {
+            T rsc = S::tab(isv + d);
 #pragma unroll
-                for (int yo = 0; yo < MAXC; yo++)
-                    if (yo < cn) {
-                        const bool self = y + yo == v;
-                        jsc = S::comb(jsc, S::add(self ? carryJ : cj[yo], tv[yo]), lt, nz);
-                        if (FL) lsc = S::comb(lsc, S::add(self ? carryL : cl[yo], tv[yo]), lt, nz);
-                    }
-                rj = S::add(jsc, e);
-                if (FL) rl = d >= 2 ? S::add(lsc, e) : e;
-            }
-            carryJ = __shfl_sync(0xffffffffu, rj, s);
-            if (FL) carryL = __shfl_sync(0xffffffffu, rl, s);
-        }
-        if (act) {
-            S::st(k.c(k.J, cur, v, d), rj);
-            if (FL) S::st(k.c(k.L, cur, v, d), rl);
+            for (int yo = 1; yo < MAXC; yo++)
+                if (yo < cn)
+                    rsc = S::comb(rsc,
+                                  max2(S::add(S::ld(k.c(k.J, cur, y + yo, d)), tv[yo]),
+                                       S::add(S::ld(k.c(k.R, cur, y + yo, d)), tv[yo])),
+                                  lt, nz);
+            S::st(k.c(k.R, cur, v, d), rsc);
         }
     }
+}
+
+// ROOT cell d of a column: the truncated begins of the penalised states y
+// (ascending) on planes J, L, R, then T (B states), into the ROOT row of the
+// column's parity; the best begin of d is kept per d across columns and
+// emitted if reportable.
+template <bool INS>
+__device__ __forceinline__ void root_cell(const Tab &t, const Deck &k, const Col &c, int d, float *vb, int *vbj,
+                                          int *vbm, int j0, float *s_bsc, int widx, float cutoff, hb::TrCand *cand,
+                                          int64_t cap, unsigned long long *ncand) {
+    using S = Sr<INS>;
+    using T = typename S::T;
+    const T Z = S::zero();
+    const bool FL = t.fill_l, FR = t.fill_r, FT = t.fill_t;
+    const int par = c.j & 1;
+    T rj = S::ld(k.rt(0, par, d)), rl = FL ? S::ld(k.rt(1, par, d)) : Z;
+    T rr = FR ? S::ld(k.rt(2, par, d)) : Z, rt = FT ? S::ld(k.rt(3, par, d)) : Z;
+    float bs = -1.0e36f;
+    int bm = hb::TRM_UNKNOWN, br = 0;
+    auto rec = [&](T sc, T &r, int mode, int y) {
+        if (sc > r) {
+            r = sc;
+            const float f = S::bits(sc);
+            if (f > bs) {
+                bs = f;
+                bm = mode;
+                br = y;
+            }
+        }
+    };
+    // the begin states in order, RU at a time with their loads issued together
+    constexpr int RU = 4;
+    for (int q0 = 0; q0 < t.npbeg; q0 += RU) {
+        T xj[RU], xl[RU], xr[RU], xt[RU];
+        int yy[RU];
+        bool ok[RU], okt[RU];
+#pragma unroll
+        for (int u = 0; u < RU; u++) {
+            const int q = q0 + u;
+            const int y = q < t.npbeg ? t.pbeg[q] : 0;
+            yy[u] = y;
+            ok[u] = q < t.npbeg && d <= t.dxcap[y];
+            okt[u] = ok[u] && FT && t.sttype[y] == B_ST;
+            const T pen = ok[u] ? S::tab(t.pty + y) : Z;
+            xj[u] = ok[u] ? S::add(S::ld(k.c(k.J, c.cur, y, d)), pen) : Z;
+            xl[u] = ok[u] && FL ? S::add(S::ld(k.c(k.L, c.cur, y, d)), pen) : Z;
+            xr[u] = ok[u] && FR ? S::add(S::ld(k.c(k.R, c.cur, y, d)), pen) : Z;
+            xt[u] = okt[u] ? S::add(S::ld(k.c(k.T, c.cur, y, d)), pen) : Z;
+        }
+#pragma unroll
+        for (int u = 0; u < RU; u++) {
+            if (!ok[u]) continue;
+            rec(xj[u], rj, hb::TRM_J, yy[u]);
+            if (FL) rec(xl[u], rl, hb::TRM_L, yy[u]);
+            if (FR) rec(xr[u], rr, hb::TRM_R, yy[u]);
+            if (okt[u]) rec(xt[u], rt, hb::TRM_T, yy[u]);
+        }
+    }
+    S::st(k.rt(0, par, d), rj);
+    if (FL) S::st(k.rt(1, par, d), rl);
+    if (FR) S::st(k.rt(2, par, d), rr);
+    if (FT) S::st(k.rt(3, par, d), rt);
+    if (bs > vb[d]) {
+        vb[d] = bs;
+        vbj[d] = c.j;
+        vbm[d] = bm;
+    }
+    if (c.j == j0 && d == j0) *s_bsc = bs;
+    if (bs >= cutoff && bs > -1.0e36f) {
+        const unsigned long long at = atomicAdd(ncand, 1ull);
+        if ((int64_t)at < cap) cand[at] = hb::TrCand{widx, c.j, d, bs, bm, br};
+    }
+}
+
+// Lane 0 polls a progress counter of another warp until it reaches `need`
+// (or a wait of this CTA gave up, or SPIN_LIMIT polls pass: then it marks
+// the error and gives up); the warp then sees every write that warp made
+// before publishing.
+__device__ __forceinline__ bool wait_for(volatile int *flag, int need, volatile int *err, int lane) {
+    int ok = 1;
+    if (lane == 0) {
+        long long it = 0;
+        while (*flag < need) {
+            if (*err) {
+                ok = 0;
+                break;
+            }
+            if (++it > SPIN_LIMIT) {
+                *err = 1;
+                ok = 0;
+                break;
+            }
+            __nanosleep(64);
+        }
+        __threadfence_block();
+    }
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    __syncwarp();
+    return ok;
+}
+
+// all of the warp's writes so far, then the new progress value
+__device__ __forceinline__ void publish(volatile int *flag, int val, int lane) {
+    __syncwarp();
+    if (lane == 0) {
+        __threadfence_block();
+        *flag = val;
+    }
+    __syncwarp();
 }
 
 template <bool INS>
 __global__ void __launch_bounds__(THREADS) trq_kernel(Tab t, const Win *__restrict__ wins, int nwin,
                                                       const uint8_t *__restrict__ dsq_all, uint32_t *decks,
                                                       int64_t deck_stride, float cutoff, int *queue, hb::TrCand *cand,
-                                                      int64_t cap, unsigned long long *ncand, Res *res) {
-    using S = Sr<INS>;
-    using T = typename S::T;
+                                                      int64_t cap, unsigned long long *ncand, Res *res, int *kerr) {
     extern __shared__ __align__(16) unsigned char smem[];
     float *vb = (float *)smem;               // per d: best begin score over the columns so far
     int *vbj = (int *)(vb + t.W + 1);        // ... the first column that reached it
@@ -406,152 +531,103 @@ __global__ void __launch_bounds__(THREADS) trq_kernel(Tab t, const Win *__restri
     uint16_t *lt = (uint16_t *)(vbm + t.W + 1);
     __shared__ int s_win;
     __shared__ float s_bsc;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    __shared__ volatile int prog[NW];        // per warp: jj * S + steps done of its current column jj
+    __shared__ volatile int s_err;
+    const int tid = threadIdx.x, wid = tid >> 5, lane = tid & 31;
     if (INS)
         for (int x = tid; x < t.ilog_nz; x += THREADS) lt[x] = t.ilog[x];
-    const T Z = S::zero();
-    const bool FL = t.fill_l, FR = t.fill_r, FT = t.fill_t;
-    const int M = t.M, nbegl = t.nbegl;
+    if (tid == 0) s_err = 0;
+    const int M = t.M, nbegl = t.nbegl, P = NW + 1;
+    const int S = t.nstep, NC = t.nc, NL = t.nl;
     uint32_t *dk = decks + (size_t)blockIdx.x * (size_t)deck_stride;
     for (;;) {
         __syncthreads();
-        if (tid == 0) s_win = atomicAdd(queue, 1);
+        if (tid == 0) s_win = s_err ? nwin : atomicAdd(queue, 1);
         __syncthreads();
         const int wq = s_win;
         if (wq >= nwin) break;
         const Win wn = wins[wq];
-        const int w = wn.w, W1 = w + 1;
-        const size_t plane = (size_t)2 * M * W1, bdeck = (size_t)W1 * nbegl * W1;
-        Deck k{dk, dk + plane, dk + 2 * plane, dk + 3 * plane, dk + 4 * plane, dk + 4 * plane + bdeck,
-               dk + 4 * plane + 2 * bdeck, W1, M, nbegl};
+        const int w = wn.w, W1 = w + 1, RG = W1 + NW;
+        const size_t plane = (size_t)P * M * W1, bdeck = (size_t)RG * nbegl * W1;
+        uint32_t *rbase = dk + 4 * plane, *bbase = rbase + 8 * (size_t)W1;
+        const Deck k{dk, dk + plane, dk + 2 * plane, dk + 3 * plane, bbase, bbase + bdeck, bbase + 2 * bdeck, rbase,
+                     W1, M, nbegl, RG};
         // every cell IMPOSSIBLE / -INFTY, then the d = 0 base cells
         const uint32_t zu = INS ? (uint32_t)(int32_t)-987654321 : __float_as_uint(-1.0e36f);
-        for (size_t x = tid; x < 4 * plane; x += THREADS) {
+        for (size_t x = tid; x < 4 * plane + 8 * (size_t)W1; x += THREADS) {
             const int d = (int)(x % W1);
             const size_t r = x / W1;
-            const int v = (int)(r % M), pl = (int)(r / (2 * (size_t)M));
-            dk[x] = (d == 0 && pl < 3) ? __ldg(t.base + (size_t)pl * M + v) : zu;
+            const int v = (int)(r % M), pl = (int)(r / ((size_t)P * M));
+            dk[x] = (d == 0 && pl < 3 && x < 4 * plane) ? __ldg(t.base + (size_t)pl * M + v) : zu;
         }
         for (size_t x = tid; x < 3 * bdeck; x += THREADS) {
             const int d = (int)(x % W1);
             const int bi = (int)((x / W1) % nbegl);
-            k.BJ[x] = (d == 0 && x < bdeck) ? __ldg(t.base + 3 * (size_t)M + bi) : zu;
+            bbase[x] = (d == 0 && x < bdeck) ? __ldg(t.base + 3 * (size_t)M + bi) : zu;
         }
         for (int d = tid; d <= w; d += THREADS) {
             vb[d] = -1.0e36f;
             vbj[d] = 0;
             vbm[d] = hb::TRM_UNKNOWN;
         }
+        if (tid < NW) prog[tid] = 0;
         if (tid == 0) s_bsc = -1.0e36f;
         __syncthreads();
         const uint8_t *dsq = dsq_all + wn.dsq_off;
-        for (int j = wn.i0; j <= wn.j0; j++) {
-            const Col c{j, j & 1, (j - 1) & 1, min(j - wn.i0 + 1, w), j % W1, dsq};
-            for (int l = 0; l < t.nlev; l++) {
-                const int u1 = t.lev_start[l + 1];
-                for (int u = t.lev_start[l] + warp; u < u1; u += NWARP) {
-                    const int2 un = t.units[u];
-                    const int v = un.x, kind = t.kind[v];
-                    const int dx = min(c.jrow, t.dxcap[v]);
-                    if (un.y == 0) {
-                        il_chain<INS>(t, k, c, lt, v, dx, lane);
+        const int ncol = wn.j0 - wn.i0 + 1, dx0 = t.dxcap[0];
+        bool ok = true;
+        for (int jj = wid; jj < ncol && ok; jj += NW) {
+            const int j = wn.i0 + jj, jrow = min(jj + 1, w);
+            const Col c{j, j % P, (j - 1) % P, jrow, j % RG, dsq};
+            const int ca = min((jrow + CH - 1) / CH, NC);
+            for (int sp = 0; sp < S; sp++) {
+                if (jj > 0 && !wait_for(&prog[(jj - 1) % NW], (jj - 1) * S + sp + 1, &s_err, lane)) {
+                    ok = false;
+                    break;
+                }
+                const int *ci = t.il_off + sp * (NC + 1), *cc = t.cu_off + sp * (NC + 1);
+                // IL chunks, one lane each
+                const int il0 = ci[0], nil = ci[ca] - il0;
+                for (int x = lane; x < nil; x += 32) {
+                    const int2 un = t.il_units[il0 + x];
+                    const int d1 = min(min(jrow, t.dxcap[un.x]), un.y + CH - 1);
+                    if (un.y <= d1) il_chunk<INS>(t, k, c, lt, un.x, un.y, d1);
+                }
+                // plain cells, then the ROOT cells of this step
+                const int c0 = cc[0], ncu = cc[ca] - c0, rc = sp - NL;
+                const bool root = rc >= 0 && rc * CH + 1 <= min(jrow, dx0);
+                const int ntot = (ncu + (root ? 1 : 0)) * CH;
+                for (int x = lane; x < ntot; x += 32) {
+                    const int u = x / CH, m = x % CH;
+                    if (u < ncu) {
+                        const int2 un = t.units[c0 + u];
+                        const int v = un.x, d = un.y + m;
+                        if (d <= min(jrow, t.dxcap[v])) cell<INS>(t, k, c, lt, v, t.kind[v], t.sttype[v], d);
                     } else {
-                        const int d = un.y + lane;
-                        if (d <= dx) cell<INS>(t, k, c, lt, v, kind, t.sttype[v], d);
+                        const int d = rc * CH + 1 + m;
+                        if (d <= min(jrow, dx0))
+                            root_cell<INS>(t, k, c, d, vb, vbj, vbm, wn.j0, &s_bsc, wn.idx, cutoff, cand, cap,
+                                           ncand);
                     }
                 }
-                __syncthreads();
+                publish(&prog[wid], jj * S + sp + 1, lane);
             }
-            // ROOT: truncated begins into the persistent row, best begin per d
-            const int dx0 = min(c.jrow, t.dxcap[0]);
-            for (int d = tid + 1; d <= dx0; d += THREADS) {
-                T rj = S::ld(k.c(k.J, c.cur, 0, d));
-                T rl = FL ? S::ld(k.c(k.L, c.cur, 0, d)) : Z;
-                T rr = FR ? S::ld(k.c(k.R, c.cur, 0, d)) : Z;
-                T rt = FT ? S::ld(k.c(k.T, c.cur, 0, d)) : Z;
-                float bs = -1.0e36f;
-                int bm = hb::TRM_UNKNOWN, br = 0;
-                for (int q = 0; q < t.npbeg; q++) {
-                    const int y = t.pbeg[q];
-                    if (d > t.dxcap[y]) continue;
-                    const T pen = S::tab(t.pty + y);
-                    T sc = S::add(S::ld(k.c(k.J, c.cur, y, d)), pen);
-                    if (sc > rj) {
-                        rj = sc;
-                        const float f = S::bits(sc);
-                        if (f > bs) {
-                            bs = f;
-                            bm = hb::TRM_J;
-                            br = y;
-                        }
-                    }
-                    if (FL) {
-                        sc = S::add(S::ld(k.c(k.L, c.cur, y, d)), pen);
-                        if (sc > rl) {
-                            rl = sc;
-                            const float f = S::bits(sc);
-                            if (f > bs) {
-                                bs = f;
-                                bm = hb::TRM_L;
-                                br = y;
-                            }
-                        }
-                    }
-                    if (FR) {
-                        sc = S::add(S::ld(k.c(k.R, c.cur, y, d)), pen);
-                        if (sc > rr) {
-                            rr = sc;
-                            const float f = S::bits(sc);
-                            if (f > bs) {
-                                bs = f;
-                                bm = hb::TRM_R;
-                                br = y;
-                            }
-                        }
-                    }
-                    if (FT && t.sttype[y] == B_ST) {
-                        sc = S::add(S::ld(k.c(k.T, c.cur, y, d)), pen);
-                        if (sc > rt) {
-                            rt = sc;
-                            const float f = S::bits(sc);
-                            if (f > bs) {
-                                bs = f;
-                                bm = hb::TRM_T;
-                                br = y;
-                            }
-                        }
-                    }
-                }
-                S::st(k.c(k.J, c.cur, 0, d), rj);
-                if (FL) S::st(k.c(k.L, c.cur, 0, d), rl);
-                if (FR) S::st(k.c(k.R, c.cur, 0, d), rr);
-                if (FT) S::st(k.c(k.T, c.cur, 0, d), rt);
-                if (bs > vb[d]) {
-                    vb[d] = bs;
-                    vbj[d] = j;
-                    vbm[d] = bm;
-                }
-                if (j == wn.j0 && d == wn.j0) s_bsc = bs;
-                if (bs >= cutoff && bs > -1.0e36f) {
-                    const unsigned long long at = atomicAdd(ncand, 1ull);
-                    if ((int64_t)at < cap) cand[at] = hb::TrCand{wn.idx, j, d, bs, bm, br};
-                }
-            }
-            // the ROOT row of this parity is read again two columns on by the
-            // same threads; the next column's levels touch neither it nor the
-            // per-d slots, and end in a barrier
         }
         __syncthreads();
         if (tid == 0) {
-            float best = -1.0e36f;
-            int bj = INT_MAX, bm = hb::TRM_UNKNOWN;
-            for (int d = 1; d <= w; d++)
-                if (vb[d] > best || (vb[d] == best && best > -1.0e36f && vbj[d] < bj)) {
-                    best = vb[d];
-                    bj = vbj[d];
-                    bm = vbm[d];
-                }
-            res[wn.idx] = Res{best, bm, s_bsc, 0};
+            if (s_err) {
+                atomicExch(kerr, 1);
+            } else {
+                float best = -1.0e36f;
+                int bj = INT_MAX, bm = hb::TRM_UNKNOWN;
+                for (int d = 1; d <= w; d++)
+                    if (vb[d] > best || (vb[d] == best && best > -1.0e36f && vbj[d] < bj)) {
+                        best = vb[d];
+                        bj = vbj[d];
+                        bm = vbm[d];
+                    }
+                res[wn.idx] = Res{best, bm, s_bsc, 0};
+            }
         }
     }
 }
@@ -758,24 +834,50 @@ int trq_batch(const cmgpu_model *mc, cudaStream_t st, int semiring, int qdbidx, 
         const int dmax = qdbidx == 0 ? W : (qdbidx == 1 ? c.dmax1[v] : c.dmax2[v]);
         dxcap[v] = std::min(dmax, W);
     }
-    std::vector<std::vector<int2>> lv(std::max(q->nlev, 1));
+    // the wavefront: unit (level l, chunk c) in step l + c over the levels
+    // that hold work, the ROOT cells as one more level; a step's units sorted
+    // by chunk (a column with fewer rows takes a prefix: cu_off / il_off),
+    // then B units first and the rest by kind
+    std::vector<int> lmap(std::max(q->nlev, 1), -1);
+    for (int v = 1; v < M; v++)
+        if (q->kind_h[v] != trq::K_SKIP && dxcap[v] >= 1) lmap[q->level[v]] = 0;
+    int nl = 0;
+    for (int &x : lmap)
+        if (x == 0) x = nl++;
+    const int NC = (W + trq::CH - 1) / trq::CH;
+    const int nstep = nl + NC;
+    struct U {
+        int c, key, v, d0;
+    };
+    std::vector<std::vector<U>> sc_cells(nstep), sc_il(nstep);
     for (int v = 1; v < M; v++) {
         const int k = q->kind_h[v];
         if (k == trq::K_SKIP || dxcap[v] < 1) continue;
-        auto &L = lv[q->level[v]];
-        if (k == trq::K_IL)
-            L.insert(L.begin(), int2{v, 0});  // the serial chains first
-        else
-            for (int d0 = 1; d0 <= dxcap[v]; d0 += 32) L.push_back(int2{v, d0});
+        for (int d0 = 1, ch = 0; d0 <= dxcap[v]; d0 += trq::CH, ch++) {
+            const int sp = lmap[q->level[v]] + ch;
+            (k == trq::K_IL ? sc_il : sc_cells)[sp].push_back(U{ch, k == trq::K_B ? 0 : k + 1, v, d0});
+        }
     }
-    std::vector<int2> units;
-    std::vector<int32_t> lev_start(1, 0);
-    for (auto &L : lv) {
-        if (L.empty()) continue;
-        units.insert(units.end(), L.begin(), L.end());
-        lev_start.push_back((int32_t)units.size());
+    std::vector<int2> units, il_units;
+    std::vector<int32_t> cu_off((size_t)nstep * (NC + 1)), il_off((size_t)nstep * (NC + 1));
+    auto lay = [&](std::vector<U> &L, std::vector<int2> &out, int32_t *off) {
+        std::sort(L.begin(), L.end(), [](const U &a, const U &b) {
+            if (a.c != b.c) return a.c < b.c;
+            if (a.key != b.key) return a.key < b.key;
+            if (a.v != b.v) return a.v < b.v;
+            return a.d0 < b.d0;
+        });
+        size_t x = 0;
+        for (int c = 0; c <= NC; c++) {
+            while (x < L.size() && L[x].c < c) x++;
+            off[c] = (int32_t)(out.size() + x);
+        }
+        for (const U &u : L) out.push_back(int2{u.v, u.d0});
+    };
+    for (int sp = 0; sp < nstep; sp++) {
+        lay(sc_cells[sp], units, cu_off.data() + (size_t)sp * (NC + 1));
+        lay(sc_il[sp], il_units, il_off.data() + (size_t)sp * (NC + 1));
     }
-    const int nlev = (int)lev_start.size() - 1;
     std::vector<int32_t> pbeg;
     std::vector<uint32_t> lm((size_t)M * KP), rm((size_t)M * KP), pty(M), base;
     for (int y = 1; y < M; y++)
@@ -828,9 +930,16 @@ int trq_batch(const cmgpu_model *mc, cudaStream_t st, int semiring, int qdbidx, 
     if (wl.empty()) return CMGPU_OK;
 
     const int nw = (int)wl.size();
+    for (const trq::Win &x : wl)
+        if ((int64_t)(x.j0 - x.i0 + 1) * nstep >= INT_MAX) {
+            set_error("truncated QDB scan: window too long for the column progress counters");
+            return CMGPU_EINVAL;
+        }
     const int W1 = wmax + 1;
     const int nbk = std::max(q->nbegl, 1);  // the kernel's BEGL deck count (one unused deck without BEGL states)
-    const int64_t deck_stride = (((int64_t)8 * M * W1 + (int64_t)3 * W1 * nbk * W1) + 63) / 64 * 64;
+    const int64_t nplane = trq::NW + 1;
+    const int64_t deck_stride =
+        ((int64_t)4 * nplane * M * W1 + (int64_t)8 * W1 + (int64_t)3 * (W1 + trq::NW) * nbk * W1 + 63) / 64 * 64;
     const size_t smem = (size_t)(W + 1) * 12 + (ins ? ((size_t)m->ilog_nz * 2 + 16) : 0);
     auto kfn = ins ? trq::trq_kernel<true> : trq::trq_kernel<false>;
     if (smem > 48 * 1024) TRQ_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -845,8 +954,8 @@ int trq_batch(const cmgpu_model *mc, cudaStream_t st, int semiring, int qdbidx, 
     int64_t grid = std::min<int64_t>({(int64_t)nw, (int64_t)occ * nsm, std::max<int64_t>(1, budget / (deck_stride * 4))});
 
     DevArena &ar = q->arena;
-    int2 *d_units;
-    int32_t *d_lev, *d_dx, *d_pbeg;
+    int2 *d_units, *d_il;
+    int32_t *d_cuoff, *d_iloff, *d_dx, *d_pbeg;
     uint32_t *d_lm, *d_rm, *d_pty, *d_base, *d_decks;
     trq::Win *d_win;
     uint8_t *d_dsq;
@@ -854,7 +963,9 @@ int trq_batch(const cmgpu_model *mc, cudaStream_t st, int semiring, int qdbidx, 
     int *d_queue;
     unsigned long long *d_nc;
     if (ar.get(0, &d_units, sizeof(int2) * std::max<size_t>(units.size(), 1)) ||
-        ar.get(1, &d_lev, sizeof(int32_t) * lev_start.size()) || ar.get(2, &d_dx, sizeof(int32_t) * M) ||
+        ar.get(1, &d_cuoff, sizeof(int32_t) * cu_off.size()) || ar.get(2, &d_dx, sizeof(int32_t) * M) ||
+        ar.get(15, &d_il, sizeof(int2) * std::max<size_t>(il_units.size(), 1)) ||
+        ar.get(16, &d_iloff, sizeof(int32_t) * il_off.size()) ||
         ar.get(3, &d_pbeg, sizeof(int32_t) * (pbeg.size() + 1)) || ar.get(4, &d_lm, sizeof(uint32_t) * lm.size()) ||
         ar.get(5, &d_rm, sizeof(uint32_t) * rm.size()) || ar.get(6, &d_pty, sizeof(uint32_t) * M) ||
         ar.get(7, &d_base, sizeof(uint32_t) * base.size()) || ar.get(8, &d_win, sizeof(trq::Win) * nw) ||
@@ -866,7 +977,10 @@ int trq_batch(const cmgpu_model *mc, cudaStream_t st, int semiring, int qdbidx, 
     }
     if (!units.empty())
         TRQ_TRY(cudaMemcpyAsync(d_units, units.data(), sizeof(int2) * units.size(), cudaMemcpyHostToDevice, st));
-    TRQ_TRY(cudaMemcpyAsync(d_lev, lev_start.data(), sizeof(int32_t) * lev_start.size(), cudaMemcpyHostToDevice, st));
+    if (!il_units.empty())
+        TRQ_TRY(cudaMemcpyAsync(d_il, il_units.data(), sizeof(int2) * il_units.size(), cudaMemcpyHostToDevice, st));
+    TRQ_TRY(cudaMemcpyAsync(d_cuoff, cu_off.data(), sizeof(int32_t) * cu_off.size(), cudaMemcpyHostToDevice, st));
+    TRQ_TRY(cudaMemcpyAsync(d_iloff, il_off.data(), sizeof(int32_t) * il_off.size(), cudaMemcpyHostToDevice, st));
     TRQ_TRY(cudaMemcpyAsync(d_dx, dxcap.data(), sizeof(int32_t) * M, cudaMemcpyHostToDevice, st));
     if (!pbeg.empty())
         TRQ_TRY(cudaMemcpyAsync(d_pbeg, pbeg.data(), sizeof(int32_t) * pbeg.size(), cudaMemcpyHostToDevice, st));
@@ -879,9 +993,10 @@ int trq_batch(const cmgpu_model *mc, cudaStream_t st, int semiring, int qdbidx, 
     const bool fill_l = pass_idx == 3 || pass_idx == 4 || pass_idx == 5;
     const bool fill_r = pass_idx == 2 || pass_idx == 4 || pass_idx == 5;
     const bool fill_t = pass_idx == 4 || pass_idx == 5;
-    const trq::Tab tab{q->sttype, q->kind, q->cfirst, q->cnum, d_dx, q->begl_idx, d_lev, d_pbeg, d_units,
-                       q->tsc[s], q->esc[s], d_lm, d_rm, d_pty, q->init_sc[s], d_base, m->ilog, m->ilog_nz, M, W,
-                       nbk, nlev, (int)pbeg.size(), qdbidx == 0, fill_l, fill_r, fill_t};
+    const trq::Tab tab{q->sttype, q->kind, q->cfirst, q->cnum, d_dx, q->begl_idx, d_pbeg, d_cuoff, d_iloff,
+                       d_units, d_il, q->tsc[s], q->esc[s], d_lm, d_rm, d_pty, q->init_sc[s], d_base, m->ilog,
+                       m->ilog_nz, M, W, nbk, (int)pbeg.size(), qdbidx == 0, fill_l, fill_r, fill_t,
+                       nl, NC, nstep};
     int64_t cap = std::max<int64_t>(4096 + 16 * (int64_t)nw, q->cand_hint);
     cudaEvent_t ev0, ev1;
     TRQ_TRY(cudaEventCreate(&ev0));
@@ -899,12 +1014,20 @@ int trq_batch(const cmgpu_model *mc, cudaStream_t st, int semiring, int qdbidx, 
         TRQ_TRY(cudaMemsetAsync(d_nc, 0, sizeof(unsigned long long), st));
         TRQ_TRY(cudaEventRecord(ev0, st));
         kfn<<<(unsigned)grid, trq::THREADS, smem, st>>>(tab, d_win, nw, d_dsq, d_decks, deck_stride, cutoff, d_queue,
-                                                       d_c, cap, d_nc, d_res);
+                                                       d_c, cap, d_nc, d_res, d_queue + 1);
         TRQ_TRY(cudaGetLastError());
         TRQ_TRY(cudaEventRecord(ev1, st));
         unsigned long long nc = 0;
+        int kerr = 0;
         TRQ_TRY(cudaMemcpyAsync(&nc, d_nc, sizeof(nc), cudaMemcpyDeviceToHost, st));
+        TRQ_TRY(cudaMemcpyAsync(&kerr, d_queue + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
         TRQ_TRY(cudaStreamSynchronize(st));
+        if (kerr) {
+            cudaEventDestroy(ev0);
+            cudaEventDestroy(ev1);
+            set_error("truncated QDB scan: a column wait of the kernel timed out");
+            return CMGPU_EDEVICE;
+        }
         float ms = 0;
         cudaEventElapsedTime(&ms, ev0, ev1);
         q->last_ms += ms;
