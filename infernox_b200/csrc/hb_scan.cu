@@ -95,8 +95,9 @@ struct State {
     int32_t ilo, hmn_min, hmx_max, pad;  // IR: first diagonal, band extremes
 };
 
-struct Row {
-    int32_t roff, hmn, hmx, pad;
+struct Row {  // 8 bytes: band rows dominate the per-call copy
+    int32_t roff;
+    int16_t hmn, hmx;
 };
 
 struct Cand {
@@ -206,7 +207,7 @@ __device__ void bif_row(const Tables &t, const State *st, const Row *rows, float
     const int y = t.cfirst[v], z = t.cnum[v];
     const State sy = st[y], sz = st[z];
     const bool inz = j >= sz.jmin && j <= sz.jmax;
-    Row rz{0, 1, 0, 0};
+    Row rz{0, 1, 0};
     if (inz) rz = rows[sz.row0 + j - sz.jmin];
     const int jpy = j - sy.jmin;
     const int kn = max(max(j - sy.jmax, rz.hmn), 0), kx = min(jpy, rz.hmx);
@@ -951,7 +952,11 @@ int64_t fill_envelope(const HostCM &c, const cmgpu_hb_task &tk, int64_t dsq_len,
                 err = "HMM-banded scan: empty END state row";
                 return -1;
             }
-            rows[nrow++] = hb::Row{(int32_t)ncells, hmn, hmx, 0};
+            if (hmn < -32768 || hmx > 32767) {
+                err = "HMM-banded scan: band row beyond the 16-bit d range";
+                return -1;
+            }
+            rows[nrow++] = hb::Row{(int32_t)ncells, (int16_t)hmn, (int16_t)hmx};
             if (hmx >= hmn) ncells += hmx - hmn + 1;
         }
         if (ncells > INT32_MAX) {

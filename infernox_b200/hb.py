@@ -53,11 +53,22 @@ class Bands:
         return Bands(np.ascontiguousarray(jmin, np.int32), np.ascontiguousarray(jmax, np.int32),
                      np.asarray(off, np.int32), cat(rows_min), cat(rows_max))
 
+    def _arrays(self):
+        k = getattr(self, "_keep", None)
+        if k is None or any(a is not b for a, b in zip(k[1], (self.jmin, self.jmax, self.hd_off, self.hdmin,
+                                                             self.hdmax))):
+            src = (self.jmin, self.jmax, self.hd_off, self.hdmin, self.hdmax)
+            arrs = [np.ascontiguousarray(a, np.int32) for a in src]
+            self._keep = k = (arrs, src, [a.ctypes.data for a in arrs])
+        return k
+
+    def pointers(self):
+        """Data addresses of jmin, jmax, hd_off, hdmin, hdmax (int32, contiguous), kept alive by self."""
+        return self._arrays()[2]
+
     def struct(self) -> N.HbBands:
         ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))
-        self._keep = [np.ascontiguousarray(a, np.int32) for a in (self.jmin, self.jmax, self.hd_off, self.hdmin,
-                                                                    self.hdmax)]
-        return N.HbBands(*[ip(a) for a in self._keep])
+        return N.HbBands(*[ip(a) for a in self._arrays()[0]])
 
 
 _E_ST = 7
@@ -134,25 +145,52 @@ def fast_finside_scan_hb(cm, bands: Bands, dsq, i0: int, j0: int, env_cutoff: fl
     return _hb_hits(sc, N.INSIDE_F32, bands, dsq, i0, j0, env_cutoff, cutoff, do_null3)
 
 
+def _task_array(tasks, nvalid):
+    """The tasks as an array laid out like cmgpu_hb_task (nvalid = 0) or
+    cmgpu_tr_task (nvalid = 4 validity pointers), filled column by column."""
+    names = ["dsq_offset", "i0", "j0", "env_cutoff", "cutoff", "p"]
+    fmts = [np.int64, np.int32, np.int32, np.float32, np.float32, (np.uint64, 5 + nvalid)]
+    dt = np.dtype({"names": names, "formats": fmts, "offsets": [0, 8, 12, 16, 20, 24],
+                   "itemsize": 24 + 8 * (5 + nvalid)})
+    a = np.zeros(len(tasks), dt)
+    if not len(tasks):
+        return a
+    cols = list(zip(*[t[:5] for t in tasks]))
+    for name, col in zip(names[:5], cols):
+        a[name] = col
+    a["p"][:, :5] = [t[5].pointers() for t in tasks]
+    return a
+
+
+def _results(res, dt):
+    return np.frombuffer(res, dt) if len(res) else np.zeros(0, dt)
+
+
+_HB_RES_DTYPE = np.dtype({"names": ["vsc_root", "nhits", "envi", "envj", "hit_first"],
+                          "formats": [np.float32, np.int32, np.int64, np.int64, np.int64],
+                          "offsets": [0, 4, 8, 16, 24], "itemsize": 32})
+
+
 def hb_scan_batch(sc: Scanner, semiring: int, report_hits: bool, do_null3: bool, buf: np.ndarray, tasks):
     """tasks: [(dsq_offset, i0, j0, env_cutoff, cutoff, Bands)] -> [(vsc, envi, envj, hits)] per task."""
     b = np.ascontiguousarray(buf, np.uint8)
-    tk = (N.HbTask * len(tasks))()
-    for q, (off, i0, j0, ec, cut, bands) in enumerate(tasks):
-        tk[q] = N.HbTask(off, i0, j0, ec, cut, bands.struct())
-    res = (N.HbResult * len(tasks))()
+    tk = _task_array(tasks, 0)
+    assert tk.dtype.itemsize == C.sizeof(N.HbTask)
+    res = (N.HbResult * max(len(tasks), 1))()
     cap = 1024 + 16 * len(tasks)
     while True:
         out = np.zeros(cap, N.HIT_DTYPE)
         n = C.c_int64()
         rc = N.lib().cmgpu_hb_scan_batch(sc._model, None, semiring, int(bool(report_hits)), int(bool(do_null3)),
-                                         b.ctypes.data, b.size, tk, len(tasks), res, out.ctypes.data, cap,
-                                         C.byref(n))
+                                         b.ctypes.data, b.size, tk.ctypes.data, len(tasks), res, out.ctypes.data,
+                                         cap, C.byref(n))
         if rc == N.CMGPU_EOVERFLOW and n.value > cap:
             cap = n.value
             continue
         N.check(rc)
-        return [(r.vsc_root, r.envi, r.envj, _hits(out[r.hit_first:], r.nhits)) for r in res]
+        r = _results(res, _HB_RES_DTYPE)[:len(tasks)]
+        hl = out[:n.value].tolist()
+        return [(float(v), int(ei), int(ej), hl[f:f + h]) for v, h, ei, ej, f in r.tolist()]
 
 
 def hb_stats(sc: Scanner):
@@ -237,31 +275,39 @@ def ftr_inside_scan_hb(cm, tri: TrInputs, bands: Bands, valid, dsq, i0: int, j0:
     return _tr_scan(sc, N.INSIDE_F32, tri, bands, valid, dsq, i0, j0, cutoff, do_null3, pass_idx, env_cutoff)
 
 
+_TR_RES_DTYPE = np.dtype({"names": ["vsc_root", "vmode", "envi", "envj", "hit_first", "nhits"],
+                          "formats": [np.float32, np.int32, np.int64, np.int64, np.int64, np.int32],
+                          "offsets": [0, 4, 8, 16, 24, 32], "itemsize": 40})
+
+
 def tr_scan_hb_batch(sc: Scanner, semiring: int, tri: TrInputs, pass_idx: int, do_null3: bool, buf: np.ndarray,
                      tasks):
     """tasks: [(dsq_offset, i0, j0, env_cutoff, cutoff, Bands, (jvalid, lvalid, rvalid, tvalid))]
     -> [(hits, vsc, vmode, envi, envj)] per task."""
     b = np.ascontiguousarray(buf, np.uint8)
-    tk = (N.TrTask * len(tasks))()
+    tk = _task_array(tasks, 4)
+    assert tk.dtype.itemsize == C.sizeof(N.TrTask)
     keep = []
-    for q, (off, i0, j0, ec, cut, bands, valid) in enumerate(tasks):
-        vs = [np.ascontiguousarray(x, np.uint8) for x in valid]
+    for q, t in enumerate(tasks):
+        vs = [np.ascontiguousarray(x, np.uint8) for x in t[6]]
         keep.append(vs)
-        tk[q] = N.TrTask(off, i0, j0, ec, cut, bands.struct(), *[_u8p(v) for v in vs])
+        tk["p"][q, 5:] = [v.ctypes.data for v in vs]
     tt = tri.struct()
-    res = (N.TrResult * len(tasks))()
+    res = (N.TrResult * max(len(tasks), 1))()
     cap = 1024 + 16 * len(tasks)
     while True:
         out = np.zeros(cap, N.TR_HIT_DTYPE)
         n = C.c_int64()
         rc = N.lib().cmgpu_tr_scan_hb_batch(sc._model, None, semiring, C.byref(tt), int(pass_idx),
-                                            int(bool(do_null3)), b.ctypes.data, b.size, tk, len(tasks), res,
-                                            out.ctypes.data, cap, C.byref(n))
+                                            int(bool(do_null3)), b.ctypes.data, b.size, tk.ctypes.data, len(tasks),
+                                            res, out.ctypes.data, cap, C.byref(n))
         if rc == N.CMGPU_EOVERFLOW and n.value > cap:
             cap = n.value
             continue
         N.check(rc)
-        return [(_tr_hits(out[r.hit_first:], r.nhits), r.vsc_root, r.vmode, r.envi, r.envj) for r in res]
+        r = _results(res, _TR_RES_DTYPE)[:len(tasks)]
+        hl = out[:n.value].tolist()
+        return [(hl[f:f + h], float(v), int(m), int(ei), int(ej)) for v, m, ei, ej, f, h in r.tolist()]
 
 
 def _trq_scan(sc, semiring, qdbidx, tri: TrInputs, dsq, i0, j0, cutoff, do_null3, pass_idx):
