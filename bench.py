@@ -367,7 +367,8 @@ def main():
             "config": config,
             "e2e": {"value": e2e, "unit": "Gcells/s",
                     "h2d_bytes_per_step": int(buf.nbytes + len(wins) * 24),
-                    "d2h_bytes_per_step": int(ncand / max(1, args.steps) * 16 + len(ref_hits) * 20)},
+                    # the two device counters, the reportable cells, the hit list
+                    "d2h_bytes_per_step": int(8 + ncand / max(1, args.steps) * 16 + len(ref_hits) * 20)},
             "seq_per_s": world * args.batch * args.steps / (total_ms_all / 1e3),
             "step_latency_ms": {"p50": statistics.median(step_lat),
                                 "p99": step_lat[min(len(step_lat) - 1, int(0.99 * len(step_lat)))]},
