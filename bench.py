@@ -382,7 +382,9 @@ def main():
             "cpu_baseline": cb,
             "clocks": clk,
             "launch_shape": {"lanes": tune["best"]["lanes"], "threads": tune["best"]["threads"],
-                             "tuned_over": [(t["lanes"], round(t["kernel_ms"], 1)) for t in tune["trials"]]},
+                             "chunk": tune["best"]["chunk"],
+                             "tuned_over": [(t["lanes"], t["chunk"], round(t["kernel_ms"], 1))
+                                            for t in tune["trials"]]},
             "hits_per_step": int(len(ref_hits)),
         }
         print(json.dumps(line))

@@ -72,24 +72,29 @@ class Scanner:
         N.check(N.lib().cmgpu_workspace_set_shape(self._ws, ctas_per_sm, threads, chunk, lanes))
 
     def autotune(self, semiring: int, qdbidx: int, buf: np.ndarray, windows: np.ndarray,
-                 cutoff: float, device_buf=None, lanes=(2, 4, 8, 16), threads=(512,)) -> dict:
-        """Pick the launch shape (work items per CTA, threads per CTA) for this
-        model and batch by timing one scan per candidate; the fastest stays
-        set on this Scanner.  Every candidate returns the same hits (checked)."""
+                 cutoff: float, device_buf=None, lanes=(4, 8, 16), threads=(512,), chunks_w=(0, 4, 8, 16)) -> dict:
+        """Pick the launch shape (work items per CTA, threads per CTA) and the
+        work-item length (0 = automatic, else that many multiples of W: longer
+        pieces repeat fewer W-1 warm-up columns, shorter ones balance the
+        tail) for this model and batch by timing one scan per candidate; the
+        fastest stays set on this Scanner.  Every candidate returns the same
+        hits (checked)."""
         best, ref, trials = None, None, []
         for th in threads:
             for ln in lanes:
-                self.set_shape(0, th, 0, ln)
-                hits = self.scan_batch(semiring, qdbidx, buf, windows, cutoff, False, device_buf=device_buf)
-                ms = self.stats()["kernel_ms"]
-                if ref is None:
-                    ref = hits
-                elif not np.array_equal(hits, ref):
-                    raise RuntimeError("launch shapes disagree")
-                trials.append({"lanes": ln, "threads": th, "kernel_ms": ms})
-                if best is None or ms < best["kernel_ms"]:
-                    best = trials[-1]
-        self.set_shape(0, best["threads"], 0, best["lanes"])
+                for cw in chunks_w:
+                    chunk = int(cw * self.cm.W)
+                    self.set_shape(0, th, chunk, ln)
+                    hits = self.scan_batch(semiring, qdbidx, buf, windows, cutoff, False, device_buf=device_buf)
+                    ms = self.stats()["kernel_ms"]
+                    if ref is None:
+                        ref = hits
+                    elif not np.array_equal(hits, ref):
+                        raise RuntimeError("launch shapes disagree")
+                    trials.append({"lanes": ln, "threads": th, "chunk": chunk, "kernel_ms": ms})
+                    if best is None or ms < best["kernel_ms"]:
+                        best = trials[-1]
+        self.set_shape(0, best["threads"], best["chunk"], best["lanes"])
         return {"best": best, "trials": trials}
 
     def stats(self) -> dict:
