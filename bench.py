@@ -204,7 +204,7 @@ def cpu_baseline(cm, w, buf, wins, budget_s):
     return {"value": tot / dt / 1e9, "unit": "Gcells/s", "cores": cores, "kind": "port",
             "sample": f"{len(take)} windows ({res} residues, {tot:.3e} cells) drawn from the same batch "
                       f"(windows shorter than half the budget on one core), {dt:.1f} s on {cores} threads",
-            "windows_per_s": len(take) / dt}
+            "windows_per_s": len(take) / dt, "cells": tot, "seconds": dt}
 
 
 def main():
@@ -237,9 +237,17 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        cb = cpu_baseline(cm, w, buf, [tuple(x) for x in wins], args.cpu_seconds)
+        per_step = max(2.0, args.cpu_seconds / max(1, args.steps))
+        for _ in range(args.warmup):
+            cpu_baseline(cm, w, buf, [tuple(x) for x in wins], per_step)
+        samples = [cpu_baseline(cm, w, buf, [tuple(x) for x in wins], per_step) for _ in range(args.steps)]
+        cells, secs = sum(x["cells"] for x in samples), sum(x["seconds"] for x in samples)
+        cb = {"value": cells / secs / 1e9, "unit": "Gcells/s", "cores": samples[0]["cores"], "kind": "port",
+              "sample": f"{args.steps} steps of {per_step:.1f} s, each a bounded random sample of the batch's "
+                        f"windows on {samples[0]['cores']} threads (after {args.warmup} warm-up samples)"}
         line = {"impl": "reference", "metric": "CYK/Inside scan Gcells/s", "value": cb["value"],
-                "unit": "Gcells/s", "n_gpus": world, "steps": 1, "warmup": 0,
+                "unit": "Gcells/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * secs / max(1, args.steps),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
                 "data": "synthetic", "config": config, "cpu_baseline": cb,
                 "e2e": {"value": cb["value"], "unit": "Gcells/s", "h2d_bytes_per_step": 0,
@@ -403,6 +411,13 @@ def main():
 # cell, plus emission add and clamp; truncated CYK: the same over the J, L
 # and R planes (T only at bifurcations).
 FILTER_OPS_PER_CELL = {"f1-ssv": 4.0, "f2-vit": 14.0, "hb-cyk": 8.0, "hb-inside": 29.0, "hb-trcyk": 24.0}
+FILTER_METRIC = {"f1-ssv": "F1 SSV window scan Gcells/s", "f2-vit": "F2 Viterbi filter Gcells/s",
+                 "hb-cyk": "HMM-banded CYK Gcells/s", "hb-inside": "HMM-banded Inside Gcells/s",
+                 "hb-trcyk": "truncated HMM-banded CYK Gcells/s (band cells, 4 planes each)",
+                 "trq-inside": "truncated non-banded TrInside Gcells/s (J-plane cells, 4 planes each)",
+                 "trq-cyk": "truncated QDB TrCYK Gcells/s (J-plane cells, 4 planes each)"}
+FILTER_DTYPE = {"f1-ssv": "u8 (packed s16x2)", "f2-vit": "i16", "hb-cyk": "f32", "hb-inside": "f32",
+                "hb-trcyk": "f32", "trq-inside": "i32", "trq-cyk": "f32"}
 
 
 def trq_work(cfg, qdb, L, fill_t=True):
@@ -511,7 +526,6 @@ def filter_main(args):
                                   f"{int(np.median(lens))} nt)",
                        "pass": "5'-and-3' (PLI_PASS_5P_AND_3P_FORCE), J/L/R/T planes",
                        "bands": "non-banded" if trq_qdb == 0 else "QDB1 (beta1)"})
-        cells_step = None  # counted by the library (J-plane cells)
     else:
         cmw = WORKLOADS["batched-uneven-max"]
         cm_s = synth.synth_cm(synth.structure(cmw["clen"], cmw["paired"], cmw["nbif"], cmw["sseed"]), cmw["pseed"],
@@ -537,6 +551,109 @@ def filter_main(args):
                        "envelopes": f"{nenv} envelopes of W residues, one sampled homolog each, CP9-shaped bands "
                                     "(per-state i/j rectangles of +-20 around the homolog's consensus coordinates)",
                        "band_cells_per_step": cells_step})
+    if kind in ("trq-inside", "trq-cyk", "hb-trcyk"):
+        tri = hb.synthetic_tr_inputs(cm_s, cfg, True)
+    if kind == "hb-trcyk":
+        ones = np.ones(cfg.M, np.uint8)
+        valid = (ones, ones, ones, ones)
+        config.update({"pass": "5'-and-3' (PLI_PASS_5P_AND_3P_FORCE), J/L/R/T planes", "planes": 4})
+    if kind in ("trq-inside", "trq-cyk"):
+        per = {}
+        for L in lens:
+            if int(L) not in per:
+                per[int(L)] = trq_work(cfg, trq_qdb, int(L))
+        cells_step = int(sum(per[int(L)][0] for L in lens))
+        tpc = sum(per[int(L)][1] for L in lens) / max(float(cells_step), 1.0)
+        FILTER_OPS_PER_CELL[kind] = tpc * (7.0 if kind == "trq-inside" else 2.0) + 2.0
+        config.update({"cells_per_step": cells_step, "child_terms_per_cell": round(tpc, 2)})
+
+    # the oracle on the host cores, one unit (window / envelope) at a time
+    import oracle
+    oracle.lib()
+    if kind == "f1-ssv":
+        units = [(int(o), int(j)) for o, _, j in wins]
+        one = lambda u: oracle.f1_msv_windows(M, prof.mat, prof.trans, maxl, mmu, mlam, buf, [u[0]], [u[1]], f1,
+                                              maxl) and u[1] * M
+    elif kind == "f2-vit":
+        units = [(int(o), int(j)) for o, _, j in wins]
+        one = lambda u: oracle.vit_score_batch(M, prof.mat, prof.trans, buf, [u[0]], [u[1]]) and u[1] * M
+    elif kind in ("trq-inside", "trq-cyk"):
+        units = list(range(len(wins)))
+        ttab = {"lmesc": tri.lmesc, "rmesc": tri.rmesc, "pty": tri.pty, "ilmesc": tri.ilmesc, "irmesc": tri.irmesc,
+                "ipty": tri.ipty, "lpos": tri.lpos, "rpos": tri.rpos, "clen": tri.clen}
+
+        def one(q):
+            o, i0, j0 = (int(x) for x in wins[q])
+            oracle.trq_scan(cfg, kind == "trq-inside", ttab, buf[o:o + j0 + 2], i0, j0, 0.0, True, trq_qdb, 4, True)
+            return int(per[j0 - i0 + 1][0])
+    elif kind == "hb-trcyk":
+        units = list(range(len(tasks)))
+        ttab = {"lmesc": tri.lmesc, "rmesc": tri.rmesc, "pty": tri.pty, "lpos": tri.lpos, "rpos": tri.rpos,
+                "clen": tri.clen}
+
+        def one(q):
+            o, i0, j0, ec, cut, b = tasks[q]
+            oracle.tr_hb_scan(cfg, False, ttab, valid, (b.jmin, b.jmax, b.hd_off, b.hdmin, b.hdmax),
+                              buf[o:o + j0 + 2], i0, j0, cut, True, 4, ec, True)
+            return int(np.maximum(b.hdmax - b.hdmin + 1, 0).sum())
+    else:
+        units = list(range(len(tasks)))
+
+        def one(q):
+            o, i0, j0, ec, cut, b = tasks[q]
+            oracle.hb_scan(cfg, kind == "hb-inside", (b.jmin, b.jmax, b.hd_off, b.hdmin, b.hdmax),
+                           buf[o:o + j0 + 2], i0, j0, ec, True, cut, True)
+            return int(np.maximum(b.hdmax - b.hdmin + 1, 0).sum())
+    cores = os.cpu_count() or 1
+    perm = np.random.default_rng(7).permutation(len(units))
+    pos = {"at": 0}
+
+    def cpu_sample(budget_s):
+        """Units of one step's inputs (seeded random order, continuing where
+        the last sample stopped) on every host core until budget_s passes."""
+        lock = threading.Lock()
+        st = {"n": 0, "cells": 0}
+        deadline = time.perf_counter() + budget_s
+
+        def worker():
+            while time.perf_counter() < deadline:
+                with lock:
+                    u = units[int(perm[pos["at"] % len(units)])]
+                    pos["at"] += 1
+                    st["n"] += 1
+                c = one(u)
+                with lock:
+                    st["cells"] += c
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(cores) as ex:
+            for _ in range(cores):
+                ex.submit(worker)
+        dt = time.perf_counter() - t0
+        return {"value": st["cells"] / dt / 1e9, "unit": "Gcells/s", "cores": cores, "kind": "port",
+                "sample": f"{st['n']} of {len(units)} units of one step's inputs, {dt:.1f} s on {cores} threads",
+                "cells": st["cells"], "seconds": dt}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        per_step = max(1.0, args.cpu_seconds / max(1, args.steps))
+        for _ in range(args.warmup):
+            cpu_sample(per_step)
+        samples = [cpu_sample(per_step) for _ in range(args.steps)]
+        cells, secs = sum(x["cells"] for x in samples), sum(x["seconds"] for x in samples)
+        val = cells / secs / 1e9
+        cb = {"value": val, "unit": "Gcells/s", "cores": cores, "kind": "port",
+              "sample": f"{args.steps} steps of {per_step:.1f} s, each a bounded sample of one step's units "
+                        f"on {cores} threads (after {args.warmup} warm-up samples)"}
+        print(json.dumps({"impl": "reference", "metric": FILTER_METRIC[kind], "value": val, "unit": "Gcells/s",
+                          "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": 1e3 * secs / max(1, args.steps), "higher_is_better": True,
+                          "scaling": "weak", "vs_baseline": None, "dtype": FILTER_DTYPE[kind], "data": "synthetic",
+                          "config": config, "cpu_baseline": cb,
+                          "e2e": {"value": val, "unit": "Gcells/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}))
+        return
+
     import torch
     torch.cuda.set_device(local_rank)
     stream = torch.cuda.current_stream()
@@ -557,28 +674,17 @@ def filter_main(args):
         from infernox_b200 import _native as N
         from infernox_b200.scan import Scanner
         sc = Scanner(cfg, device=local_rank)
-        tri = hb.synthetic_tr_inputs(cm_s, cfg, True)
         sr = N.INSIDE_I32 if kind == "trq-inside" else N.CYK_F32
         call = lambda: hb.tr_qdb_scan_batch(sc, sr, trq_qdb, tri, 4, True, buf, wins, 0.0)
         stats = lambda: hb.tr_qdb_stats(sc)
         call()
-        cells_step = stats()[1]
-        per = {}
-        for L in lens:
-            if int(L) not in per:
-                per[int(L)] = trq_work(cfg, trq_qdb, int(L))
-        tpc = sum(per[int(L)][1] for L in lens) / max(sum(per[int(L)][0] for L in lens), 1.0)
-        FILTER_OPS_PER_CELL[kind] = tpc * (7.0 if kind == "trq-inside" else 2.0) + 2.0
-        config.update({"cells_per_step": int(cells_step), "child_terms_per_cell": round(tpc, 2)})
+        if stats()[1] != cells_step:
+            raise RuntimeError("J-plane cell counts of the library and of trq_work differ")
         h2d = buf.nbytes + len(wins) * 16 + cfg.M * (2 * 18 + 1) * 4
     elif kind == "hb-trcyk":
         from infernox_b200.scan import Scanner
         sc = Scanner(cfg, device=local_rank)
-        tri = hb.synthetic_tr_inputs(cm_s, cfg, True)
-        ones = np.ones(cfg.M, np.uint8)
-        valid = (ones, ones, ones, ones)
         ttasks = [t + (valid,) for t in tasks]
-        config.update({"pass": "5'-and-3' (PLI_PASS_5P_AND_3P_FORCE), J/L/R/T planes", "planes": 4})
         call = lambda: hb.tr_scan_hb_batch(sc, 0, tri, 4, True, buf, ttasks)
         stats = lambda: hb.hb_stats(sc)
         h2d = buf.nbytes + sum(t[5].hdmin.nbytes + t[5].hdmax.nbytes + 3 * t[5].jmin.nbytes + 4 * cfg.M
@@ -618,75 +724,12 @@ def filter_main(args):
     nsm = torch.cuda.get_device_properties(local_rank).multi_processor_count
     peak = nsm * 128 * sm_mhz * 1e6 / 1e9
     achieved = FILTER_OPS_PER_CELL[kind] * cells_step / (kernel_ms / 1e3) / 1e9
-    # CPU: the oracle on all host cores over a bounded sample of the same inputs
-    import oracle
-    oracle.lib()
-    cores = os.cpu_count() or 1
-    if kind == "f1-ssv":
-        units = [(int(o), int(j)) for o, _, j in wins]
-        one = lambda u: oracle.f1_msv_windows(M, prof.mat, prof.trans, maxl, mmu, mlam, buf, [u[0]], [u[1]], f1,
-                                              maxl) and u[1] * M
-    elif kind == "f2-vit":
-        units = [(int(o), int(j)) for o, _, j in wins]
-        one = lambda u: oracle.vit_score_batch(M, prof.mat, prof.trans, buf, [u[0]], [u[1]]) and u[1] * M
-    elif kind in ("trq-inside", "trq-cyk"):
-        units = list(range(len(wins)))
-        ttab = {"lmesc": tri.lmesc, "rmesc": tri.rmesc, "pty": tri.pty, "ilmesc": tri.ilmesc, "irmesc": tri.irmesc,
-                "ipty": tri.ipty, "lpos": tri.lpos, "rpos": tri.rpos, "clen": tri.clen}
-        def one(q):
-            o, i0, j0 = (int(x) for x in wins[q])
-            oracle.trq_scan(cfg, kind == "trq-inside", ttab, buf[o:o + j0 + 2], i0, j0, 0.0, True, trq_qdb, 4, True)
-            return int(per[j0 - i0 + 1][0])
-    elif kind == "hb-trcyk":
-        units = list(range(len(tasks)))
-        ttab = {"lmesc": tri.lmesc, "rmesc": tri.rmesc, "pty": tri.pty, "lpos": tri.lpos, "rpos": tri.rpos,
-                "clen": tri.clen}
-
-        def one(q):
-            o, i0, j0, ec, cut, b = tasks[q]
-            oracle.tr_hb_scan(cfg, False, ttab, valid, (b.jmin, b.jmax, b.hd_off, b.hdmin, b.hdmax),
-                              buf[o:o + j0 + 2], i0, j0, cut, True, 4, ec, True)
-            return int(np.maximum(b.hdmax - b.hdmin + 1, 0).sum())
-    else:
-        units = list(range(len(tasks)))
-
-        def one(q):
-            o, i0, j0, ec, cut, b = tasks[q]
-            oracle.hb_scan(cfg, kind == "hb-inside", (b.jmin, b.jmax, b.hd_off, b.hdmin, b.hdmax),
-                           buf[o:o + j0 + 2], i0, j0, ec, True, cut, True)
-            return int(np.maximum(b.hdmax - b.hdmin + 1, 0).sum())
-    order = [units[int(k)] for k in np.random.default_rng(7).permutation(len(units))]
-    lock = threading.Lock()
-    st = {"next": 0, "cells": 0}
-    deadline = time.perf_counter() + args.cpu_seconds
-
-    def worker():
-        while time.perf_counter() < deadline:
-            with lock:
-                if st["next"] >= len(order):
-                    return
-                u = order[st["next"]]
-                st["next"] += 1
-            c = one(u)
-            with lock:
-                st["cells"] += c
-    t0 = time.perf_counter()
-    with ThreadPoolExecutor(cores) as ex:
-        for _ in range(cores):
-            ex.submit(worker)
-    dt = time.perf_counter() - t0
-    cb = {"value": st["cells"] / dt / 1e9, "unit": "Gcells/s", "cores": cores, "kind": "port",
-          "sample": f"{st['next']} of {len(units)} units of one step's inputs, {dt:.1f} s on {cores} threads"}
-    metric = {"f1-ssv": "F1 SSV window scan Gcells/s", "f2-vit": "F2 Viterbi filter Gcells/s",
-              "hb-cyk": "HMM-banded CYK Gcells/s", "hb-inside": "HMM-banded Inside Gcells/s",
-              "hb-trcyk": "truncated HMM-banded CYK Gcells/s (band cells, 4 planes each)",
-              "trq-inside": "truncated non-banded TrInside Gcells/s (J-plane cells, 4 planes each)",
-              "trq-cyk": "truncated QDB TrCYK Gcells/s (J-plane cells, 4 planes each)"}[kind]
+    cb = cpu_sample(args.cpu_seconds)
+    metric = FILTER_METRIC[kind]
     line = {"metric": metric, "value": value, "unit": "Gcells/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": statistics.mean(times), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": {"f1-ssv": "u8 (packed s16x2)", "f2-vit": "i16", "hb-cyk": "f32", "hb-inside": "f32",
-                      "hb-trcyk": "f32", "trq-inside": "i32", "trq-cyk": "f32"}[kind],
+            "dtype": FILTER_DTYPE[kind],
             "data": "synthetic", "config": config,
             "e2e": {"value": e2e, "unit": "Gcells/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": None},
             "gpu_launches": launches,
