@@ -387,6 +387,12 @@ int cmgpu_tr_qdb_scan_batch(const cmgpu_model *m, void *stream, int semiring, in
                             const cmgpu_tr_tables *tt, int pass_idx, int do_null3, const uint8_t *dsq_all,
                             int64_t dsq_len, const cmgpu_window *wins, int32_t nwin, float cutoff,
                             cmgpu_trq_result *results, cmgpu_tr_hit *hits, int64_t cap, int64_t *n_out);
+/* Test hook for failure detection: in the next truncated QDB call the warp
+ * that runs column `column` (0-based within each window) never publishes its
+ * progress, so the next column's bounded wait runs out (about a second) and
+ * the call fails with CMGPU_EDEVICE instead of hanging; -1 clears it.  The
+ * model stays usable. */
+int cmgpu_tr_qdb_inject_stall(cmgpu_model *m, int32_t column);
 /* Device time, J-plane cells and launches of the last truncated QDB call. */
 int cmgpu_tr_qdb_stats(const cmgpu_model *m, double *kernel_ms, int64_t *cells, int32_t *launches);
 

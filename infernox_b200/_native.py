@@ -217,6 +217,7 @@ def lib() -> C.CDLL:
     L.cmgpu_tr_qdb_scan_batch.argtypes = [vp, vp, C.c_int, C.c_int, P(TrTables), C.c_int, C.c_int, vp, C.c_int64,
                                           vp, C.c_int32, C.c_float, vp, vp, C.c_int64, P(C.c_int64)]
     L.cmgpu_tr_qdb_stats.argtypes = [vp, P(C.c_double), P(C.c_int64), P(C.c_int32)]
+    L.cmgpu_tr_qdb_inject_stall.argtypes = [vp, C.c_int32]
     L.cmgpu_count_work.argtypes = [P(Cm), C.c_int, C.c_int, C.c_int32, P(C.c_double),
                                    P(C.c_double)]
     _lib = L
@@ -240,5 +241,5 @@ EXPORTED = [
     "cmgpu_msv_score_batch", "cmgpu_f1_msv_windows", "cmgpu_ssv_diagonals", "cmgpu_msv_filter_stats",
     "cmgpu_fast_cyk_scan_hb", "cmgpu_hb_scan_hits", "cmgpu_hb_scan_batch", "cmgpu_hb_stats",
     "cmgpu_tr_scan_hb", "cmgpu_tr_scan_hb_batch", "cmgpu_tr_qdb_scan", "cmgpu_tr_qdb_scan_batch",
-    "cmgpu_tr_qdb_stats",
+    "cmgpu_tr_qdb_stats", "cmgpu_tr_qdb_inject_stall",
 ]

@@ -75,6 +75,7 @@ struct TrqDev {
     double last_ms = 0;
     int64_t last_cells = 0;
     int32_t last_launches = 0;
+    int32_t stall_col = -1;  // test hook: this column never publishes its progress (next call only)
 };
 
 void trq_free(TrqDev *t) {
@@ -125,6 +126,7 @@ struct Tab {
     const uint16_t *ilog;
     int ilog_nz, M, W, nbegl, npbeg, nonbanded, fill_l, fill_r, fill_t;
     int nl, nc, nstep;  // levels, chunks, steps per column
+    int stall_col;      // test hook (-1 off): the column whose warp never publishes
 };
 
 template <bool INS>
@@ -610,7 +612,10 @@ __global__ void __launch_bounds__(THREADS) trq_kernel(Tab t, const Win *__restri
                                            ncand);
                     }
                 }
-                publish(&prog[wid], jj * S + sp + 1, lane);
+                if (jj != t.stall_col)
+                    publish(&prog[wid], jj * S + sp + 1, lane);
+                else
+                    __syncwarp();
             }
         }
         __syncthreads();
@@ -996,7 +1001,8 @@ int trq_batch(const cmgpu_model *mc, cudaStream_t st, int semiring, int qdbidx, 
     const trq::Tab tab{q->sttype, q->kind, q->cfirst, q->cnum, d_dx, q->begl_idx, d_pbeg, d_cuoff, d_iloff,
                        d_units, d_il, q->tsc[s], q->esc[s], d_lm, d_rm, d_pty, q->init_sc[s], d_base, m->ilog,
                        m->ilog_nz, M, W, nbk, (int)pbeg.size(), qdbidx == 0, fill_l, fill_r, fill_t,
-                       nl, NC, nstep};
+                       nl, NC, nstep, q->stall_col};
+    q->stall_col = -1;
     int64_t cap = std::max<int64_t>(4096 + 16 * (int64_t)nw, q->cand_hint);
     cudaEvent_t ev0, ev1;
     TRQ_TRY(cudaEventCreate(&ev0));
@@ -1122,6 +1128,15 @@ extern "C" int cmgpu_tr_qdb_scan(const cmgpu_model *m, int semiring, int qdbidx,
         return CMGPU_EOVERFLOW;
     }
     if (hits) std::copy(all.begin(), all.end(), hits);
+    return CMGPU_OK;
+}
+
+extern "C" int cmgpu_tr_qdb_inject_stall(cmgpu_model *m, int32_t column) {
+    if (!m || column < -1) return CMGPU_EINVAL;
+    TrqDev *q = nullptr;
+    int rc = trq_prepare(m, &q);
+    if (rc) return rc;
+    q->stall_col = column;
     return CMGPU_OK;
 }
 
