@@ -9,8 +9,9 @@
 //
 // Device side: one warp per window, rows i in order.  Model positions
 // k = 1..M are split into blocks of B = ceil(M/32) consecutive positions, lane
-// l owning block l; the rows of M, I and D live in shared memory with a
-// padded lane stride (conflict-free).  M and I cells read only the previous
+// l owning block l; the rows of M, I and D live in registers (B <= 8, i.e.
+// M <= 256) or, for longer models, in shared memory with a padded lane
+// stride (conflict-free).  M and I cells read only the previous
 // row; xE is a warp max.  D cells form a serial chain along k in the same row
 // (D(i,k) from M(i,k-1) and D(i,k-1)); each lane walks its block serially
 // from an incoming value and the warp repeats until no incoming value
@@ -257,6 +258,108 @@ __global__ void __launch_bounds__(256) vit_kernel(const int16_t *__restrict__ ta
     }
 }
 
+// The same recurrence with each lane's B (<= 8) cells of the M, I and D rows
+// held in registers instead of shared memory: identical operations in the
+// same order, with the neighbouring lane's last cell passed by shuffle.
+template <int BB>
+__global__ void __launch_bounds__(256) vit_kernel_reg(const int16_t *__restrict__ tab, int M, int base_w,
+                                                      int e_move, int e_loop, const uint8_t *__restrict__ dsq,
+                                                      const VitWin *__restrict__ wins, int nwin, int *out,
+                                                      uint8_t *status) {
+    extern __shared__ int vsm[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int tstride = M + 2;  // entries per table column (k = 0..M, padded)
+    int16_t *tabT = reinterpret_cast<int16_t *>(vsm);
+    for (int q = threadIdx.x; q < (M + 1) * 26; q += blockDim.x) {
+        const int k = q / 26, c = q - k * 26;
+        tabT[c * tstride + k] = tab[q];
+    }
+    __syncthreads();
+    auto T = [&](int c, int k) -> int { return tabT[c * tstride + k]; };
+    const int k0 = 1 + lane * BB;  // first position of this lane's block
+    const unsigned FULL = 0xffffffffu;
+    for (int w = blockIdx.x * nw + warp; w < nwin; w += gridDim.x * nw) {
+        const VitWin win = wins[w];
+        const uint8_t *frame = dsq + win.off;
+        int mv[BB], iv[BB], dv[BB];
+#pragma unroll
+        for (int b = 0; b < BB; b++) mv[b] = iv[b] = dv[b] = -32768;
+        int xn = base_w, xb = adds16(base_w, win.xw_move), xj = -32768, xc = -32768;
+        bool overflow = false;
+        for (int i = win.i0; i <= win.j0; i++) {
+            int x = frame[i];
+            x = x > 17 ? 17 : x;
+            // previous-row values at k0-1 (lane-1's last cell; -inf at k = 0)
+            int pm = __shfl_up_sync(FULL, mv[BB - 1], 1);
+            int pi = __shfl_up_sync(FULL, iv[BB - 1], 1);
+            int pd = __shfl_up_sync(FULL, dv[BB - 1], 1);
+            if (lane == 0) pm = pi = pd = -32768;
+            int xe = -32768;
+            int mn[BB], in[BB], dn[BB];
+#pragma unroll
+            for (int b = 0; b < BB; b++) {
+                const int k = k0 + b;
+                int vm = -32768, vi = -32768;
+                if (k <= M) {
+                    int sc = adds16(xb, T(18, k));
+                    sc = max(sc, adds16(pm, T(19, k - 1)));
+                    sc = max(sc, adds16(pi, T(20, k - 1)));
+                    sc = max(sc, adds16(pd, T(21, k - 1)));
+                    vm = adds16(sc, T(x, k));
+                    vi = max(adds16(mv[b], T(22, k)), adds16(iv[b], T(23, k)));
+                    xe = max(xe, vm);
+                }
+                pm = mv[b];
+                pi = iv[b];
+                pd = dv[b];
+                mn[b] = vm;
+                in[b] = vi;
+            }
+            for (int o = 16; o > 0; o >>= 1) xe = max(xe, __shfl_xor_sync(FULL, xe, o));
+            // D chain along k: d(k) = max(M(i,k-1)+MD(k-1), d(k-1)+DD(k-1))
+            int m_in = __shfl_up_sync(FULL, mn[BB - 1], 1);
+            if (lane == 0) m_in = -32768;
+            int din = -32768, din_prev = -32768;
+            for (int it = 0; it < 34; it++) {
+                int d = din, mprev = m_in;
+#pragma unroll
+                for (int b = 0; b < BB; b++) {
+                    const int k = k0 + b;
+                    int v = -32768;
+                    if (k <= M) v = max(adds16(mprev, T(24, k - 1)), adds16(d, T(25, k - 1)));
+                    dn[b] = v;
+                    d = v;
+                    mprev = mn[b];
+                }
+                const bool has = k0 <= M;
+                const int dlast = has ? d : -32768;
+                const bool same = !has || din == din_prev;
+                if (it > 0 && __all_sync(FULL, same)) break;
+                din_prev = din;
+                int up = __shfl_up_sync(FULL, dlast, 1);
+                din = lane == 0 ? -32768 : up;
+            }
+            if (xe >= 32767) {
+                overflow = true;
+                break;
+            }
+            xc = max(xc, adds16(xe, e_move));
+            xj = max(xj, adds16(xe, e_loop));
+            xb = max(adds16(xj, win.xw_move), adds16(xn, win.xw_move));
+#pragma unroll
+            for (int b = 0; b < BB; b++) {
+                mv[b] = mn[b];
+                iv[b] = in[b];
+                dv[b] = dn[b];
+            }
+        }
+        if (lane == 0) {
+            out[w] = xc;
+            status[w] = overflow ? 0 : 1;
+        }
+    }
+}
+
 }  // namespace dev
 }  // namespace cmx
 
@@ -378,12 +481,31 @@ extern "C" int cmgpu_vit_score_batch(const cmgpu_vit_filter *f, void *stream_ptr
         set_error(std::string("cmgpu_vit_score_batch: ") + cudaGetErrorString(e));
         return CMGPU_EDEVICE;
     }
+    // models up to 256 positions keep each lane's block of the rows in
+    // registers; longer ones use the shared-memory rows
+    auto launch_reg = [&](auto kern) {
+        const int g = (int)std::min<int64_t>((nwin + 7) / 8, (int64_t)sms * 8);
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tab_bytes);
+        kern<<<g, 256, tab_bytes, st>>>(f->d_tab, M, f->host.base_w, f->host.e_move, f->host.e_loop, d_dsq, d_w,
+                                        nwin, d_out, d_st);
+    };
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEventCreate(&ev0);
     cudaEventCreate(&ev1);
     cudaEventRecord(ev0, st);
-    dev::vit_kernel<<<grid, warps * 32, smem, st>>>(f->d_tab, M, f->host.base_w, f->host.e_move, f->host.e_loop,
-                                                  d_dsq, d_w, nwin, d_out, d_st);
+    switch (B) {
+    case 1: launch_reg(dev::vit_kernel_reg<1>); break;
+    case 2: launch_reg(dev::vit_kernel_reg<2>); break;
+    case 3: launch_reg(dev::vit_kernel_reg<3>); break;
+    case 4: launch_reg(dev::vit_kernel_reg<4>); break;
+    case 5: launch_reg(dev::vit_kernel_reg<5>); break;
+    case 6: launch_reg(dev::vit_kernel_reg<6>); break;
+    case 7: launch_reg(dev::vit_kernel_reg<7>); break;
+    case 8: launch_reg(dev::vit_kernel_reg<8>); break;
+    default:
+        dev::vit_kernel<<<grid, warps * 32, smem, st>>>(f->d_tab, M, f->host.base_w, f->host.e_move, f->host.e_loop,
+                                                      d_dsq, d_w, nwin, d_out, d_st);
+    }
     cudaEventRecord(ev1, st);
     if ((e = cudaGetLastError()) != cudaSuccess ||
         (e = cudaMemcpyAsync(out.data(), d_out, sizeof(int) * nwin, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
