@@ -11,7 +11,8 @@ reference's own properties (src/cm_dpsearch_trunc.rs):
   marginal emissions and penalties here are rounded stand-ins of the float
   ones, not Prob2Score of the marginal probabilities;
 * QDB bands never raise the non-banded TrCYK score (:2568-2581 restated for
-  the truncated scan).
+  the truncated scan);
+* the wide-band pins again in the local configuration, passes 2-5.
 The HB oracle restates tr_cyk_scan_hb / ftr_inside_scan_hb and the
 non-banded one generic_tr_scan; they share no code."""
 import numpy as np
@@ -69,3 +70,24 @@ def test_truncated_qdb_le_nonbanded(name):
         for q in (1, 2):
             _, vb, _, _ = oracle.trq_scan(g, False, tt, f, 1, L, -1e30, False, q, p, False)
             assert vb <= vn + 1e-6
+
+
+@pytest.mark.parametrize("name", ["trna", "small0", "small2", "mb3", "cfg2"])
+def test_wideband_equals_nonbanded_local(name):
+    """The same pins in the local configuration (local truncation rules,
+    local begins/ends), passes 5'-only, 3'-only, 5'-and-3' and 5'-and-3'-any:
+    TrCYK equal within 1e-4 with the same mode; float HB TrInside against the
+    integer non-banded TrInside with the same mode and within 0.5 bits (the
+    local tables carry more rounded stand-in terms than the global ones)."""
+    cm, g, l = models(name)
+    f, L = _window(cm, l, 5)
+    ones = np.ones(l.M, np.uint8)
+    for p in (2, 3, 4, 5):
+        tt = tr_tables(cm, l, p, True)
+        wb = as_tuple(wide_bands(l, 1, L))
+        _, vq, mq, _ = oracle.trq_scan(l, False, tt, f, 1, L, -1e30, False, 0, p, True)
+        _, vh, mh, _, _ = oracle.tr_hb_scan(l, False, tt, (ones,) * 4, wb, f, 1, L, -1e30, False, p, -1e30, True)
+        assert abs(vq - vh) < 1e-4 and mq == mh, (p, vq, vh, mq, mh)
+        _, vq, mq, _ = oracle.trq_scan(l, True, tt, f, 1, L, -1e30, False, 0, p, True)
+        _, vh, mh, _, _ = oracle.tr_hb_scan(l, True, tt, (ones,) * 4, wb, f, 1, L, -1e30, False, p, -1e30, True)
+        assert abs(vq - vh) < 0.5 and mq == mh, (p, vq, vh, mq, mh)
