@@ -7,9 +7,11 @@
 // with the best begin of every earlier column of the same parity), cells
 // outside a state's band keep what an earlier column left there, and the
 // BEGL decks are a ring over the last w+1 columns.  So one CTA runs one
-// window, column by column, on exactly the reference's layout in HBM:
-//   J/L/R/T planes [2][M][w+1] and BEGL decks J/L/R [w+1][nbegl][w+1],
-// with the d = 0 cells set once when the window starts.  The states are
+// window, in HBM, on the reference's cell layout -- J/L/R/T planes of M
+// state rows of w+1 cells per column, BEGL decks J/L/R of nbegl rows of w+1
+// cells per column -- with the d = 0 cells set once when the window starts
+// (the reference keeps two columns of planes and w+1 of BEGL decks; the
+// column pipeline below keeps more, see there).  The states are
 // grouped in dependency levels (one more than the deepest child; END states
 // are level 0).  Every read of a cell (v, d) of the current column is of a
 // lower level at d' <= d or of v's own cell d-1 (IL's self-loop); every read
@@ -53,7 +55,6 @@
 #include <climits>
 #include <cstring>
 #include <mutex>
-#include <numeric>
 #include <string>
 #include <vector>
 
