@@ -5,8 +5,8 @@
  * The library replaces the QDB-banded CYK / Inside window scanner of infernox
  * (src/cm_nohmm.rs) behind plain C entry points: POD structs, raw pointers and
  * sizes, int status codes, no exceptions and no torch types.  A Rust caller
- * binds these with an `extern "C"` block; the Python
- * package `infernox_b200` binds them with ctypes.
+ * binds these with an `extern "C"` block; the Python package `infernox_b200`
+ * binds them with ctypes.
  *
  * Conventions
  *   - Every entry point returns CMGPU_OK (0) or a negative CMGPU_E* code;
@@ -182,16 +182,18 @@ int cmgpu_qdb_scan(const cmgpu_model *m, cmgpu_workspace *ws, int semiring,
                    int32_t cap, int32_t *n_out);
 
 /* Window scan that allocates no device memory.  It has no counterpart in the
- * reference; it exists for callers that cannot call cudaMalloc during a scan:
- * code running while a stream is captured into a CUDA graph, services whose
- * device memory belongs to a framework's pool or budget, and latency-bound
- * loops that cannot afford an allocation and the synchronisation it implies.
- * Same arguments and results as cmgpu_qdb_scan, minus the workspace; stream
- * is a cudaStream_t (NULL: the default stream) and the call returns after the
- * scan has finished on it.  Its scratch -- a copy of the scan plan, the
- * residues, work items, counters, reportable cells and, when they do not fit
- * in shared memory, the decks -- lives in one 16 MiB `static __device__` array
- * that every GPU loading the library holds until the process exits.  Requests
+ * reference.  It serves callers that cannot call cudaMalloc or cudaFree: a
+ * process whose device memory belongs to a framework's caching allocator or
+ * to a fixed per-tenant budget, where a raw allocation fails or escapes the
+ * accounting, and a process running other streams on the GPU that cannot
+ * accept the device-wide synchronisation cudaFree implies.  Same arguments
+ * and results as cmgpu_qdb_scan, minus the workspace; stream is a
+ * cudaStream_t (NULL: the default stream).  The call waits for its stream
+ * and returns with the scan finished; the calling thread's current device is
+ * unchanged on return.  Its scratch -- a copy of the scan plan, the residues,
+ * work items, counters, reportable cells and, when they do not fit in shared
+ * memory, the decks -- lives in one 16 MiB `static __device__` array that
+ * every GPU loading the library holds until the process exits.  Requests
  * that do not fit return CMGPU_ENOSPACE.  The first call on a device looks up
  * the array's address (set-up), so make it before any stream capture.  All
  * calls on a device share the array: calls that overlap on the GPU race, so
@@ -390,7 +392,7 @@ int cmgpu_tr_qdb_scan_batch(const cmgpu_model *m, void *stream, int semiring, in
 /* Test hook for failure detection: in the next truncated QDB call the warp
  * that runs column `column` (0-based within each window) never publishes its
  * progress, so the next column's bounded wait runs out (about a second) and
- * the call fails with CMGPU_EDEVICE instead of hanging; -1 clears it.  The
+ * the call fails with CMGPU_ETIMEOUT instead of hanging; -1 clears it.  The
  * model stays usable. */
 int cmgpu_tr_qdb_inject_stall(cmgpu_model *m, int32_t column);
 /* Device time, J-plane cells and launches of the last truncated QDB call. */

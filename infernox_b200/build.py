@@ -18,7 +18,6 @@ NVCC_FLAGS = [
     "-lineinfo", "-O3", "-std=c++17",
     "-fmad=false",                      # no contraction in device float math
     "-Xcompiler", "-fPIC,-ffp-contract=off,-fno-fast-math",
-    "--shared",
 ]
 
 
@@ -33,14 +32,28 @@ def _stale() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compiles every source to an object file (in parallel), then links the
+    shared library; the objects live in a temporary folder."""
     if not force and not _stale():
         return LIB
+    import tempfile
+    from concurrent.futures import ThreadPoolExecutor
+
     os.makedirs(LIBDIR, exist_ok=True)
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc] + NVCC_FLAGS + ["-o", LIB + ".tmp"] + [os.path.join(CSRC, s) for s in SOURCES]
-    if verbose:
-        print(" ".join(cmd), file=sys.stderr)
-    subprocess.run(cmd, check=True)
+    with tempfile.TemporaryDirectory(prefix="cmscan_obj_") as tmp:
+        def compile_one(src: str) -> str:
+            obj = os.path.join(tmp, os.path.splitext(src)[0] + ".o")
+            cmd = [nvcc] + NVCC_FLAGS + ["-c", "-o", obj, os.path.join(CSRC, src)]
+            if verbose:
+                print(" ".join(cmd), file=sys.stderr)
+            subprocess.run(cmd, check=True)
+            return obj
+
+        with ThreadPoolExecutor(max_workers=min(len(SOURCES), os.cpu_count() or 1)) as ex:
+            objs = list(ex.map(compile_one, SOURCES))
+        cmd = [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "--shared", "-o", LIB + ".tmp"] + objs
+        subprocess.run(cmd, check=True)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

@@ -135,6 +135,9 @@ struct cmgpu_model {
     std::vector<float> flog;  // host FLogsum table for null3
     cmx::HbDev *hb = nullptr;  // built on the first HMM-banded scan
     cmx::TrqDev *trq = nullptr;  // built on the first truncated QDB / non-banded scan
+    // host-only scan plans of the allocation-free entry point (key semiring*8 + qdbidx)
+    mutable std::mutex noalloc_mu;
+    mutable std::map<int, std::unique_ptr<cmx::Plan>> noalloc_plans;
     ~cmgpu_model() {
         cudaFree(ilog);
         cmx::hb_free(hb);

@@ -1,13 +1,13 @@
 // cmgpu_qdb_scan_noalloc: the window scan of cmgpu_qdb_scan for callers that
 // must not allocate device memory.
 //
-// Who needs it: code that runs where cudaMalloc is off limits -- inside a
-// region that is being captured into a CUDA graph (an allocation there either
-// fails or breaks the capture), in a service whose device memory is owned by
-// a framework's memory pool or budget that forbids raw allocations, or in a
-// latency-bound loop that cannot pay for cudaMalloc/cudaFree and the device
-// synchronisation they imply.  The regular entry points grow per-workspace
-// buffers with cudaMalloc; this one never does.
+// Who needs it: a process whose device memory is owned by someone else -- a
+// framework's caching allocator that has reserved most of the GPU, or a
+// server that gives each tenant a fixed device-memory budget -- where a raw
+// cudaMalloc fails or escapes the accounting; and a process that runs other
+// streams on the same GPU and cannot accept the device-wide synchronisation
+// that cudaFree implies.  The regular entry points grow per-workspace
+// buffers with cudaMalloc and cudaFree; this one never calls either.
 //
 // Where its scratch lives: one file-scope `static __device__` array of
 // NOALLOC_SCRATCH_BYTES (16 MiB).  Every GPU that loads this library reserves
@@ -18,9 +18,14 @@
 // request that does not fit is rejected with CMGPU_ENOSPACE before any copy.
 //
 // Set-up: the host needs the array's device address (its name in host code
-// is only a host-side stand-in).  The first call on a device makes that device
-// current and looks the address up once with cudaGetSymbolAddress; that first
-// call should therefore come before any stream capture begins.
+// is only a host-side stand-in).  The first call on a device looks the
+// address up once with cudaGetSymbolAddress, with that device current; make
+// that first call before any stream capture begins.
+//
+// Blocking: the call copies its inputs, launches the scan and waits for its
+// stream (it reads the cell count back to size the result), so it returns
+// with the scan finished.  The calling thread's current device is the same on
+// return as on entry.
 //
 // Sharing: all calls on one device use the same array, which keeps whatever
 // the previous call left there.  The counters are cleared on every call and
@@ -65,6 +70,34 @@ static int noalloc_scratch(int device, unsigned char **out) {
     }
     *out = g_noalloc_ptr[device];
     return CMGPU_OK;
+}
+
+// Makes `device` current for the life of the guard and restores the caller's
+// current device afterwards.
+struct DeviceGuard {
+    int prev = -1;
+    cudaError_t err = cudaSuccess;
+    explicit DeviceGuard(int device) {
+        err = cudaGetDevice(&prev);
+        if (err == cudaSuccess && prev != device) err = cudaSetDevice(device);
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+// The model's host scan plan for (semiring, qdbidx), built on first use and
+// kept with the model (host memory only).
+static const Plan *noalloc_plan(const cmgpu_model *m, int semiring, int qdbidx) {
+    std::lock_guard<std::mutex> lk(m->noalloc_mu);
+    const int key = semiring * 8 + qdbidx;
+    auto it = m->noalloc_plans.find(key);
+    if (it != m->noalloc_plans.end()) return it->second.get();
+    std::unique_ptr<Plan> pl(new Plan());
+    if (!build_plan(&m->cm.view, semiring, qdbidx, *pl)) return nullptr;
+    const Plan *out = pl.get();
+    m->noalloc_plans[key] = std::move(pl);
+    return out;
 }
 
 // Bump allocator over a region of the scratch array (offsets only; nothing
@@ -112,14 +145,19 @@ extern "C" int cmgpu_qdb_scan_noalloc(const cmgpu_model *m, void *stream_ptr, in
         }
     if (j0 < i0) return CMGPU_OK;
     cudaStream_t st = (cudaStream_t)stream_ptr;
-    NA_TRY(cudaSetDevice(m->device));
+    DeviceGuard dg(m->device);
+    NA_TRY(dg.err);
     unsigned char *scratch = nullptr;
     int rc = noalloc_scratch(m->device, &scratch);
     if (rc) return rc;
 
-    // scan plan, built on the host and copied into the scratch array
-    Plan pl;
-    if (!build_plan(&m->cm.view, semiring, qdbidx, pl)) return CMGPU_EINVAL;
+    // scan plan: built on the host once per model, copied into the scratch array
+    const Plan *plp = noalloc_plan(m, semiring, qdbidx);
+    if (!plp) {
+        set_error(std::string("cmgpu_qdb_scan_noalloc: scan plan: ") + cmgpu_last_error());
+        return CMGPU_EINVAL;
+    }
+    const Plan &pl = *plp;
     const int W = pl.W;
 
     // work items: the window in pieces of `chunk` reported columns

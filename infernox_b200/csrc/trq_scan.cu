@@ -1033,7 +1033,7 @@ int trq_batch(const cmgpu_model *mc, cudaStream_t st, int semiring, int qdbidx, 
             cudaEventDestroy(ev0);
             cudaEventDestroy(ev1);
             set_error("truncated QDB scan: a column wait of the kernel timed out");
-            return CMGPU_EDEVICE;
+            return CMGPU_ETIMEOUT;
         }
         float ms = 0;
         cudaEventElapsedTime(&ms, ev0, ev1);

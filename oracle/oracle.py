@@ -27,12 +27,24 @@ def build() -> str:
     return LIB_PATH
 
 
+def use_native() -> str:
+    """Load the -march=native build (the timed CPU baseline) instead of the
+    portable one; builds it on this machine.  Call before the first lib()."""
+    global LIB_PATH
+    if _lib is not None:
+        raise RuntimeError("oracle.use_native() must come before the first oracle call")
+    subprocess.run(["make", "-s", "-C", HERE, "native"], check=True)
+    LIB_PATH = os.path.join(HERE, "_build_native", "liboracle.so")
+    return LIB_PATH
+
+
 def lib():
     global _lib
     if _lib is None:
         srcs = [os.path.join(HERE, f) for f in ("qdb_oracle.c", "hb_oracle.c", "tr_oracle.c", "trq_oracle.c", "p7_oracle.c", "msv_oracle.c")]
         if not os.path.exists(LIB_PATH) or any(os.path.getmtime(LIB_PATH) < os.path.getmtime(f) for f in srcs):
-            build()
+            native = os.path.basename(os.path.dirname(LIB_PATH)) == "_build_native"
+            subprocess.run(["make", "-s", "-C", HERE] + (["native"] if native else []), check=True)
         L = C.CDLL(LIB_PATH)
         vp = C.c_void_p
         P = C.POINTER

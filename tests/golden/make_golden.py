@@ -4,12 +4,12 @@
   reference's own unit tests, parsed from its sources (src/cp9.rs tests
   `ilogsum_sentinel_and_bounds`, `ilogsum_table_matches_c_dump`,
   `ilogsum_table_endpoints_match_c_formula`; src/cm_qdband.rs
-  `test_state_delta`).  Needs the reference checkout (REFERENCE_ROOT, default
-  /root/reference); run it only where that exists.
+  `test_state_delta`).  Needs the reference checkout: set REFERENCE_ROOT to
+  its path; run it only where that exists.
 * scan_small.json: the oracle's hits on one fixed seeded model and sequence,
   a regression lock for the oracle itself.
 
-Usage: python tests/golden/make_golden.py
+Usage: REFERENCE_ROOT=<reference checkout> python tests/golden/make_golden.py
 """
 import json
 import os
@@ -18,7 +18,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("REFERENCE_ROOT", "/root/reference")
+REF = os.environ.get("REFERENCE_ROOT")
 
 
 def ilogsum_kats():
@@ -68,7 +68,9 @@ def scan_small():
 
 
 def main():
-    if os.path.isdir(REF):
+    if not REF or not os.path.isdir(REF):
+        print("REFERENCE_ROOT is not set to a reference checkout: only scan_small.json is regenerated")
+    else:
         with open(os.path.join(HERE, "ilogsum_kat.json"), "w") as f:
             json.dump(ilogsum_kats(), f, indent=1)
         with open(os.path.join(HERE, "state_delta_kat.json"), "w") as f:

@@ -52,4 +52,3 @@ def test_bad_arguments_are_rejected_without_gpu():
     assert L.cmgpu_prep_configure(None, 0, 0, 1e-7, 1e-15, 1e-7, None) == -1
     m = C.c_void_p()
     assert L.cmgpu_model_upload(None, 0, C.byref(m)) == -1
-    assert L.cmgpu_set_shape if False else True

@@ -145,7 +145,7 @@ def test_trq_edge_windows_and_passes(name, loc, qdb):
 def test_trq_column_wait_times_out_and_reports():
     """Failure detection without a GPU fault: the warp of one column never
     publishes its progress (the test hook), the next column's bounded wait
-    runs out, the call fails with CMGPU_EDEVICE, and the model scans
+    runs out, the call fails with CMGPU_ETIMEOUT, and the model scans
     correctly afterwards."""
     cm, g, l = models("small2")
     sc = Scanner(l)
@@ -153,6 +153,7 @@ def test_trq_column_wait_times_out_and_reports():
     f, i0, j0 = truncated_window(cm, l, 4, 77, max_len=l.W + 10, flank=60)
     assert j0 - i0 + 1 > 12
     N.check(N.lib().cmgpu_tr_qdb_inject_stall(sc._model, 3))
-    with pytest.raises(N.CmgpuError, match="timed out"):
+    with pytest.raises(N.CmgpuError, match="timed out") as ei:
         ref_tr_cyk_scan(sc, tri_of(tt, True), f, i0, j0, -5.0, N.NOQDB, True, 4)
+    assert ei.value.rc == -6  # CMGPU_ETIMEOUT
     check(l, sc, tt, True, f, i0, j0, N.NOQDB, 4, -5.0, True, "after a timeout")

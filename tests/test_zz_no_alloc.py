@@ -1,13 +1,14 @@
 """The allocation-free window scan (cmgpu_qdb_scan_noalloc) against the
 regular one (cmgpu_qdb_scan), through the C ABI.
 
-The no-allocation entry point serves callers that may not call cudaMalloc
-while they scan (graph capture, pooled or budgeted device memory, tight
-latency loops); it keeps its scratch in a fixed 16 MiB device array shared by
-every call on a GPU.  Its hits must equal the regular entry point's exactly,
-and two calls in a row must not see each other's leftovers.  This file is
-collected last so that a run stopping at the first failure has run every
-other test first.
+The no-allocation entry point serves callers that cannot call cudaMalloc or
+cudaFree while they scan: processes whose device memory belongs to a
+framework's caching allocator or a fixed budget, and processes running other
+streams that cannot accept the device-wide synchronisation of cudaFree.  It
+keeps its scratch in a fixed 16 MiB device array shared by every call on a
+GPU.  Its hits must equal the regular entry point's exactly, and two calls in
+a row must not see each other's leftovers.  This file is collected last so
+that a run stopping at the first failure has run every other test first.
 """
 import ctypes as C
 
@@ -51,10 +52,24 @@ def test_noalloc_matches_regular_scan_two_calls_in_a_row():
     assert got2 == regular_scan(sc, CYK_F32, QDB1, b, 101, 2900, 0.0, True) and got2
 
 
+def one_lane_fits_in_smem(cfg, semiring, band) -> bool:
+    """Whether one work item's decks fit in shared memory: the criterion both
+    the regular path (with one lane forced) and the no-allocation path use."""
+    sc = Scanner(cfg)
+    try:
+        sc.set_shape(1, 512, 0, 1)
+        dsq = np.concatenate([[255], np.zeros(300, np.uint8), [255]]).astype(np.uint8)
+        sc.generic_scan(semiring, band, dsq, 1, 300, 1e9, False)
+        return bool(sc.stats()["deck_in_smem"])
+    finally:
+        sc.close()
+
+
 def test_noalloc_global_decks_two_calls_in_a_row():
     """A model whose non-banded decks do not fit in shared memory: the decks
     live in the static array; the second call must not see the first's."""
     cm, g, l = models("cfg2")
+    assert not one_lane_fits_in_smem(l, INSIDE_I32, NOQDB), "this case must take the global-deck branch"
     sc = Scanner(l)
     a = frame(planted_seq(cm, 1500, 0.45, 2, seed=903))
     for _ in range(2):
