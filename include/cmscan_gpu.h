@@ -134,7 +134,18 @@ typedef struct cmgpu_stats {
     int32_t deck_in_smem; /* 1 when the rolling decks live in shared memory */
     int32_t ctas;
     int32_t lanes;        /* work items per CTA                            */
+    int32_t kernel;       /* CMGPU_KERNEL_LEVEL or CMGPU_KERNEL_SWEEP       */
 } cmgpu_stats;
+
+/* Scan kernels of the QDB scanner (cmgpu_workspace_set_kernel).  Both give
+ * the same results.  LEVEL: one CTA scans up to 16 work items side by side,
+ * state by state in dependency levels with CTA barriers (qdb_scan.cu).
+ * SWEEP: one warp scans one work item node by node with no CTA barrier
+ * (sweep_scan.cu); it needs W <= 255 and the node-local state topology of
+ * CMs built by cmbuild.  AUTO picks SWEEP where it applies. */
+#define CMGPU_KERNEL_AUTO 0
+#define CMGPU_KERNEL_LEVEL 1
+#define CMGPU_KERNEL_SWEEP 2
 
 typedef struct cmgpu_model cmgpu_model;
 typedef struct cmgpu_workspace cmgpu_workspace;
@@ -171,6 +182,11 @@ int cmgpu_workspace_stats(const cmgpu_workspace *ws, cmgpu_stats *out);
  * scanned side by side per CTA (1..8). */
 int cmgpu_workspace_set_shape(cmgpu_workspace *ws, int ctas_per_sm, int threads, int chunk,
                               int lanes);
+/* Kernel choice for the scans of this workspace (CMGPU_KERNEL_*).  A scan
+ * with CMGPU_KERNEL_SWEEP on a model outside that kernel's scope fails with
+ * CMGPU_EINVAL.  With SWEEP, set_shape's `lanes` is the warps per CTA (1..12)
+ * and `chunk` the residues per work item. */
+int cmgpu_workspace_set_kernel(cmgpu_workspace *ws, int kernel);
 
 /* ---- scanner entry points ----------------------------------------------- */
 

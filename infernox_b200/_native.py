@@ -18,6 +18,7 @@ CMGPU_OK = 0
 CMGPU_EOVERFLOW = -4
 CYK_F32, INSIDE_I32, INSIDE_F32 = 0, 1, 2
 NOQDB, QDB1, QDB2 = 0, 1, 2
+KERNEL_AUTO, KERNEL_LEVEL, KERNEL_SWEEP = 0, 1, 2
 
 P = C.POINTER
 
@@ -126,6 +127,7 @@ class Stats(C.Structure):
         ("work_items", C.c_int64), ("candidates", C.c_int64),
         ("kernel_ms", C.c_float), ("kernel_launches", C.c_int32),
         ("deck_in_smem", C.c_int32), ("ctas", C.c_int32), ("lanes", C.c_int32),
+        ("kernel", C.c_int32),
     ]
 
 
@@ -165,6 +167,7 @@ def lib() -> C.CDLL:
     L.cmgpu_workspace_free.restype = None
     L.cmgpu_workspace_stats.argtypes = [vp, P(Stats)]
     L.cmgpu_workspace_set_shape.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int]
+    L.cmgpu_workspace_set_kernel.argtypes = [vp, C.c_int]
     L.cmgpu_qdb_scan.argtypes = [vp, vp, C.c_int, C.c_int, P(C.c_uint8), C.c_int32, C.c_int32,
                                  C.c_int32, C.c_float, C.c_int, vp, C.c_int32, P(C.c_int32)]
     L.cmgpu_qdb_scan_noalloc.argtypes = [vp, vp, C.c_int, C.c_int, P(C.c_uint8), C.c_int32, C.c_int32,
@@ -233,7 +236,7 @@ def check(rc: int) -> None:
 EXPORTED = [
     "cmgpu_last_error", "cmgpu_version", "cmgpu_prep_configure", "cmgpu_ilogsum_table",
     "cmgpu_flogsum_table", "cmgpu_model_upload", "cmgpu_model_free", "cmgpu_workspace_create",
-    "cmgpu_workspace_free", "cmgpu_workspace_stats", "cmgpu_workspace_set_shape",
+    "cmgpu_workspace_free", "cmgpu_workspace_stats", "cmgpu_workspace_set_shape", "cmgpu_workspace_set_kernel",
     "cmgpu_qdb_scan", "cmgpu_qdb_scan_noalloc", "cmgpu_qdb_scan_cells", "cmgpu_cyk_seq_filter", "cmgpu_final_stage_inside_opt",
     "cmgpu_scan_batch", "cmgpu_scan_batch_device", "cmgpu_scan_plain", "cmgpu_count_work",
     "cmgpu_vit_filter_build", "cmgpu_vit_filter_free", "cmgpu_vit_filter_tables", "cmgpu_vit_score_batch",

@@ -27,6 +27,7 @@
 #include "model_internal.h"
 #include "qdb_kernel.h"
 #include "qdb_plan.h"
+#include "sweep_kernel.h"
 
 namespace cmx {
 
@@ -72,6 +73,8 @@ struct cmgpu_workspace {
     int *d_counters = nullptr;  // [0] next item, [1] candidate count
     uint32_t *d_deck = nullptr;
     size_t deck_cap = 0;  // elements
+    uint32_t *d_sweep = nullptr;  // node-sweep kernel: per-warp decks and BEGL rings
+    size_t sweep_cap = 0;         // elements
     // host staging
     Cand *h_cands = nullptr;
     size_t h_cands_cap = 0;
@@ -81,6 +84,7 @@ struct cmgpu_workspace {
     int ctas_per_sm = 0;  // 0 = tuned
     int chunk = 0;        // 0 = auto
     int lanes = 0;        // 0 = tuned
+    int kernel = 0;       // CMGPU_KERNEL_*
     int sm_count = 148;
     cmgpu_stats stats{};
     ~cmgpu_workspace() {
@@ -89,6 +93,7 @@ struct cmgpu_workspace {
         cudaFree(d_cands);
         cudaFree(d_counters);
         cudaFree(d_deck);
+        cudaFree(d_sweep);
         cudaFreeHost(h_cands);
         cudaFreeHost(h_counters);
         if (ev0) cudaEventDestroy(ev0);
@@ -127,6 +132,22 @@ static int get_plan(cmgpu_model *m, int semiring, int qdbidx, DevPlan **out) {
     if ((rc = upload_vec(&dp->esc, p.esc))) return rc;
     if ((rc = upload_vec(&dp->el_sca, p.el_sca))) return rc;
     if ((rc = upload_vec(&dp->esc_c, p.esc_c))) return rc;
+    // node-sweep plan
+    {
+        std::string why;
+        dp->sw_ok = build_sweep_plan(&m->cm.view, p, qdbidx, dp->sw, &why);
+        dp->sw_why = why;
+        if ((rc = upload_vec(&dp->init0, p.init0))) return rc;
+        if (dp->sw_ok) {
+            std::vector<uint8_t> kid = dp->sw.kid;
+            kid.resize((kid.size() + 3) & ~(size_t)3, 0);
+            if ((rc = upload_vec(&dp->sw_st, dp->sw.st))) return rc;
+            if ((rc = upload_vec(&dp->sw_kid, kid))) return rc;
+            if ((rc = upload_vec(&dp->sw_nodes, dp->sw.nodes))) return rc;
+            if ((rc = upload_vec(&dp->sw_io, dp->sw.io))) return rc;
+            if ((rc = upload_vec(&dp->sw_bifs, dp->sw.bifs))) return rc;
+        }
+    }
     // per-column work counts by row limit
     const int W = p.W;
     dp->cells_prefix.assign(W + 1, 0.0);
@@ -367,21 +388,75 @@ static int run_scan(cmgpu_model *m, cmgpu_workspace *ws, int semiring, int qdbid
     sp.dsq = d_dsq;
     sp.cutoff = cutoff;
 
-    // launch shape: lanes (work items per CTA) x CTAs per SM.  Decks go to
-    // shared memory when at least 3 lanes fit per SM; otherwise to global
-    // memory (L2-resident) with 8 lanes per CTA, which keeps more
-    // independent work in flight per SM.
-    const int threads = ws->threads;
+    // kernel choice
+    if (ws->kernel == CMGPU_KERNEL_SWEEP && !dp->sw_ok) {
+        set_error("node-sweep kernel does not apply to this model: " + dp->sw_why);
+        return CMGPU_EINVAL;
+    }
+    const bool sweep = dp->sw_ok && ws->kernel != CMGPU_KERNEL_LEVEL;
     const size_t SMEM_CAP = 227 * 1024 - 1024, SM_CAP = 228 * 1024;
+    const int threads = ws->threads;
     int best_c = 0, best_l = 0;
     bool deck_smem = false;
-    auto occ_for = [&](int l, bool smem_deck) {
-        sp.lanes = l;
-        sp.deck_smem = smem_deck ? 1 : 0;
-        sp.lay = scan_layout(sp, l, smem_deck);
-        return scan_occupancy(sp, threads);
-    };
-    if (!plain) {
+    SweepParams swp{};
+    if (sweep) {
+        // one CTA per SM with as many warps (one work item each) as fit
+        const SweepPlan &sw = dp->sw;
+        swp.st = dp->sw_st;
+        swp.kid = dp->sw_kid;
+        swp.nodes = dp->sw_nodes;
+        swp.io = dp->sw_io;
+        swp.bifs = dp->sw_bifs;
+        swp.tsc = dp->tsc;
+        swp.endsc = dp->endsc;
+        swp.init0 = dp->init0;
+        swp.bsv = dp->beginsc_all;
+        swp.esc = dp->esc;
+        swp.esc_c = dp->esc_c;
+        swp.el_sca = dp->el_sca;
+        swp.ilog = m->ilog;
+        swp.ilog_nz = m->ilog_nz;
+        swp.M = pl.M;
+        swp.W = pl.W;
+        swp.S = sw.S;
+        swp.RW = sw.RW;
+        swp.nnodes = (int)sw.nodes.size();
+        swp.nio = (int)sw.io.size();
+        swp.nbif = (int)sw.bifs.size();
+        swp.n_esc_c = (int)pl.esc_c.size();
+        swp.local = pl.local ? 1 : 0;
+        swp.inside = sp.inside;
+        swp.dsq = d_dsq;
+        swp.cutoff = cutoff;
+        swp.deck_words = sw.deck_words;
+        swp.gstride = ((sw.deck_words + sw.ring_words) + 63) & ~(int64_t)63;
+        const int wmax = ws->lanes > 0 ? std::min(ws->lanes, SW_MAX_WARPS) : SW_MAX_WARPS;
+        for (int w = wmax; w >= 1; w--) {
+            swp.warps = w;
+            swp.lay = sweep_layout(swp, w);
+            if ((size_t)swp.lay.words * 4 > SMEM_CAP) continue;
+            if (sweep_occupancy(swp, w * 32) < 1) continue;
+            best_l = w;
+            break;
+        }
+        if (best_l < 1) {
+            set_error("node-sweep kernel: the model tables leave no room for a warp in shared memory");
+            return CMGPU_EDEVICE;
+        }
+        swp.warps = best_l;
+        swp.lay = sweep_layout(swp, best_l);
+        best_c = 1;
+    } else {
+        // launch shape: lanes (work items per CTA) x CTAs per SM.  Decks go to
+        // shared memory when at least 3 lanes fit per SM; otherwise to global
+        // memory (L2-resident) with 8 lanes per CTA, which keeps more
+        // independent work in flight per SM.
+        auto occ_for = [&](int l, bool smem_deck) {
+            sp.lanes = l;
+            sp.deck_smem = smem_deck ? 1 : 0;
+            sp.lay = scan_layout(sp, l, smem_deck);
+            return scan_occupancy(sp, threads);
+        };
         for (int c = 1; c <= 4; c++) {
             if (ws->ctas_per_sm > 0 && c != ws->ctas_per_sm) continue;
             size_t cap = std::min(SMEM_CAP, SM_CAP / c - 1024);
@@ -397,55 +472,58 @@ static int run_scan(cmgpu_model *m, cmgpu_workspace *ws, int semiring, int qdbid
         }
         bool forced = ws->lanes > 0 || ws->ctas_per_sm > 0;
         if (best_c * best_l < 3 && !(forced && best_c > 0)) best_c = 0;
-    } else if ((size_t)scan_layout(sp, 1, true).words * 4 <= SMEM_CAP) {
-        best_c = 1;
-        best_l = 1;
+        if (best_c > 0) {
+            deck_smem = true;
+        } else {
+            best_l = ws->lanes > 0 ? ws->lanes : MAX_LANES;
+            best_c = ws->ctas_per_sm > 0 ? ws->ctas_per_sm : 1;
+        }
+        int occ = occ_for(best_l, deck_smem);
+        if (occ < 1) {
+            set_error("scan kernel cannot be resident with this shape");
+            return CMGPU_EDEVICE;
+        }
+        best_c = std::min(best_c, occ);
     }
-    if (best_c > 0) {
-        deck_smem = true;
-    } else {
-        best_l = plain ? 1 : (ws->lanes > 0 ? ws->lanes : MAX_LANES);
-        best_c = ws->ctas_per_sm > 0 ? ws->ctas_per_sm : 1;
-    }
-    int occ = occ_for(best_l, deck_smem);
-    if (occ < 1) {
-        set_error("scan kernel cannot be resident with this shape");
-        return CMGPU_EDEVICE;
-    }
-    int per_sm = std::min(best_c, occ);
-    int max_ctas = ws->sm_count * per_sm;
+    const int max_ctas = ws->sm_count * best_c;
 
-    // work items
+    // work items: pieces of `chunk` reported columns plus W-1 warm-up columns.
+    // The batch shares one cost-ordered queue; the plain comparator launches
+    // once per window over that window's own pieces.
     std::vector<WorkItem> items;
+    std::vector<size_t> win_first;  // plain: first item of each window
     int64_t total_cols = 0;
     for (auto &w : wins) total_cols += std::max<int64_t>(0, (int64_t)w.j0 - w.i0 + 1);
     const int W = pl.W;
-    int64_t chunk = ws->chunk;
-    if (chunk <= 0) {
-        // about four items per lane slot, but no piece shorter than 2W (the
-        // W-1 warm-up columns are overhead) and none longer than 32768
-        chunk = total_cols / std::max<int64_t>(1, (int64_t)max_ctas * best_l * 4);
-        chunk = std::max<int64_t>(chunk, 2 * (int64_t)W);
-        chunk = std::min<int64_t>(chunk, 32768);
-    }
+    auto chunk_for = [&](int64_t cols) -> int64_t {
+        int64_t chunk = ws->chunk;
+        if (chunk <= 0) {
+            // about four items per lane slot, but no piece shorter than 2W (the
+            // W-1 warm-up columns are overhead) and none longer than 32768
+            chunk = cols / std::max<int64_t>(1, (int64_t)max_ctas * best_l * 4);
+            chunk = std::max<int64_t>(chunk, 2 * (int64_t)W);
+            chunk = std::min<int64_t>(chunk, 32768);
+        }
+        return chunk;
+    };
+    const int64_t batch_chunk = chunk_for(total_cols);
     for (size_t wi = 0; wi < wins.size(); wi++) {
         const WinDesc &w = wins[wi];
+        win_first.push_back(items.size());
         if (w.j0 < w.i0) continue;
         double c = 0, t = 0;
         window_work(dp, (int64_t)w.j0 - w.i0 + 1, c, t);
         ws->stats.cells += c;
         ws->stats.terms += t;
         ws->stats.residues += (double)w.j0 - w.i0 + 1;
-        if (plain) {
-            items.push_back(WorkItem{w.off, w.i0, w.j0, w.i0, (int32_t)wi});
-            continue;
-        }
+        const int64_t chunk = plain ? chunk_for((int64_t)w.j0 - w.i0 + 1) : batch_chunk;
         for (int64_t r0 = w.i0; r0 <= w.j0; r0 += chunk) {
             int64_t r1 = std::min<int64_t>(w.j0, r0 + chunk - 1);
             int64_t js = std::max<int64_t>(w.i0, r0 - (W - 1));
             items.push_back(WorkItem{w.off, (int32_t)js, (int32_t)r1, (int32_t)r0, (int32_t)wi});
         }
     }
+    win_first.push_back(items.size());
     if (!plain)
         std::stable_sort(items.begin(), items.end(), [](const WorkItem &a, const WorkItem &b) {
             return (a.jend - a.jstart) > (b.jend - b.jstart);
@@ -453,6 +531,7 @@ static int run_scan(cmgpu_model *m, cmgpu_workspace *ws, int semiring, int qdbid
     ws->stats.work_items = (int64_t)items.size();
     ws->stats.deck_in_smem = deck_smem ? 1 : 0;
     ws->stats.lanes = best_l;
+    ws->stats.kernel = sweep ? CMGPU_KERNEL_SWEEP : CMGPU_KERNEL_LEVEL;
     if (items.empty()) return CMGPU_OK;
 
     if ((rc = ensure_dev(&ws->d_items, &ws->items_cap, items.size()))) return rc;
@@ -460,38 +539,58 @@ static int run_scan(cmgpu_model *m, cmgpu_workspace *ws, int semiring, int qdbid
                              ws->stream));
     size_t cand_cap = std::max<size_t>(ws->cands_cap, 1 << 16);
     if ((rc = ensure_dev(&ws->d_cands, &ws->cands_cap, cand_cap))) return rc;
-    int ctas = plain ? 1 : (int)std::min<int64_t>(((int64_t)items.size() + best_l - 1) / best_l, max_ctas);
+    const int ctas = (int)std::min<int64_t>(((int64_t)items.size() + best_l - 1) / best_l, max_ctas);
     ws->stats.ctas = ctas;
-    if (!deck_smem) {
+    if (sweep) {
+        if ((rc = ensure_dev(&ws->d_sweep, &ws->sweep_cap, (size_t)swp.gstride * (size_t)ctas * (size_t)best_l)))
+            return rc;
+        swp.gmem = ws->d_sweep;
+        swp.next_item = ws->d_counters;
+        swp.cand_count = ws->d_counters + 1;
+    } else if (!deck_smem) {
         size_t stride = ((size_t)pl.deck_elems + 31) & ~(size_t)31;
         if ((rc = ensure_dev(&ws->d_deck, &ws->deck_cap, stride * (size_t)ctas * (size_t)best_l))) return rc;
         sp.deck_global = ws->d_deck;
         sp.deck_stride = (int64_t)stride;
     }
-    sp.items = ws->d_items;
     sp.next_item = ws->d_counters;
     sp.cand_count = ws->d_counters + 1;
 
-    size_t ncand = 0;
-    for (int attempt = 0; attempt < 3; attempt++) {
+    // one launch over items [first, first + n) on `grid` CTAs
+    auto launch = [&](size_t first, size_t n, int grid) -> cudaError_t {
+        if (sweep) {
+            swp.items = ws->d_items + first;
+            swp.nitems = (int)n;
+            swp.item_base = (int)first;
+            swp.cands = ws->d_cands;
+            swp.cand_cap = (int)std::min<size_t>(ws->cands_cap, (size_t)INT32_MAX);
+            return sweep_launch(swp, grid, ws->stream);
+        }
+        sp.items = ws->d_items + first;
+        sp.nitems = (int)n;
+        sp.item_base = (int)first;
         sp.cands = ws->d_cands;
         sp.cand_cap = (int)std::min<size_t>(ws->cands_cap, (size_t)INT32_MAX);
+        return scan_launch(sp, grid, threads, ws->stream);
+    };
+    size_t ncand = 0;
+    for (int attempt = 0; attempt < 3; attempt++) {
         CUDA_TRY(cudaMemsetAsync(ws->d_counters, 0, 2 * sizeof(int), ws->stream));
         CUDA_TRY(cudaEventRecord(ws->ev0, ws->stream));
         if (plain) {
-            // one launch per window, one CTA: the per-window comparator
-            for (size_t k = 0; k < items.size(); k++) {
-                sp.items = ws->d_items + k;
-                sp.nitems = 1;
-                sp.item_base = (int)k;
+            // one launch per window over its own pieces: the per-window comparator
+            int launches = 0;
+            for (size_t w = 0; w + 1 < win_first.size(); w++) {
+                size_t f = win_first[w], n = win_first[w + 1] - f;
+                if (n == 0) continue;
+                int grid = (int)std::min<int64_t>(((int64_t)n + best_l - 1) / best_l, max_ctas);
                 CUDA_TRY(cudaMemsetAsync(ws->d_counters, 0, sizeof(int), ws->stream));
-                CUDA_TRY(scan_launch(sp, 1, threads, ws->stream));
+                CUDA_TRY(launch(f, n, grid));
+                launches++;
             }
-            ws->stats.kernel_launches = (int)items.size();
+            ws->stats.kernel_launches = launches;
         } else {
-            sp.nitems = (int)items.size();
-            sp.item_base = 0;
-            CUDA_TRY(scan_launch(sp, ctas, threads, ws->stream));
+            CUDA_TRY(launch(0, items.size(), ctas));
             ws->stats.kernel_launches = 1;
         }
         CUDA_TRY(cudaEventRecord(ws->ev1, ws->stream));
@@ -508,7 +607,6 @@ static int run_scan(cmgpu_model *m, cmgpu_workspace *ws, int semiring, int qdbid
             set_error("candidate buffer overflow");
             return CMGPU_ENOSPACE;
         }
-        if (plain) sp.items = ws->d_items;
     }
     ws->stats.candidates = (int64_t)ncand;
     if ((rc = ensure_host_cands(ws, ncand + 1))) return rc;
@@ -652,6 +750,12 @@ void cmgpu_workspace_free(cmgpu_workspace *ws) { delete ws; }
 int cmgpu_workspace_stats(const cmgpu_workspace *ws, cmgpu_stats *out) {
     if (!ws || !out) return CMGPU_EINVAL;
     *out = ws->stats;
+    return CMGPU_OK;
+}
+
+int cmgpu_workspace_set_kernel(cmgpu_workspace *ws, int kernel) {
+    if (!ws || kernel < CMGPU_KERNEL_AUTO || kernel > CMGPU_KERNEL_SWEEP) return CMGPU_EINVAL;
+    ws->kernel = kernel;
     return CMGPU_OK;
 }
 

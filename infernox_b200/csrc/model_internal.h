@@ -14,6 +14,7 @@
 #include "cm_internal.h"
 #include "qdb_kernel.h"
 #include "qdb_plan.h"
+#include "sweep_plan.h"
 
 namespace cmx {
 
@@ -102,7 +103,23 @@ struct DevPlan {
              *esc_c = nullptr, *init_val = nullptr, *beginsc_all = nullptr;
     std::vector<double> cells_prefix, terms_prefix;  // per jrow, prefix over jrow = 1..W
     double cells_full = 0, terms_full = 0;
+    // node-sweep kernel (sweep_scan.cu); sw_ok false when the model is outside its scope
+    bool sw_ok = false;
+    std::string sw_why;
+    SweepPlan sw;
+    SwState *sw_st = nullptr;
+    uint8_t *sw_kid = nullptr;
+    SwNode *sw_nodes = nullptr;
+    SwIO *sw_io = nullptr;
+    SwBif *sw_bifs = nullptr;
+    uint32_t *init0 = nullptr;
     ~DevPlan() {
+        cudaFree(sw_st);
+        cudaFree(sw_kid);
+        cudaFree(sw_nodes);
+        cudaFree(sw_io);
+        cudaFree(sw_bifs);
+        cudaFree(init0);
         cudaFree(states);
         cudaFree(chunks);
         cudaFree(begins);

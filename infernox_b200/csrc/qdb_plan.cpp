@@ -12,6 +12,7 @@
 #include "../../include/cmscan_gpu.h"
 #include "cm_internal.h"
 #include "qdb_plan.h"
+#include "sweep_plan.h"
 
 namespace cmx {
 
@@ -390,6 +391,228 @@ bool count_work(const cmgpu_cm *cm, int semiring, int qdbidx, int64_t L, double 
         cells += c * (double)(L - warm);
         terms += t * (double)(L - warm);
     }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// sweep plan
+// ---------------------------------------------------------------------------
+namespace {
+
+// unique state ids (src/constants.rs:46-81)
+enum {
+    UID_ROOT_S = 0, UID_ROOT_IL, UID_ROOT_IR, UID_BEGL_S, UID_BEGR_S, UID_BEGR_IL, UID_MATP_MP, UID_MATP_ML,
+    UID_MATP_MR, UID_MATP_D, UID_MATP_IL, UID_MATP_IR, UID_MATL_ML, UID_MATL_D, UID_MATL_IL, UID_MATR_MR,
+    UID_MATR_D, UID_MATR_IR, UID_BIF_B, UID_END_E
+};
+
+struct NodeShape {
+    int type, nst, nsplit;  // node type, states, split (non-insert) states
+    int ids[6];             // unique state ids in state order
+};
+
+// The node a state id starts, with its state list (src/cm_modelmaker.rs:979-1110).
+bool node_shape(int first_id, NodeShape &ns) {
+    switch (first_id) {
+    case UID_ROOT_S: ns = {ROOT_ND, 3, 1, {UID_ROOT_S, UID_ROOT_IL, UID_ROOT_IR}}; return true;
+    case UID_BEGL_S: ns = {BEGL_ND, 1, 1, {UID_BEGL_S}}; return true;
+    case UID_BEGR_S: ns = {BEGR_ND, 2, 1, {UID_BEGR_S, UID_BEGR_IL}}; return true;
+    case UID_MATP_MP:
+        ns = {MATP_ND, 6, 4, {UID_MATP_MP, UID_MATP_ML, UID_MATP_MR, UID_MATP_D, UID_MATP_IL, UID_MATP_IR}};
+        return true;
+    case UID_MATL_ML: ns = {MATL_ND, 3, 2, {UID_MATL_ML, UID_MATL_D, UID_MATL_IL}}; return true;
+    case UID_MATR_MR: ns = {MATR_ND, 3, 2, {UID_MATR_MR, UID_MATR_D, UID_MATR_IR}}; return true;
+    case UID_BIF_B: ns = {BIF_ND, 1, 1, {UID_BIF_B}}; return true;
+    case UID_END_E: ns = {END_ND, 1, 1, {UID_END_E}}; return true;
+    default: return false;
+    }
+}
+
+}  // namespace
+
+bool build_sweep_plan(const cmgpu_cm *cm, const Plan &p, int qdbidx, SweepPlan &sp, std::string *why) {
+    auto fail = [&](const std::string &m) {
+        if (why) *why = m;
+        return false;
+    };
+    const int M = cm->M, W = cm->W;
+    if (W + 1 > SW_MAX_S) return fail("W above the sweep kernel's limit");
+    sp = SweepPlan();
+    sp.M = M;
+    sp.W = W;
+    sp.S = ((W + 1 + 31) / 32) * 32;
+    sp.RW = W + 1;
+    Bands b = select_bands(cm, qdbidx);
+
+    // nodes from the unique state ids
+    std::vector<NodeShape> shape;
+    std::vector<int> v0s, node_of(M, -1);
+    for (int v = 0; v < M;) {
+        NodeShape ns;
+        if (!node_shape(cm->stid[v], ns)) return fail("state list does not start a node where expected");
+        if (v + ns.nst > M) return fail("truncated node");
+        for (int q = 0; q < ns.nst; q++) {
+            if (cm->stid[v + q] != ns.ids[q]) return fail("unexpected state order inside a node");
+            node_of[v + q] = (int)shape.size();
+        }
+        shape.push_back(ns);
+        v0s.push_back(v);
+        v += ns.nst;
+    }
+    const int nn = (int)shape.size();
+    if (nn > 32767 || M > 32767) return fail("model too large");
+    if (shape[0].type != ROOT_ND) return fail("first node is not ROOT");
+
+    // children: own inserts, then the split states of node n+1
+    auto is_insert = [&](int v) { return cm->sttype[v] == IL_ST || cm->sttype[v] == IR_ST; };
+    std::vector<int> bif_of_begl(M, -1), bif_of_begr(M, -1);
+    for (int v = 0; v < M; v++) {
+        const int st = cm->sttype[v], n = node_of[v];
+        if (st == E_ST) continue;
+        if (st == B_ST) {
+            int wl = cm->cfirst[v], y = cm->cnum[v];
+            if (wl != v + 1 || cm->stid[wl] != UID_BEGL_S || y <= v || y >= M || cm->stid[y] != UID_BEGR_S)
+                return fail("bifurcation children are not BEGL_S / BEGR_S");
+            SwBif bf{};
+            bf.kdn_y = (int16_t)std::min(b.dmin[y], W);
+            bf.kdx_y = (int16_t)std::min(b.dmax[y], W);
+            bf.kdn_w = (int16_t)std::min(b.dmin[wl], W);
+            bf.kdx_w = (int16_t)std::min(b.dmax[wl], W);
+            bf.begl = (int16_t)wl;
+            bf.begr = (int16_t)y;
+            bf.b = (int16_t)v;
+            bif_of_begl[wl] = bif_of_begr[y] = (int)sp.bifs.size();
+            sp.bifs.push_back(bf);
+            continue;
+        }
+        if (n + 1 >= nn) return fail("a non-END last node");
+        std::vector<int> kids;
+        const int v0 = v0s[n];
+        for (int q = 0; q < shape[n].nst; q++) {
+            int u = v0 + q;
+            if (!is_insert(u)) continue;
+            if (is_insert(v) && u < v) continue;  // an insert's children start at itself
+            kids.push_back(u);
+        }
+        for (int q = 0; q < shape[n + 1].nsplit; q++) kids.push_back(v0s[n + 1] + q);
+        if ((int)kids.size() != cm->cnum[v] || kids[0] != cm->cfirst[v])
+            return fail("children are not the node's inserts followed by the next node's split states");
+    }
+    if (sp.bifs.size() > 255) return fail("too many bifurcations");
+
+    // cell ranges: own band plus every index a reader uses (as build_plan)
+    std::vector<int> lo(M, 1 << 30), hi(M, -1);
+    auto cover = [&](int y, int a, int c) {
+        if (c < a) return;
+        lo[y] = std::min(lo[y], a);
+        hi[y] = std::max(hi[y], c);
+    };
+    for (int v = 0; v < M; v++) {
+        const int st = cm->sttype[v];
+        const int width = std::max(0, b.dxcap[v] - b.dn[v] + 1);
+        if (st == E_ST) continue;
+        if (v == 0) {
+            for (int yo = 0; yo < cm->cnum[0]; yo++) cover(cm->cfirst[0] + yo, b.dn[0], b.dxcap[0]);
+            continue;
+        }
+        if (width <= 0) continue;
+        cover(v, b.dn[v], b.dxcap[v]);
+        if (st == B_ST) {
+            int wl = cm->cfirst[v], y = cm->cnum[v];
+            cover(y, std::max(0, std::min(b.dmin[y], W)), std::min(b.dmax[y], W));
+            cover(wl, std::max(0, std::min(b.dmin[wl], W)), std::min(b.dmax[wl], W));
+        } else {
+            const int sd = state_delta(st);
+            for (int yo = 0; yo < cm->cnum[v]; yo++) cover(cm->cfirst[v] + yo, b.dn[v] - sd, b.dxcap[v] - sd);
+        }
+    }
+
+    // per-state metadata
+    sp.st.assign(M, SwState());
+    for (int v = 0; v < M; v++) {
+        const StateDev &sd = p.states[v];
+        SwState &s = sp.st[v];
+        s.lo = (int16_t)(hi[v] >= lo[v] ? lo[v] : 1);
+        s.hi = (int16_t)(hi[v] >= lo[v] ? hi[v] : 0);
+        s.dn = sd.dn;
+        s.dxcap = sd.dxcap;
+        s.type = sd.type;
+        s.flags = sd.flags & (SF_ENDSC | SF_BEGIN);
+        s.cnum = sd.cnum;
+        s.sd = sd.sd;
+        if (sd.escoff > 32767) return fail("emission table too large");
+        s.escoff = (int16_t)sd.escoff;
+        s.slot = (uint8_t)(v - v0s[node_of[v]]);
+        if (v == 0) s.flags |= SWF_ROOT;
+        if (cm->stid[v] == UID_BEGL_S) s.flags |= SWF_BEGL;
+        if (cm->stid[v] == UID_BEGR_S) s.flags |= SWF_BEGR;
+    }
+
+    // previous-column reads, deck slots and child locations
+    sp.kid.assign((size_t)M * MAXC, 0);
+    sp.nodes.assign(nn, SwNode());
+    int64_t deck = 0;
+    for (int n = 0; n < nn; n++) {
+        SwNode &nd = sp.nodes[n];
+        const int v0 = v0s[n];
+        nd.type = (uint8_t)shape[n].type;
+        nd.nst = (uint8_t)shape[n].nst;
+        nd.v0 = (int16_t)v0;
+        nd.io0 = (int16_t)sp.io.size();
+        nd.aux = 0;
+        if (shape[n].type == BIF_ND) {
+            for (size_t k = 0; k < sp.bifs.size(); k++)
+                if (sp.bifs[k].b == v0) nd.aux = (uint8_t)k;
+        } else if (shape[n].type == BEGL_ND) {
+            nd.aux = (uint8_t)bif_of_begl[v0];
+        } else if (shape[n].type == BEGR_ND) {
+            nd.aux = (uint8_t)bif_of_begr[v0];
+        }
+        std::vector<int> prev;  // states read in the previous column, ascending
+        for (int q = 0; q < shape[n].nst; q++) {
+            const int v = v0 + q, st = cm->sttype[v];
+            if (!right_emitter(st)) continue;
+            for (int yo = 0; yo < cm->cnum[v]; yo++) prev.push_back(cm->cfirst[v] + yo);
+        }
+        std::sort(prev.begin(), prev.end());
+        prev.erase(std::unique(prev.begin(), prev.end()), prev.end());
+        if (prev.size() > (size_t)SW_SLOTS) return fail("too many previous-column reads in one node");
+        for (size_t k = 0; k < prev.size(); k++) {
+            const int y = prev[k];
+            if (cm->stid[y] == UID_BEGL_S || cm->stid[y] == UID_BEGR_S)
+                return fail("a right emitter reads a subtree start state");
+            SwIO e{};
+            e.y = (int16_t)y;
+            e.pslot = (uint8_t)k;
+            e.cur = node_of[y] == n ? (uint8_t)(y - v0) : (uint8_t)(8 + y - v0s[n + 1]);
+            e.lo = sp.st[y].lo;
+            e.hi = sp.st[y].hi;
+            e.deck = (int32_t)deck;
+            deck += sp.S;
+            sp.io.push_back(e);
+        }
+        nd.nio = (uint8_t)prev.size();
+        for (int q = 0; q < shape[n].nst; q++) {
+            const int v = v0 + q, st = cm->sttype[v];
+            if (st == E_ST || st == B_ST) continue;
+            for (int yo = 0; yo < cm->cnum[v]; yo++) {
+                const int y = cm->cfirst[v] + yo;
+                uint8_t code;
+                if (right_emitter(st)) {
+                    size_t k = std::find(prev.begin(), prev.end(), y) - prev.begin();
+                    code = (uint8_t)(KID_PREV * 8 + k);
+                } else if (node_of[y] == n) {
+                    code = (uint8_t)(KID_OWN * 8 + (y - v0));
+                } else {
+                    code = (uint8_t)(KID_NEXT * 8 + (y - v0s[n + 1]));
+                }
+                sp.kid[(size_t)v * MAXC + yo] = code;
+            }
+        }
+    }
+    if (deck > ((int64_t)1 << 30)) return fail("deck too large");
+    sp.deck_words = deck;
+    sp.ring_words = (int64_t)sp.bifs.size() * sp.RW * sp.S;
     return true;
 }
 

@@ -26,6 +26,7 @@ RawHit = namedtuple("RawHit", "i j score bias")
 
 CYK_F32, INSIDE_I32 = N.CYK_F32, N.INSIDE_I32
 NOQDB, QDB1, QDB2 = N.NOQDB, N.QDB1, N.QDB2
+KERNEL_AUTO, KERNEL_LEVEL, KERNEL_SWEEP = N.KERNEL_AUTO, N.KERNEL_LEVEL, N.KERNEL_SWEEP
 SMX_QDB1_TIGHT, SMX_QDB2_LOOSE = QDB1, QDB2
 
 
@@ -70,6 +71,10 @@ class Scanner:
 
     def set_shape(self, ctas_per_sm: int = 0, threads: int = 0, chunk: int = 0, lanes: int = 0) -> None:
         N.check(N.lib().cmgpu_workspace_set_shape(self._ws, ctas_per_sm, threads, chunk, lanes))
+
+    def set_kernel(self, kernel: int) -> None:
+        """KERNEL_AUTO, KERNEL_LEVEL (CTA level schedule) or KERNEL_SWEEP (warp node sweep)."""
+        N.check(N.lib().cmgpu_workspace_set_kernel(self._ws, kernel))
 
     def autotune(self, semiring: int, qdbidx: int, buf: np.ndarray, windows: np.ndarray,
                  cutoff: float, device_buf=None, lanes=(4, 8, 16), threads=(512,), chunks_w=(0, 4, 8, 16)) -> dict:

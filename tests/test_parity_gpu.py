@@ -9,11 +9,21 @@ import pytest
 
 import oracle
 from infernox_b200 import scan
-from infernox_b200.scan import CYK_F32, INSIDE_I32, NOQDB, QDB1, QDB2
+from infernox_b200.scan import CYK_F32, INSIDE_I32, KERNEL_LEVEL, KERNEL_SWEEP, NOQDB, QDB1, QDB2
 
 from helpers import frame, models, planted_seq
 
 pytestmark = pytest.mark.gpu
+
+# both scan kernels must reproduce the oracle: the CTA level schedule and the
+# warp node sweep
+KERNELS = pytest.mark.parametrize("kernel", [KERNEL_LEVEL, KERNEL_SWEEP], ids=["level", "sweep"])
+
+
+def scanner(cfg, kernel):
+    s = scan.Scanner(cfg)
+    s.set_kernel(kernel)
+    return s
 
 
 def hits_equal(gpu, ref):
@@ -41,30 +51,33 @@ CASES = [
 ]
 
 
+@KERNELS
 @pytest.mark.parametrize("case", CASES, ids=lambda c: f"{c[0]}-{'L' if c[1] else 'G'}-s{c[2]}-b{c[3]}")
-def test_generic_scan_matches_oracle(case):
+def test_generic_scan_matches_oracle(case, kernel):
     name, local, sr, band, n, cutoff, null3, degen = case
     cm, g, l = models(name)
     c = l if local else g
     seq = planted_seq(cm, n, 0.5, 3, seed=17 + CASES.index(case), degenerate=degen)
     dsq = frame(seq)
     ref, _, _, _ = oracle.qdb_scan(c, sr, band, dsq, 1, n, cutoff, null3)
-    s = scan.Scanner(c)
+    s = scanner(c, kernel)
     got = s.generic_scan(sr, band, dsq, 1, n, cutoff, null3)
+    assert s.stats()["kernel"] == kernel
     assert len(ref) > 0
     assert hits_equal(got, ref), (got[:5], ref[:5])
 
 
+@KERNELS
 @pytest.mark.parametrize("shape", [(0, 0, 0, 0), (0, 0, 200, 1), (0, 256, 200, 3), (2, 128, 1000, 2),
                                    (1, 512, 300, 8)])
-def test_subchunked_windows_match(shape):
+def test_subchunked_windows_match(shape, kernel):
     """Forced small work items, several items per CTA: warm-up restarts and
     lane refills must not change any hit."""
     ctas, threads, chunk, lanes = shape
     cm, g, l = models("trna")
     n = 6000
     dsq = frame(planted_seq(cm, n, 0.45, 6, seed=7))
-    s = scan.Scanner(l)
+    s = scanner(l, kernel)
     s.set_shape(ctas_per_sm=ctas, threads=threads, chunk=chunk, lanes=lanes)
     for sr, band in ((CYK_F32, QDB1), (INSIDE_I32, QDB2)):
         ref, _, _, _ = oracle.qdb_scan(l, sr, band, dsq, 1, n, -3.0, True)
@@ -72,12 +85,13 @@ def test_subchunked_windows_match(shape):
         assert hits_equal(got, ref)
 
 
-def test_window_inside_frame():
+@KERNELS
+def test_window_inside_frame(kernel):
     """Windows [i0, j0] strictly inside the frame (as envelopes are)."""
     cm, g, l = models("small2")
     n = 3000
     dsq = frame(planted_seq(cm, n, 0.5, 4, seed=9))
-    s = scan.Scanner(l)
+    s = scanner(l, kernel)
     for (i0, j0) in ((1, 1), (5, 40), (700, 1900), (2990, 3000), (1, 3000)):
         ref, _, _, _ = oracle.qdb_scan(l, INSIDE_I32, QDB2, dsq, i0, j0, -10.0, True)
         got = s.generic_scan(INSIDE_I32, QDB2, dsq, i0, j0, -10.0, True)
@@ -99,7 +113,8 @@ def test_cyk_filter_and_final_stage():
         assert hits_equal(got, ref)
 
 
-def test_batch_uneven_windows_match_per_window():
+@KERNELS
+def test_batch_uneven_windows_match_per_window(kernel):
     """Many windows of uneven length in one launch == each window alone."""
     cm, g, l = models("small2")
     rng = np.random.default_rng(42)
@@ -112,7 +127,7 @@ def test_batch_uneven_windows_match_per_window():
         off += len(f)
     buf = np.concatenate(frames)
     W = np.array(wins, dtype=[("dsq_offset", np.int64), ("i0", np.int32), ("j0", np.int32)])
-    s = scan.Scanner(l)
+    s = scanner(l, kernel)
     for sr, band in ((INSIDE_I32, NOQDB), (CYK_F32, QDB1)):
         got = s.scan_batch(sr, band, buf, W, 0.0, True)
         plain = s.scan_batch(sr, band, buf, W, 0.0, True, plain=True)
@@ -148,8 +163,9 @@ CELL_CASES = [
 ]
 
 
+@KERNELS
 @pytest.mark.parametrize("case", CELL_CASES, ids=lambda c: f"{c[0]}-{'L' if c[1] else 'G'}-s{c[2]}-b{c[3]}")
-def test_all_cells_match_oracle(case):
+def test_all_cells_match_oracle(case, kernel):
     """Every ROOT cell (j, d) above a very low cutoff, bit for bit."""
     name, local, sr, band = case
     cm, g, l = models(name)
@@ -157,7 +173,7 @@ def test_all_cells_match_oracle(case):
     n = 400
     dsq = frame(planted_seq(cm, n, 0.5, 1, seed=55))
     _, ref, _, _ = oracle.qdb_scan(c, sr, band, dsq, 1, n, -1e30, False, want_cands=True)
-    got = scan.Scanner(c).scan_cells(sr, band, dsq, 1, n, -1e30)
+    got = scanner(c, kernel).scan_cells(sr, band, dsq, 1, n, -1e30)
     rmap = {(j, d): s for j, d, s in ref}
     gmap = {(j, d): s for j, d, s in got}
     bad = [(k, gmap.get(k), rmap.get(k)) for k in sorted(set(rmap) | set(gmap))

@@ -16,7 +16,7 @@ import numpy as np
 import pytest
 
 from infernox_b200 import _native as N
-from infernox_b200.scan import CYK_F32, INSIDE_I32, NOQDB, QDB1, QDB2, Scanner
+from infernox_b200.scan import CYK_F32, INSIDE_I32, KERNEL_LEVEL, NOQDB, QDB1, QDB2, Scanner
 
 from helpers import frame, models, planted_seq
 
@@ -54,9 +54,11 @@ def test_noalloc_matches_regular_scan_two_calls_in_a_row():
 
 def one_lane_fits_in_smem(cfg, semiring, band) -> bool:
     """Whether one work item's decks fit in shared memory: the criterion both
-    the regular path (with one lane forced) and the no-allocation path use."""
+    the regular path (level kernel, one lane forced) and the no-allocation
+    path use."""
     sc = Scanner(cfg)
     try:
+        sc.set_kernel(KERNEL_LEVEL)
         sc.set_shape(1, 512, 0, 1)
         dsq = np.concatenate([[255], np.zeros(300, np.uint8), [255]]).astype(np.uint8)
         sc.generic_scan(semiring, band, dsq, 1, 300, 1e9, False)
