@@ -142,7 +142,7 @@ typedef struct cmgpu_stats {
  * state by state in dependency levels with CTA barriers (qdb_scan.cu).
  * SWEEP: one warp scans one work item node by node with no CTA barrier
  * (sweep_scan.cu); it needs W <= 255 and the node-local state topology of
- * CMs built by cmbuild.  AUTO picks SWEEP where it applies. */
+ * CMs built by cmbuild.  AUTO picks LEVEL. */
 #define CMGPU_KERNEL_AUTO 0
 #define CMGPU_KERNEL_LEVEL 1
 #define CMGPU_KERNEL_SWEEP 2

@@ -393,7 +393,8 @@ static int run_scan(cmgpu_model *m, cmgpu_workspace *ws, int semiring, int qdbid
         set_error("node-sweep kernel does not apply to this model: " + dp->sw_why);
         return CMGPU_EINVAL;
     }
-    const bool sweep = dp->sw_ok && ws->kernel != CMGPU_KERNEL_LEVEL;
+    // AUTO takes the level kernel: measured faster on every workload here
+    const bool sweep = dp->sw_ok && ws->kernel == CMGPU_KERNEL_SWEEP;
     const size_t SMEM_CAP = 227 * 1024 - 1024, SM_CAP = 228 * 1024;
     const int threads = ws->threads;
     int best_c = 0, best_l = 0;

@@ -12,8 +12,9 @@
 // of six state slots in shared memory hold them, swapping roles every node.
 // Right emitters (MP, MR, IR) read the previous column instead
 // (jp_y = prv, src/cm_nohmm.rs:575): the states they read keep a slot in the
-// warp's deck in global memory; before node n runs those slots are copied to
-// a previous-column buffer, and after it the current values overwrite them.
+// warp's deck in global memory; while node n+1 runs, cp.async copies node
+// n's slots into one of two previous-column buffers, and after node n ran
+// its current values overwrite them.
 // A bifurcation reads its BEGR_S from a per-warp row in shared memory and its
 // BEGL_S from a ring of W+1 columns in global memory (alpha_begl,
 // src/cm_nohmm.rs:578-600).  Local begins are a MAX (src/cm_nohmm.rs:
@@ -41,7 +42,30 @@ using dev::IMPOSSIBLE_D;
 using dev::reduce_c;
 using dev::reduce_c_noself;
 
+#ifndef SW_NC
+#define SW_NC 2
+#endif
+
 constexpr unsigned FULL = 0xffffffffu;
+
+// Integer Inside with ILogsum (src/cp9.rs:65-75) written without branches:
+// the cases that add nothing (min at -INFTY, difference beyond the table)
+// index the zero entry the kernel stores at tbl[nz].
+struct SemInsBF : Sem<true> {
+    __device__ static __forceinline__ int32_t comb(int32_t a, int32_t b, const uint16_t *tbl, int nz) {
+        const int32_t mx0 = max(a, b), mn = min(a, b);
+        const uint32_t diff = (uint32_t)mx0 - (uint32_t)mn;
+        const int32_t mx = max(mx0, -dev::INFTY_D);
+        const uint32_t idx = mn <= -dev::INFTY_D ? (uint32_t)nz : min(diff, (uint32_t)nz);
+        return (int32_t)((uint32_t)mx + (uint32_t)tbl[idx]);
+    }
+};
+#ifdef SW_COMB_BRANCHY
+template <bool INS> struct SemSel { typedef Sem<INS> type; };
+#else
+template <bool INS> struct SemSel { typedef Sem<false> type; };
+template <> struct SemSel<true> { typedef SemInsBF type; };
+#endif
 constexpr int B_ST_D = 8, E_ST_D = 7, IL_ST_D = 4;  // sttype codes (cm_internal.h)
 
 struct St {  // unpacked SwState
@@ -71,7 +95,7 @@ struct Ctx {
     const uint16_t *tbl;
     const int4 *nodes, *io, *bifs;
     int nz;
-    uint32_t *buf;    // two node buffers (12 S) followed by the previous-column buffer (6 S)
+    uint32_t *buf;    // two node buffers (12 S), then two previous-column buffers (12 S)
     uint32_t *begr;   // nbif rows of S
     uint32_t *bmax;   // S: local-begin maxima of the current column
     uint8_t *ring;    // residues
@@ -98,12 +122,21 @@ __device__ __forceinline__ typename Sm::T esc2(const Ctx &c, int v, int escoff, 
     return Sm::ldg(c.p->esc + v * 324 + a * 18 + b);
 }
 
-// Base of a child's current-column cells (code = kind * 8 + slot).
-__device__ __forceinline__ const uint32_t *kid_base(const Ctx &c, int code, int par) {
+// Base of a child's current-column cells (code = kind * 8 + slot); pb is
+// the previous-column buffer of the node being computed.
+__device__ __forceinline__ const uint32_t *kid_base(const Ctx &c, int code, int par, int pb) {
     const int kind = code >> 3, slot = code & 7;
-    const int buf = kind == KID_PREV ? 12 : ((kind == KID_OWN ? par : par ^ 1) * SW_SLOTS);
+    const int buf = kind == KID_PREV ? 12 + pb * SW_SLOTS : ((kind == KID_OWN ? par : par ^ 1) * SW_SLOTS);
     return c.buf + (buf + slot) * c.S;
 }
+
+// Asynchronous 4-byte copy global -> shared (cp.async, sm_80+).
+__device__ __forceinline__ void cp_async4(uint32_t *dst, const uint32_t *src) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 // Local begin (MAX into the ROOT row) of a begin state's cell d.
 template <class Sm>
@@ -115,10 +148,58 @@ __device__ __forceinline__ void begin_fold(const Ctx &c, int d, typename Sm::T x
     if (b < cand) Sm::st(c.bmax + d, cand);
 }
 
+// reduce_c (reduce_c_order for Inside, any bracketing for CYK) of NC
+// independent cells at once: one switch on cnum, the NC fold chains side by
+// side inside each case so that their latencies overlap.
+template <class Sm, int NC>
+__device__ __forceinline__ void reduce_n(int cnum, const typename Sm::T (&t)[NC][6], const typename Sm::T (&init)[NC],
+                                         typename Sm::T (&o)[NC], const uint16_t *tb, int nz) {
+#define CB(a, b) Sm::comb(a, b, tb, nz)
+    if (!Sm::ORDERED) {
+#pragma unroll
+        for (int q = 0; q < NC; q++) o[q] = reduce_c<Sm>(cnum, t[q], init[q], tb, nz);
+        return;
+    }
+    switch (cnum) {
+    case 1:
+#pragma unroll
+        for (int q = 0; q < NC; q++) o[q] = CB(init[q], t[q][0]);
+        break;
+    case 2:
+#pragma unroll
+        for (int q = 0; q < NC; q++) o[q] = CB(CB(t[q][1], init[q]), t[q][0]);
+        break;
+    case 3:
+#pragma unroll
+        for (int q = 0; q < NC; q++) o[q] = CB(CB(CB(t[q][2], t[q][1]), init[q]), t[q][0]);
+        break;
+    case 4:
+#pragma unroll
+        for (int q = 0; q < NC; q++) o[q] = CB(CB(CB(CB(t[q][3], t[q][2]), init[q]), t[q][1]), t[q][0]);
+        break;
+    case 5:
+#pragma unroll
+        for (int q = 0; q < NC; q++)
+            o[q] = CB(CB(CB(CB(CB(t[q][4], t[q][3]), init[q]), t[q][1]), t[q][2]), t[q][0]);
+        break;
+    case 6:
+#pragma unroll
+        for (int q = 0; q < NC; q++)
+            o[q] = CB(CB(CB(CB(CB(CB(t[q][5], init[q]), t[q][4]), t[q][3]), t[q][2]), t[q][1]), t[q][0]);
+        break;
+    default:  // cnum is 1..6 for every non-B, non-E state of a CM
+#pragma unroll
+        for (int q = 0; q < NC; q++) o[q] = init[q];
+    }
+#undef CB
+}
+
 // An ordinary state (not E, B, IL, ROOT_S): cells lo..hi, band cells
-// computed, the rest the fill of the reference's decks.
+// computed, the rest the fill of the reference's decks.  Two cells per lane
+// per step (d and d+32), evaluated side by side.
 template <class Sm>
-__device__ __forceinline__ void do_plain(const Ctx &c, const Col &C, int v, const St &s, int par, uint32_t *dst) {
+__device__ __forceinline__ void do_plain(const Ctx &c, const Col &C, int v, const St &s, int par, int pb,
+                                         uint32_t *dst) {
     typedef typename Sm::T T;
     const T ZERO = Sm::zero();
     const uint32_t *kp[6];
@@ -128,7 +209,7 @@ __device__ __forceinline__ void do_plain(const Ctx &c, const Col &C, int v, cons
         kp[yo] = c.buf;
         ts[yo] = ZERO;
         if (yo < s.cnum) {
-            kp[yo] = kid_base(c, c.kid[v * 6 + yo], par) - s.sd;
+            kp[yo] = kid_base(c, c.kid[v * 6 + yo], par, pb) - s.sd;
             ts[yo] = Sm::ld(c.tsc + v * 6 + yo);
         }
     }
@@ -141,36 +222,68 @@ __device__ __forceinline__ void do_plain(const Ctx &c, const Col &C, int v, cons
     const bool natural = s.flags & SWF_BEGL;  // BEGL_S folds its children in natural order
     const int t = s.type;
     const T ej = (t == 3 || t == 5) ? esc1<Sm>(c, v, s.escoff, C.resj) : ZERO;
-    for (int d = s.lo + c.lane; d <= s.hi; d += 32) {
-        T val;
-        if (d >= s.dn && d <= dx) {
-            T terms[6];
+    // computed cells: [clo, chi] = band within the written range
+    const int clo = max(s.lo, s.dn), chi = min(s.hi, dx);
+    constexpr int NC = SW_NC;
+    for (int d0 = s.lo; d0 <= s.hi; d0 += 32 * NC) {
+        int dd[NC];
+        bool live[NC], inb[NC];
+        T terms[NC][6], init[NC], sc[NC];
 #pragma unroll
-            for (int yo = 0; yo < 6; yo++)
-                if (yo < s.cnum) terms[yo] = Sm::add(Sm::ld(kp[yo] + d), ts[yo]);
-            const T init = endsc ? Sm::add(Sm::ld(c.el + d - s.sd), es) : ZERO;
-            T sc;
-            if (natural) {
-                sc = init;
+        for (int q = 0; q < NC; q++) {
+            dd[q] = d0 + c.lane + 32 * q;
+            live[q] = dd[q] <= s.hi;
+            inb[q] = dd[q] >= clo && dd[q] <= chi;
+            // cells outside the band are evaluated at a band cell (discarded)
+            const int e = chi >= clo ? min(max(dd[q], clo), chi) : s.dn;
+#pragma unroll
+            for (int yo = 0; yo < 6; yo++) terms[q][yo] = ZERO;
+            if (chi >= clo) {
 #pragma unroll
                 for (int yo = 0; yo < 6; yo++)
-                    if (yo < s.cnum) sc = Sm::comb(sc, terms[yo], c.tbl, c.nz);
+                    if (yo < s.cnum) terms[q][yo] = Sm::add(Sm::ld(kp[yo] + e), ts[yo]);
+                init[q] = endsc ? Sm::add(Sm::ld(c.el + e - s.sd), es) : ZERO;
             } else {
-                sc = reduce_c<Sm>(s.cnum, terms, init, c.tbl, c.nz);
+                init[q] = ZERO;
             }
-            if (t == 2 || t == 4) {  // ML, IL: residue i = j-d+1
-                sc = Sm::add(sc, esc1<Sm>(c, v, s.escoff, c.ring[(C.j - d + 1) & c.rmask]));
-            } else if (t == 3 || t == 5) {  // MR, IR: residue j
-                sc = Sm::add(sc, ej);
-            } else if (t == 1) {  // MP
-                sc = Sm::add(sc, esc2<Sm>(c, v, s.escoff, c.ring[(C.j - d + 1) & c.rmask], C.resj));
-            }
-            val = sc;
-            if (begin) begin_fold<Sm>(c, d, val, bsc);
-        } else {
-            val = d == 0 ? base0 : ZERO;
         }
-        Sm::st(dst + d, val);
+        if (chi >= clo) {
+            if (natural) {
+#pragma unroll
+                for (int q = 0; q < NC; q++) {
+                    sc[q] = init[q];
+#pragma unroll
+                    for (int yo = 0; yo < 6; yo++)
+                        if (yo < s.cnum) sc[q] = Sm::comb(sc[q], terms[q][yo], c.tbl, c.nz);
+                }
+            } else {
+                reduce_n<Sm, NC>(s.cnum, terms, init, sc, c.tbl, c.nz);
+            }
+#pragma unroll
+            for (int q = 0; q < NC; q++) {
+                const int e = min(max(dd[q], clo), chi);
+                if (t == 2 || t == 4) {  // ML, IL: residue i = j-d+1
+                    sc[q] = Sm::add(sc[q], esc1<Sm>(c, v, s.escoff, c.ring[(C.j - e + 1) & c.rmask]));
+                } else if (t == 3 || t == 5) {  // MR, IR: residue j
+                    sc[q] = Sm::add(sc[q], ej);
+                } else if (t == 1) {  // MP
+                    sc[q] = Sm::add(sc[q], esc2<Sm>(c, v, s.escoff, c.ring[(C.j - e + 1) & c.rmask], C.resj));
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < NC; q++) {
+            if (!live[q]) continue;
+            const int d = dd[q];
+            T val;
+            if (inb[q]) {
+                val = sc[q];
+                if (begin) begin_fold<Sm>(c, d, val, bsc);
+            } else {
+                val = d == 0 ? base0 : ZERO;
+            }
+            Sm::st(dst + d, val);
+        }
     }
 }
 
@@ -241,7 +354,7 @@ __device__ __forceinline__ void do_il(const Ctx &c, const Col &C, int v, const S
         kp[yo] = c.buf;
         ts[yo] = ZERO;
         if (yo < s.cnum) {
-            kp[yo] = kid_base(c, c.kid[v * 6 + yo], par) - 1;
+            kp[yo] = kid_base(c, c.kid[v * 6 + yo], par, 0) - 1;  // IL reads no previous column
             ts[yo] = Sm::ld(c.tsc + v * 6 + yo);
         }
     }
@@ -253,14 +366,19 @@ __device__ __forceinline__ void do_il(const Ctx &c, const Col &C, int v, const S
     const int n = dx - dn + 1;
     if (n > 0) {
         const int kk = (n + 31) >> 5;
-        if (kk == 1)
-            il_relax<Sm, 1>(c, C, v, s, kp, ts, endsc, es, begin, bsc, dst, dn, dx, kk);
-        else if (kk == 2)
-            il_relax<Sm, 2>(c, C, v, s, kp, ts, endsc, es, begin, bsc, dst, dn, dx, kk);
-        else if (kk <= 4)
-            il_relax<Sm, 4>(c, C, v, s, kp, ts, endsc, es, begin, bsc, dst, dn, dx, kk);
-        else
-            il_relax<Sm, 8>(c, C, v, s, kp, ts, endsc, es, begin, bsc, dst, dn, dx, kk);
+#define IL_CASE(KC) \
+    case KC: il_relax<Sm, KC>(c, C, v, s, kp, ts, endsc, es, begin, bsc, dst, dn, dx, kk); break;
+        switch (kk) {
+            IL_CASE(1)
+            IL_CASE(2)
+            IL_CASE(3)
+            IL_CASE(4)
+            IL_CASE(5)
+            IL_CASE(6)
+            IL_CASE(7)
+            default: il_relax<Sm, 8>(c, C, v, s, kp, ts, endsc, es, begin, bsc, dst, dn, dx, kk);
+        }
+#undef IL_CASE
     }
     const T base0 = Sm::ld(c.init0 + v);
     for (int d = s.lo + c.lane; d <= s.hi; d += 32)
@@ -297,13 +415,29 @@ __device__ __forceinline__ void do_bif(const Ctx &c, const Col &C, int v, const 
         const int K1 = __reduce_max_sync(FULL, act ? kmax : INT_MIN);
         T sc = (inb && endsc) ? Sm::add(Sm::ld(c.el + d), es) : ZERO;
         if (K0 <= K1) {
+            // eight steps at a time: the ring loads of a batch are issued
+            // before its folds, which stay in ascending k
+            constexpr int KB = 8;
             int col = C.jm - K0;
             if (col < 0) col += c.RW;
-            for (int k = K0; k <= K1; k++) {
-                if (act && k >= kmin && k <= kmax)
-                    sc = Sm::comb(sc, Sm::add(Sm::ld(ring + (size_t)col * c.S + d - k), Sm::ld(begr + k)), c.tbl,
-                                  c.nz);
-                col = col == 0 ? c.RW - 1 : col - 1;
+            for (int k0 = K0; k0 <= K1; k0 += KB) {
+                T lv[KB], rv[KB];
+#pragma unroll
+                for (int u = 0; u < KB; u++) {
+                    const int k = k0 + u;
+                    int cc = col - u;
+                    if (cc < 0) cc += c.RW;
+                    const bool on = act && k >= kmin && k <= kmax;
+                    lv[u] = on ? Sm::ld(ring + (size_t)cc * c.S + d - k) : ZERO;
+                    rv[u] = on ? Sm::ld(begr + k) : ZERO;
+                }
+#pragma unroll
+                for (int u = 0; u < KB; u++) {
+                    const int k = k0 + u;
+                    if (act && k >= kmin && k <= kmax) sc = Sm::comb(sc, Sm::add(lv[u], rv[u]), c.tbl, c.nz);
+                }
+                col -= KB;
+                if (col < 0) col += c.RW;
             }
         }
         if (live) {
@@ -327,7 +461,7 @@ __device__ __forceinline__ void do_root(const Ctx &c, const Col &C, const St &s,
         kp[yo] = c.buf;
         ts[yo] = ZERO;
         if (yo < s.cnum) {
-            kp[yo] = kid_base(c, c.kid[yo], par);
+            kp[yo] = kid_base(c, c.kid[yo], par, 0);  // ROOT_S reads the current column
             ts[yo] = Sm::ld(c.tsc + yo);
         }
     }
@@ -373,39 +507,54 @@ __device__ __forceinline__ void do_root(const Ctx &c, const Col &C, const St &s,
     }
 }
 
+// Previous-column values node n reads: deck slots -> previous-column buffer
+// pb, with cp.async (completion awaited before node n runs); in the first
+// column of a work item the reference's initial deck fill instead.
+template <class Sm>
+__device__ __forceinline__ void prefetch(const Ctx &c, const Col &C, int n, int pb) {
+    const int4 nq = c.nodes[n];
+    const int nio = (nq.x >> 16) & 0xff, io0 = (int16_t)((uint32_t)nq.y >> 16);
+    const uint32_t zero = Sm::u(Sm::zero());
+    for (int e = 0; e < nio; e++) {
+        const int4 q = c.io[io0 + e];
+        const int y = (int16_t)(q.x & 0xffff), pslot = (q.x >> 16) & 0xff;
+        const int lo = (int16_t)(q.y & 0xffff), hi = (int16_t)((uint32_t)q.y >> 16);
+        uint32_t *dstb = c.buf + (12 + pb * SW_SLOTS + pslot) * c.S;
+        if (C.first) {
+            const uint32_t b0 = c.init0[y];
+            for (int d = lo + c.lane; d <= hi; d += 32) dstb[d] = d == 0 ? b0 : zero;
+        } else {
+            const uint32_t *g = c.deck + q.z;
+            for (int d = lo + c.lane; d <= hi; d += 32) cp_async4(dstb + d, g + d);
+        }
+    }
+    cp_async_commit();
+}
+
 template <class Sm>
 __device__ __forceinline__ void do_column(const Ctx &c, const Col &C) {
-    typedef typename Sm::T T;
-    const T ZERO = Sm::zero();
     const SweepParams &p = *c.p;
     const int S = c.S;
+    int pb = 0;
+    prefetch<Sm>(c, C, p.nnodes - 1, pb);
     for (int n = p.nnodes - 1; n >= 0; n--) {
         const int4 nq = c.nodes[n];
         const int nst = (nq.x >> 8) & 0xff, nio = (nq.x >> 16) & 0xff;
         const int aux = ((uint32_t)nq.x >> 24) & 0xff;
         const int v0 = (int16_t)(nq.y & 0xffff), io0 = (int16_t)((uint32_t)nq.y >> 16);
         const int par = n & 1;
-        // previous-column values this node reads
-        for (int e = 0; e < nio; e++) {
-            const int4 q = c.io[io0 + e];
-            const int y = (int16_t)(q.x & 0xffff), pslot = (q.x >> 16) & 0xff;
-            const int lo = (int16_t)(q.y & 0xffff), hi = (int16_t)((uint32_t)q.y >> 16);
-            uint32_t *pb = c.buf + (12 + pslot) * S;
-            if (C.first) {
-                const uint32_t b0 = c.init0[y];
-                for (int d = lo + c.lane; d <= hi; d += 32) pb[d] = d == 0 ? b0 : Sm::u(ZERO);
-            } else {
-                const uint32_t *g = c.deck + q.z;
-                for (int d = lo + c.lane; d <= hi; d += 32) pb[d] = g[d];
-            }
-        }
+        // this node's previous-column values have arrived; fetch the next
+        // node's while this one computes
+        cp_async_wait_all();
         __syncwarp();
+        if (n > 0) prefetch<Sm>(c, C, n - 1, pb ^ 1);
         for (int v = v0 + nst - 1; v >= v0; v--) {
             const St s = unpack(c.st[v]);
             if (s.type == E_ST_D) {
                 uint32_t *dst = c.buf + (par * SW_SLOTS + s.slot) * S;
                 const uint32_t b0 = c.init0[v];
-                for (int d = s.lo + c.lane; d <= s.hi; d += 32) dst[d] = d == 0 ? b0 : Sm::u(ZERO);
+                const uint32_t zero = Sm::u(Sm::zero());
+                for (int d = s.lo + c.lane; d <= s.hi; d += 32) dst[d] = d == 0 ? b0 : zero;
             } else if (s.type == B_ST_D) {
                 do_bif<Sm>(c, C, v, s, par, aux);
             } else if (s.flags & SWF_ROOT) {
@@ -420,7 +569,7 @@ __device__ __forceinline__ void do_column(const Ctx &c, const Col &C) {
                     dst = c.begr + aux * S;
                 else
                     dst = c.buf + (par * SW_SLOTS + s.slot) * S;
-                do_plain<Sm>(c, C, v, s, par, dst);
+                do_plain<Sm>(c, C, v, s, par, pb, dst);
             }
             __syncwarp();
         }
@@ -435,12 +584,13 @@ __device__ __forceinline__ void do_column(const Ctx &c, const Col &C) {
             for (int d = lo + c.lane; d <= hi; d += 32) g[d] = src[d];
         }
         __syncwarp();
+        pb ^= 1;
     }
 }
 
 template <bool INS>
 __global__ void __launch_bounds__(SW_MAX_WARPS * 32, 1) sweep_kernel(SweepParams p) {
-    typedef Sem<INS> Sm;
+    typedef typename SemSel<INS>::type Sm;
     extern __shared__ __align__(16) uint32_t smem[];
     const SwLayout &ly = p.lay;
     const int tid = threadIdx.x, bs = blockDim.x;
@@ -457,7 +607,15 @@ __global__ void __launch_bounds__(SW_MAX_WARPS * 32, 1) sweep_kernel(SweepParams
         copy32(ly.bsv, p.bsv, p.M);
         copy32(ly.escc, p.esc_c, p.n_esc_c);
         copy32(ly.el, p.el_sca, p.W + 1);
-        if (INS) copy32(ly.tbl, p.ilog, (p.ilog_nz + 1) / 2);
+        if (INS) {
+            copy32(ly.tbl, p.ilog, p.ilog_nz / 2);
+            // the last (odd) entry, then the zero entry at nz
+            if (tid == 0) {
+                uint16_t *t16 = reinterpret_cast<uint16_t *>(smem + ly.tbl);
+                if (p.ilog_nz & 1) t16[p.ilog_nz - 1] = p.ilog[p.ilog_nz - 1];
+                t16[p.ilog_nz] = 0;
+            }
+        }
         copy32(ly.nodes, p.nodes, p.nnodes * 4);
         copy32(ly.io, p.io, p.nio * 4);
         copy32(ly.bifs, p.bifs, p.nbif * 4);
@@ -483,7 +641,7 @@ __global__ void __launch_bounds__(SW_MAX_WARPS * 32, 1) sweep_kernel(SweepParams
     c.lane = lane;
     uint32_t *wsm = smem + ly.warp0 + (size_t)warp * ly.wwords;
     c.buf = wsm;
-    c.begr = wsm + 18 * p.S;
+    c.begr = wsm + 24 * p.S;
     c.bmax = c.begr + p.nbif * p.S;
     c.ring = reinterpret_cast<uint8_t *>(c.bmax + p.S);
     c.rmask = ly.ring_len - 1;
@@ -560,14 +718,14 @@ SwLayout sweep_layout(const SweepParams &p, int warps) {
     L.bsv = take(p.M);
     L.escc = take(p.n_esc_c);
     L.el = take(p.W + 1);
-    L.tbl = take(p.inside ? (p.ilog_nz + 1) / 2 : 0);
+    L.tbl = take(p.inside ? p.ilog_nz / 2 + 1 : 0);
     L.nodes = take((int64_t)p.nnodes * 4);
     L.io = take((int64_t)p.nio * 4);
     L.bifs = take((int64_t)p.nbif * 4);
     int r = 32;
     while (r < p.W + 33) r <<= 1;
     L.ring_len = r;
-    L.wwords = (int)(((int64_t)(18 + p.nbif + 1) * p.S + r / 4 + 3) & ~(int64_t)3);
+    L.wwords = (int)(((int64_t)(24 + p.nbif + 1) * p.S + r / 4 + 3) & ~(int64_t)3);
     L.warp0 = (int)w;
     w += (int64_t)warps * L.wwords;
     L.words = w;
