@@ -46,8 +46,9 @@ sys.path.insert(0, ROOT)
 WORKLOADS = {
     # name: (clen, paired fraction, bifurcations, structure seed, param seed,
     #        semiring, band set, median length, sigma, lo, hi, gc)
+    # sigma 0.78: about 99% of log-normal lengths with median 1500 fall in [200, 20000]
     "batched-uneven-max": dict(clen=120, paired=0.5, nbif=3, sseed=5, pseed=23, semiring=1, band=0,
-                               median=1500, sigma=1.0, lo=200, hi=20000, gc=0.45),
+                               median=1500, sigma=0.78, lo=200, hi=20000, gc=0.45),
     "nohmm-cyk-filter": dict(clen=72, paired=None, nbif=2, sseed=0, pseed=11, semiring=0, band=1,
                              median=100000, sigma=0.0, lo=100000, hi=100000, gc=0.50),
 }
@@ -154,57 +155,114 @@ class ClockSampler:
 
 
 def cpu_baseline(cm, w, buf, wins, budget_s):
-    """The oracle (C restatement of the reference scanner) on the host cores,
-    threads over windows, on a bounded prefix of the batch."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
-    from concurrent.futures import ThreadPoolExecutor
-    oracle.lib()
+    """The oracle (C restatement of the reference scanner, built -O3
+    -march=native on this host) on all host cores, threads over windows.
+
+    Every thread takes windows of the batch in a seeded random order until
+    the time budget is spent; a window started before the deadline is
+    finished (the longest, 20 kb, takes a few seconds on one core), and the
+    rate is the cells of all finished windows over the elapsed time."""
+    oracle = _oracle()
     cores = os.cpu_count() or 1
-    # every core takes seeded-random windows of the batch from a shared queue
-    # until the time budget is spent; the cells of finished windows count
-    # calibrate on the shortest window; windows that would take one core more
-    # than half the budget are left out so the sample ends near the budget
-    order = sorted(range(len(wins)), key=lambda k: wins[k][2] - wins[k][1])
-    o, i0, j0 = wins[order[0]]
-    t1 = time.perf_counter()
-    oracle.qdb_scan(cm, w["semiring"], w["band"], buf[o:o + j0 + 2], i0, j0, CUTOFF_BITS, True)
-    t1 = time.perf_counter() - t1
-    rate1 = cm.count_work(w["semiring"], w["band"], j0 - i0 + 1)[0] / max(t1, 1e-6)
-    fits = [k for k in range(len(wins))
-            if cm.count_work(w["semiring"], w["band"], wins[k][2] - wins[k][1] + 1)[0] / rate1 <= budget_s / 2]
-    perm = [fits[int(k)] for k in np.random.default_rng(7).permutation(len(fits))]
+    perm = [int(k) for k in np.random.default_rng(7).permutation(len(wins))]
     lock = threading.Lock()
-    state = {"next": 0, "cells": 0.0, "res": 0, "n": 0}
+    state = {"next": 0, "cells": 0.0, "res": 0, "n": 0, "maxlen": 0}
     deadline = time.perf_counter() + budget_s
 
-    def worker():
+    rates = [0.0] * cores
+
+    def worker(t):
+        mine, t_start = 0.0, time.perf_counter()
         while time.perf_counter() < deadline:
             with lock:
                 if state["next"] >= len(perm):
-                    return
+                    break
                 k = perm[state["next"]]
                 state["next"] += 1
             o, i0, j0 = wins[k]
             oracle.qdb_scan(cm, w["semiring"], w["band"], buf[o:o + j0 + 2], i0, j0, CUTOFF_BITS, True)
             c, _ = cm.count_work(w["semiring"], w["band"], j0 - i0 + 1)
+            mine += c
             with lock:
                 state["cells"] += c
                 state["res"] += j0 - i0 + 1
                 state["n"] += 1
+                state["maxlen"] = max(state["maxlen"], j0 - i0 + 1)
+        # this thread's own rate: its cells over the time it was busy
+        rates[t] = mine / max(time.perf_counter() - t_start, 1e-9)
 
     t0 = time.perf_counter()
-    ths = [threading.Thread(target=worker) for _ in range(cores)]
+    ths = [threading.Thread(target=worker, args=(t,)) for t in range(cores)]
     for t in ths:
         t.start()
     for t in ths:
         t.join()
     dt = time.perf_counter() - t0
-    tot, res, take = state["cells"], state["res"], [None] * state["n"]
-    return {"value": tot / dt / 1e9, "unit": "Gcells/s", "cores": cores, "kind": "port",
-            "sample": f"{len(take)} windows ({res} residues, {tot:.3e} cells) drawn from the same batch "
-                      f"(windows shorter than half the budget on one core), {dt:.1f} s on {cores} threads",
-            "windows_per_s": len(take) / dt, "cells": tot, "seconds": dt}
+    tot, res, n = state["cells"], state["res"], state["n"]
+    # all cores busy: the sum of the threads' own rates (the last windows of
+    # a sample finish at different times; counting each thread over its own
+    # busy time keeps that tail from diluting the rate)
+    return {"value": sum(rates) / 1e9, "unit": "Gcells/s", "cores": cores, "kind": "port",
+            "build": "gcc -O3 -march=native -ffp-contract=off",
+            "sample": f"{n} windows in seeded random order, every length (longest {state['maxlen']} nt; "
+                      f"{res} residues, {tot:.3e} cells) from the same batch, {dt:.1f} s on {cores} threads",
+            "windows_per_s": n / dt, "cells": tot, "seconds": dt}
+
+
+def _renumber(hits, idx):
+    """Batch hits numbered within a rank's windows -> numbered by job window."""
+    out = hits.copy()
+    out["win"] = np.asarray(idx)[hits["win"]]
+    return out
+
+
+def _oracle():
+    """The oracle, the -march=native build (the timed CPU baseline)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    if oracle._lib is None:
+        oracle.use_native()
+    oracle.lib()
+    return oracle
+
+
+def config2_job(sc, cm, w, nseq, check, stream, flush):
+    """The batched-uneven-windows workload as stated: `nseq` sequences, both
+    strands, every window in ONE persistent launch (device-resident
+    residues).  A seeded sample of `check` windows is scanned by the oracle
+    and must give the same hits."""
+    import torch
+    oracle = _oracle()
+    buf, wins, lens = make_batch(w, nseq, seed=4242)
+    d_buf = torch.from_numpy(buf).cuda()
+    sr, band = w["semiring"], w["band"]
+    flush.fill_(1)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    hits = sc.scan_batch(sr, band, buf, wins, CUTOFF_BITS, True, device_buf=d_buf.data_ptr())
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    st = sc.stats()
+    rng = np.random.default_rng(99)
+    sample = sorted(rng.choice(len(wins), size=min(check, len(wins)), replace=False).tolist())
+    same = True
+    for k in sample:
+        o, i0, j0 = (int(x) for x in wins[k])
+        ref, _, _, _ = oracle.qdb_scan(cm, sr, band, buf[o:o + j0 + 2], i0, j0, CUTOFF_BITS, True)
+        mine = hits[hits["win"] == k]
+        got = [(int(h["i"]), int(h["j"]), h["score"].tobytes(), h["bias"].tobytes()) for h in mine]
+        exp = [(r[0], r[1], np.float32(r[2]).tobytes(), np.float32(r[3]).tobytes()) for r in ref]
+        same = same and got == exp
+    if not same:
+        raise RuntimeError("full-job hits differ from the oracle on the checked windows")
+    del d_buf
+    return {"sequences": int(nseq), "windows": int(len(wins)), "residues": int(2 * lens.sum()),
+            "launches": int(st["kernel_launches"]), "ms": ms, "kernel_ms": st["kernel_ms"],
+            "value": st["cells"] / (ms / 1e3) / 1e9, "unit": "Gcells/s",
+            "seq_per_s": nseq / (ms / 1e3), "cells": st["cells"], "hits": int(len(hits)),
+            "oracle_checked_windows": len(sample), "oracle_identical": bool(same),
+            "timing": "one launch, CUDA events on the library's stream, L2 flushed before"}
 
 
 def main():
@@ -215,7 +273,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="batched-uneven-max",
                     choices=sorted(WORKLOADS) + list(FILTER_WORKLOADS))
-    ap.add_argument("--batch", type=int, default=300, help="sequences per step per rank")
+    ap.add_argument("--batch", type=int, default=500, help="sequences per step per rank")
+    ap.add_argument("--job-seqs", type=int, default=10000,
+                    help="sequences of the full one-launch job measured once at N=1 (0: skip)")
+    ap.add_argument("--job-check", type=int, default=24, help="windows of the full job checked by the oracle")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--plain-windows", type=int, default=16)
@@ -226,13 +287,32 @@ def main():
     w = WORKLOADS[args.workload]
     rank, world, local_rank = env_rank()
     cm = make_model(w)
-    buf, wins, lens = make_batch(w, args.batch, seed=1000 + rank)
+    # one job of world x batch sequences; every rank scans its cost-balanced
+    # share of the job's windows (infernox_b200.shard) and rank 0 gathers the
+    # hits: per-rank work stays fixed as ranks are added (weak scaling)
+    from infernox_b200 import shard
+    job_buf, job_wins, job_lens = make_batch(w, args.batch * world, seed=1000)
+    parts = shard.split_windows(
+        shard.window_cost_fn(cm, w["semiring"], w["band"])(job_wins["j0"] - job_wins["i0"] + 1), world)
+    mine = parts[rank]
+    frames, wl, off = [], [], 0
+    for k in mine:
+        o, i0, j0 = (int(x) for x in job_wins[k])
+        frames.append(job_buf[o:o + j0 + 2])
+        wl.append((off, i0, j0))
+        off += j0 + 2
+    buf = np.concatenate(frames)
+    wins = np.array(wl, dtype=job_wins.dtype)
     config = {"workload": args.workload, "model": f"synthetic CM clen={cm.clen} M={cm.M} W={cm.W}",
               "scan": {0: "CYK f32", 1: "Inside i32"}[w["semiring"]] + " " +
                       {0: "non-banded", 1: "QDB1", 2: "QDB2"}[w["band"]],
               "sequences_per_step_per_rank": int(args.batch), "windows_per_step_per_rank": int(len(wins)),
-              "residues_per_step_per_rank": int(2 * lens.sum()), "cutoff_bits": CUTOFF_BITS,
-              "parallelism": f"dp{world}", "l2": "flushed (256 MB write) before each timed step"}
+              "residues_per_step_per_rank": int((wins["j0"] - wins["i0"] + 1).sum()),
+              "sequences_per_step_job": int(args.batch * world), "cutoff_bits": CUTOFF_BITS,
+              "lengths": f"log-normal median {w['median']} sigma {w['sigma']} clipped to [{w['lo']}, {w['hi']}], "
+                         f"both strands",
+              "parallelism": f"dp{world}: cost-balanced window split, hits gathered to rank 0",
+              "l2": "flushed (256 MB write) before each timed step"}
 
     if args.impl == "reference":
         if rank != 0:
@@ -242,9 +322,12 @@ def main():
             cpu_baseline(cm, w, buf, [tuple(x) for x in wins], per_step)
         samples = [cpu_baseline(cm, w, buf, [tuple(x) for x in wins], per_step) for _ in range(args.steps)]
         cells, secs = sum(x["cells"] for x in samples), sum(x["seconds"] for x in samples)
-        cb = {"value": cells / secs / 1e9, "unit": "Gcells/s", "cores": samples[0]["cores"], "kind": "port",
-              "sample": f"{args.steps} steps of {per_step:.1f} s, each a bounded random sample of the batch's "
-                        f"windows on {samples[0]['cores']} threads (after {args.warmup} warm-up samples)"}
+        rate = sum(x["value"] * x["seconds"] for x in samples) / secs
+        cb = {"value": rate, "unit": "Gcells/s", "cores": samples[0]["cores"], "kind": "port",
+              "build": samples[0]["build"],
+              "sample": f"{args.steps} steps of about {per_step:.1f} s, each a seeded random sample of the "
+                        f"batch's windows of every length on {samples[0]['cores']} threads (after "
+                        f"{args.warmup} warm-up samples); rate = sum of the threads' own rates"}
         line = {"impl": "reference", "metric": "CYK/Inside scan Gcells/s", "value": cb["value"],
                 "unit": "Gcells/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": 1e3 * secs / max(1, args.steps),
@@ -280,7 +363,10 @@ def main():
     def step_e2e():
         return sc.scan_batch(sr, band, buf, wins, CUTOFF_BITS, True)
 
-    tune = sc.autotune(sr, band, buf, wins, CUTOFF_BITS, device_buf=d_buf.data_ptr())
+    # launch shape tuned on the first 400 windows of the step's batch
+    tw = wins[: min(len(wins), 400)]
+    tb = buf[: int(tw[-1]["dsq_offset"]) + int(tw[-1]["j0"]) + 2]
+    tune = sc.autotune(sr, band, tb, tw, CUTOFF_BITS, device_buf=d_buf.data_ptr())
     for _ in range(args.warmup):
         hits = step_device()
     ref_hits = hits
@@ -307,12 +393,13 @@ def main():
     if not np.array_equal(hits, ref_hits):
         raise RuntimeError("hit lists differ between steps")
     total_ms = sum(times)
-    # e2e through the host-buffer API
+    # e2e through the host-buffer API (up to 5 steps)
+    e2e_steps = min(args.steps, 5)
     for _ in range(1):
         step_e2e()
     barrier()
     etimes = []
-    for _ in range(args.steps):
+    for _ in range(e2e_steps):
         flush.fill_(1)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -323,14 +410,17 @@ def main():
     barrier()
     if not np.array_equal(eh, ref_hits):
         raise RuntimeError("e2e hits differ from the device-resident path")
-    e2e_ms = sum(etimes)
+    e2e_ms = sum(etimes) * args.steps / e2e_steps  # scaled to the timed step count
 
     total_ms_all, e2e_ms_all, cells_all = aggregate_ranks(dist, total_ms, e2e_ms, cells)
+
+    # the job's hits: every rank's, numbered by job window, gathered to rank 0
+    job_hits = shard.finalize(shard.gather_hits(dist, _renumber(ref_hits, mine), rank, world) or [])
 
     plain = None
     cb = None
     if rank == 0 and args.plain_windows > 0:
-        # plain comparator: one launch and one CTA per window, same windows
+        # plain comparator: one launch per window over its own work items, same windows
         k = min(args.plain_windows, len(wins))
         sub = wins[:k]
         sc.scan_batch(sr, band, buf, sub, CUTOFF_BITS, True, plain=True)
@@ -346,13 +436,16 @@ def main():
             raise RuntimeError("plain and batched scans differ")
         plain = {"value": pst["cells"] / (pms / 1e3) / 1e9, "unit": "Gcells/s", "windows": k,
                  "launches": pst["kernel_launches"], "ms": pms}
+    job = None
+    if rank == 0 and world == 1 and args.job_seqs > 0:
+        job = config2_job(sc, cm, w, args.job_seqs, args.job_check, stream, flush)
     if rank == 0:
         if not args.no_cpu:
             cb = cpu_baseline(cm, w, buf, [tuple(x) for x in wins], args.cpu_seconds)
 
     if rank == 0:
         value = cells_all / (total_ms_all / 1e3) / 1e9
-        e2e = cells_all / (e2e_ms_all / 1e3) / 1e9
+        e2e = cells_all / (e2e_ms_all / 1e3) / 1e9  # e2e_ms is scaled to the same step count
         kernel_ms = sum(kms) / max(1, launches)
         ops_launch = (terms * OPS_PER_TERM[sr] + cells * OPS_PER_CELL) / max(1, launches)
         sm_mhz = clk["sm_mhz"]
@@ -394,6 +487,9 @@ def main():
                              "tuned_over": [(t["lanes"], t["chunk"], round(t["kernel_ms"], 1))
                                             for t in tune["trials"]]},
             "hits_per_step": int(len(ref_hits)),
+            "hits_per_job_step": int(len(job_hits)),
+            "e2e_steps": e2e_steps,
+            "config2_job": job,
         }
         print(json.dumps(line))
     sc.close()

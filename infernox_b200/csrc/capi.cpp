@@ -383,6 +383,10 @@ static int run_scan(cmgpu_model *m, cmgpu_workspace *ws, int semiring, int qdbid
         sp.beginsc_all = dp->beginsc_all;
     }
     sp.deck_elems = pl.deck_elems;
+    // per-state tables in global memory when they alone would fill most of
+    // the shared memory (models of a few thousand states)
+    sp.tables_global = 0;
+    if ((size_t)scan_layout(sp, 1, false).words * 4 > 120 * 1024) sp.tables_global = 1;
     sp.ilog = m->ilog;
     sp.ilog_nz = m->ilog_nz;
     sp.dsq = d_dsq;
@@ -540,7 +544,23 @@ static int run_scan(cmgpu_model *m, cmgpu_workspace *ws, int semiring, int qdbid
                              ws->stream));
     size_t cand_cap = std::max<size_t>(ws->cands_cap, 1 << 16);
     if ((rc = ensure_dev(&ws->d_cands, &ws->cands_cap, cand_cap))) return rc;
-    const int ctas = (int)std::min<int64_t>(((int64_t)items.size() + best_l - 1) / best_l, max_ctas);
+    if (!sweep && !deck_smem && (int64_t)items.size() < best_l) {
+        // fewer work items than lanes: no deck for lanes that would stay idle
+        best_l = (int)items.size();
+        sp.lanes = best_l;
+        sp.lay = scan_layout(sp, best_l, false);
+        ws->stats.lanes = best_l;
+    }
+    int ctas = (int)std::min<int64_t>(((int64_t)items.size() + best_l - 1) / best_l, max_ctas);
+    if (!sweep && !deck_smem) {
+        // global decks of large models: keep them within half of the free device memory
+        size_t freeb = 0, totalb = 0;
+        CUDA_TRY(cudaMemGetInfo(&freeb, &totalb));
+        const size_t per_cta = (((size_t)pl.deck_elems + 31) & ~(size_t)31) * 4 * (size_t)best_l;
+        const size_t have = freeb / 2 + (ws->deck_cap * 4);
+        const int fit = (int)std::max<size_t>(1, have / std::max<size_t>(per_cta, 1));
+        ctas = std::min(ctas, fit);
+    }
     ws->stats.ctas = ctas;
     if (sweep) {
         if ((rc = ensure_dev(&ws->d_sweep, &ws->sweep_cap, (size_t)swp.gstride * (size_t)ctas * (size_t)best_l)))

@@ -72,6 +72,9 @@ struct ScanParams {
     int cand_cap;
     int *cand_count;
     float cutoff;
+    // per-state tables read from global memory instead of shared memory
+    // (models whose tables would not leave room for a lane)
+    int tables_global;
     // lanes per CTA and deck placement
     int lanes;
     int deck_smem;

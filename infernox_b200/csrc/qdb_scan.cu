@@ -332,16 +332,31 @@ __global__ void __launch_bounds__(512, 1) qdb_scan_kernel(ScanParams p) {
     k.nz = p.ilog_nz;
     k.s.el = smem + ly.el;
     k.s.tbl = reinterpret_cast<const uint16_t *>(smem + ly.tbl);
-    k.s.info = reinterpret_cast<const int4 *>(smem + ly.info);
-    k.s.wb = reinterpret_cast<const int32_t *>(smem + ly.wb);
-    k.s.cb = reinterpret_cast<const int32_t *>(smem + ly.cb);
-    k.s.tsc = smem + ly.tsc;
-    k.s.endsc = smem + ly.endsc;
-    k.s.escc = smem + ly.escc;
-    k.s.chunks = reinterpret_cast<const int2 *>(smem + ly.chunks);
-    k.s.lvl = reinterpret_cast<const int32_t *>(smem + ly.lvl);
-    k.s.begin = reinterpret_cast<const int4 *>(smem + ly.begin);
-    k.s.beginsc = smem + ly.beginsc;
+    if (p.tables_global) {
+        // large models: the per-state tables are read from global memory
+        // (read-only, cached in L1) instead of being copied to shared memory
+        k.s.info = reinterpret_cast<const int4 *>(p.states);
+        k.s.wb = p.wb;
+        k.s.cb = p.cb;
+        k.s.tsc = p.tsc;
+        k.s.endsc = p.endsc;
+        k.s.escc = p.esc_c;
+        k.s.chunks = reinterpret_cast<const int2 *>(p.chunks);
+        k.s.lvl = p.level_start;
+        k.s.begin = reinterpret_cast<const int4 *>(p.begins);
+        k.s.beginsc = p.beginsc;
+    } else {
+        k.s.info = reinterpret_cast<const int4 *>(smem + ly.info);
+        k.s.wb = reinterpret_cast<const int32_t *>(smem + ly.wb);
+        k.s.cb = reinterpret_cast<const int32_t *>(smem + ly.cb);
+        k.s.tsc = smem + ly.tsc;
+        k.s.endsc = smem + ly.endsc;
+        k.s.escc = smem + ly.escc;
+        k.s.chunks = reinterpret_cast<const int2 *>(smem + ly.chunks);
+        k.s.lvl = reinterpret_cast<const int32_t *>(smem + ly.lvl);
+        k.s.begin = reinterpret_cast<const int4 *>(smem + ly.begin);
+        k.s.beginsc = smem + ly.beginsc;
+    }
     k.s.ring = reinterpret_cast<uint8_t *>(smem + ly.ring);
     k.s.lane = reinterpret_cast<int32_t *>(smem + ly.lane);
     k.s.bsv = smem + ly.bsv;
@@ -363,16 +378,18 @@ __global__ void __launch_bounds__(512, 1) qdb_scan_kernel(ScanParams p) {
         };
         copy32(ly.el, p.el_sca, p.W + 1);
         if (INS) copy32(ly.tbl, p.ilog, (p.ilog_nz + 1) / 2);
-        copy32(ly.info, p.states, p.M * 4);
-        copy32(ly.wb, p.wb, p.M * 2);
-        copy32(ly.cb, p.cb, p.M * 12);
-        copy32(ly.tsc, p.tsc, p.M * 6);
-        copy32(ly.endsc, p.endsc, p.M);
-        copy32(ly.escc, p.esc_c, p.n_esc_c);
-        copy32(ly.chunks, p.chunks, p.nchunks * 2);
-        copy32(ly.lvl, p.level_start, p.nlev + 1);
-        copy32(ly.begin, p.begins, p.nbegin * 4);
-        copy32(ly.beginsc, p.beginsc, p.nbegin);
+        if (!p.tables_global) {
+            copy32(ly.info, p.states, p.M * 4);
+            copy32(ly.wb, p.wb, p.M * 2);
+            copy32(ly.cb, p.cb, p.M * 12);
+            copy32(ly.tsc, p.tsc, p.M * 6);
+            copy32(ly.endsc, p.endsc, p.M);
+            copy32(ly.escc, p.esc_c, p.n_esc_c);
+            copy32(ly.chunks, p.chunks, p.nchunks * 2);
+            copy32(ly.lvl, p.level_start, p.nlev + 1);
+            copy32(ly.begin, p.begins, p.nbegin * 4);
+            copy32(ly.beginsc, p.beginsc, p.nbegin);
+        }
         if (INS && p.fuse_begin) {
             copy32(ly.bsv, p.beginsc_all, p.M);
             for (int x = tid; x < lanes * (p.root_dxcap + 1); x += bs) k.s.bmax[x] = -INFTY_D;
@@ -607,16 +624,17 @@ SmemLayout scan_layout(const ScanParams &p, int lanes, bool deck_smem) {
     };
     L.el = take(p.W + 1);
     L.tbl = take(p.inside ? (p.ilog_nz + 1) / 2 : 0);
-    L.info = take((int64_t)p.M * 4);
-    L.wb = take((int64_t)p.M * 2);
-    L.cb = take((int64_t)p.M * 12);
-    L.tsc = take((int64_t)p.M * 6);
-    L.endsc = take(p.M);
-    L.escc = take(p.n_esc_c);
-    L.chunks = take((int64_t)p.nchunks * 2);
-    L.lvl = take(p.nlev + 1);
-    L.begin = take((int64_t)p.nbegin * 4);
-    L.beginsc = take(p.nbegin);
+    const int64_t g = p.tables_global ? 0 : 1;  // per-state tables in shared memory?
+    L.info = take(g * p.M * 4);
+    L.wb = take(g * p.M * 2);
+    L.cb = take(g * p.M * 12);
+    L.tsc = take(g * p.M * 6);
+    L.endsc = take(g * p.M);
+    L.escc = take(g * p.n_esc_c);
+    L.chunks = take(g * p.nchunks * 2);
+    L.lvl = take(g * (p.nlev + 1));
+    L.begin = take(g * p.nbegin * 4);
+    L.beginsc = take(g * p.nbegin);
     int r = 1;
     while (r < p.W + 64) r <<= 1;
     L.ring_len = r;

@@ -42,6 +42,14 @@ def models(name: str):
         cm = synth.synth_cm(synth.structure(120, 0.5, 3, 5), 23, name=name)
     elif name == "mb3":
         cm = synth.synth_cm(synth.structure(90, 0.4, 3, 6, layout="multibranch"), 24, name=name)
+    elif name == "cfg0":
+        # the --nohmm CYK workload's model shape: 72 columns, a 7 bp closing
+        # stem around three 5 bp hairpins (a 4-stem multibranch)
+        cm = synth.synth_cm(synth.trna_like(), 11, name=name)
+    elif name == "cfg3":
+        # the bifurcation-heavy truncated workload's model shape: 1500
+        # columns, 60% paired, 25 bifurcations
+        cm = synth.synth_cm(synth.structure(1500, 0.6, 25, 31), 33, name=name)
     else:
         raise KeyError(name)
     r = (cm, model.configure(cm, local=False), model.configure(cm, local=True))
