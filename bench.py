@@ -274,6 +274,8 @@ def main():
     ap.add_argument("--workload", default="batched-uneven-max",
                     choices=sorted(WORKLOADS) + list(FILTER_WORKLOADS))
     ap.add_argument("--batch", type=int, default=500, help="sequences per step per rank")
+    ap.add_argument("--kernel", default="auto", choices=["auto", "level", "sweep"],
+                    help="QDB scan kernel (CMGPU_KERNEL_*)")
     ap.add_argument("--job-seqs", type=int, default=10000,
                     help="sequences of the full one-launch job measured once at N=1 (0: skip)")
     ap.add_argument("--job-check", type=int, default=24, help="windows of the full job checked by the oracle")
@@ -348,6 +350,7 @@ def main():
     from infernox_b200 import scan
     stream = torch.cuda.current_stream()
     sc = scan.Scanner(cm, device=local_rank, stream=stream.cuda_stream)
+    sc.set_kernel({"auto": scan.KERNEL_AUTO, "level": scan.KERNEL_LEVEL, "sweep": scan.KERNEL_SWEEP}[args.kernel])
     d_buf = torch.from_numpy(buf).cuda()
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device="cuda")
     sr, band = w["semiring"], w["band"]
@@ -486,6 +489,7 @@ def main():
                              "chunk": tune["best"]["chunk"],
                              "tuned_over": [(t["lanes"], t["chunk"], round(t["kernel_ms"], 1))
                                             for t in tune["trials"]]},
+            "kernel": {1: "level", 2: "sweep"}.get(sc.stats()["kernel"], "?"),
             "hits_per_step": int(len(ref_hits)),
             "hits_per_job_step": int(len(job_hits)),
             "e2e_steps": e2e_steps,
