@@ -652,7 +652,7 @@ def filter_main(args):
                                     "(per-state i/j rectangles of +-20 around the homolog's consensus coordinates)",
                        "band_cells_per_step": cells_step})
     if kind in ("trq-inside", "trq-cyk", "hb-trcyk"):
-        tri = hb.synthetic_tr_inputs(cm_s, cfg, True)
+        tri = hb.tr_inputs(cm_s, cfg, 4, True)
     if kind == "hb-trcyk":
         ones = np.ones(cfg.M, np.uint8)
         valid = (ones, ones, ones, ones)

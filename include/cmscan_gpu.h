@@ -165,6 +165,24 @@ int cmgpu_prep_configure(const cmgpu_cm_params *p, int local, int32_t W_in,
                          double beta1, double beta2, double betaW,
                          cmgpu_cm_scores *out);
 
+/* Inputs of the truncated scanners for a configured CM, all caller
+ * allocated: the marginal emission scores (fill_marginal_emissions,
+ * src/cp9.rs:4441) lmesc/rmesc and ilmesc/irmesc [M*18]; the truncated-begin
+ * penalties of the local (local != 0) or global configuration
+ * (TrPenalties::new, src/cm_trunc.rs:192, from the expected state occupancy
+ * of src/cp9.rs:752 and the emit map of src/cp9.rs:144) as rows [3][M] --
+ * 5'-and-3', 5'-only, 3'-only, the order of pty_idx_for_pass -- in pty (log2)
+ * and ipty (Prob2Score); and the node span lpos/rpos [M] allow_truncation
+ * reads for each state (src/cm_dpsearch_trunc.rs:2395-2406). */
+typedef struct cmgpu_tr_prep {
+    float *lmesc, *rmesc;
+    int32_t *ilmesc, *irmesc;
+    float *pty;
+    int32_t *ipty;
+    int32_t *lpos, *rpos;
+} cmgpu_tr_prep;
+int cmgpu_prep_truncated(const cmgpu_cm_params *p, int local, cmgpu_tr_prep *out);
+
 /* ILogsum table (src/cp9.rs:28-44): tbl[0..n) with n <= 23000. */
 int cmgpu_ilogsum_table(int32_t *tbl, int32_t n);
 /* FLogsum table (src/cp9.rs:5391-5400). */

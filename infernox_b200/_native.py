@@ -36,6 +36,15 @@ class CmParams(C.Structure):
     ]
 
 
+class TrPrep(C.Structure):
+    _fields_ = [
+        ("lmesc", P(C.c_float)), ("rmesc", P(C.c_float)),
+        ("ilmesc", P(C.c_int32)), ("irmesc", P(C.c_int32)),
+        ("pty", P(C.c_float)), ("ipty", P(C.c_int32)),
+        ("lpos", P(C.c_int32)), ("rpos", P(C.c_int32)),
+    ]
+
+
 class Cm(C.Structure):
     _fields_ = [
         ("M", C.c_int32), ("W", C.c_int32), ("flags", C.c_uint32),
@@ -157,6 +166,7 @@ def lib() -> C.CDLL:
     L.cmgpu_version.restype = C.c_char_p
     L.cmgpu_prep_configure.argtypes = [P(CmParams), C.c_int, C.c_int32, C.c_double, C.c_double,
                                        C.c_double, P(CmScores)]
+    L.cmgpu_prep_truncated.argtypes = [P(CmParams), C.c_int, P(TrPrep)]
     L.cmgpu_ilogsum_table.argtypes = [P(C.c_int32), C.c_int32]
     L.cmgpu_flogsum_table.argtypes = [P(C.c_float), C.c_int32]
     L.cmgpu_model_upload.argtypes = [P(Cm), C.c_int, P(vp)]
@@ -234,7 +244,7 @@ def check(rc: int) -> None:
 
 # symbols declared in include/cmscan_gpu.h (checked by the CPU test suite)
 EXPORTED = [
-    "cmgpu_last_error", "cmgpu_version", "cmgpu_prep_configure", "cmgpu_ilogsum_table",
+    "cmgpu_last_error", "cmgpu_version", "cmgpu_prep_configure", "cmgpu_prep_truncated", "cmgpu_ilogsum_table",
     "cmgpu_flogsum_table", "cmgpu_model_upload", "cmgpu_model_free", "cmgpu_workspace_create",
     "cmgpu_workspace_free", "cmgpu_workspace_stats", "cmgpu_workspace_set_shape", "cmgpu_workspace_set_kernel",
     "cmgpu_qdb_scan", "cmgpu_qdb_scan_noalloc", "cmgpu_qdb_scan_cells", "cmgpu_cyk_seq_filter", "cmgpu_final_stage_inside_opt",

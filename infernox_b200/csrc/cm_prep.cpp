@@ -441,3 +441,292 @@ extern "C" int cmgpu_flogsum_table(float *tbl, int32_t n) {
     }
     return CMGPU_OK;
 }
+
+// ===========================================================================
+// Truncated-scan inputs: marginal emission scores and truncated-begin
+// penalties of a configured CM.
+// ===========================================================================
+namespace {
+
+// unique state ids (src/constants.rs:46-81)
+constexpr int ID_MATP_MP = 6, ID_MATP_IL = 10, ID_MATL_ML = 12, ID_MATR_MR = 15, ID_BIF_B = 18, ID_END_E = 19;
+
+// Prob2Score of the CP9/truncation code (src/cp9.rs:977-997, src/cm_trunc.rs:
+// 176-185): the ratio in f32, sreLOG2 in f64, -INFTY for p == 0 and for a
+// non-finite result, never below -INFTY.
+int prob2score_f(float p, float null) {
+    if (p == 0.0f) return -INFTY;
+    float ratio = p / null;
+    double v = std::floor(0.5 + 1000.0 * sre_log2((double)ratio));
+    if (!std::isfinite(v)) return -INFTY;
+    double c = std::max(v, (double)INT32_MIN);
+    c = std::min(c, (double)INT32_MAX);
+    return std::max((int)c, -INFTY);
+}
+
+// esl_abc_FExpectScore / IExpectScore over the background (src/cp9.rs:4380-4420)
+float fexpect(int x, const float *sc, const float *p) {
+    if (!is_residue(x)) return 0.0f;
+    float r = 0.0f, den = 0.0f;
+    for (int i = 0; i < K; i++)
+        if (degen(x, i)) {
+            r += sc[i] * p[i];
+            den += p[i];
+        }
+    return r / den;
+}
+int iexpect(int x, const int *sc, const float *p) {
+    if (!is_residue(x)) return 0;
+    float r = 0.0f, den = 0.0f;
+    for (int i = 0; i < K; i++)
+        if (degen(x, i)) {
+            r += (float)sc[i] * p[i];
+            den += p[i];
+        }
+    r /= den;
+    return r < 0.0f ? (int)(r - 0.5f) : (int)(r + 0.5f);
+}
+
+// fill_marginal_emissions (src/cp9.rs:4441-4530): [M][18] left / right
+// marginal scores, float and integer.
+void marginals(const Model &cm, float *lm, float *rm, int32_t *ilm, int32_t *irm) {
+    for (int v = 0; v < cm.M; v++) {
+        float *L = lm + (size_t)v * KP, *R = rm + (size_t)v * KP;
+        int32_t *IL = ilm + (size_t)v * KP, *IR = irm + (size_t)v * KP;
+        for (int x = 0; x < KP; x++) {
+            L[x] = R[x] = 0.0f;
+            IL[x] = IR[x] = 0;
+        }
+        for (int x : {K, KP - 2, KP - 1}) {
+            L[x] = R[x] = IMPOSSIBLE;
+            IL[x] = IR[x] = -INFTY;
+        }
+        const int st = cm.sttype[v];
+        const float *e = &cm.e[(size_t)v * 16];
+        if (st == MP_ST) {
+            float l4[K] = {0, 0, 0, 0}, r4[K] = {0, 0, 0, 0};
+            for (int x = 0; x < K; x++)
+                for (int y = 0; y < K; y++) {
+                    l4[x] += e[x * K + y];
+                    r4[y] += e[x * K + y];
+                }
+            for (int x = 0; x < K; x++) {
+                IL[x] = prob2score_f(l4[x], cm.null[x]);
+                IR[x] = prob2score_f(r4[x], cm.null[x]);
+                L[x] = (float)sre_log2((double)(l4[x] / cm.null[x]));
+                R[x] = (float)sre_log2((double)(r4[x] / cm.null[x]));
+            }
+            for (int x = K + 1; x <= KP - 3; x++) {
+                L[x] = fexpect(x, L, cm.null);
+                R[x] = fexpect(x, R, cm.null);
+                IL[x] = iexpect(x, IL, cm.null);
+                IR[x] = iexpect(x, IR, cm.null);
+            }
+        } else if (st == ML_ST || st == IL_ST || st == MR_ST || st == IR_ST) {
+            const bool left = st == ML_ST || st == IL_ST;
+            float *F = left ? L : R;
+            int32_t *I = left ? IL : IR;
+            for (int x = 0; x < K; x++) {
+                F[x] = (float)sre_log2((double)(e[x] / cm.null[x]));
+                I[x] = prob2score_f(e[x], cm.null[x]);
+            }
+            for (int x = K + 1; x <= KP - 3; x++) {
+                F[x] = fexpect(x, F, cm.null);
+                I[x] = iexpect(x, I, cm.null);
+            }
+        }
+    }
+}
+
+// CreateEmitMap (src/cp9.rs:144-208): left / right consensus column per node.
+void emit_map(const Model &cm, const std::vector<int32_t> &ndidx, std::vector<int> &lpos, std::vector<int> &rpos) {
+    lpos.assign(cm.nodes, -1);
+    rpos.assign(cm.nodes, -1);
+    int cpos = 0;
+    std::vector<std::pair<int, int>> stack{{0, 0}};  // (on_right, node)
+    while (!stack.empty()) {
+        auto [on_right, nd] = stack.back();
+        stack.pop_back();
+        const int t = cm.ndtype[nd];
+        if (on_right) {
+            rpos[nd] = cpos + 1;
+            if (t == MATP_ND || t == MATR_ND) cpos++;
+            continue;
+        }
+        if (t == MATP_ND || t == MATL_ND) cpos++;
+        lpos[nd] = cpos;
+        stack.push_back({1, nd});
+        if (t == BIF_ND) {
+            const int s = cm.nodemap[nd];
+            stack.push_back({0, ndidx[cm.cnum[s]]});
+            stack.push_back({0, ndidx[cm.cfirst[s]]});
+        } else if (t != END_ND) {
+            stack.push_back({0, nd + 1});
+        }
+    }
+}
+
+}  // namespace
+
+namespace {
+
+// cm_ExpectedStateOccupancy (src/cp9.rs:752-838) of the global CM: psi[v],
+// the expected number of times a parse enters state v.  The transition from
+// parent x to v is x's child offset of v (the reference's transition map
+// gives the same index for every parent / child pair of a CM).
+bool state_occupancy(const Model &cm, const int32_t *plast, const int32_t *pnum, std::vector<double> &psi) {
+    psi.assign(cm.M, 0.0);
+    for (int v = 0; v < cm.M; v++) {
+        const int st = cm.sttype[v];
+        if (st == S_ST) {
+            psi[v] = 1.0;
+            continue;
+        }
+        const int ins = (st == IL_ST || st == IR_ST) ? 1 : 0;
+        for (int y = pnum[v] - 1; y >= ins; y--) {
+            const int x = plast[v] - y;
+            const int off = v - cm.cfirst[x];
+            if (x < 0 || off < 0 || off >= cm.cnum[x]) return false;
+            psi[v] += psi[x] * (double)cm.t[(size_t)x * MAXC + off];
+        }
+        if (ins) {
+            const double t0 = (double)cm.t[(size_t)v * MAXC];
+            psi[v] += psi[v] * (t0 / (1.0 - t0));
+        }
+    }
+    return true;
+}
+
+// InsertsGivenNodeIndex (src/cm_trunc.rs:111-124)
+std::pair<int, int> inserts_of(const Model &cm, int nd) {
+    if (nd < 0) return {-1, -1};
+    const int v = cm.nodemap[nd];
+    switch (cm.ndtype[nd]) {
+    case MATP_ND: return {v + 4, v + 5};
+    case MATL_ND:
+    case MATR_ND: return {v + 2, -1};
+    case BEGR_ND: return {v + 1, -1};
+    case ROOT_ND: return {v + 1, v + 2};
+    default: return {-1, -1};
+    }
+}
+
+// cm_tr_penalties_Create with ignore_inserts = FALSE (TrPenalties::new,
+// src/cm_trunc.rs:192-385): truncated-begin penalties [3][M] (rows
+// 5'-and-3', 5'-only, 3'-only), global g / ig and local l / il.
+void tr_penalties(const Model &cm, const int32_t *ndidx, const int32_t *plast, const std::vector<int> &elpos,
+                  const std::vector<int> &erpos, const std::vector<double> &psi, std::vector<float> &g,
+                  std::vector<int32_t> &ig, std::vector<float> &l, std::vector<int32_t> &il) {
+    const int M = cm.M, clen = cm.clen;
+    g.assign((size_t)3 * M, IMPOSSIBLE);
+    l.assign((size_t)3 * M, IMPOSSIBLE);
+    ig.assign((size_t)3 * M, -INFTY);
+    il.assign((size_t)3 * M, -INFTY);
+    const float g53 = (float)(2.0 / (double)(clen * (clen + 1)));
+    const float g5or3 = (float)(1.0 / (double)clen);
+    // local begin probabilities with the C float / double mix
+    std::vector<float> begin(M, 0.0f);
+    int nstarts = 0;
+    for (int nd = 2; nd < cm.nodes; nd++) {
+        const int t = cm.ndtype[nd];
+        if (t == MATP_ND || t == MATL_ND || t == MATR_ND || t == BIF_ND) nstarts++;
+    }
+    if (cm.nodes > 1) begin[cm.nodemap[1]] = (float)(1.0 - (double)cm.pbegin);
+    const float pb = cm.pbegin / (float)nstarts;
+    for (int nd = 2; nd < cm.nodes; nd++) {
+        const int t = cm.ndtype[nd];
+        if (t == MATP_ND || t == MATL_ND || t == MATR_ND || t == BIF_ND) begin[cm.nodemap[nd]] = pb;
+    }
+    float prv5 = 0.0f, prv3 = 0.0f, prv53 = 0.0f;
+    for (int nd = 0; nd < cm.nodes; nd++) {
+        const int t = cm.ndtype[nd];
+        const int lpos = (t == MATP_ND || t == MATL_ND) ? elpos[nd] : elpos[nd] + 1;
+        const int rpos = (t == MATP_ND || t == MATR_ND) ? erpos[nd] : erpos[nd] - 1;
+        if (t == END_ND) {
+            prv5 = prv3 = prv53 = 0.0f;
+        } else if (t == BEGL_ND || t == BEGR_ND) {
+            const int b = plast[cm.nodemap[nd]];
+            prv5 = t == BEGL_ND ? 0.0f : l[(size_t)1 * M + b];
+            prv3 = t == BEGR_ND ? 0.0f : l[(size_t)2 * M + b];
+            prv53 = l[b];
+        } else if (t == MATP_ND || t == MATL_ND || t == MATR_ND || t == BIF_ND) {
+            const int m = cm.nodemap[nd];
+            const auto ins = inserts_of(cm, nd - 1);
+            const float m_psi = (float)psi[m];
+            const float i1_psi = ins.first >= 0 ? (float)psi[ins.first] : 0.0f;
+            const float i2_psi = ins.second >= 0 ? (float)psi[ins.second] : 0.0f;
+            const float summed = m_psi + i1_psi + i2_psi;
+            auto set = [&](std::vector<float> &a, int row, float prob) {
+                a[(size_t)row * M + m] = (m_psi / summed) * prob;
+                if (ins.first >= 0) a[(size_t)row * M + ins.first] = (i1_psi / summed) * prob;
+                if (ins.second >= 0) a[(size_t)row * M + ins.second] = (i2_psi / summed) * prob;
+            };
+            set(g, 0, g53);
+            if (rpos == clen) set(g, 1, g5or3);
+            if (lpos == 1) set(g, 2, g5or3);
+            const int sub = rpos - lpos + 1;
+            const int nfrag53 = (sub * (sub + 1)) / 2;
+            const float cur5 = begin[m] / (float)sub + prv5;
+            const float cur3 = begin[m] / (float)sub + prv3;
+            const float cur53 = begin[m] / (float)nfrag53 + prv53;
+            set(l, 0, cur53);
+            set(l, 1, cur5);
+            set(l, 2, cur3);
+            prv5 = t == MATL_ND ? cur5 : 0.0f;
+            prv3 = t == MATR_ND ? cur3 : 0.0f;
+            prv53 = cur53;
+        }
+    }
+    for (int v = 0; v < M; v++) {
+        const int id = cm.stid[v], st = cm.sttype[v];
+        const bool detached = v + 1 < M && cm.stid[v + 1] == ID_END_E;
+        const bool qualifies = id == ID_MATP_MP || id == ID_MATL_ML || id == ID_MATR_MR || id == ID_BIF_B ||
+                               ((st == IL_ST || st == IR_ST) && !detached);
+        if (!qualifies) continue;
+        if (id == ID_MATP_IL && cm.ndtype[ndidx[v] + 1] == END_ND) continue;
+        for (int r = 0; r < 3; r++) {
+            float &x = g[(size_t)r * M + v];
+            if (x > IMPOSSIBLE + 1.0f) {
+                ig[(size_t)r * M + v] = prob2score_f(x, 1.0f);
+                x = (float)sre_log2((double)x);
+            }
+            float &y = l[(size_t)r * M + v];
+            il[(size_t)r * M + v] = prob2score_f(y, 1.0f);
+            y = (float)sre_log2((double)y);
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" int cmgpu_prep_truncated(const cmgpu_cm_params *p, int local, cmgpu_tr_prep *out) {
+    if (!p || !out || p->M < 2 || p->nodes < 2 || !p->sttype || !p->t || !p->e || !p->plast || !p->pnum ||
+        !p->ndidx || !out->lmesc || !out->rmesc || !out->ilmesc || !out->irmesc || !out->pty || !out->ipty ||
+        !out->lpos || !out->rpos) {
+        cmx::set_error("cmgpu_prep_truncated: bad arguments");
+        return CMGPU_EINVAL;
+    }
+    Model cm = load(p);
+    marginals(cm, out->lmesc, out->rmesc, out->ilmesc, out->irmesc);
+    std::vector<int32_t> ndidx(p->ndidx, p->ndidx + cm.M);
+    std::vector<int> elpos, erpos;
+    emit_map(cm, ndidx, elpos, erpos);
+    std::vector<double> psi;
+    if (!state_occupancy(cm, p->plast, p->pnum, psi)) {
+        cmx::set_error("cmgpu_prep_truncated: a parent does not list the state among its children");
+        return CMGPU_EINVAL;
+    }
+    std::vector<float> g, l;
+    std::vector<int32_t> ig, il;
+    tr_penalties(cm, p->ndidx, p->plast, elpos, erpos, psi, g, ig, l, il);
+    const std::vector<float> &pt = local ? l : g;
+    const std::vector<int32_t> &ipt = local ? il : ig;
+    std::copy(pt.begin(), pt.end(), out->pty);
+    std::copy(ipt.begin(), ipt.end(), out->ipty);
+    for (int v = 0; v < cm.M; v++) {
+        const int nd = ndidx[v], t = cm.ndtype[nd];
+        out->lpos[v] = (t == MATP_ND || t == MATL_ND) ? elpos[nd] : elpos[nd] + 1;
+        out->rpos[v] = (t == MATP_ND || t == MATR_ND) ? erpos[nd] : erpos[nd] - 1;
+    }
+    return CMGPU_OK;
+}

@@ -373,72 +373,36 @@ def tr_qdb_stats(sc: Scanner):
     return ms.value, cells.value, launches.value
 
 
-# canonical residues (bit a = residue a) of each RNA code 0..17
-_DEGEN_BITS = [0x1, 0x2, 0x4, 0x8, 0x0, 0x5, 0xA, 0x3, 0xC, 0x6, 0x9, 0xB, 0xE, 0x7, 0xD, 0xF, 0x0, 0x0]
+# row of the truncated-begin penalties a pass uses (pty_idx_for_pass,
+# src/cm_trunc.rs:99-107): 5'-and-3' (forced or any), 5'-only, 3'-only
+PTY_ROW = {2: 1, 3: 2, 4: 0, 5: 0}
 
 
-def synthetic_tr_inputs(cm_s, cfg, local: bool) -> TrInputs:
-    """Truncated-scan inputs for a synthetic CM (synth.SynthCM + its
-    configuration): marginal emissions laid out as fill_marginal_emissions
-    lays them out (src/cp9.rs:4441 -- MP rows the log-odds of the summed
-    left/right pair marginals, degenerate codes the mean over their residues;
-    ML/IL their own emissions on the left and 0 on the right, MR/IR the
-    reverse; gap / non-residue / missing codes IMPOSSIBLE), the node spans
-    allow_truncation reads, and a stand-in for the pass's truncation
-    penalties: log2(2 / (clen (clen + 1))) on the states the reference
-    penalises (MATP_MP, MATL_ML, MATR_MR, BIF_B and insert states), which is
-    the global 5'-and-3' penalty with every such state weighted equally."""
-    from . import synth
-    st = cm_s.st
-    M = cfg.M
-    imp = np.float32(-1e36)
-    lm = np.zeros((M, 18), np.float32)
-    rm = np.zeros((M, 18), np.float32)
-    for v in range(M):
-        lm[v, [4, 16, 17]] = imp
-        rm[v, [4, 16, 17]] = imp
-        t = int(cfg.sttype[v])
-        if t == 1:
-            e = np.asarray(cm_s.e[v][:16], np.float64).reshape(4, 4)
-            for x in range(4):
-                lm[v, x] = np.float32(np.log2(e[x].sum() / float(cfg.null[x])))
-                rm[v, x] = np.float32(np.log2(e[:, x].sum() / float(cfg.null[x])))
-            for code in range(5, 16):
-                bset = [b for b in range(4) if _DEGEN_BITS[code] >> b & 1]
-                lm[v, code] = np.float32(np.mean([lm[v, b] for b in bset]))
-                rm[v, code] = np.float32(np.mean([rm[v, b] for b in bset]))
-        elif t in (2, 4):
-            lm[v] = cfg.oesc[v, :18]
-        elif t in (3, 5):
-            rm[v] = cfg.oesc[v, :18]
-    lpos_n, rpos_n = synth.emit_map(st)
-    nd = np.asarray(st.ndidx)
-    ndt = np.asarray(st.ndtype)[nd]
-    lpos = np.where(np.isin(ndt, (synth.MATP_ND, synth.MATL_ND)), lpos_n[nd], lpos_n[nd] + 1).astype(np.int32)
-    rpos = np.where(np.isin(ndt, (synth.MATP_ND, synth.MATR_ND)), rpos_n[nd], rpos_n[nd] - 1).astype(np.int32)
-    clen = int(cfg.clen)
-    pen = np.float32(np.log2(2.0 / (clen * (clen + 1))))
-    qual = np.isin(np.asarray(cfg.stid), (synth.MATP_MP, synth.MATL_ML, synth.MATR_MR, synth.BIF_B)) | \
-        np.isin(np.asarray(cfg.sttype), (4, 5))
-    pty = np.where(qual, pen, imp).astype(np.float32)
-    pty[0] = imp
-    # integer tables: the states' own integer emissions on their side, the
-    # MP marginals and the penalty scaled as Prob2Score scales (x1000, rounded)
-    ninf = -987654321
-    ilm = np.zeros((M, 18), np.int32)
-    irm = np.zeros((M, 18), np.int32)
-    for v in range(M):
-        t = int(cfg.sttype[v])
-        if t in (2, 4):
-            ilm[v] = cfg.ioesc[v, :18]
-        elif t in (3, 5):
-            irm[v] = cfg.ioesc[v, :18]
-        else:
-            for src, dst in ((lm[v], ilm[v]), (rm[v], irm[v])):
-                x = np.floor(0.5 + 1000.0 * src.astype(np.float64))
-                dst[:] = np.where(src <= -1e35, ninf, np.clip(x, ninf, 1e9)).astype(np.int64)
-        ilm[v, [4, 16, 17]] = ninf
-        irm[v, [4, 16, 17]] = ninf
-    ipty = np.where(qual, int(np.floor(0.5 + 1000.0 * float(pen))), ninf).astype(np.int32)
-    ipty[0] = ninf
-    return TrInputs(lm.ravel(), rm.ravel(), pty, lpos, rpos, clen, bool(local), ilm.ravel(), irm.ravel(), ipty)
+def truncated_tables(cm_s, local: bool) -> dict:
+    """The truncated scanners' inputs of a CM (cmgpu_prep_truncated): marginal
+    emissions lmesc/rmesc/ilmesc/irmesc [M*18], the penalty rows pty/ipty
+    [3, M] of the local or global configuration, and lpos/rpos [M]."""
+    from .model import params_struct
+    M = cm_s.M
+    out = dict(lmesc=np.zeros(M * 18, np.float32), rmesc=np.zeros(M * 18, np.float32),
+               ilmesc=np.zeros(M * 18, np.int32), irmesc=np.zeros(M * 18, np.int32),
+               pty=np.zeros((3, M), np.float32), ipty=np.zeros((3, M), np.int32),
+               lpos=np.zeros(M, np.int32), rpos=np.zeros(M, np.int32))
+    p, keep = params_struct(cm_s)
+    t = N.TrPrep()
+    for k in ("lmesc", "rmesc", "pty"):
+        setattr(t, k, N.ptr(out[k], C.c_float))
+    for k in ("ilmesc", "irmesc", "ipty", "lpos", "rpos"):
+        setattr(t, k, N.ptr(out[k], C.c_int32))
+    N.check(N.lib().cmgpu_prep_truncated(C.byref(p), int(bool(local)), C.byref(t)))
+    del keep
+    return out
+
+
+def tr_inputs(cm_s, cfg, pass_idx: int, local: bool) -> TrInputs:
+    """TrInputs of one truncated pass (PLI_PASS_*: 2 5'-only, 3 3'-only,
+    4/5 5'-and-3') in the local or global configuration."""
+    t = truncated_tables(cm_s, local)
+    r = PTY_ROW[int(pass_idx)]
+    return TrInputs(t["lmesc"], t["rmesc"], t["pty"][r].copy(), t["lpos"], t["rpos"], int(cfg.clen), bool(local),
+                    t["ilmesc"], t["irmesc"], t["ipty"][r].copy())

@@ -1,5 +1,6 @@
 """TEST INFRASTRUCTURE ONLY: ctypes binding of the oracle (qdb_oracle.c,
-hb_oracle.c, tr_oracle.c, trq_oracle.c, p7_oracle.c, msv_oracle.c).
+hb_oracle.c, tr_oracle.c, trq_oracle.c, p7_oracle.c, msv_oracle.c,
+prep_oracle.c).
 
 Used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as
 the checker of the GPU scanner.  The product package never imports it.
@@ -41,7 +42,8 @@ def use_native() -> str:
 def lib():
     global _lib
     if _lib is None:
-        srcs = [os.path.join(HERE, f) for f in ("qdb_oracle.c", "hb_oracle.c", "tr_oracle.c", "trq_oracle.c", "p7_oracle.c", "msv_oracle.c")]
+        srcs = [os.path.join(HERE, f) for f in ("qdb_oracle.c", "hb_oracle.c", "tr_oracle.c", "trq_oracle.c",
+                                                "p7_oracle.c", "msv_oracle.c", "prep_oracle.c")]
         if not os.path.exists(LIB_PATH) or any(os.path.getmtime(LIB_PATH) < os.path.getmtime(f) for f in srcs):
             native = os.path.basename(os.path.dirname(LIB_PATH)) == "_build_native"
             subprocess.run(["make", "-s", "-C", HERE] + (["native"] if native else []), check=True)
@@ -311,3 +313,61 @@ def trq_scan(cm, inside, tt, dsq, i0, j0, cutoff, do_null3, qdbidx, pass_idx, lo
                    for h in hits[:n]]
             return out, vsc.value, vmode.value, bfull.value
         cap = n
+
+
+# ---------------------------------------------------------------------------
+# model preparation (prep_oracle.c)
+# ---------------------------------------------------------------------------
+def prep_configure(cm_s, local, W=0, beta1=1e-7, beta2=1e-15, betaW=1e-7):
+    """The oracle's score tables and bands of a synthetic CM, as a dict of
+    arrays with the fields of cmgpu_cm_scores (plus W, flags, el_selfsc,
+    iel_selfsc)."""
+    from infernox_b200 import _native as N
+    from infernox_b200.model import params_struct
+    M = cm_s.M
+    out = dict(tsc=np.zeros((M, 6), np.float32), oesc=np.zeros((M, 324), np.float32),
+               endsc=np.zeros(M, np.float32), beginsc=np.zeros(M, np.float32),
+               itsc=np.zeros((M, 6), np.int32), ioesc=np.zeros((M, 324), np.int32),
+               iendsc=np.zeros(M, np.int32), ibeginsc=np.zeros(M, np.int32),
+               dmin1=np.zeros(M, np.int32), dmax1=np.zeros(M, np.int32),
+               dmin2=np.zeros(M, np.int32), dmax2=np.zeros(M, np.int32),
+               t_local=np.zeros((M, 6), np.float32))
+    p, keep = params_struct(cm_s)
+    s = N.CmScores()
+    for k in ("tsc", "oesc", "endsc", "beginsc", "t_local"):
+        setattr(s, k, N.ptr(out[k], C.c_float))
+    for k in ("itsc", "ioesc", "iendsc", "ibeginsc", "dmin1", "dmax1", "dmin2", "dmax2"):
+        setattr(s, k, N.ptr(out[k], C.c_int32))
+    L = lib()
+    L.oracle_prep_configure.argtypes = [C.c_void_p, C.c_int, C.c_int32, C.c_double, C.c_double, C.c_double,
+                                        C.c_void_p]
+    rc = L.oracle_prep_configure(C.byref(p), int(bool(local)), int(W), beta1, beta2, betaW, C.byref(s))
+    if rc != 0:
+        raise RuntimeError(f"oracle_prep_configure: {rc}")
+    del keep
+    out.update(W=int(s.W), flags=int(s.flags), el_selfsc=float(s.el_selfsc), iel_selfsc=int(s.iel_selfsc))
+    return out
+
+
+def prep_truncated(cm_s, local):
+    """The oracle's truncated-scan inputs (the fields of cmgpu_tr_prep)."""
+    from infernox_b200 import _native as N
+    from infernox_b200.model import params_struct
+    M = cm_s.M
+    out = dict(lmesc=np.zeros(M * 18, np.float32), rmesc=np.zeros(M * 18, np.float32),
+               ilmesc=np.zeros(M * 18, np.int32), irmesc=np.zeros(M * 18, np.int32),
+               pty=np.zeros((3, M), np.float32), ipty=np.zeros((3, M), np.int32),
+               lpos=np.zeros(M, np.int32), rpos=np.zeros(M, np.int32))
+    p, keep = params_struct(cm_s)
+    t = N.TrPrep()
+    for k in ("lmesc", "rmesc", "pty"):
+        setattr(t, k, N.ptr(out[k], C.c_float))
+    for k in ("ilmesc", "irmesc", "ipty", "lpos", "rpos"):
+        setattr(t, k, N.ptr(out[k], C.c_int32))
+    L = lib()
+    L.oracle_prep_truncated.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+    rc = L.oracle_prep_truncated(C.byref(p), int(bool(local)), C.byref(t))
+    if rc != 0:
+        raise RuntimeError(f"oracle_prep_truncated: {rc}")
+    del keep
+    return out

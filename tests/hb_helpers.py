@@ -153,9 +153,10 @@ def ragged_bands(cm, i0, j0, seed, trim=4):
 
 # ---- truncated-scan inputs ----------------------------------------------
 def tr_tables(cm_s, cfg, pass_idx, local):
-    """Per-pass truncated-scan inputs as a dict (see hb.synthetic_tr_inputs)."""
-    from infernox_b200.hb import synthetic_tr_inputs
-    t = synthetic_tr_inputs(cm_s, cfg, local)
+    """Per-pass truncated-scan inputs as a dict (hb.tr_inputs: the restated
+    marginal emissions and truncated-begin penalties of the pass)."""
+    from infernox_b200.hb import tr_inputs
+    t = tr_inputs(cm_s, cfg, pass_idx, local)
     return {"lmesc": t.lmesc, "rmesc": t.rmesc, "pty": t.pty, "lpos": t.lpos, "rpos": t.rpos, "clen": t.clen,
             "ilmesc": t.ilmesc, "irmesc": t.irmesc, "ipty": t.ipty}
 

@@ -55,3 +55,29 @@ def models(name: str):
     r = (cm, model.configure(cm, local=False), model.configure(cm, local=True))
     _cache[name] = r
     return r
+
+
+_ocache = {}
+
+
+def oracle_cfg(name: str, local: bool):
+    """The model configured from the oracle's own table builders
+    (oracle/prep_oracle.c) instead of the library's: the oracle side of a
+    parity test then shares no table with the GPU side."""
+    key = (name, local)
+    if key in _ocache:
+        return _ocache[key]
+    import oracle
+    from infernox_b200.model import ConfiguredCM
+    cm, g, l = models(name)
+    t = oracle.prep_configure(cm, local)
+    c = ConfiguredCM(
+        name=cm.name, M=cm.M, W=t["W"], flags=t["flags"], clen=cm.clen,
+        sttype=np.ascontiguousarray(cm.st.sttype, np.int8), stid=np.ascontiguousarray(cm.st.stid, np.int8),
+        cfirst=np.ascontiguousarray(cm.st.cfirst, np.int32), cnum=np.ascontiguousarray(cm.st.cnum, np.int32),
+        el_selfsc=t["el_selfsc"], iel_selfsc=t["iel_selfsc"], null=np.asarray(cm.null, np.float32),
+        n3_omega=float(np.float32(cm.n3_omega)),
+        **{k: t[k] for k in ("tsc", "oesc", "endsc", "beginsc", "itsc", "ioesc", "iendsc", "ibeginsc",
+                             "dmin1", "dmax1", "dmin2", "dmax2", "t_local")})
+    _ocache[key] = c
+    return c

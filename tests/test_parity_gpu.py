@@ -11,7 +11,7 @@ import oracle
 from infernox_b200 import scan
 from infernox_b200.scan import CYK_F32, INSIDE_I32, KERNEL_LEVEL, KERNEL_SWEEP, NOQDB, QDB1, QDB2
 
-from helpers import frame, models, planted_seq
+from helpers import frame, models, oracle_cfg, planted_seq
 
 pytestmark = pytest.mark.gpu
 
@@ -59,7 +59,8 @@ def test_generic_scan_matches_oracle(case, kernel):
     c = l if local else g
     seq = planted_seq(cm, n, 0.5, 3, seed=17 + CASES.index(case), degenerate=degen)
     dsq = frame(seq)
-    ref, _, _, _ = oracle.qdb_scan(c, sr, band, dsq, 1, n, cutoff, null3)
+    # the oracle scans with its own tables; the GPU with the library's
+    ref, _, _, _ = oracle.qdb_scan(oracle_cfg(name, local), sr, band, dsq, 1, n, cutoff, null3)
     s = scanner(c, kernel)
     got = s.generic_scan(sr, band, dsq, 1, n, cutoff, null3)
     assert s.stats()["kernel"] == kernel
