@@ -272,8 +272,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="batched-uneven-max",
-                    choices=sorted(WORKLOADS) + list(FILTER_WORKLOADS))
+                    choices=sorted(WORKLOADS) + list(FILTER_WORKLOADS) + ["serve"])
     ap.add_argument("--batch", type=int, default=500, help="sequences per step per rank")
+    ap.add_argument("--models", type=int, default=200, help="serve: CMs in the library")
+    ap.add_argument("--requests", type=int, default=16, help="serve: queries")
+    ap.add_argument("--rate", type=float, default=200.0, help="serve: Poisson arrivals per second")
+    ap.add_argument("--serve-budget", type=int, default=8_000_000, help="serve: active residues (both strands)")
+    ap.add_argument("--serve-check", type=int, default=2, help="serve: requests checked alone vs mixed")
     ap.add_argument("--kernel", default="auto", choices=["auto", "level", "sweep"],
                     help="QDB scan kernel (CMGPU_KERNEL_*)")
     ap.add_argument("--job-seqs", type=int, default=10000,
@@ -286,6 +291,8 @@ def main():
     args = ap.parse_args()
     if args.workload in FILTER_WORKLOADS:
         return filter_main(args)
+    if args.workload == "serve":
+        return serve_main(args)
     w = WORKLOADS[args.workload]
     rank, world, local_rank = env_rank()
     cm = make_model(w)
@@ -840,6 +847,164 @@ def filter_main(args):
             "cpu_baseline": cb, "clocks": clk}
     if rank == 0:
         print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# serving loop (cmscan-style)
+# ---------------------------------------------------------------------------
+def serve_library(nmodels, seed=77):
+    """nmodels synthetic CMs of 40-400 consensus columns, 30-50% paired,
+    0-6 bifurcations (no more than one per 40 columns), local configuration."""
+    from infernox_b200 import model, synth
+    rng = np.random.default_rng(seed)
+    cms, cfgs = [], []
+    for k in range(nmodels):
+        clen = int(rng.integers(40, 401))
+        nb = int(rng.integers(0, min(6, clen // 40) + 1))
+        ss = synth.structure(clen, float(rng.uniform(0.3, 0.5)), nb, int(rng.integers(1 << 30)))
+        cm = synth.synth_cm(ss, int(rng.integers(1 << 30)), name=f"lib{k}")
+        cms.append(cm)
+        cfgs.append(model.configure(cm, local=True))
+    return cms, cfgs
+
+
+def serve_requests(cms, n, rate, seed=78):
+    """n queries with Poisson arrivals at `rate` per second, lengths
+    log-uniform in [100, 100000], GC uniform in [0.4, 0.6], 30% with one
+    homolog sampled from a random library model planted at a random place."""
+    from infernox_b200 import serve, synth
+    rng = np.random.default_rng(seed)
+    t, reqs = 0.0, []
+    for k in range(n):
+        t += float(rng.exponential(1.0 / rate))
+        L = int(np.exp(rng.uniform(np.log(100), np.log(100000))))
+        seq = synth.random_dsq(L, float(rng.uniform(0.4, 0.6)), rng)
+        if rng.random() < 0.3:
+            h = synth.emit(cms[int(rng.integers(len(cms)))], rng)
+            if 0 < len(h) < L:
+                p = int(rng.integers(0, L - len(h)))
+                seq[p:p + len(h)] = h
+        reqs.append(serve.Request(k, seq, arrival=t))
+    return reqs
+
+
+def serve_main(args):
+    rank, world, local_rank = env_rank()
+    if rank != 0:
+        return
+    from infernox_b200 import serve
+    t_build = time.perf_counter()
+    cms, cfgs = serve_library(args.models)
+    t_build = time.perf_counter() - t_build
+    reqs = serve_requests(cms, args.requests, args.rate)
+    config = {"workload": "serve", "library": f"{len(cfgs)} synthetic CMs, clen 40-400, 0-6 bifurcations, local",
+              "requests": len(reqs), "arrivals": f"Poisson, {args.rate:g} per second",
+              "query_lengths": "log-uniform 100-100000 nt, both strands; 30% carry one planted homolog",
+              "scan": "--nohmm per window: QDB1 CYK filter, QDB2 Inside on its envelopes",
+              "cutoffs_bits": {"f6": 0.0, "final": CUTOFF_BITS},
+              "residues": int(sum(r.residues for r in reqs)), "library_build_s": round(t_build, 1)}
+    if args.impl == "reference":
+        # the oracle on the host cores: the per-query, per-model loop of cmscan
+        # on a bounded sample (the first requests, all models), one thread per model
+        oracle = _oracle()
+        from concurrent.futures import ThreadPoolExecutor
+        from infernox_b200.synth import revcomp
+        cores = os.cpu_count() or 1
+        sample = sorted(reqs, key=lambda r: len(r.seq))[: max(1, min(args.steps, 4))]
+
+        def one(k_req):
+            k, r = k_req
+            for s in (r.seq, revcomp(r.seq)):
+                dsq = np.concatenate([[255], s, [255]]).astype(np.uint8)
+                envs = oracle.cyk_seq_filter(cfgs[k], dsq, len(s), 0.0, True)
+                if envs:
+                    oracle.final_stage_inside_opt(cfgs[k], dsq, envs, CUTOFF_BITS, True, False)
+
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(cores) as ex:
+            list(ex.map(one, [(k, r) for r in sample for k in range(len(cfgs))]))
+        dt = time.perf_counter() - t0
+        value = len(sample) / dt
+        line = {"impl": "reference", "metric": "served sequences/s (cmscan --nohmm, CM library)", "value": value,
+                "unit": "seq/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * dt / max(1, len(sample)), "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32+int32", "data": "synthetic", "config": config,
+                "cpu_baseline": {"value": value, "unit": "seq/s", "cores": cores, "kind": "port",
+                                 "sample": f"the {len(sample)} shortest queries ({sum(len(r.seq) for r in sample)} nt) "
+                                           f"against all {len(cfgs)} models, threads over models"},
+                "e2e": {"value": value, "unit": "seq/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    torch.cuda.set_device(local_rank)
+    srv = serve.Server(cfgs, device=local_rank, budget_residues=args.serve_budget)
+    # warm-up: every model's plans built and uploaded by a few short queries
+    warm = serve_requests(cms, max(1, args.warmup), 1e6, seed=79)
+    for r in warm:
+        r.seq = r.seq[:300]
+        srv.submit(r)
+    while not srv.idle():
+        srv.step()
+    srv.finished.clear()
+    cells = [0.0]
+
+    def step_counted():
+        srv.step()
+        for sc in srv.scanners[srv.cursor - 1: srv.cursor] if srv.cursor else srv.scanners[-1:]:
+            cells[0] += sc.stats()["cells"]
+
+    # real time: requests enter the queue at their arrival times
+    torch.cuda.synchronize()
+    srv.t0 = time.perf_counter()
+    pending = sorted(reqs, key=lambda r: r.arrival)
+    nxt = 0
+    steps = 0
+    while nxt < len(pending) or not srv.idle():
+        now = srv.clock()
+        while nxt < len(pending) and pending[nxt].arrival <= now:
+            srv.submit(pending[nxt])
+            nxt += 1
+        if srv.idle():
+            time.sleep(max(0.0, min(0.01, pending[nxt].arrival - now)))
+            continue
+        srv.step()
+        steps += 1
+    torch.cuda.synchronize()
+    wall = srv.clock()
+    done = [r for r in srv.finished if r.status == serve.OK]
+    lat = sorted(r.done - r.arrival for r in done)
+    span = max(r.done for r in done) - min(r.arrival for r in done)
+    value = len(done) / span
+    # identity check on a few requests: alone == in the mix
+    same = all(serve.scan_alone(srv, r) == r.hits for r in done[: args.serve_check])
+    if not same:
+        raise RuntimeError("a served request's hits differ from the same request scanned alone")
+    # plain comparator: the same queries, one launch per window per stage
+    # (scan_alone), timed on a subset
+    sub = [r for r in done if len(r.seq) <= 20000][: max(1, args.serve_check)]
+    t0 = time.perf_counter()
+    for r in sub:
+        serve.scan_alone(srv, r)
+    torch.cuda.synchronize()
+    plain_dt = time.perf_counter() - t0
+    plain = {"value": len(sub) / plain_dt, "unit": "seq/s", "requests": len(sub),
+             "residues": int(sum(r.residues for r in sub)), "s": plain_dt}
+    line = {"metric": "served sequences/s (cmscan --nohmm, CM library)", "value": value, "unit": "seq/s",
+            "n_gpus": 1, "steps": steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / max(1, steps),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+int32",
+            "data": "synthetic", "config": config,
+            "e2e": {"value": value, "unit": "seq/s", "h2d_bytes_per_step": int(config["residues"] / max(1, steps)),
+                    "d2h_bytes_per_step": 0},
+            "latency_s": {"p50": statistics.median(lat), "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
+                          "max": lat[-1]},
+            "residues_per_s": config["residues"] / span,
+            "gpu_launches": srv.launches, "model_steps": srv.model_steps,
+            "plain_gpu": plain, "served_over_plain_residue_rate":
+                (config["residues"] / span) / (plain["residues"] / plain_dt),
+            "identity_checked_requests": min(len(done), args.serve_check)}
+    print(json.dumps(line))
+    srv.close()
 
 
 if __name__ == "__main__":
