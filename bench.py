@@ -56,6 +56,11 @@ FILTER_WORKLOADS = ("f1-ssv", "f2-vit", "hb-cyk", "hb-inside", "hb-trcyk", "trq-
 OPS_PER_TERM = {0: 2.0, 1: 7.0}   # CYK: FADD + select; Inside: 6 INT + 1 LDS
 OPS_PER_CELL = 2.0                # emission add + store
 CUTOFF_BITS = 15.0                # stands in for the E-value threshold
+# DRAM bytes (read + write) per DP cell of the scan kernel, from one ncu
+# capture of this bench's default step (profiles/qdb_scan_inside_nonbanded_
+# traffic.txt: 1.438e12 bytes over 1.058e11 cells in one launch); the
+# roofline's traffic is this times the cells of a launch
+TRAFFIC_B_PER_CELL = {("level", 1, 0): 13.59}
 
 
 def env_rank():
@@ -275,7 +280,7 @@ def main():
                     choices=sorted(WORKLOADS) + list(FILTER_WORKLOADS) + ["serve"])
     ap.add_argument("--batch", type=int, default=500, help="sequences per step per rank")
     ap.add_argument("--models", type=int, default=200, help="serve: CMs in the library")
-    ap.add_argument("--requests", type=int, default=16, help="serve: queries")
+    ap.add_argument("--requests", type=int, default=12, help="serve: queries")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: Poisson arrivals per second")
     ap.add_argument("--serve-budget", type=int, default=8_000_000, help="serve: active residues (both strands)")
     ap.add_argument("--serve-check", type=int, default=2, help="serve: requests checked alone vs mixed")
@@ -400,6 +405,7 @@ def main():
         ncand += st["candidates"]
     barrier()
     clk = clocks.stop()
+    kern_used = sc.stats()["kernel"]
     if not np.array_equal(hits, ref_hits):
         raise RuntimeError("hit lists differ between steps")
     total_ms = sum(times)
@@ -469,6 +475,7 @@ def main():
         nsm = torch.cuda.get_device_properties(local_rank).multi_processor_count
         peak = nsm * 128 * sm_mhz * 1e6 / 1e9  # Gop/s
         achieved = ops_launch / (kernel_ms / 1e3) / 1e9
+        kern_name = {1: "level", 2: "sweep"}.get(kern_used, "?")
         step_lat = sorted(times)
         line = {
             "metric": "CYK/Inside scan Gcells/s", "value": value, "unit": "Gcells/s",
@@ -485,7 +492,10 @@ def main():
                                 "p99": step_lat[min(len(step_lat) - 1, int(0.99 * len(step_lat)))]},
             "gpu_launches": launches,
             "roofline": {"bound": "issue", "achieved": achieved, "peak": peak, "unit": "Gop/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak,
+                         "traffic": (TRAFFIC_B_PER_CELL[(kern_name, sr, band)] * cells / max(1, launches)
+                                     if (kern_name, sr, band) in TRAFFIC_B_PER_CELL else None),
+                         "traffic_unit": "DRAM bytes per launch (ncu-measured bytes per cell x cells)",
                          "note": f"INT32/FP32 lane-op issue: {nsm} SMs x 128 lanes x {sm_mhz:.0f} MHz "
                                  f"({peak_src}); ops = {OPS_PER_TERM[sr]:.0f}/term + 2/cell"},
             "plain_gpu": plain,
@@ -496,7 +506,7 @@ def main():
                              "chunk": tune["best"]["chunk"],
                              "tuned_over": [(t["lanes"], t["chunk"], round(t["kernel_ms"], 1))
                                             for t in tune["trials"]]},
-            "kernel": {1: "level", 2: "sweep"}.get(sc.stats()["kernel"], "?"),
+            "kernel": kern_name,
             "hits_per_step": int(len(ref_hits)),
             "hits_per_job_step": int(len(job_hits)),
             "e2e_steps": e2e_steps,
@@ -901,7 +911,8 @@ def serve_main(args):
               "requests": len(reqs), "arrivals": f"Poisson, {args.rate:g} per second",
               "query_lengths": "log-uniform 100-100000 nt, both strands; 30% carry one planted homolog",
               "scan": "--nohmm per window: QDB1 CYK filter, QDB2 Inside on its envelopes",
-              "cutoffs_bits": {"f6": 0.0, "final": CUTOFF_BITS},
+              "cutoffs_bits": {"f6": 12.0, "final": CUTOFF_BITS, "note": "bit cutoffs stand in for the "
+                               "E-value thresholds (no calibration)"},
               "residues": int(sum(r.residues for r in reqs)), "library_build_s": round(t_build, 1)}
     if args.impl == "reference":
         # the oracle on the host cores: the per-query, per-model loop of cmscan
@@ -916,7 +927,7 @@ def serve_main(args):
             k, r = k_req
             for s in (r.seq, revcomp(r.seq)):
                 dsq = np.concatenate([[255], s, [255]]).astype(np.uint8)
-                envs = oracle.cyk_seq_filter(cfgs[k], dsq, len(s), 0.0, True)
+                envs = oracle.cyk_seq_filter(cfgs[k], dsq, len(s), 12.0, True)
                 if envs:
                     oracle.final_stage_inside_opt(cfgs[k], dsq, envs, CUTOFF_BITS, True, False)
 

@@ -384,7 +384,9 @@ typedef struct cmgpu_tr_result {
 
 /* tr_cyk_scan_hb (CMGPU_CYK_F32, src/cm_dpsearch_trunc.rs:264) and
  * ftr_inside_scan_hb (CMGPU_INSIDE_F32, :1055) of residues i0..j0 of dsq
- * in pass pass_idx (PLI_PASS_*: 2 5'-only, 3 3'-only, 4/5 5'-and-3'):
+ * in pass pass_idx (PLI_PASS_*: 2 5'-only, 3 3'-only, 4/5 5'-and-3'; other
+ * passes return CMGPU_EINVAL, as the reference's truncated scanners refuse
+ * them):
  * vsc_root and its mode, the envelope (-1 when none) and the hits after
  * overlap removal, as the reference returns them. */
 int cmgpu_tr_scan_hb(const cmgpu_model *m, int semiring, const cmgpu_tr_tables *tt, const cmgpu_hb_bands *bands,

@@ -1334,8 +1334,11 @@ int tr_batch(const cmgpu_model *mc, cudaStream_t st, int semiring, const cmgpu_t
         set_error("truncated HMM-banded scan: missing truncation tables");
         return CMGPU_EINVAL;
     }
-    if (pass_idx < 1 || pass_idx > 6) {
-        set_error("truncated HMM-banded scan: pass index must be 1..6 (PLI_PASS_*)");
+    // the truncated scanners take the truncated passes only: the reference
+    // picks the pass's penalty row with pty_idx_for_pass(..).expect("truncated
+    // pass") (src/cm_dpsearch_trunc.rs:219, src/cm_trunc.rs:99-107)
+    if (pass_idx < 2 || pass_idx > 5) {
+        set_error("truncated HMM-banded scan: pass index must be a truncated pass 2..5 (PLI_PASS_*)");
         return CMGPU_EINVAL;
     }
     for (int32_t e = 0; e < ntask; e++) {

@@ -80,7 +80,7 @@ class Server:
     """The request loop over a library of configured CMs on one GPU."""
 
     def __init__(self, models, device: int = 0, budget_residues: int = 4_000_000, max_queue: int = 1024,
-                 f6_cutoff: float = 0.0, final_cutoff: float = 15.0, do_null3: bool = True):
+                 f6_cutoff: float = 12.0, final_cutoff: float = 15.0, do_null3: bool = True):
         self.models = list(models)
         self.device = device
         self._scanners = None  # uploaded on the first scan (queueing needs no GPU)

@@ -128,18 +128,24 @@ def test_trq_rejects_bad_inputs():
 
 @pytest.mark.parametrize("name,loc,qdb", [("trna", True, N.NOQDB), ("small2", False, N.QDB2), ("small0", True, N.QDB1)])
 def test_trq_edge_windows_and_passes(name, loc, qdb):
-    """Pass 1 (the standard pass: J plane only), windows of 1 and 2 residues,
-    IUPAC degenerate residues in the window, and a model without
-    bifurcations (small0)."""
+    """Every truncated pass, windows of 1 and 2 residues, IUPAC degenerate
+    residues in the window, and a model without bifurcations (small0); the
+    standard pass 1 and pass 6, which the reference's truncated scanners do
+    not take (pty_idx_for_pass(..).expect), are refused."""
     from helpers import planted_seq
     cm, g, l = models(name)
     cfg = l if loc else g
     sc = Scanner(cfg)
     f = frame(planted_seq(cm, 400, 0.45, 2, seed=31, degenerate=0.1))
-    for pass_idx in (1, 2, 4, 5):
+    for pass_idx in (2, 3, 4, 5):
         tt = tr_tables(cm, cfg, pass_idx, loc)
         for i0, j0 in ((50, 50), (50, 51), (10, 10 + cfg.W // 2), (100, 100 + cfg.W + 20)):
             check(cfg, sc, tt, loc, f, i0, j0, qdb, pass_idx, -20.0, True, ("edge", i0, j0))
+    tt = tr_tables(cm, cfg, 4, loc)
+    for bad in (1, 6):
+        with pytest.raises(N.CmgpuError, match="truncated pass") as ei:
+            ref_tr_cyk_scan(sc, tri_of(tt, loc), f, 50, 90, -20.0, qdb, True, bad)
+        assert ei.value.rc == -1  # CMGPU_EINVAL
 
 
 def test_trq_column_wait_times_out_and_reports():
