@@ -277,8 +277,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="batched-uneven-max",
-                    choices=sorted(WORKLOADS) + list(FILTER_WORKLOADS) + ["serve"])
+                    choices=sorted(WORKLOADS) + list(FILTER_WORKLOADS) + ["serve", "calibrate"])
     ap.add_argument("--batch", type=int, default=500, help="sequences per step per rank")
+    ap.add_argument("--calib-mb", type=float, default=1.6, help="calibrate: Mb of random sequence (-L)")
     ap.add_argument("--models", type=int, default=200, help="serve: CMs in the library")
     ap.add_argument("--requests", type=int, default=12, help="serve: queries")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: Poisson arrivals per second")
@@ -298,6 +299,8 @@ def main():
         return filter_main(args)
     if args.workload == "serve":
         return serve_main(args)
+    if args.workload == "calibrate":
+        return calibrate_main(args)
     w = WORKLOADS[args.workload]
     rank, world, local_rank = env_rank()
     cm = make_model(w)
@@ -1017,6 +1020,167 @@ def serve_main(args):
     print(json.dumps(line))
     srv.close()
 
+
+
+# ---------------------------------------------------------------------------
+# cmcalibrate
+# ---------------------------------------------------------------------------
+def calibrate_main(args):
+    """One JSON line for --workload calibrate: cmcalibrate's default run
+    (calibrate_cm, src/cm_calibrate.rs:1102) of the 72-column tRNA-like CM --
+    L = 1.6 Mb = 160 random genomic 10 kb sequences, QDB bands at beta 1e-15,
+    four exp modes (glocal / local x CYK / Inside), null3, tail fits.  A step
+    is one whole calibration through cmgpu_calibrate (host generator,
+    configuration, four batched scans, fits); each rank calibrates its own
+    copy of the model with its own seed (weak scaling, no exchange).
+
+    value  DP cells of the four scans / their device time (library events)
+    e2e    the same cells / the wall time of the whole synchronous call"""
+    from concurrent.futures import ThreadPoolExecutor
+    rank, world, local_rank = env_rank()
+    from infernox_b200 import calibrate as cal
+    from infernox_b200 import model, synth
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    cm_s = synth.synth_cm(synth.trna_like(), 11, name="cfg0")
+    W = model.configure(cm_s, local=False).W
+    ccfg = cal.CalibrateConfig(seed=181 + rank, l_mb=args.calib_mb)
+    nseq = cal.n_sequences(ccfg)
+    g, l = cal.calibration_configs(cm_s, W, ccfg)
+    config = {"workload": "calibrate", "model": f"synthetic CM clen={g.clen} M={g.M} W={W} (tRNA-like, "
+                                                f"4-stem multibranch)",
+              "calibration": f"-L {ccfg.l_mb} Mb = {nseq} random genomic sequences of 10 kb (five-state genomic "
+                             f"HMM, seed {ccfg.seed}), QDB2 bands at beta {ccfg.beta:g}, 4 exp modes "
+                             f"(glocal/local x CYK/Inside), cutoff -inf, null3, tails gtailn {ccfg.gtailn} / "
+                             f"ltailn {ccfg.ltailn}",
+              "parallelism": f"dp{world}", "l2": "flushed (256 MB write) before each timed step"}
+    # CPU: the oracle's restatement of collect_scores's scan, one (sequence,
+    # mode) unit at a time on every host core (the reference runs them on one)
+    import oracle
+    oracle.lib()
+    frames = cal.sample_genomic_sequences(ccfg.seed, cal.EXPTAIL_CHUNKLEN, nseq)
+    flen = cal.EXPTAIL_CHUNKLEN + 2
+    units = [(s, m) for s in range(nseq) for m in range(4)]
+    perm = np.random.default_rng(7).permutation(len(units))
+    cores = os.cpu_count() or 1
+    pos = {"at": 0}
+
+    def one(u):
+        s, m = u
+        c = l if cal.exp_mode_is_local(m) else g
+        _, cells = oracle.calib_scan(c, int(cal.exp_mode_is_inside(m)), 2, frames[s * flen:(s + 1) * flen], 1,
+                                     cal.EXPTAIL_CHUNKLEN, True, want_cells=True)
+        return cells
+
+    def cpu_sample(budget_s):
+        lock = threading.Lock()
+        st = {"n": 0, "cells": 0.0}
+        deadline = time.perf_counter() + budget_s
+
+        def worker():
+            while time.perf_counter() < deadline:
+                with lock:
+                    u = units[int(perm[pos["at"] % len(units)])]
+                    pos["at"] += 1
+                    st["n"] += 1
+                c = one(u)
+                with lock:
+                    st["cells"] += c
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(cores) as ex:
+            for _ in range(cores):
+                ex.submit(worker)
+        dt = time.perf_counter() - t0
+        return {"value": st["cells"] / dt / 1e9, "unit": "Gcells/s", "cores": cores, "kind": "port",
+                "sample": f"{st['n']} of {len(units)} (sequence, mode) scans of one calibration, {dt:.1f} s on "
+                          f"{cores} threads (the reference runs them one after another on one core)",
+                "cells": st["cells"], "seconds": dt}
+
+    metric = "cmcalibrate scan Gcells/s (4 exp modes, bit-exact)"
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        per_step = max(1.0, args.cpu_seconds / max(1, args.steps))
+        for _ in range(args.warmup):
+            cpu_sample(per_step)
+        samples = [cpu_sample(per_step) for _ in range(args.steps)]
+        cells, secs = sum(x["cells"] for x in samples), sum(x["seconds"] for x in samples)
+        val = cells / secs / 1e9
+        cb = {"value": val, "unit": "Gcells/s", "cores": cores, "kind": "port",
+              "sample": f"{args.steps} steps of {per_step:.1f} s, each a bounded sample of one calibration's "
+                        f"(sequence, mode) scans on {cores} threads"}
+        print(json.dumps({"impl": "reference", "metric": metric, "value": val, "unit": "Gcells/s",
+                          "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": 1e3 * secs / max(1, args.steps), "higher_is_better": True,
+                          "scaling": "weak", "vs_baseline": None, "dtype": "f32/int32", "data": "synthetic",
+                          "config": config, "cpu_baseline": cb,
+                          "e2e": {"value": val, "unit": "Gcells/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}))
+        return
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local_rank)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device="cuda")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def call():
+        return cal.calibrate_cm(cm_s, ccfg, W=W, device=local_rank)
+
+    for _ in range(args.warmup):
+        ref = call()
+    clocks = ClockSampler(local_rank)
+    barrier()
+    clocks.start()
+    walls, kms, cells, terms, launches = [], [], 0.0, 0.0, 0
+    for _ in range(args.steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = call()
+        walls.append(1e3 * (time.perf_counter() - t0))
+        kms.append(out["kernel_ms"])
+        cells, terms = out["cells"], out["terms"]
+        launches += out["launches"]
+    barrier()
+    clk = clocks.stop()
+    if [e["mu"] for e in out["exp"]] != [e["mu"] for e in ref["exp"]]:
+        raise RuntimeError("calibrations differ between steps")
+    total_ms, e2e_ms, all_cells = aggregate_ranks(dist, sum(kms), sum(walls), cells * args.steps)
+    value = all_cells / (total_ms / 1e3) / 1e9
+    e2e = all_cells / (e2e_ms / 1e3) / 1e9
+    sm_mhz = clk["sm_mhz"] or 1965.0
+    nsm = torch.cuda.get_device_properties(local_rank).multi_processor_count
+    peak = nsm * 128 * sm_mhz * 1e6 / 1e9
+    # lane-ops: half the modes CYK (2 per term), half Inside (7 per term), 2 per cell
+    ops = 4.5 * terms + OPS_PER_CELL * cells
+    achieved = ops / (statistics.mean(kms) / 1e3) / 1e9
+    cb = cpu_sample(args.cpu_seconds) if (rank == 0 and not args.no_cpu) else None
+    line = {"metric": metric, "value": value, "unit": "Gcells/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": statistics.mean(walls), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32/int32", "data": "synthetic", "config": config,
+            "e2e": {"value": e2e, "unit": "Gcells/s", "h2d_bytes_per_step": 4 * nseq * flen,
+                    "d2h_bytes_per_step": None, "timing": "host clock around the synchronous cmgpu_calibrate call"},
+            "gpu_launches": launches,
+            "calibration": {"exp": out["exp"], "nhits": out["nhits"], "kernel_ms_per_step": statistics.mean(kms),
+                            "wall_ms_per_step": statistics.mean(walls)},
+            "roofline": {"bound": "issue", "achieved": achieved, "peak": peak, "unit": "Gop/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "note": f"2 (CYK) / 7 (Inside) lane-ops per child term + 2 per cell; {nsm} SMs x 128 "
+                                 f"lanes x {sm_mhz:.0f} MHz"},
+            "cpu_baseline": cb, "clocks": clk}
+    if rank == 0:
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
 
 if __name__ == "__main__":
     main()

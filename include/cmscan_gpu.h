@@ -229,7 +229,7 @@ int cmgpu_qdb_scan(const cmgpu_model *m, cmgpu_workspace *ws, int semiring,
  * memory, the decks -- lives in one 16 MiB `static __device__` array that
  * every GPU loading the library holds until the process exits.  Requests
  * that do not fit return CMGPU_ENOSPACE.  The first call on a device looks up
- * the array's address (set-up), so make it before any stream capture.  All
+ * the array's address with cudaGetSymbolAddress (a one-time set-up).  All
  * calls on a device share the array: calls that overlap on the GPU race, so
  * serialise them.  The model must already be uploaded (cmgpu_model_upload). */
 int cmgpu_qdb_scan_noalloc(const cmgpu_model *m, void *stream, int semiring, int qdbidx,
@@ -285,6 +285,68 @@ int cmgpu_scan_plain(const cmgpu_model *m, cmgpu_workspace *ws, int semiring,
                      const cmgpu_window *wins, int32_t nwin, float cutoff,
                      int do_null3, cmgpu_batch_hit *hits, int32_t cap,
                      int32_t *n_out);
+
+/* ---- cmcalibrate (src/cm_calibrate.rs) ------------------------------------
+ * The exponential-tail E-value fit of a CM in its four modes, indexed
+ * GC, GI, LC, LI = glocal CYK, glocal Inside, local CYK, local Inside
+ * (EXP_CM_*, src/cm_calibrate.rs:38-42). */
+typedef struct cmgpu_calibrate_config {
+    uint32_t seed;        /* generator seed (181)                              */
+    double l_mb;          /* Mb of random sequence, in 10 kb sequences (1.6)   */
+    double beta;          /* tail loss of both QDB band sets (1e-15)           */
+    int32_t nonbanded;    /* full d-range instead of QDB bands                 */
+    int32_t gtailn;       /* tail hits per Mb fitted, glocal modes (250)       */
+    int32_t ltailn;       /* tail hits per Mb fitted, local modes (750)        */
+    float tailp;          /* > 0: fixed tail mass instead of gtailn / ltailn   */
+    int32_t do_null3;     /* null3 correction of the hit scores (1)            */
+} cmgpu_calibrate_config;
+
+/* ExpParams (src/evalue.rs:8-17) as set_exp_info fills it: mu is the
+ * extrapolated location, mu_orig the fitted one. */
+typedef struct cmgpu_exp_params {
+    double lambda, mu, dbsize, mu_orig, tailp;
+    int32_t nrandhits;
+} cmgpu_exp_params;
+
+typedef struct cmgpu_calibrate_result {
+    cmgpu_exp_params exp[4];  /* GC, GI, LC, LI                               */
+    int32_t nhits[4];         /* hits in each mode's histogram                */
+    double dbsize;            /* residues scored per mode                     */
+    double cells;             /* DP cells of the four scans                   */
+    double terms;             /* child relaxations of the four scans          */
+    float kernel_ms;          /* device time of the four scans                */
+    int32_t launches;         /* scan kernel launches                         */
+} cmgpu_calibrate_result;
+
+/* generate_sequences / SampleGenomicSequenceFromHMM (src/cm_calibrate.rs:
+ * 184-200, 1113-1124): nseq frames of L residues drawn from the five-state
+ * genomic HMM with easel's Mersenne Twister seeded with `seed`, written
+ * back to back as [255, L codes 0..3, 255].  No GPU. */
+int cmgpu_genomic_sample(uint32_t seed, int32_t L, int32_t nseq, uint8_t *frames);
+
+/* fit_histogram + SetExpInfo (src/cm_calibrate.rs:1000-1099): the tail mass
+ * (tailp > 0, else the mode's tail hits per Mb of nseq x L residues), the
+ * top floor(n * tailp) scores and the complete-data exponential fit.
+ * CMGPU_ERANGE where the reference returns an error (too few tail points,
+ * tailn too large, non-finite lambda or score).  No GPU. */
+int cmgpu_exp_fit(const float *scores, int64_t n, int exp_mode, int32_t nseq, int32_t L, int32_t gtailn,
+                  int32_t ltailn, float tailp, double dbsize, cmgpu_exp_params *out);
+
+/* collect_scores's scan (src/cm_calibrate.rs:441-989): each window scanned
+ * as cmcalibrate's generic_scan does -- cutoff -inf, local begins compared
+ * in bit scores -- with the kept hits of every window, in window order.  The
+ * device emits only the ROOT cells the greedy report could take. */
+int cmgpu_calibrate_scan_batch(const cmgpu_model *m, cmgpu_workspace *ws, int semiring, int qdbidx,
+                               const uint8_t *dsq_all, int64_t dsq_len, const cmgpu_window *wins,
+                               int32_t nwin, int do_null3, cmgpu_batch_hit *hits, int32_t cap,
+                               int32_t *n_out);
+
+/* calibrate_cm (src/cm_calibrate.rs:1102-1182): a probability-level CM with
+ * window length W; the global and local configurations with both band sets
+ * at cfg->beta, the random sequences, one batched scan per mode on `device`
+ * and the four fits. */
+int cmgpu_calibrate(const cmgpu_cm_params *p, int32_t W, int device, const cmgpu_calibrate_config *cfg,
+                    cmgpu_calibrate_result *out);
 
 /* ---- HMM-banded (CP9-banded) scanners ------------------------------------
  * Bands of one envelope as CP9Bands holds them (src/cp9.rs:1450-1495): for

@@ -140,6 +140,21 @@ class Stats(C.Structure):
     ]
 
 
+class CalibrateConfig(C.Structure):
+    _fields_ = [("seed", C.c_uint32), ("l_mb", C.c_double), ("beta", C.c_double), ("nonbanded", C.c_int32),
+                ("gtailn", C.c_int32), ("ltailn", C.c_int32), ("tailp", C.c_float), ("do_null3", C.c_int32)]
+
+
+class ExpParams(C.Structure):
+    _fields_ = [("lambda_", C.c_double), ("mu", C.c_double), ("dbsize", C.c_double), ("mu_orig", C.c_double),
+                ("tailp", C.c_double), ("nrandhits", C.c_int32)]
+
+
+class CalibrateResult(C.Structure):
+    _fields_ = [("exp", ExpParams * 4), ("nhits", C.c_int32 * 4), ("dbsize", C.c_double), ("cells", C.c_double),
+                ("terms", C.c_double), ("kernel_ms", C.c_float), ("launches", C.c_int32)]
+
+
 def ptr(a: np.ndarray, ctype):
     return a.ctypes.data_as(P(ctype))
 
@@ -233,6 +248,12 @@ def lib() -> C.CDLL:
     L.cmgpu_tr_qdb_inject_stall.argtypes = [vp, C.c_int32]
     L.cmgpu_count_work.argtypes = [P(Cm), C.c_int, C.c_int, C.c_int32, P(C.c_double),
                                    P(C.c_double)]
+    L.cmgpu_genomic_sample.argtypes = [C.c_uint32, C.c_int32, C.c_int32, vp]
+    L.cmgpu_exp_fit.argtypes = [vp, C.c_int64, C.c_int, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_float,
+                                C.c_double, P(ExpParams)]
+    L.cmgpu_calibrate_scan_batch.argtypes = [vp, vp, C.c_int, C.c_int, vp, C.c_int64, vp, C.c_int32, C.c_int, vp,
+                                             C.c_int32, P(C.c_int32)]
+    L.cmgpu_calibrate.argtypes = [P(CmParams), C.c_int32, C.c_int, P(CalibrateConfig), P(CalibrateResult)]
     _lib = L
     return L
 
@@ -254,5 +275,6 @@ EXPORTED = [
     "cmgpu_msv_score_batch", "cmgpu_f1_msv_windows", "cmgpu_ssv_diagonals", "cmgpu_msv_filter_stats",
     "cmgpu_fast_cyk_scan_hb", "cmgpu_hb_scan_hits", "cmgpu_hb_scan_batch", "cmgpu_hb_stats",
     "cmgpu_tr_scan_hb", "cmgpu_tr_scan_hb_batch", "cmgpu_tr_qdb_scan", "cmgpu_tr_qdb_scan_batch",
-    "cmgpu_tr_qdb_stats", "cmgpu_tr_qdb_inject_stall",
+    "cmgpu_tr_qdb_stats", "cmgpu_tr_qdb_inject_stall", "cmgpu_genomic_sample", "cmgpu_exp_fit",
+    "cmgpu_calibrate_scan_batch", "cmgpu_calibrate",
 ]

@@ -236,23 +236,25 @@ static inline float raw_bits(int semiring, uint32_t raw) {
     return f;
 }
 
-// remove_overlaps_greedy (src/cp9.rs:6544-6574)
+// remove_overlaps_greedy (src/cp9.rs:6544-6574): hits sorted by score
+// (descending, stable) then start; a hit is removed when it overlaps an
+// earlier hit that was kept.  The kept hits are disjoint, so they are held
+// in a map ordered by start: the only kept hit that can overlap [i, j] is the
+// one with the largest start <= j, and it overlaps when its end >= i.  Same
+// result as the pairwise scan, in O(n log n).
 static void remove_overlaps(std::vector<cmgpu_hit> &h) {
     std::stable_sort(h.begin(), h.end(), [](const cmgpu_hit &a, const cmgpu_hit &b) {
         if (a.score != b.score) return a.score > b.score;
         return a.i < b.i;
     });
-    std::vector<char> removed(h.size(), 0);
-    for (size_t i = 0; i < h.size(); i++) {
-        if (removed[i]) continue;
-        for (size_t j = i + 1; j < h.size(); j++) {
-            if (removed[j]) continue;
-            if (!(h[j].j < h[i].i) && !(h[i].j < h[j].i)) removed[j] = 1;
-        }
-    }
+    std::map<int32_t, int32_t> kept;  // start -> end
     size_t o = 0;
-    for (size_t i = 0; i < h.size(); i++)
-        if (!removed[i]) h[o++] = h[i];
+    for (size_t x = 0; x < h.size(); x++) {
+        auto it = kept.upper_bound(h[x].j);
+        if (it != kept.begin() && std::prev(it)->second >= h[x].i) continue;
+        kept.emplace(h[x].i, h[x].j);
+        h[o++] = h[x];
+    }
     h.resize(o);
 }
 
@@ -326,7 +328,7 @@ struct WinDesc {
 static int run_scan(cmgpu_model *m, cmgpu_workspace *ws, int semiring, int qdbidx, const uint8_t *d_dsq,
                     const uint8_t *h_dsq, int64_t dsq_len, const std::vector<WinDesc> &wins, float cutoff,
                     int do_null3, bool plain, std::vector<std::vector<cmgpu_hit>> &hits_per_win,
-                    std::vector<Cand> *cells_out = nullptr) {
+                    std::vector<Cand> *cells_out = nullptr, bool calib = false) {
     if (semiring != CMGPU_CYK_F32 && semiring != CMGPU_INSIDE_I32) {
         set_error("unknown semiring");
         return CMGPU_EINVAL;
@@ -383,6 +385,13 @@ static int run_scan(cmgpu_model *m, cmgpu_workspace *ws, int semiring, int qdbid
         sp.beginsc_all = dp->beginsc_all;
     }
     sp.deck_elems = pl.deck_elems;
+    // cmcalibrate's scan: bit-score order of the local begins, and the
+    // report pre-filter (its cutoff of -inf makes every ROOT cell reportable)
+    sp.begin_key = calib ? 1 : 0;
+    sp.prefilter = calib ? 1 : 0;
+    sp.do_null3 = do_null3 ? 1 : 0;
+    for (int a = 0; a < 4; a++) sp.pf_null[a] = m->cm.view.null[a];
+    sp.pf_omega = m->cm.view.n3_omega;
     // per-state tables in global memory when they alone would fill most of
     // the shared memory (models of a few thousand states)
     sp.tables_global = 0;
@@ -393,6 +402,10 @@ static int run_scan(cmgpu_model *m, cmgpu_workspace *ws, int semiring, int qdbid
     sp.cutoff = cutoff;
 
     // kernel choice
+    if (calib && ws->kernel == CMGPU_KERNEL_SWEEP) {
+        set_error("cmcalibrate's scan runs on the level kernel only");
+        return CMGPU_EINVAL;
+    }
     if (ws->kernel == CMGPU_KERNEL_SWEEP && !dp->sw_ok) {
         set_error("node-sweep kernel does not apply to this model: " + dp->sw_why);
         return CMGPU_EINVAL;
@@ -916,7 +929,8 @@ int cmgpu_final_stage_inside_opt(const cmgpu_model *mc, cmgpu_workspace *ws, con
 
 static int batch_common(const cmgpu_model *mc, cmgpu_workspace *ws, int semiring, int qdbidx, const uint8_t *h_dsq,
                         const uint8_t *d_dsq, int64_t dsq_len, const cmgpu_window *wins, int32_t nwin, float cutoff,
-                        int do_null3, bool plain, cmgpu_batch_hit *hits, int32_t cap, int32_t *n_out) {
+                        int do_null3, bool plain, cmgpu_batch_hit *hits, int32_t cap, int32_t *n_out,
+                        bool calib = false) {
     cmgpu_model *m = const_cast<cmgpu_model *>(mc);
     if (!m || !ws || !n_out || nwin < 0 || (nwin > 0 && !wins) || (cap > 0 && !hits)) return CMGPU_EINVAL;
     *n_out = 0;
@@ -933,7 +947,7 @@ static int batch_common(const cmgpu_model *mc, cmgpu_workspace *ws, int semiring
         d_dsq = ws->d_dsq;
     }
     std::vector<std::vector<cmgpu_hit>> hpw;
-    rc = run_scan(m, ws, semiring, qdbidx, d_dsq, h_dsq, dsq_len, wv, cutoff, do_null3, plain, hpw);
+    rc = run_scan(m, ws, semiring, qdbidx, d_dsq, h_dsq, dsq_len, wv, cutoff, do_null3, plain, hpw, nullptr, calib);
     if (rc) return rc;
     size_t n = 0;
     for (auto &v : hpw) n += v.size();
@@ -970,6 +984,20 @@ int cmgpu_scan_plain(const cmgpu_model *m, cmgpu_workspace *ws, int semiring, in
     if (!dsq_all) return CMGPU_EINVAL;
     return batch_common(m, ws, semiring, qdbidx, dsq_all, nullptr, dsq_len, wins, nwin, cutoff, do_null3, true, hits,
                         cap, n_out);
+}
+
+// collect_scores's scan (src/cm_calibrate.rs:953-989): every window with
+// cutoff -inf, local begins in bit-score order
+int cmgpu_calibrate_scan_batch(const cmgpu_model *m, cmgpu_workspace *ws, int semiring, int qdbidx,
+                               const uint8_t *dsq_all, int64_t dsq_len, const cmgpu_window *wins, int32_t nwin,
+                               int do_null3, cmgpu_batch_hit *hits, int32_t cap, int32_t *n_out) {
+    if (!dsq_all) return CMGPU_EINVAL;
+    if (ws && ws->kernel == CMGPU_KERNEL_SWEEP) {
+        set_error("cmcalibrate's scan runs on the level kernel only");
+        return CMGPU_EINVAL;
+    }
+    return batch_common(m, ws, semiring, qdbidx, dsq_all, nullptr, dsq_len, wins, nwin, -INFINITY, do_null3, false,
+                        hits, cap, n_out, true);
 }
 
 }  // extern "C"

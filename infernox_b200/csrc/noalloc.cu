@@ -19,8 +19,7 @@
 //
 // Set-up: the host needs the array's device address (its name in host code
 // is only a host-side stand-in).  The first call on a device looks the
-// address up once with cudaGetSymbolAddress, with that device current; make
-// that first call before any stream capture begins.
+// address up once with cudaGetSymbolAddress, with that device current.
 //
 // Blocking: the call copies its inputs, launches the scan and waits for its
 // stream (it reads the cell count back to size the result), so it returns

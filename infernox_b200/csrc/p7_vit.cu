@@ -8,16 +8,19 @@
 // the per-length N/C/J move cost of vit_score_scalar (:305-385).
 //
 // Device side: one warp per window, rows i in order.  Model positions
-// k = 1..M are split into blocks of B = ceil(M/32) consecutive positions, lane
-// l owning block l; the rows of M, I and D live in registers (B <= 8, i.e.
-// M <= 256) or, for longer models, in shared memory with a padded lane
-// stride (conflict-free).  M and I cells read only the previous
-// row; xE is a warp max.  D cells form a serial chain along k in the same row
-// (D(i,k) from M(i,k-1) and D(i,k-1)); each lane walks its block serially
-// from an incoming value and the warp repeats until no incoming value
-// changes -- the values then satisfy the serial chain, so they equal the
-// scalar full DD sweep bit for bit (and the SSE lazy-F result, which the
-// reference shows is the same).  All arithmetic is 16-bit saturating.
+// k = 1..M are split into blocks of consecutive positions, lane l owning
+// block l.  For M <= 256 each lane keeps its block of the M, I and D rows in
+// registers as packed pairs of int16 cells, and every saturating add and max
+// acts on two cells at once (the sm_90+ add/max/min.s16x2 instructions, with
+// the saturation done by clamping the operand first); longer models keep the
+// rows in shared memory with a padded lane stride (conflict-free), one cell
+// per 32-bit lane op.  M and I cells read only the previous row; xE is a warp
+// max.  D cells form a serial chain along k in the same row (D(i,k) from
+// M(i,k-1) and D(i,k-1)); each lane walks its block serially from an incoming
+// value and the warp repeats until no incoming value changes -- the values
+// then satisfy the serial chain, so they equal the scalar full DD sweep bit
+// for bit (and the SSE lazy-F result, which the reference shows is the
+// same).  All arithmetic is 16-bit saturating.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -258,85 +261,161 @@ __global__ void __launch_bounds__(256) vit_kernel(const int16_t *__restrict__ ta
     }
 }
 
-// The same recurrence with each lane's B (<= 8) cells of the M, I and D rows
-// held in registers instead of shared memory: identical operations in the
-// same order, with the neighbouring lane's last cell passed by shuffle.
-template <int BB>
-__global__ void __launch_bounds__(256) vit_kernel_reg(const int16_t *__restrict__ tab, int M, int base_w,
-                                                      int e_move, int e_loop, const uint8_t *__restrict__ dsq,
-                                                      const VitWin *__restrict__ wins, int nwin, int *out,
-                                                      uint8_t *status) {
-    extern __shared__ int vsm[];
+// Packed kernel for models up to 256 positions: lane l owns the 2*NP
+// positions k = 1 + 2*NP*l .. 2*NP*(l+1), held as NP registers of two int16
+// cells each (the lower half is position k, the upper half k+1), for each of
+// the M, I and D rows.  Every saturating step acts on two cells at once with
+// the sm_90+ s16x2 instructions:
+//   sat(a + b) = add(min(max(a, lo_b), hi_b), b),  lo_b = max(-32768 - b, -32768),
+//                hi_b = min(32767 - b, 32767),
+// which is exact: a is moved just far enough that a + b lands on the
+// saturation bound, and otherwise left alone.  Transitions are never positive
+// (they are capped at 0 or -1), so for them the upper clamp is the identity
+// and only max + add remain.  The operations and their order per cell are
+// those of the scalar recurrence, so the result is the same bit for bit.
+__device__ __forceinline__ uint32_t pk16(int lo, int hi) { return ((uint32_t)lo & 0xffffu) | ((uint32_t)hi << 16); }
+__device__ __forceinline__ int lo16(uint32_t x) { return (int)(int16_t)(x & 0xffffu); }
+__device__ __forceinline__ int hi16(uint32_t x) { return (int)(int16_t)(x >> 16); }
+__device__ __forceinline__ uint32_t vadd2(uint32_t a, uint32_t b) {
+    uint32_t r;
+    asm("add.s16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
+}
+__device__ __forceinline__ uint32_t vmax2(uint32_t a, uint32_t b) {
+    uint32_t r;
+    asm("max.s16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
+}
+__device__ __forceinline__ uint32_t vmin2(uint32_t a, uint32_t b) {
+    uint32_t r;
+    asm("min.s16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
+}
+// lower clamp of a non-positive addend: -32768 - b (b <= 0, so it fits)
+__host__ __device__ __forceinline__ int lo_clamp(int b) { return b < 0 ? -32768 - b : -32768; }
+__host__ __device__ __forceinline__ int hi_clamp(int b) { return b > 0 ? 32767 - b : 32767; }
+// saturating add of a non-positive pair b, with lb its lower clamps
+__device__ __forceinline__ uint32_t addsat_np(uint32_t a, uint32_t b, uint32_t lb) { return vadd2(vmax2(a, lb), b); }
+
+template <int NP>
+__global__ void __launch_bounds__(256) vit_kernel_pk(const int16_t *__restrict__ tab, int M, int base_w,
+                                                     int e_move, int e_loop, const uint8_t *__restrict__ dsq,
+                                                     const VitWin *__restrict__ wins, int nwin, int *out,
+                                                     uint8_t *status) {
+    // emission pairs [18][NP][32] as (b, lo_b, hi_b) triples, lane-minor so a
+    // warp's reads of one entry hit 32 distinct banks
+    extern __shared__ uint32_t psm[];
+    constexpr int BB = 2 * NP;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const int tstride = M + 2;  // entries per table column (k = 0..M, padded)
-    int16_t *tabT = reinterpret_cast<int16_t *>(vsm);
-    for (int q = threadIdx.x; q < (M + 1) * 26; q += blockDim.x) {
-        const int k = q / 26, c = q - k * 26;
-        tabT[c * tstride + k] = tab[q];
+    auto tv = [&](int k, int c) -> int { return (k >= 0 && k <= M) ? (int)tab[k * 26 + c] : -32768; };
+    for (int q = threadIdx.x; q < 18 * NP * 32; q += blockDim.x) {
+        const int x = q / (NP * 32), r = q - x * (NP * 32), qq = r >> 5, l = r & 31;
+        const int k = 1 + l * BB + 2 * qq;
+        const int a = tv(k, x), b = tv(k + 1, x);
+        psm[3 * q] = pk16(a, b);
+        psm[3 * q + 1] = pk16(lo_clamp(a), lo_clamp(b));
+        psm[3 * q + 2] = pk16(hi_clamp(a), hi_clamp(b));
+    }
+    const int k0 = 1 + lane * BB;
+    // transition pairs and their lower clamps; the ones read at k-1 are
+    // stored shifted, (k-1, k) for the pair (k, k+1)
+    uint32_t tb[NP], lb[NP], tmm[NP], lmm[NP], tim[NP], lim[NP], tdm[NP], ldm[NP];
+    uint32_t tmi[NP], lmi[NP], tii[NP], lii[NP], tmd[NP], lmd[NP], tdd[NP], ldd[NP], inv[NP];
+#pragma unroll
+    for (int q = 0; q < NP; q++) {
+        const int k = k0 + 2 * q;
+#define VIT_PAIR(t, l, c, k1)                          \
+    {                                                  \
+        const int a_ = tv(k1, c), b_ = tv(k1 + 1, c);  \
+        t[q] = pk16(a_, b_);                           \
+        l[q] = pk16(lo_clamp(a_), lo_clamp(b_));       \
+    }
+        VIT_PAIR(tb, lb, 18, k)
+        VIT_PAIR(tmm, lmm, 19, k - 1)
+        VIT_PAIR(tim, lim, 20, k - 1)
+        VIT_PAIR(tdm, ldm, 21, k - 1)
+        VIT_PAIR(tmi, lmi, 22, k)
+        VIT_PAIR(tii, lii, 23, k)
+        VIT_PAIR(tmd, lmd, 24, k - 1)
+        VIT_PAIR(tdd, ldd, 25, k - 1)
+#undef VIT_PAIR
+        inv[q] = (k > M ? 0x0000ffffu : 0u) | (k + 1 > M ? 0xffff0000u : 0u);
     }
     __syncthreads();
-    auto T = [&](int c, int k) -> int { return tabT[c * tstride + k]; };
-    const int k0 = 1 + lane * BB;  // first position of this lane's block
     const unsigned FULL = 0xffffffffu;
+    const uint32_t NEG = 0x80008000u;
     for (int w = blockIdx.x * nw + warp; w < nwin; w += gridDim.x * nw) {
         const VitWin win = wins[w];
         const uint8_t *frame = dsq + win.off;
-        int mv[BB], iv[BB], dv[BB];
+        uint32_t mv[NP], iv[NP], dv[NP];
 #pragma unroll
-        for (int b = 0; b < BB; b++) mv[b] = iv[b] = dv[b] = -32768;
+        for (int q = 0; q < NP; q++) mv[q] = iv[q] = dv[q] = NEG;
         int xn = base_w, xb = adds16(base_w, win.xw_move), xj = -32768, xc = -32768;
         bool overflow = false;
         for (int i = win.i0; i <= win.j0; i++) {
             int x = frame[i];
             x = x > 17 ? 17 : x;
-            // previous-row values at k0-1 (lane-1's last cell; -inf at k = 0)
-            int pm = __shfl_up_sync(FULL, mv[BB - 1], 1);
-            int pi = __shfl_up_sync(FULL, iv[BB - 1], 1);
-            int pd = __shfl_up_sync(FULL, dv[BB - 1], 1);
-            if (lane == 0) pm = pi = pd = -32768;
-            int xe = -32768;
-            int mn[BB], in[BB], dn[BB];
+            const uint32_t *E = psm + 3 * (x * NP * 32 + lane);
+            // previous-row cells at k0-1 (lane-1's last cell; -inf at k = 0)
+            uint32_t pm = __shfl_up_sync(FULL, mv[NP - 1], 1);
+            uint32_t pi = __shfl_up_sync(FULL, iv[NP - 1], 1);
+            uint32_t pd = __shfl_up_sync(FULL, dv[NP - 1], 1);
+            if (lane == 0) pm = pi = pd = NEG;
+            const uint32_t XB = pk16(xb, xb);
+            uint32_t mn[NP], in[NP], dn[NP], xe2 = NEG;
 #pragma unroll
-            for (int b = 0; b < BB; b++) {
-                const int k = k0 + b;
-                int vm = -32768, vi = -32768;
-                if (k <= M) {
-                    int sc = adds16(xb, T(18, k));
-                    sc = max(sc, adds16(pm, T(19, k - 1)));
-                    sc = max(sc, adds16(pi, T(20, k - 1)));
-                    sc = max(sc, adds16(pd, T(21, k - 1)));
-                    vm = adds16(sc, T(x, k));
-                    vi = max(adds16(mv[b], T(22, k)), adds16(iv[b], T(23, k)));
-                    xe = max(xe, vm);
-                }
-                pm = mv[b];
-                pi = iv[b];
-                pd = dv[b];
-                mn[b] = vm;
-                in[b] = vi;
+            for (int q = 0; q < NP; q++) {
+                // previous row at (k-1, k): upper half of the pair before, lower half of this one
+                const uint32_t sm = __byte_perm(pm, mv[q], 0x5432);
+                const uint32_t si = __byte_perm(pi, iv[q], 0x5432);
+                const uint32_t sd = __byte_perm(pd, dv[q], 0x5432);
+                uint32_t sc = addsat_np(XB, tb[q], lb[q]);
+                sc = vmax2(sc, addsat_np(sm, tmm[q], lmm[q]));
+                sc = vmax2(sc, addsat_np(si, tim[q], lim[q]));
+                sc = vmax2(sc, addsat_np(sd, tdm[q], ldm[q]));
+                const uint32_t eb = E[96 * q], el = E[96 * q + 1], eh = E[96 * q + 2];
+                uint32_t vm = vadd2(vmin2(vmax2(sc, el), eh), eb);
+                uint32_t vi = vmax2(addsat_np(mv[q], tmi[q], lmi[q]), addsat_np(iv[q], tii[q], lii[q]));
+                vm = (vm & ~inv[q]) | (NEG & inv[q]);
+                vi = (vi & ~inv[q]) | (NEG & inv[q]);
+                xe2 = vmax2(xe2, vm);
+                pm = mv[q];
+                pi = iv[q];
+                pd = dv[q];
+                mn[q] = vm;
+                in[q] = vi;
             }
+            int xe = max(lo16(xe2), hi16(xe2));
             for (int o = 16; o > 0; o >>= 1) xe = max(xe, __shfl_xor_sync(FULL, xe, o));
-            // D chain along k: d(k) = max(M(i,k-1)+MD(k-1), d(k-1)+DD(k-1))
-            int m_in = __shfl_up_sync(FULL, mn[BB - 1], 1);
-            if (lane == 0) m_in = -32768;
+            // D chain along k: d(k) = max(M(i,k-1)+MD(k-1), d(k-1)+DD(k-1));
+            // the M terms of every pair first (independent of d), then the chain
+            uint32_t m_in = __shfl_up_sync(FULL, mn[NP - 1], 1);
+            if (lane == 0) m_in = NEG;
+            uint32_t mt[NP];
+#pragma unroll
+            for (int q = 0; q < NP; q++) {
+                const uint32_t smn = __byte_perm(q == 0 ? m_in : mn[q > 0 ? q - 1 : 0], mn[q], 0x5432);
+                mt[q] = addsat_np(smn, tmd[q], lmd[q]);
+            }
             int din = -32768, din_prev = -32768;
             for (int it = 0; it < 34; it++) {
-                int d = din, mprev = m_in;
+                uint32_t d = pk16(din, din);  // the chain value in both halves
 #pragma unroll
-                for (int b = 0; b < BB; b++) {
-                    const int k = k0 + b;
-                    int v = -32768;
-                    if (k <= M) v = max(adds16(mprev, T(24, k - 1)), adds16(d, T(25, k - 1)));
-                    dn[b] = v;
-                    d = v;
-                    mprev = mn[b];
+                for (int q = 0; q < NP; q++) {
+                    const uint32_t r1 = vmax2(mt[q], addsat_np(d, tdd[q], ldd[q]));   // lower half: d(k)
+                    const uint32_t d1 = __byte_perm(r1, 0, 0x1010);
+                    const uint32_t r2 = vmax2(mt[q], addsat_np(d1, tdd[q], ldd[q]));  // upper half: d(k+1)
+                    uint32_t v = __byte_perm(r1, r2, 0x7610);
+                    v = (v & ~inv[q]) | (NEG & inv[q]);
+                    dn[q] = v;
+                    d = __byte_perm(v, 0, 0x3232);
                 }
                 const bool has = k0 <= M;
-                const int dlast = has ? d : -32768;
+                const int dlast = has ? hi16(d) : -32768;
                 const bool same = !has || din == din_prev;
                 if (it > 0 && __all_sync(FULL, same)) break;
                 din_prev = din;
-                int up = __shfl_up_sync(FULL, dlast, 1);
+                const int up = __shfl_up_sync(FULL, dlast, 1);
                 din = lane == 0 ? -32768 : up;
             }
             if (xe >= 32767) {
@@ -347,10 +426,10 @@ __global__ void __launch_bounds__(256) vit_kernel_reg(const int16_t *__restrict_
             xj = max(xj, adds16(xe, e_loop));
             xb = max(adds16(xj, win.xw_move), adds16(xn, win.xw_move));
 #pragma unroll
-            for (int b = 0; b < BB; b++) {
-                mv[b] = mn[b];
-                iv[b] = in[b];
-                dv[b] = dn[b];
+            for (int q = 0; q < NP; q++) {
+                mv[q] = mn[q];
+                iv[q] = in[q];
+                dv[q] = dn[q];
             }
         }
         if (lane == 0) {
@@ -482,26 +561,24 @@ extern "C" int cmgpu_vit_score_batch(const cmgpu_vit_filter *f, void *stream_ptr
         return CMGPU_EDEVICE;
     }
     // models up to 256 positions keep each lane's block of the rows in
-    // registers; longer ones use the shared-memory rows
-    auto launch_reg = [&](auto kern) {
+    // registers as packed int16 pairs; longer ones use the shared-memory rows
+    const int NP = (B + 1) / 2;
+    auto launch_pk = [&](auto kern) {
         const int g = (int)std::min<int64_t>((nwin + 7) / 8, (int64_t)sms * 8);
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tab_bytes);
-        kern<<<g, 256, tab_bytes, st>>>(f->d_tab, M, f->host.base_w, f->host.e_move, f->host.e_loop, d_dsq, d_w,
-                                        nwin, d_out, d_st);
+        const size_t pk_smem = (size_t)18 * NP * 32 * 3 * sizeof(uint32_t);
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pk_smem);
+        kern<<<g, 256, pk_smem, st>>>(f->d_tab, M, f->host.base_w, f->host.e_move, f->host.e_loop, d_dsq, d_w,
+                                      nwin, d_out, d_st);
     };
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEventCreate(&ev0);
     cudaEventCreate(&ev1);
     cudaEventRecord(ev0, st);
-    switch (B) {
-    case 1: launch_reg(dev::vit_kernel_reg<1>); break;
-    case 2: launch_reg(dev::vit_kernel_reg<2>); break;
-    case 3: launch_reg(dev::vit_kernel_reg<3>); break;
-    case 4: launch_reg(dev::vit_kernel_reg<4>); break;
-    case 5: launch_reg(dev::vit_kernel_reg<5>); break;
-    case 6: launch_reg(dev::vit_kernel_reg<6>); break;
-    case 7: launch_reg(dev::vit_kernel_reg<7>); break;
-    case 8: launch_reg(dev::vit_kernel_reg<8>); break;
+    switch (B <= 8 ? NP : 0) {
+    case 1: launch_pk(dev::vit_kernel_pk<1>); break;
+    case 2: launch_pk(dev::vit_kernel_pk<2>); break;
+    case 3: launch_pk(dev::vit_kernel_pk<3>); break;
+    case 4: launch_pk(dev::vit_kernel_pk<4>); break;
     default:
         dev::vit_kernel<<<grid, warps * 32, smem, st>>>(f->d_tab, M, f->host.base_w, f->host.e_move, f->host.e_loop,
                                                       d_dsq, d_w, nwin, d_out, d_st);

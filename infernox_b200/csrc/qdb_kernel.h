@@ -31,6 +31,7 @@ struct Cand {
 struct SmemLayout {
     int el, tbl, info, wb, cb, tsc, endsc, escc, chunks, lvl, begin, beginsc, ring, lane, deck;
     int bsv, bmax;     // fused local begins: per-state begin score, per-lane ROOT row
+    int prow;          // report pre-filter: per-lane ROOT row of raw values
     int ring_len;      // residues per lane ring (power of two >= W + 64)
     int64_t words;     // total
 };
@@ -76,6 +77,17 @@ struct ScanParams {
     // (models whose tables would not leave room for a lane)
     int tables_global;
     // lanes per CTA and deck placement
+    // cmcalibrate's scan (src/cm_calibrate.rs:441-780): local begins are
+    // compared in bits, so -INFTY orders below every other integer value
+    // (scorify maps it to IMPOSSIBLE, and nothing else)
+    int begin_key;
+    // report pre-filter: of the ROOT cells of a column only those that the
+    // greedy report (with null3) could report are emitted; the rest can be
+    // neither reported nor raise the running maximum of reported scores
+    int prefilter;
+    int do_null3;
+    float pf_null[4];
+    float pf_omega;
     int lanes;
     int deck_smem;
     uint32_t *deck_global;  // when !deck_smem: [ctas][lanes][deck_stride]

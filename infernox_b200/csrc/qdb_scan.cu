@@ -70,6 +70,7 @@ struct Smem {
     const uint32_t *tsc, *endsc, *escc, *beginsc;
     const uint32_t *bsv;  // [M] begin score per state (fused begins)
     int32_t *bmax;        // [lanes][bstride] ROOT-row begin maxima (fused begins)
+    uint32_t *prow;       // [lanes][bstride] ROOT-row raw values (report pre-filter)
     int bstride;
     const int32_t *lvl;
     const int4 *begin;
@@ -154,6 +155,19 @@ __device__ __forceinline__ typename S::T cell_value(const K &k, const Lane &L, i
     return sc;
 }
 
+// Local-begin comparison: `a < cand` on the raw values (src/cm_nohmm.rs:
+// 720-742), or, for cmcalibrate's scan (src/cm_calibrate.rs:720-745), on
+// their bit scores, where -INFTY (IMPOSSIBLE) sits below every other integer.
+template <class S>
+__device__ __forceinline__ bool begin_less(int key, typename S::T a, typename S::T cand) {
+    if (S::ORDERED && key) {
+        const int32_t ka = (int32_t)S::u(a) == -INFTY_D ? INT32_MIN : (int32_t)S::u(a);
+        const int32_t kc = (int32_t)S::u(cand) == -INFTY_D ? INT32_MIN : (int32_t)S::u(cand);
+        return ka < kc;
+    }
+    return a < cand;
+}
+
 // Fused local begins (integer Inside): ROOT cell d takes the maximum of
 // cell(v, d) + beginsc[v] over the begin states v, and a maximum needs no
 // order, so each begin state posts its cells as it computes them.
@@ -162,7 +176,8 @@ __device__ __forceinline__ void post_begin(const K &k, const Lane &L, const SInf
                                            typename S::T x) {
     if (S::ORDERED && k.p->fuse_begin && (sv.flags & SF_BEGIN) && d >= k.p->root_dn &&
         d <= min(L.jrow, k.p->root_dxcap)) {
-        const int32_t c = (int32_t)((uint32_t)S::u(x) + k.s.bsv[v]);
+        int32_t c = (int32_t)((uint32_t)S::u(x) + k.s.bsv[v]);
+        if (k.p->begin_key && c == -INFTY_D) c = INT32_MIN;
         atomicMax(k.s.bmax + L.l * k.s.bstride + d, c);
     }
 }
@@ -319,6 +334,133 @@ __device__ __forceinline__ void do_il(const K &k, const Lane &L, int v, const SI
 enum { LS_ITEM = 0, LS_JB, LS_JSTART, LS_JEND, LS_JREPORT, LS_OFFLO, LS_OFFHI, LS_JM };
 constexpr int LS_W = 8;
 
+// Appends the cells of the warp's lanes with hit set to the candidate buffer
+// (one atomic per warp); entries past cand_cap are counted, not written.
+__device__ __forceinline__ void emit_cand(const ScanParams &p, int wl, bool hit, int item, int j, int d,
+                                          uint32_t raw) {
+    const unsigned m = __ballot_sync(0xffffffffu, hit);
+    if (!m) return;
+    const int leader = __ffs(m) - 1;
+    int base = 0;
+    if (wl == leader) base = atomicAdd(p.cand_count, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (hit) {
+        const int pos = base + __popc(m & ((1u << wl) - 1));
+        if (pos < p.cand_cap) {
+            Cand cd;
+            cd.item = item;
+            cd.j = j;
+            cd.d = d;
+            cd.raw = raw;
+            p.cands[pos] = cd;
+        }
+    }
+}
+
+// Null3 correction of a hit of length len with residue counts n[4]
+// (score_correction_null3, src/cp9.rs:6516-6528), computed as the host does
+// but with the device's log and, for the final FLogsum(0, x), the exact
+// log2(1 + 2^-x) instead of the 0.001-step table: used only to decide which
+// cells the host must look at, within a margin that covers both differences.
+__device__ float null3_approx(const ScanParams &p, const uint32_t *n, int len) {
+    float comp[4], sum = 0.0f;
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+        comp[a] = (float)n[a];
+        sum = __fadd_rn(sum, comp[a]);
+    }
+#pragma unroll
+    for (int a = 0; a < 4; a++) comp[a] = sum > 0.0f ? __fdiv_rn(comp[a], sum) : 0.25f;
+    float score = 0.0f;
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+        const double q = (double)__fdiv_rn(comp[a], p.pf_null[a]);
+        const double t = (q > 0.0 ? log(q) * 1.44269504 : -1.0e36) * (double)comp[a] * (double)len;
+        score = (float)((double)score + t);
+    }
+    const double om = (double)p.pf_omega;
+    score = (float)((double)score + (om > 0.0 ? log(om) * 1.44269504 : -1.0e36));
+    const float mx = fmaxf(0.0f, score), mn = fminf(0.0f, score);
+    if (mx - mn >= 23.0f) return mx;
+    return mx + (float)log2(1.0 + exp2(-(double)(mx - mn)));
+}
+
+// Margin of an approximate corrected score: FLogsum's table step (<= 5e-4
+// bits) plus the double-precision log differences (relative ~1e-15) plus
+// f32 rounding of the sums (a few ulps of |x|), with room to spare.
+__device__ __forceinline__ float pf_margin(float x) { return 2.0e-3f + 1.0e-5f * fabsf(x); }
+
+// Report pre-filter of one lane's column (one warp): the greedy report
+// (src/cm_nohmm.rs:769-812) walks d ascending and reports a cell when its
+// corrected score c(d) is >= cutoff and above every reported score so far,
+// i.e. above R(d) = max{c(d') : d' < d, c(d') >= cutoff}, since the largest
+// such c(d') is always reported.  With approximate scores c~ within margin
+// m of c, a cell with c~(d) + m(d) <= R~(d) - m(R~), or c~(d) + m(d) < cutoff,
+// can neither be reported nor change R, where R~ is the maximum of c~(d')
+// over the cells with c~(d') - m(d') >= cutoff.  Every other cell with a
+// possible score is emitted, and the host replays the exact rule on them.
+// Residue counts of j-d+1..j come from a warp prefix sum over d.
+template <class S>
+__device__ void prefilter_row(const K &k, int l, int step, int wl) {
+    const ScanParams &p = *k.p;
+    const unsigned FULL = 0xffffffffu;
+    const int32_t *ls = k.s.lane + l * LS_W;
+    const int j = ls[LS_JB] + step;
+    if (ls[LS_ITEM] < 0 || j > ls[LS_JEND] || j < ls[LS_JREPORT]) return;
+    const int jrow = min(j - ls[LS_JSTART] + 1, p.W);
+    const int dn0 = p.root_dn, dx0 = min(jrow, p.root_dxcap);
+    const uint8_t *ring = k.s.ring + l * p.lay.ring_len;
+    const uint32_t *row = k.s.prow + l * k.s.bstride;
+    const int item = p.item_base + ls[LS_ITEM];
+    uint32_t c01 = 0, c23 = 0;  // counts of residues 0,1 / 2,3 in j-d+1..j, 16 bits each
+    float run = -INFINITY;
+    for (int base = 1; base <= dx0; base += 32) {
+        const int d = base + wl;
+        const bool in = d <= dx0;
+        const int r = in ? ring[(j - d + 1) & k.rmask] : 4;
+        uint32_t x01 = (r == 0 ? 1u : 0u) | (r == 1 ? 0x10000u : 0u);
+        uint32_t x23 = (r == 2 ? 1u : 0u) | (r == 3 ? 0x10000u : 0u);
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y01 = __shfl_up_sync(FULL, x01, o), y23 = __shfl_up_sync(FULL, x23, o);
+            if (wl >= o) {
+                x01 += y01;
+                x23 += y23;
+            }
+        }
+        x01 += c01;
+        x23 += c23;
+        c01 = __shfl_sync(FULL, x01, 31);
+        c23 = __shfl_sync(FULL, x23, 31);
+        uint32_t raw = 0;
+        float c = -INFINITY;
+        if (in && d >= dn0) {
+            raw = row[d];
+            const float bits = S::bits(S::ld(row + d));
+            if (bits > IMPOSSIBLE_D + 1.0f) {
+                c = bits;
+                if (p.do_null3) {
+                    const uint32_t n[4] = {x01 & 0xffffu, x01 >> 16, x23 & 0xffffu, x23 >> 16};
+                    c = __fsub_rn(c, null3_approx(p, n, d));
+                }
+            }
+        }
+        const float m = pf_margin(c);
+        float inc = (c > -INFINITY && c - m >= p.cutoff) ? c : -INFINITY;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const float y = __shfl_up_sync(FULL, inc, o);
+            if (wl >= o) inc = fmaxf(inc, y);
+        }
+        float ex = __shfl_up_sync(FULL, inc, 1);
+        if (wl == 0) ex = -INFINITY;
+        ex = fmaxf(ex, run);
+        run = fmaxf(run, __shfl_sync(FULL, inc, 31));
+        const bool hit = c > -INFINITY && c + m >= p.cutoff && (ex == -INFINITY || c + m > ex - pf_margin(ex));
+        emit_cand(p, wl, hit, item, j, d, raw);
+    }
+}
+
 template <bool INS, bool DECK_SMEM>
 __global__ void __launch_bounds__(512, 1) qdb_scan_kernel(ScanParams p) {
     typedef Sem<INS> S;
@@ -361,6 +503,7 @@ __global__ void __launch_bounds__(512, 1) qdb_scan_kernel(ScanParams p) {
     k.s.lane = reinterpret_cast<int32_t *>(smem + ly.lane);
     k.s.bsv = smem + ly.bsv;
     k.s.bmax = reinterpret_cast<int32_t *>(smem + ly.bmax);
+    k.s.prow = smem + ly.prow;
     k.s.bstride = p.root_dxcap + 1;
     k.rmask = ly.ring_len - 1;
 
@@ -392,7 +535,8 @@ __global__ void __launch_bounds__(512, 1) qdb_scan_kernel(ScanParams p) {
         }
         if (INS && p.fuse_begin) {
             copy32(ly.bsv, p.beginsc_all, p.M);
-            for (int x = tid; x < lanes * (p.root_dxcap + 1); x += bs) k.s.bmax[x] = -INFTY_D;
+            for (int x = tid; x < lanes * (p.root_dxcap + 1); x += bs)
+                k.s.bmax[x] = p.begin_key ? INT32_MIN : -INFTY_D;
         }
         if (tid < MAX_LANES * LS_W) k.s.lane[tid] = tid % LS_W == LS_ITEM ? -1 : 0;
     }
@@ -534,8 +678,8 @@ __global__ void __launch_bounds__(512, 1) qdb_scan_kernel(ScanParams p) {
                             if (INS && p.fuse_begin) {
                                 int32_t *bm = k.s.bmax + l * k.s.bstride + d;
                                 const T cand = (T)*bm;
-                                *bm = -INFTY_D;
-                                if (a < cand) a = cand;
+                                *bm = p.begin_key ? INT32_MIN : -INFTY_D;
+                                if (begin_less<S>(p.begin_key, a, cand)) a = cand;
                             } else if (p.local) {
                                 for (int b = 0; b < p.nbegin; b++) {
                                     const int4 bd = k.s.begin[b];
@@ -549,34 +693,23 @@ __global__ void __launch_bounds__(512, 1) qdb_scan_kernel(ScanParams p) {
                                         rb = par ? bd.z : bd.y;
                                     }
                                     T cand = S::add(S::ld(deck + rb + d), S::ld(k.s.beginsc + b));
-                                    if (a < cand) a = cand;
+                                    if (begin_less<S>(p.begin_key, a, cand)) a = cand;
                                 }
                             }
-                            if (j >= ls[LS_JREPORT]) {
+                            if (p.prefilter) {
+                                k.s.prow[l * k.s.bstride + d] = S::u(a);
+                            } else if (j >= ls[LS_JREPORT]) {
                                 float sc = S::bits(a);
                                 hit = sc >= p.cutoff && sc > IMPOSSIBLE_D + 1.0f;
                             }
                         }
                     }
                 }
-                unsigned m = __ballot_sync(0xffffffffu, hit);
-                if (m) {
-                    int leader = __ffs(m) - 1;
-                    int base = 0;
-                    if (wl == leader) base = atomicAdd(p.cand_count, __popc(m));
-                    base = __shfl_sync(0xffffffffu, base, leader);
-                    if (hit) {
-                        int pos = base + __popc(m & ((1u << wl) - 1));
-                        if (pos < p.cand_cap) {
-                            Cand cd;
-                            cd.item = p.item_base + k.s.lane[l * LS_W + LS_ITEM];
-                            cd.j = j;
-                            cd.d = d;
-                            cd.raw = S::u(a);
-                            p.cands[pos] = cd;
-                        }
-                    }
-                }
+                emit_cand(p, wl, hit, hit ? p.item_base + k.s.lane[l * LS_W + LS_ITEM] : 0, j, d, S::u(a));
+            }
+            if (p.prefilter) {
+                __syncthreads();
+                for (int l = warp; l < lanes; l += nwarps) prefilter_row<S>(k, l, step, wl);
             }
             if (INS && p.fuse_begin) __syncthreads();  // ROOT-row resets before the next column's posts
         }
@@ -642,6 +775,7 @@ SmemLayout scan_layout(const ScanParams &p, int lanes, bool deck_smem) {
     L.lane = take((int64_t)MAX_LANES * 8);
     L.bsv = take(p.fuse_begin ? p.M : 0);
     L.bmax = take(p.fuse_begin ? (int64_t)lanes * (p.root_dxcap + 1) : 0);
+    L.prow = take(p.prefilter ? (int64_t)lanes * (p.root_dxcap + 1) : 0);
     L.deck = take(deck_smem ? (int64_t)lanes * p.deck_elems : 0);
     L.words = w;
     return L;

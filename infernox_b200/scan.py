@@ -39,25 +39,56 @@ def _frame(dsq) -> np.ndarray:
     return a
 
 
+class Workspace:
+    """A device workspace (decks, work queue, candidate buffers, stream) that
+    several Scanners of one thread may share, so a library of models keeps
+    one set of scratch buffers sized for the largest scan instead of one per
+    model."""
+
+    def __init__(self, device: int = 0, stream: int | None = None):
+        self.handle = C.c_void_p()
+        N.check(N.lib().cmgpu_workspace_create(device, C.c_void_p(stream) if stream else None,
+                                               C.byref(self.handle)))
+
+    def close(self) -> None:
+        if self.handle:
+            N.lib().cmgpu_workspace_free(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Scanner:
-    """A configured CM uploaded to one GPU, with a private workspace.
+    """A configured CM uploaded to one GPU, with a private workspace or a
+    shared one (`workspace`, owned by the caller).
 
-    One Scanner must be used by one thread at a time; build one per thread
-    (the device model is read-only and cheap to re-upload)."""
+    One Scanner -- and one Workspace -- must be used by one thread at a time;
+    build one per thread (the device model is read-only and cheap to
+    re-upload)."""
 
-    def __init__(self, cm: ConfiguredCM, device: int = 0, stream: int | None = None):
+    def __init__(self, cm: ConfiguredCM, device: int = 0, stream: int | None = None,
+                 workspace: Workspace | None = None):
         L = N.lib()
         self.cm = cm
         self._model = C.c_void_p()
         N.check(L.cmgpu_model_upload(C.byref(cm.as_struct()), device, C.byref(self._model)))
-        self._ws = C.c_void_p()
-        N.check(L.cmgpu_workspace_create(device, C.c_void_p(stream) if stream else None,
-                                         C.byref(self._ws)))
+        self._shared = workspace
+        if workspace is not None:
+            self._ws = workspace.handle
+        else:
+            self._ws = C.c_void_p()
+            N.check(L.cmgpu_workspace_create(device, C.c_void_p(stream) if stream else None,
+                                             C.byref(self._ws)))
 
     def close(self) -> None:
         L = N.lib()
         if self._ws:
-            L.cmgpu_workspace_free(self._ws)
+            if self._shared is None:
+                L.cmgpu_workspace_free(self._ws)
             self._ws = C.c_void_p()
         if self._model:
             L.cmgpu_model_free(self._model)
@@ -185,6 +216,22 @@ class Scanner:
         return self.final_stage_inside_opt(dsq, envs, cutoff, do_null3, False)
 
     # ------------------------------------------------------------------
+    def calibrate_scan_batch(self, semiring: int, qdbidx: int, buf: np.ndarray, windows: np.ndarray,
+                             do_null3: bool) -> np.ndarray:
+        """cmcalibrate's scan of every window (cutoff -inf, local begins in
+        bit-score order, src/cm_calibrate.rs:441-989): the kept hits of each
+        window, BATCH_HIT_DTYPE in window order."""
+        w = np.ascontiguousarray(windows, N.WINDOW_DTYPE)
+        b = np.ascontiguousarray(buf, np.uint8)
+        # kept hits of a window are disjoint: at most one per residue
+        cap = max(1024, int((w["j0"] - w["i0"] + 1).clip(0).sum()) + len(w))
+        out = np.zeros(cap, N.BATCH_HIT_DTYPE)
+        nout = C.c_int32()
+        N.check(N.lib().cmgpu_calibrate_scan_batch(self._model, self._ws, semiring, qdbidx, b.ctypes.data,
+                                                   int(b.size), w.ctypes.data, len(w), int(bool(do_null3)),
+                                                   out.ctypes.data, cap, C.byref(nout)))
+        return out[: nout.value].copy()
+
     def scan_batch(self, semiring: int, qdbidx: int, buf: np.ndarray, windows: np.ndarray,
                    cutoff: float, do_null3: bool, plain: bool = False, device_buf=None) -> np.ndarray:
         """Scan many windows of one residue buffer in one launch.

@@ -4,7 +4,9 @@ library of CMs, with continuous batching.
 The reference runs cmscan as a serial loop over queries and, for each, over
 the models of the library (src/bin/cmscan.rs:833-834), with parallelism only
 inside one search (src/cm_search.rs:1300-1315).  Here every model of the
-library stays uploaded with its scan plans, and requests share the GPU:
+library stays uploaded with its scan plans, all models share one device
+workspace (decks and buffers sized once for the largest scan), and requests
+share the GPU:
 
 * Admission.  A submitted request waits in a bounded FIFO queue; it becomes
   active when the residues of all active requests (both strands) stay within
@@ -34,7 +36,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _native as N
-from .scan import CYK_F32, INSIDE_I32, QDB1, QDB2, Scanner
+from .scan import CYK_F32, INSIDE_I32, QDB1, QDB2, Scanner, Workspace
 from .synth import revcomp
 
 OK, REFUSED_TOO_LARGE, REFUSED_QUEUE_FULL, CANCELLED = 0, 1, 2, 3
@@ -84,6 +86,7 @@ class Server:
         self.models = list(models)
         self.device = device
         self._scanners = None  # uploaded on the first scan (queueing needs no GPU)
+        self._ws = None        # one workspace shared by every model's scanner
         self.budget = int(budget_residues)
         self.max_queue = int(max_queue)
         self.f6_cutoff, self.final_cutoff, self.do_null3 = float(f6_cutoff), float(final_cutoff), bool(do_null3)
@@ -101,13 +104,17 @@ class Server:
     @property
     def scanners(self):
         if self._scanners is None:
-            self._scanners = [Scanner(cm, device=self.device) for cm in self.models]
+            self._ws = Workspace(self.device)
+            self._scanners = [Scanner(cm, device=self.device, workspace=self._ws) for cm in self.models]
         return self._scanners
 
     def close(self):
         for s in self._scanners or []:
             s.close()
         self._scanners = None
+        if self._ws is not None:
+            self._ws.close()
+            self._ws = None
 
     # -- requests ----------------------------------------------------------
     def submit(self, req: Request) -> int:

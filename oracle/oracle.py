@@ -1,6 +1,6 @@
 """TEST INFRASTRUCTURE ONLY: ctypes binding of the oracle (qdb_oracle.c,
 hb_oracle.c, tr_oracle.c, trq_oracle.c, p7_oracle.c, msv_oracle.c,
-prep_oracle.c).
+prep_oracle.c, calib_oracle.c).
 
 Used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as
 the checker of the GPU scanner.  The product package never imports it.
@@ -43,7 +43,7 @@ def lib():
     global _lib
     if _lib is None:
         srcs = [os.path.join(HERE, f) for f in ("qdb_oracle.c", "hb_oracle.c", "tr_oracle.c", "trq_oracle.c",
-                                                "p7_oracle.c", "msv_oracle.c", "prep_oracle.c")]
+                                                "p7_oracle.c", "msv_oracle.c", "prep_oracle.c", "calib_oracle.c")]
         if not os.path.exists(LIB_PATH) or any(os.path.getmtime(LIB_PATH) < os.path.getmtime(f) for f in srcs):
             native = os.path.basename(os.path.dirname(LIB_PATH)) == "_build_native"
             subprocess.run(["make", "-s", "-C", HERE] + (["native"] if native else []), check=True)
@@ -79,6 +79,11 @@ def lib():
         L.oracle_ilogsum_table.argtypes = [P(C.c_int32), C.c_int]
         L.oracle_ilogsum.argtypes = [C.c_int32, C.c_int32]
         L.oracle_ilogsum.restype = C.c_int32
+        L.oracle_calib_scan.argtypes = [vp, C.c_int, C.c_int, P(C.c_uint8), C.c_int32, C.c_int32, C.c_int, vp,
+                                        C.c_int32, P(C.c_int32), P(C.c_double)]
+        L.oracle_genomic_sample.argtypes = [C.c_uint32, C.c_int32, C.c_int32, vp]
+        L.oracle_exp_fit.argtypes = [vp, C.c_int64, C.c_int, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_float,
+                                     C.c_double, vp]
         _lib = L
     return _lib
 
@@ -371,3 +376,42 @@ def prep_truncated(cm_s, local):
         raise RuntimeError(f"oracle_prep_truncated: {rc}")
     del keep
     return out
+
+
+# ---- cmcalibrate (calib_oracle.c, oracle_calib_scan in qdb_oracle.c) ------
+
+EXP_DTYPE = np.dtype([("lambda", np.float64), ("mu", np.float64), ("dbsize", np.float64), ("mu_orig", np.float64),
+                      ("tailp", np.float64), ("nrandhits", np.int32), ("pad", np.int32)])
+
+
+def calib_scan(cm, semiring, qdbidx, dsq, i0, j0, do_null3, want_cells=False):
+    """collect_scores's scan of one window: kept hits (i, j, score, bias)
+    (and the DP cells computed, with want_cells)."""
+    L = lib()
+    a, pa = _u8(dsq)
+    cap = max(64, (j0 - i0 + 1) + 64)
+    hits = np.zeros(cap, HIT_DTYPE)
+    n = C.c_int32()
+    cells = C.c_double()
+    rc = L.oracle_calib_scan(C.byref(cm.as_struct()), semiring, qdbidx, pa, i0, j0, int(bool(do_null3)),
+                             hits.ctypes.data, cap, C.byref(n), C.byref(cells))
+    if rc != 0:
+        raise RuntimeError(f"oracle overflow rc={rc}")
+    out = [(int(h["i"]), int(h["j"]), float(h["score"]), float(h["bias"])) for h in hits[: n.value]]
+    return (out, cells.value) if want_cells else out
+
+
+def genomic_sample(seed, L, nseq):
+    """nseq frames [255, L residues, 255] of the genomic HMM, back to back."""
+    out = np.zeros(nseq * (L + 2), np.uint8)
+    lib().oracle_genomic_sample(seed, L, nseq, out.ctypes.data)
+    return out
+
+
+def exp_fit(scores, exp_mode, n_seqs, L, gtailn=250, ltailn=750, tailp=0.0, dbsize=0.0):
+    """fit_histogram + set_exp_info; None where the reference errors."""
+    s = np.ascontiguousarray(scores, np.float32)
+    out = np.zeros(1, EXP_DTYPE)
+    rc = lib().oracle_exp_fit(s.ctypes.data, len(s), exp_mode, n_seqs, L, gtailn, ltailn, float(tailp),
+                              float(dbsize), out.ctypes.data)
+    return None if rc else out[0]

@@ -37,6 +37,11 @@
 enum { D_ST = 0, MP_ST, ML_ST, MR_ST, IL_ST, IR_ST, S_ST, E_ST, B_ST };
 #define BEGL_S 3
 
+/* cmcalibrate's copy of the scanner (src/cm_calibrate.rs:441-780) compares
+ * local begins by their bit scores (S::scbits(a) < S::scbits(cand)); the
+ * search scanner compares the raw values.  Set for oracle_calib_scan only. */
+static int g_calib_begins = 0;
+
 static int32_t g_ilog[LOGSUM_TBL];
 static float g_flog[LOGSUM_TBL];
 static int g_tables_ready = 0;
@@ -511,13 +516,15 @@ static void NAME(const cmgpu_cm *cm, const uint8_t *dsq, int32_t i0, int32_t j0,
                     int bi = begl_idx[y];                                                               \
                     for (int32_t d = dn; d <= dx; d++) {                                                \
                         T cand = ADDV(abegl[(jpy * nb + bi) * W1 + (size_t)d], BEGINSC[y]);             \
-                        if (a0row[d] < cand) a0row[d] = cand;                                           \
+                        if (g_calib_begins ? SCBITS(a0row[d]) < SCBITS(cand) : a0row[d] < cand)         \
+                            a0row[d] = cand;                                                            \
                         if (wc) wc->terms += 1;                                                         \
                     }                                                                                   \
                 } else {                                                                                \
                     for (int32_t d = dn; d <= dx; d++) {                                                \
                         T cand = ADDV(alpha[(cur * (size_t)M + y) * W1 + (size_t)d], BEGINSC[y]);       \
-                        if (a0row[d] < cand) a0row[d] = cand;                                           \
+                        if (g_calib_begins ? SCBITS(a0row[d]) < SCBITS(cand) : a0row[d] < cand)         \
+                            a0row[d] = cand;                                                            \
                         if (wc) wc->terms += 1;                                                         \
                     }                                                                                   \
                 }                                                                                       \
@@ -594,6 +601,17 @@ int oracle_qdb_scan(const cmgpu_cm *cm, int semiring, int qdbidx, const uint8_t 
     free(cv.j);
     free(cv.d);
     free(cv.sc);
+    return rc;
+}
+
+/* collect_scores's scan (src/cm_calibrate.rs:953-989): cutoff -inf and
+ * local begins compared in bits; the kept hits of the window. */
+int oracle_calib_scan(const cmgpu_cm *cm, int semiring, int qdbidx, const uint8_t *dsq, int32_t i0, int32_t j0,
+                      int do_null3, cmgpu_hit *hits, int32_t cap, int32_t *n_out, double *cells) {
+    g_calib_begins = 1;
+    int rc = oracle_qdb_scan(cm, semiring, qdbidx, dsq, i0, j0, -INFINITY, do_null3, hits, cap, n_out, NULL, NULL,
+                             NULL, 0, NULL, cells, NULL);
+    g_calib_begins = 0;
     return rc;
 }
 

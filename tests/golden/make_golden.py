@@ -6,6 +6,9 @@
   `ilogsum_table_endpoints_match_c_formula`; src/cm_qdband.rs
   `test_state_delta`).  Needs the reference checkout: set REFERENCE_ROOT to
   its path; run it only where that exists.
+* genomic_kat.json: the random genomic sequences of cmcalibrate's generator
+  for seed 181 that the reference's test `rng_sample_matches_c` pins against
+  C Infernal (src/cm_calibrate.rs:1253-1268).
 * scan_small.json: the oracle's hits on one fixed seeded model and sequence,
   a regression lock for the oracle itself.
 
@@ -50,6 +53,16 @@ def state_delta_kats():
     return {"source": "src/cm_qdband.rs:639-652", "state_delta": pairs}
 
 
+def genomic_kats():
+    src = open(os.path.join(REF, "src", "cm_calibrate.rs")).read()
+    body = src[src.index("fn rng_sample_matches_c"):]
+    body = body[: body.index("}\n")]
+    seed = int(re.search(r"EslRandom::new\((\d+)\)", body).group(1))
+    length = int(re.search(r"sample_genomic_sequence_from_hmm\(&mut r, &ghmm, (\d+)\)", body).group(1))
+    seqs = re.findall(r'assert_eq!\(d\d, "([0-3]+)"\)', body)
+    return {"source": "src/cm_calibrate.rs:1253-1268", "seed": seed, "L": length, "sequences": seqs}
+
+
 def scan_small():
     sys.path.insert(0, ROOT)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -75,6 +88,8 @@ def main():
             json.dump(ilogsum_kats(), f, indent=1)
         with open(os.path.join(HERE, "state_delta_kat.json"), "w") as f:
             json.dump(state_delta_kats(), f, indent=1)
+        with open(os.path.join(HERE, "genomic_kat.json"), "w") as f:
+            json.dump(genomic_kats(), f, indent=1)
     with open(os.path.join(HERE, "scan_small.json"), "w") as f:
         json.dump(scan_small(), f, indent=1)
 

@@ -62,3 +62,19 @@ def test_truncated_penalties_are_probabilities_in_log_space():
     assert (loc["pty"][:, fin] < 0).all()
     assert (glb["pty"][0][fin] > -1e30).all()
     assert loc["pty"][0][0] < -1e30 and glb["pty"][0][0] < -1e30
+
+
+@pytest.mark.parametrize("name", ["cfg0", "small2", "mb3", "cfg2"])
+def test_calibration_configurations_match_oracle(name):
+    """cmcalibrate's two configurations (both band sets at beta 1e-15 on the
+    global transitions, the model's W kept) against the oracle's builders."""
+    from infernox_b200 import calibrate as cal
+    cm, g, l = models(name)
+    ccfg = cal.CalibrateConfig()
+    for local, mine in zip((False, True), cal.calibration_configs(cm, g.W, ccfg)):
+        ref = oracle.prep_configure(cm, local, g.W, ccfg.beta, ccfg.beta)
+        bad = [k for k in CONFIG_FIELDS if not same_bits(getattr(mine, k), ref[k])]
+        assert not bad, bad
+        assert mine.W == ref["W"] == g.W
+        # the tighter beta widens every band
+        assert (mine.dmax2 >= g.dmax2).all() and (mine.dmin2 <= g.dmin2).all()

@@ -44,7 +44,7 @@ def test_vit_matches_oracle_on_reference_grid():
     assert n == 21 * 8 * len(LS)
 
 
-@pytest.mark.parametrize("m", [48, 256, 350, 1500])
+@pytest.mark.parametrize("m", [33, 48, 97, 150, 190, 256, 257, 350, 1500])
 def test_vit_long_windows_and_large_models(m):
     rng = Lcg(1000 + m)
     p = random_profile(rng, m)
