@@ -955,12 +955,16 @@ def serve_main(args):
     srv = serve.Server(cfgs, device=local_rank, budget_residues=args.serve_budget)
     # warm-up: every model's plans built and uploaded by a few short queries
     warm = serve_requests(cms, max(1, args.warmup), 1e6, seed=79)
+    t_warm = time.perf_counter()
     for r in warm:
         r.seq = r.seq[:300]
         srv.submit(r)
     while not srv.idle():
         srv.step()
     srv.finished.clear()
+    print(f"serve: library of {len(cfgs)} built in {t_build:.1f} s, warm-up pass {time.perf_counter() - t_warm:.1f} s "
+          f"(kernel {srv.kernel_ms / 1e3:.1f} s)", file=sys.stderr, flush=True)
+    srv.kernel_ms = 0.0
     cells = [0.0]
 
     def step_counted():
@@ -984,6 +988,10 @@ def serve_main(args):
             continue
         srv.step()
         steps += 1
+        if steps % 50 == 0:
+            print(f"serve: {srv.clock():.1f} s, {steps} model steps, {len(srv.active)} active, "
+                  f"{len(srv.queue)} queued, {len(srv.finished)} done, kernel {srv.kernel_ms / 1e3:.1f} s",
+                  file=sys.stderr, flush=True)
     torch.cuda.synchronize()
     wall = srv.clock()
     done = [r for r in srv.finished if r.status == serve.OK]
@@ -1013,7 +1021,7 @@ def serve_main(args):
             "latency_s": {"p50": statistics.median(lat), "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
                           "max": lat[-1]},
             "residues_per_s": config["residues"] / span,
-            "gpu_launches": srv.launches, "model_steps": srv.model_steps,
+            "gpu_launches": srv.launches, "model_steps": srv.model_steps, "kernel_s": srv.kernel_ms / 1e3,
             "plain_gpu": plain, "served_over_plain_residue_rate":
                 (config["residues"] / span) / (plain["residues"] / plain_dt),
             "identity_checked_requests": min(len(done), args.serve_check)}

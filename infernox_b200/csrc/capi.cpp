@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -20,6 +21,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/cmscan_gpu.h"
@@ -649,37 +651,86 @@ static int run_scan(cmgpu_model *m, cmgpu_workspace *ws, int semiring, int qdbid
                                  ws->stream));
     CUDA_TRY(cudaStreamSynchronize(ws->stream));
 
-    // map items to windows, order by (window, j, d)
-    std::vector<Cand> cs(ws->h_cands, ws->h_cands + ncand);
-    for (auto &c : cs) c.item = items[c.item].win;
-    std::sort(cs.begin(), cs.end(), [](const Cand &a, const Cand &b) {
-        if (a.item != b.item) return a.item < b.item;
-        if (a.j != b.j) return a.j < b.j;
-        return a.d < b.d;
-    });
+    // Order the cells by (window, j, d) in O(n): items ranked window by
+    // window in column order, then a stable counting sort by item rank.  A
+    // lane scans its item's columns in order, so an item's cells usually
+    // arrive already in (j, d) order; a range that does not is sorted.
+    std::vector<int32_t> rank(items.size());
+    {
+        std::vector<int32_t> ord(items.size());
+        for (size_t x = 0; x < items.size(); x++) ord[x] = (int32_t)x;
+        std::sort(ord.begin(), ord.end(), [&](int32_t a, int32_t b) {
+            if (items[a].win != items[b].win) return items[a].win < items[b].win;
+            return items[a].jreport < items[b].jreport;
+        });
+        for (size_t r = 0; r < ord.size(); r++) rank[ord[r]] = (int32_t)r;
+    }
+    std::vector<size_t> start(items.size() + 1, 0);
+    for (size_t c = 0; c < ncand; c++) start[rank[ws->h_cands[c].item] + 1]++;
+    for (size_t r = 0; r < items.size(); r++) start[r + 1] += start[r];
+    std::vector<Cand> cs(ncand);
+    {
+        std::vector<size_t> pos(start.begin(), start.end() - 1);
+        for (size_t c = 0; c < ncand; c++) {
+            Cand x = ws->h_cands[c];
+            const int32_t r = rank[x.item];
+            x.item = items[x.item].win;
+            cs[pos[r]++] = x;
+        }
+    }
+    auto jd_less = [](const Cand &a, const Cand &b) { return a.j != b.j ? a.j < b.j : a.d < b.d; };
+    for (size_t r = 0; r < items.size(); r++)
+        if (!std::is_sorted(cs.begin() + start[r], cs.begin() + start[r + 1], jd_less))
+            std::sort(cs.begin() + start[r], cs.begin() + start[r + 1], jd_less);
     if (cells_out) {
         *cells_out = cs;
         return CMGPU_OK;
     }
-    std::vector<uint8_t> frame_buf;
-    size_t k = 0;
-    while (k < cs.size()) {
+    // windows' ranges, and their frames on the host for null3
+    struct Range {
+        size_t b, e;
+        int32_t win;
+        const uint8_t *frame;
+    };
+    std::vector<Range> ranges;
+    for (size_t k = 0; k < cs.size();) {
         size_t e = k;
         while (e < cs.size() && cs[e].item == cs[k].item) e++;
-        const WinDesc &w = wins[cs[k].item];
-        const uint8_t *frame = nullptr;
-        if (do_null3) {
+        ranges.push_back(Range{k, e, cs[k].item, nullptr});
+        k = e;
+    }
+    std::vector<std::vector<uint8_t>> frame_bufs;
+    if (do_null3) {
+        if (!h_dsq) frame_bufs.resize(ranges.size());
+        for (size_t r = 0; r < ranges.size(); r++) {
+            const WinDesc &w = wins[ranges[r].win];
             if (h_dsq) {
-                frame = h_dsq + w.off;
+                ranges[r].frame = h_dsq + w.off;
             } else {
-                frame_buf.resize((size_t)w.j0 + 2);
-                CUDA_TRY(cudaMemcpy(frame_buf.data(), d_dsq + w.off, (size_t)w.j0 + 1, cudaMemcpyDeviceToHost));
-                frame = frame_buf.data();
+                frame_bufs[r].resize((size_t)w.j0 + 2);
+                CUDA_TRY(cudaMemcpy(frame_bufs[r].data(), d_dsq + w.off, (size_t)w.j0 + 1, cudaMemcpyDeviceToHost));
+                ranges[r].frame = frame_bufs[r].data();
             }
         }
-        report_window(m, semiring, cs.data() + k, e - k, frame, w.i0, cutoff, do_null3,
-                      hits_per_win[cs[k].item]);
-        k = e;
+    }
+    // report_hits_greedily + overlap removal per window: windows are
+    // independent, so they are replayed on the host's cores
+    auto replay = [&](size_t r) {
+        const Range &g = ranges[r];
+        report_window(m, semiring, cs.data() + g.b, g.e - g.b, g.frame, wins[g.win].i0, cutoff, do_null3,
+                      hits_per_win[g.win]);
+    };
+    const size_t nthr = std::min<size_t>(ranges.size(), std::max(1u, std::thread::hardware_concurrency()));
+    if (nthr <= 1 || cs.size() < (1u << 16)) {
+        for (size_t r = 0; r < ranges.size(); r++) replay(r);
+    } else {
+        std::atomic<size_t> next{0};
+        std::vector<std::thread> pool;
+        for (size_t t = 0; t < nthr; t++)
+            pool.emplace_back([&]() {
+                for (size_t r; (r = next.fetch_add(1)) < ranges.size();) replay(r);
+            });
+        for (auto &th : pool) th.join();
     }
     (void)dsq_len;
     return CMGPU_OK;
@@ -743,7 +794,9 @@ int cmgpu_model_upload(const cmgpu_cm *cm, int device, cmgpu_model **out) {
     int nz = 0;
     for (int i = 0; i < LOGSUM_TBL; i++)
         if (t[i] != 0) nz = i + 1;
-    std::vector<uint16_t> t16(nz);
+    // entries 0..nz-1, then zeros: the kernels index tbl[nz] (= 0) for the
+    // ILogsum cases that add nothing and copy whole 32-bit words
+    std::vector<uint16_t> t16(nz + 2, 0);
     for (int i = 0; i < nz; i++) t16[i] = (uint16_t)t[i];
     m->ilog_nz = nz;
     int rc = upload_vec(&m->ilog, t16);

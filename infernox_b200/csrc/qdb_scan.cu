@@ -92,6 +92,9 @@ struct K {
     Smem s;
     int nz;
     int rmask;
+    // scalars the per-cell code reads, held in registers
+    const uint32_t *esc_g;  // full emission rows [M][324] (IUPAC codes)
+    int fuse_begin, begin_key, root_dn, root_dxcap, W1;
 };
 
 // Emission score of a single residue / a pair; canonical residues come from
@@ -99,12 +102,12 @@ struct K {
 template <class S>
 __device__ __forceinline__ typename S::T esc1(const K &k, int v, int escoff, int c) {
     if (c < 4) return S::ld(k.s.escc + escoff + c);
-    return S::ldg(k.p->esc + v * 324 + c);
+    return S::ldg(k.esc_g + v * 324 + c);
 }
 template <class S>
 __device__ __forceinline__ typename S::T esc2(const K &k, int v, int escoff, int a, int b) {
     if ((a | b) < 4) return S::ld(k.s.escc + escoff + a * 4 + b);
-    return S::ldg(k.p->esc + v * 324 + a * 18 + b);
+    return S::ldg(k.esc_g + v * 324 + a * 18 + b);
 }
 
 // Child terms of cell d: deck[cb[v][yo][par] + d] + tsc[v][yo].  The padded
@@ -127,23 +130,24 @@ __device__ __forceinline__ typename S::T init_sc(const K &k, const SInfo &sv, in
 
 __device__ __forceinline__ int resid(const Lane &L, int x, int rmask) { return L.ring[x & rmask]; }
 
-// Value of cell d of an ordinary state (not B, not IL), before the store.
-template <class S>
+// Value of cell d of an ordinary state (not B, not IL) with CN children,
+// before the store.  CN is a compile-time constant, so the child loop and the
+// reduce_c_order switch unroll to exactly the state's children.
+template <class S, int CN>
 __device__ __forceinline__ typename S::T cell_value(const K &k, const Lane &L, int v, const SInfo &sv, int d) {
     typedef typename S::T T;
     const int t = sv.type;
     T terms[6];
-    child_terms<S>(k, v, sv.cnum, L.deck, L.par, d, terms, 0);
+    child_terms<S>(k, v, CN, L.deck, L.par, d, terms, 0);
     const int idx = d - sv.sd;
     T sc;
     if (sv.flags & SF_BEGL) {
         // BEGL_S folds its children in natural order (src/cm_nohmm.rs:601-611)
         sc = init_sc<S>(k, sv, v, idx);
 #pragma unroll
-        for (int yo = 0; yo < 6; yo++)
-            if (yo < sv.cnum) sc = S::comb(sc, terms[yo], k.s.tbl, k.nz);
+        for (int yo = 0; yo < CN; yo++) sc = S::comb(sc, terms[yo], k.s.tbl, k.nz);
     } else {
-        sc = reduce_c<S>(sv.cnum, terms, init_sc<S>(k, sv, v, idx), k.s.tbl, k.nz);
+        sc = reduce_c<S>(CN, terms, init_sc<S>(k, sv, v, idx), k.s.tbl, k.nz);
     }
     if (t == 2 || t == 4) {  // ML, IL: residue i = j-d+1
         sc = S::add(sc, esc1<S>(k, v, sv.escoff, resid(L, L.j - d + 1, k.rmask)));
@@ -174,10 +178,9 @@ __device__ __forceinline__ bool begin_less(int key, typename S::T a, typename S:
 template <class S>
 __device__ __forceinline__ void post_begin(const K &k, const Lane &L, const SInfo &sv, int v, int d,
                                            typename S::T x) {
-    if (S::ORDERED && k.p->fuse_begin && (sv.flags & SF_BEGIN) && d >= k.p->root_dn &&
-        d <= min(L.jrow, k.p->root_dxcap)) {
+    if (S::ORDERED && k.fuse_begin && (sv.flags & SF_BEGIN) && d >= k.root_dn && d <= min(L.jrow, k.root_dxcap)) {
         int32_t c = (int32_t)((uint32_t)S::u(x) + k.s.bsv[v]);
-        if (k.p->begin_key && c == -INFTY_D) c = INT32_MIN;
+        if (k.begin_key && c == -INFTY_D) c = INT32_MIN;
         atomicMax(k.s.bmax + L.l * k.s.bstride + d, c);
     }
 }
@@ -185,20 +188,33 @@ __device__ __forceinline__ void post_begin(const K &k, const Lane &L, const SInf
 // One warp-wide chunk of an ordinary state (not B, not IL): 64 cells, two per
 // lane (d0+lane and d0+32+lane).  Both values are computed before either is
 // stored, so the two dependency chains overlap.
-template <class S>
-__device__ __forceinline__ void do_chunk(const K &k, const Lane &L, int v, const SInfo &sv, int d0, int lane) {
+template <class S, int CN>
+__device__ __forceinline__ void do_chunk_c(const K &k, const Lane &L, int v, const SInfo &sv, int d0, int lane) {
     typedef typename S::T T;
     const int dx = min(L.jrow, sv.dxcap);
     const int da = d0 + lane, db = da + 32;
     if (da > dx) return;
     const bool has_b = db <= dx;
-    T va = cell_value<S>(k, L, v, sv, da);
-    T vb = has_b ? cell_value<S>(k, L, v, sv, db) : va;
+    T va = cell_value<S, CN>(k, L, v, sv, da);
+    T vb = has_b ? cell_value<S, CN>(k, L, v, sv, db) : va;
     const int wbase = (sv.flags & SF_BEGL) ? k.s.wb[v * 2] + L.jm * sv.span : k.s.wb[v * 2 + L.par];
     S::st(L.deck + wbase + da, va);
     if (has_b) S::st(L.deck + wbase + db, vb);
     post_begin<S>(k, L, sv, v, da, va);
     if (has_b) post_begin<S>(k, L, sv, v, db, vb);
+}
+
+// cnum is 1..6 for every non-B, non-E state of a CM
+template <class S>
+__device__ __forceinline__ void do_chunk(const K &k, const Lane &L, int v, const SInfo &sv, int d0, int lane) {
+    switch (sv.cnum) {
+    case 1: do_chunk_c<S, 1>(k, L, v, sv, d0, lane); break;
+    case 2: do_chunk_c<S, 2>(k, L, v, sv, d0, lane); break;
+    case 3: do_chunk_c<S, 3>(k, L, v, sv, d0, lane); break;
+    case 4: do_chunk_c<S, 4>(k, L, v, sv, d0, lane); break;
+    case 5: do_chunk_c<S, 5>(k, L, v, sv, d0, lane); break;
+    default: do_chunk_c<S, 6>(k, L, v, sv, d0, lane); break;
+    }
 }
 
 // Bifurcation cell: alpha[v][d] = init (+) over k ascending of
@@ -211,7 +227,7 @@ __device__ __forceinline__ typename S::T bif_value(const K &k, const Lane &L, in
     const int kmin = max(0, max(kdn_y, d - kdx_w));
     const int kmax = min(kdx_y, d - kdn_w);
     T sc = init_sc<S>(k, sv, v, d);
-    const int W1 = k.p->W + 1;
+    const int W1 = k.W1;
     int col = L.jm - kmin;
     if (col < 0) col += W1;
     const uint32_t *left = L.deck + begl + d;
@@ -461,7 +477,9 @@ __device__ void prefilter_row(const K &k, int l, int step, int wl) {
     }
 }
 
-template <bool INS, bool DECK_SMEM>
+// TG: the per-state tables stay in global memory (large models); otherwise
+// they are copied to shared memory, and the compiler sees shared addresses.
+template <bool INS, bool DECK_SMEM, bool TG>
 __global__ void __launch_bounds__(512, 1) qdb_scan_kernel(ScanParams p) {
     typedef Sem<INS> S;
     typedef typename S::T T;
@@ -472,9 +490,15 @@ __global__ void __launch_bounds__(512, 1) qdb_scan_kernel(ScanParams p) {
     K k;
     k.p = &p;
     k.nz = p.ilog_nz;
+    k.esc_g = p.esc;
+    k.fuse_begin = p.fuse_begin;
+    k.begin_key = p.begin_key;
+    k.root_dn = p.root_dn;
+    k.root_dxcap = p.root_dxcap;
+    k.W1 = p.W + 1;
     k.s.el = smem + ly.el;
     k.s.tbl = reinterpret_cast<const uint16_t *>(smem + ly.tbl);
-    if (p.tables_global) {
+    if (TG) {
         // large models: the per-state tables are read from global memory
         // (read-only, cached in L1) instead of being copied to shared memory
         k.s.info = reinterpret_cast<const int4 *>(p.states);
@@ -520,8 +544,8 @@ __global__ void __launch_bounds__(512, 1) qdb_scan_kernel(ScanParams p) {
             for (int x = tid; x < n; x += bs) smem[dst + x] = __ldg(g + x);
         };
         copy32(ly.el, p.el_sca, p.W + 1);
-        if (INS) copy32(ly.tbl, p.ilog, (p.ilog_nz + 1) / 2);
-        if (!p.tables_global) {
+        if (INS) copy32(ly.tbl, p.ilog, (p.ilog_nz + 2) / 2);  // entries 0..nz, tbl[nz] = 0
+        if (!TG) {
             copy32(ly.info, p.states, p.M * 4);
             copy32(ly.wb, p.wb, p.M * 2);
             copy32(ly.cb, p.cb, p.M * 12);
@@ -725,9 +749,9 @@ __global__ void __launch_bounds__(512, 1) qdb_scan_kernel(ScanParams p) {
     }
 }
 
-template <bool INS, bool DS>
+template <bool INS, bool DS, bool TG>
 static cudaError_t launch_t(const ScanParams &p, int ctas, int threads, cudaStream_t s) {
-    auto kern = qdb_scan_kernel<INS, DS>;
+    auto kern = qdb_scan_kernel<INS, DS, TG>;
     size_t smem = (size_t)p.lay.words * 4;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -735,10 +759,10 @@ static cudaError_t launch_t(const ScanParams &p, int ctas, int threads, cudaStre
     return cudaGetLastError();
 }
 
-template <bool INS, bool DS>
+template <bool INS, bool DS, bool TG>
 static int occupancy_t(const ScanParams &p, int threads) {
     int n = 0;
-    auto kern = qdb_scan_kernel<INS, DS>;
+    auto kern = qdb_scan_kernel<INS, DS, TG>;
     size_t smem = (size_t)p.lay.words * 4;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, threads, smem) != cudaSuccess) return 0;
@@ -756,7 +780,7 @@ SmemLayout scan_layout(const ScanParams &p, int lanes, bool deck_smem) {
         return (int)o;
     };
     L.el = take(p.W + 1);
-    L.tbl = take(p.inside ? (p.ilog_nz + 1) / 2 : 0);
+    L.tbl = take(p.inside ? (p.ilog_nz + 2) / 2 : 0);
     const int64_t g = p.tables_global ? 0 : 1;  // per-state tables in shared memory?
     L.info = take(g * p.M * 4);
     L.wb = take(g * p.M * 2);
@@ -782,17 +806,31 @@ SmemLayout scan_layout(const ScanParams &p, int lanes, bool deck_smem) {
 }
 
 int scan_occupancy(const ScanParams &p, int threads) {
-    if (p.inside)
-        return p.deck_smem ? dev::occupancy_t<true, true>(p, threads) : dev::occupancy_t<true, false>(p, threads);
-    return p.deck_smem ? dev::occupancy_t<false, true>(p, threads) : dev::occupancy_t<false, false>(p, threads);
+    const int sel = (p.inside ? 4 : 0) | (p.deck_smem ? 2 : 0) | (p.tables_global ? 1 : 0);
+    switch (sel) {
+    case 0: return dev::occupancy_t<false, false, false>(p, threads);
+    case 1: return dev::occupancy_t<false, false, true>(p, threads);
+    case 2: return dev::occupancy_t<false, true, false>(p, threads);
+    case 3: return dev::occupancy_t<false, true, true>(p, threads);
+    case 4: return dev::occupancy_t<true, false, false>(p, threads);
+    case 5: return dev::occupancy_t<true, false, true>(p, threads);
+    case 6: return dev::occupancy_t<true, true, false>(p, threads);
+    default: return dev::occupancy_t<true, true, true>(p, threads);
+    }
 }
 
 cudaError_t scan_launch(const ScanParams &p, int ctas, int threads, cudaStream_t s) {
-    if (p.inside)
-        return p.deck_smem ? dev::launch_t<true, true>(p, ctas, threads, s)
-                           : dev::launch_t<true, false>(p, ctas, threads, s);
-    return p.deck_smem ? dev::launch_t<false, true>(p, ctas, threads, s)
-                       : dev::launch_t<false, false>(p, ctas, threads, s);
+    const int sel = (p.inside ? 4 : 0) | (p.deck_smem ? 2 : 0) | (p.tables_global ? 1 : 0);
+    switch (sel) {
+    case 0: return dev::launch_t<false, false, false>(p, ctas, threads, s);
+    case 1: return dev::launch_t<false, false, true>(p, ctas, threads, s);
+    case 2: return dev::launch_t<false, true, false>(p, ctas, threads, s);
+    case 3: return dev::launch_t<false, true, true>(p, ctas, threads, s);
+    case 4: return dev::launch_t<true, false, false>(p, ctas, threads, s);
+    case 5: return dev::launch_t<true, false, true>(p, ctas, threads, s);
+    case 6: return dev::launch_t<true, true, false>(p, ctas, threads, s);
+    default: return dev::launch_t<true, true, true>(p, ctas, threads, s);
+    }
 }
 
 }  // namespace cmx

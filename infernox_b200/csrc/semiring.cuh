@@ -38,16 +38,17 @@ struct Sem<true> {  // Inside: i32 wrapping adds, ILogsum
     static constexpr bool ORDERED = true;
     __device__ static __forceinline__ T zero() { return -INFTY_D; }
     __device__ static __forceinline__ T add(T a, T b) { return (int32_t)((uint32_t)a + (uint32_t)b); }
-    // ILogsum (src/cp9.rs:65-75): max + tbl[max-min]; the table is stored up
-    // to its last nonzero entry (nz), beyond which it adds 0 like the rule
-    // (max-min) >= LOGSUM_TBL does.
+    // ILogsum (src/cp9.rs:65-75): max + tbl[max-min], written without
+    // branches.  The table is stored up to its last nonzero entry plus one
+    // zero entry, tbl[nz] = 0; the two cases where the rule adds nothing --
+    // min at or below -INFTY, and max-min >= LOGSUM_TBL (beyond nz the table
+    // is 0 anyway) -- index that zero entry.
     __device__ static __forceinline__ T comb(T a, T b, const uint16_t *tbl, int nz) {
-        int32_t mx = a > b ? a : b;
-        if (mx < -INFTY_D) mx = -INFTY_D;
-        int32_t mn = a < b ? a : b;
-        uint32_t diff = (uint32_t)mx - (uint32_t)mn;
-        if (mn <= -INFTY_D || diff >= (uint32_t)nz) return mx;
-        return (int32_t)((uint32_t)mx + (uint32_t)tbl[diff]);
+        const int32_t mx = max(max(a, b), -INFTY_D);
+        const int32_t mn = min(a, b);
+        const uint32_t diff = (uint32_t)mx - (uint32_t)mn;
+        const uint32_t idx = mn <= -INFTY_D ? (uint32_t)nz : min(diff, (uint32_t)nz);
+        return (int32_t)((uint32_t)mx + (uint32_t)tbl[idx]);
     }
     __device__ static __forceinline__ T ld(const uint32_t *p) { return (int32_t)*p; }
     __device__ static __forceinline__ T ldg(const uint32_t *p) { return (int32_t)__ldg(p); }

@@ -97,6 +97,7 @@ class Server:
         self.t0 = time.perf_counter()
         self.launches = 0
         self.model_steps = 0
+        self.kernel_ms = 0.0  # device time of the scans
 
     def clock(self) -> float:
         return time.perf_counter() - self.t0
@@ -176,6 +177,7 @@ class Server:
         # F6: QDB1 CYK over every window, one launch
         cyk = sc.scan_batch(CYK_F32, QDB1, buf, W, self.f6_cutoff, self.do_null3)
         self.launches += 1
+        self.kernel_ms += sc.stats()["kernel_ms"]
         envw, env_owner = [], []
         for w, (r, strand, n, o) in enumerate(owners):
             h = cyk[cyk["win"] == w]
@@ -188,6 +190,7 @@ class Server:
             E = np.array(envw, dtype=N.WINDOW_DTYPE)
             fin = sc.scan_batch(INSIDE_I32, QDB2, buf, E, self.final_cutoff, self.do_null3)
             self.launches += 1
+            self.kernel_ms += sc.stats()["kernel_ms"]
             for x in fin:
                 per_window[env_owner[int(x["win"])]].append(
                     (int(x["i"]), int(x["j"]), float(x["score"]), float(x["bias"])))
