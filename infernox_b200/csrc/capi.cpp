@@ -515,9 +515,20 @@ static int run_scan(cmgpu_model *m, cmgpu_workspace *ws, int semiring, int qdbid
     int64_t total_cols = 0;
     for (auto &w : wins) total_cols += std::max<int64_t>(0, (int64_t)w.j0 - w.i0 + 1);
     const int W = pl.W;
+    // Small batches -- too few columns to give every lane slot one piece of
+    // 2W -- are latency bound: a lane scans its item's columns one after
+    // another, and a CTA's time per column grows with its lanes.  Such a
+    // batch is cut into about one piece per CTA, and each CTA takes only the
+    // few lanes the pieces need (below).
+    const bool small_batch = !sweep && !deck_smem && !plain && ws->chunk <= 0 && ws->lanes <= 0 &&
+                             total_cols < (int64_t)max_ctas * best_l * 2 * W;
     auto chunk_for = [&](int64_t cols) -> int64_t {
         int64_t chunk = ws->chunk;
-        if (chunk <= 0) {
+        if (chunk <= 0 && small_batch) {
+            chunk = (cols + max_ctas - 1) / max_ctas;
+            chunk = std::max<int64_t>(chunk, 2 * (int64_t)W);
+            chunk = std::min<int64_t>(chunk, 32768);
+        } else if (chunk <= 0) {
             // about four items per lane slot, but no piece shorter than 2W (the
             // W-1 warm-up columns are overhead) and none longer than 32768
             chunk = cols / std::max<int64_t>(1, (int64_t)max_ctas * best_l * 4);
@@ -565,6 +576,15 @@ static int run_scan(cmgpu_model *m, cmgpu_workspace *ws, int semiring, int qdbid
         sp.lanes = best_l;
         sp.lay = scan_layout(sp, best_l, false);
         ws->stats.lanes = best_l;
+    } else if (small_batch) {
+        // a small batch: spread its pieces over every SM, a few lanes each
+        const int l = (int)std::min<int64_t>(best_l, ((int64_t)items.size() + max_ctas - 1) / max_ctas);
+        if (l < best_l) {
+            best_l = std::max(1, l);
+            sp.lanes = best_l;
+            sp.lay = scan_layout(sp, best_l, false);
+            ws->stats.lanes = best_l;
+        }
     }
     int ctas = (int)std::min<int64_t>(((int64_t)items.size() + best_l - 1) / best_l, max_ctas);
     if (!sweep && !deck_smem) {
