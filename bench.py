@@ -14,7 +14,8 @@ cores beside it.
 Workload (default "batched-uneven-max"): the batched uneven-window Inside scan
 of the --max path.  One 120-consensus-column CM with 3 bifurcations (seeded
 synthetic, local configuration), sequences with log-normal lengths clipped to
-[200, 20000] nt (median 1.5 kb, i.i.d. 45% GC), both strands, every window
+[200, 20000] nt (median 1.5 kb, i.i.d. 45% GC, a tenth of them carrying one
+homolog sampled from the model), both strands, every window
 scanned with the non-banded integer Inside scanner (final_stage_inside_opt
 with nonbanded=true).  A step is one pass over a batch of --batch sequences
 (both strands) drawn from that distribution; each rank scans its own batch
@@ -83,20 +84,30 @@ def aggregate_ranks(dist, total_ms, e2e_ms, cells, device="cuda"):
     return tmax[0].item(), tmax[1].item(), tsum[2].item()
 
 
-def make_model(w):
-    from infernox_b200 import model, synth
+PLANT_FRACTION = 0.1  # sequences that carry one homolog sampled from the model
+
+
+def make_cm(w):
+    from infernox_b200 import synth
     if w["paired"] is None:
         ss = synth.trna_like()
     else:
         ss = synth.structure(w["clen"], w["paired"], w["nbif"], w["sseed"])
-    cm = synth.synth_cm(ss, w["pseed"], name="bench")
-    return model.configure(cm, local=True)
+    return synth.synth_cm(ss, w["pseed"], name="bench")
+
+
+def make_model(w):
+    from infernox_b200 import model
+    return model.configure(make_cm(w), local=True)
 
 
 def make_batch(w, nseq, seed):
-    """Concatenated window frames for nseq sequences, top and bottom strand."""
+    """Concatenated window frames for nseq sequences, top and bottom strand;
+    PLANT_FRACTION of them carry one homolog sampled from the model at a
+    random place (lengths, and so cells, are unchanged)."""
     from infernox_b200 import synth
     rng = np.random.default_rng(seed)
+    cm = make_cm(w)
     if w["sigma"] > 0:
         lens = np.clip(rng.lognormal(np.log(w["median"]), w["sigma"], nseq), w["lo"], w["hi"]).astype(int)
     else:
@@ -104,6 +115,11 @@ def make_batch(w, nseq, seed):
     frames, wins, off = [], [], 0
     for L in lens:
         top = synth.random_dsq(int(L), w["gc"], rng)
+        if rng.random() < PLANT_FRACTION:
+            h = synth.emit(cm, rng)
+            if 0 < len(h) < L:
+                p = int(rng.integers(0, int(L) - len(h) + 1))
+                top[p:p + len(h)] = h
         for s in (top, synth.revcomp(top)):
             f = np.concatenate([[255], s, [255]]).astype(np.uint8)
             frames.append(f)
@@ -328,6 +344,7 @@ def main():
               "sequences_per_step_job": int(args.batch * world), "cutoff_bits": CUTOFF_BITS,
               "lengths": f"log-normal median {w['median']} sigma {w['sigma']} clipped to [{w['lo']}, {w['hi']}], "
                          f"both strands",
+              "homologs": f"{PLANT_FRACTION:.0%} of the sequences carry one homolog sampled from the model",
               "parallelism": f"dp{world}: cost-balanced window split, hits gathered to rank 0",
               "l2": "flushed (256 MB write) before each timed step"}
 

@@ -344,7 +344,9 @@ int cmgpu_calibrate_scan_batch(const cmgpu_model *m, cmgpu_workspace *ws, int se
 /* calibrate_cm (src/cm_calibrate.rs:1102-1182): a probability-level CM with
  * window length W; the global and local configurations with both band sets
  * at cfg->beta, the random sequences, one batched scan per mode on `device`
- * and the four fits. */
+ * and the four fits.  The modes run on two host threads with a workspace
+ * each, so one mode's host work overlaps another's scan; kernel_ms is the
+ * sum of the four scans' device times. */
 int cmgpu_calibrate(const cmgpu_cm_params *p, int32_t W, int device, const cmgpu_calibrate_config *cfg,
                     cmgpu_calibrate_result *out);
 

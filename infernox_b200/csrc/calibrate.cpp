@@ -14,9 +14,11 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/cmscan_gpu.h"
@@ -297,39 +299,69 @@ int cmgpu_calibrate(const cmgpu_cm_params *p, int32_t W, int device, const cmgpu
     if ((rc = g.build(p, 0, W, cfg->beta, cfg->nonbanded))) return rc;
     if ((rc = l.build(p, 1, W, cfg->beta, cfg->nonbanded))) return rc;
     cmgpu_model *gm = nullptr, *lm = nullptr;
-    cmgpu_workspace *ws = nullptr;
+    cmgpu_workspace *ws[2] = {nullptr, nullptr};
     auto done = [&](int code) {
-        cmgpu_workspace_free(ws);
+        cmgpu_workspace_free(ws[0]);
+        cmgpu_workspace_free(ws[1]);
         cmgpu_model_free(gm);
         cmgpu_model_free(lm);
         return code;
     };
     if ((rc = cmgpu_model_upload(&g.view, device, &gm))) return done(rc);
     if ((rc = cmgpu_model_upload(&l.view, device, &lm))) return done(rc);
-    if ((rc = cmgpu_workspace_create(device, nullptr, &ws))) return done(rc);
-    // kept hits of a window are disjoint, so a window holds at most CHUNK
-    std::vector<cmgpu_batch_hit> hits((size_t)nseq * CHUNK);
-    std::vector<float> scores;
+    for (int w = 0; w < 2; w++)
+        if ((rc = cmgpu_workspace_create(device, nullptr, &ws[w]))) return done(rc);
+    // The four modes run on two host threads, each with its own workspace and
+    // stream, taking modes from a shared counter (slowest first): one mode's
+    // host work -- ordering the reportable cells, the greedy report with
+    // null3, overlap removal, the fit -- overlaps another mode's scan.
+    static const int ORDER[4] = {EXP_GI, EXP_LI, EXP_GC, EXP_LC};
+    std::atomic<int> next{0};
+    int rcs[2] = {CMGPU_OK, CMGPU_OK};
+    std::string errs[2];
+    cmgpu_stats stats[4] = {};
+    auto worker = [&](int w) {
+        // kept hits of a window are disjoint, so a window holds at most CHUNK
+        std::vector<cmgpu_batch_hit> hits((size_t)nseq * CHUNK);
+        std::vector<float> scores;
+        cudaSetDevice(device);
+        for (int q; (q = next.fetch_add(1)) < 4;) {
+            const int mode = ORDER[q];
+            const bool local = mode == EXP_LC || mode == EXP_LI;
+            const int semiring = (mode == EXP_GI || mode == EXP_LI) ? CMGPU_INSIDE_I32 : CMGPU_CYK_F32;
+            int32_t nh = 0;
+            int r = cmgpu_calibrate_scan_batch(local ? lm : gm, ws[w], semiring, CMGPU_QDB2, frames.data(),
+                                               (int64_t)frames.size(), wins.data(), nseq, cfg->do_null3, hits.data(),
+                                               (int32_t)hits.size(), &nh);
+            if (!r) {
+                cmgpu_workspace_stats(ws[w], &stats[mode]);
+                scores.resize((size_t)nh);
+                for (int32_t k = 0; k < nh; k++) scores[k] = hits[k].score;
+                out->nhits[mode] = nh;
+                r = cmgpu_exp_fit(scores.data(), nh, mode, nseq, CHUNK, cfg->gtailn, cfg->ltailn, cfg->tailp,
+                                  dbsize, &out->exp[mode]);
+            }
+            if (r) {
+                rcs[w] = r;
+                errs[w] = cmgpu_last_error();
+                next.store(4);
+                return;
+            }
+        }
+    };
+    std::thread other(worker, 1);
+    worker(0);
+    other.join();
+    for (int w = 0; w < 2; w++)
+        if (rcs[w]) {
+            set_error(errs[w]);
+            return done(rcs[w]);
+        }
     for (int mode = 0; mode < 4; mode++) {
-        const bool local = mode == EXP_LC || mode == EXP_LI;
-        const int semiring = (mode == EXP_GI || mode == EXP_LI) ? CMGPU_INSIDE_I32 : CMGPU_CYK_F32;
-        cmgpu_model *m = local ? lm : gm;
-        int32_t nh = 0;
-        rc = cmgpu_calibrate_scan_batch(m, ws, semiring, CMGPU_QDB2, frames.data(), (int64_t)frames.size(),
-                                        wins.data(), nseq, cfg->do_null3, hits.data(), (int32_t)hits.size(), &nh);
-        if (rc) return done(rc);
-        cmgpu_stats st{};
-        cmgpu_workspace_stats(ws, &st);
-        out->cells += st.cells;
-        out->terms += st.terms;
-        out->kernel_ms += st.kernel_ms;
-        out->launches += st.kernel_launches;
-        scores.resize((size_t)nh);
-        for (int32_t k = 0; k < nh; k++) scores[k] = hits[k].score;
-        out->nhits[mode] = nh;
-        rc = cmgpu_exp_fit(scores.data(), nh, mode, nseq, CHUNK, cfg->gtailn, cfg->ltailn, cfg->tailp, dbsize,
-                           &out->exp[mode]);
-        if (rc) return done(rc);
+        out->cells += stats[mode].cells;
+        out->terms += stats[mode].terms;
+        out->kernel_ms += stats[mode].kernel_ms;
+        out->launches += stats[mode].kernel_launches;
     }
     return done(CMGPU_OK);
 }

@@ -168,6 +168,7 @@ struct cmgpu_msv_filter {
     mutable int64_t last_cells = 0;
     mutable int32_t last_launches = 0;
     mutable cmx::DevArena arena;  // per-call buffers, reused
+    mutable cmx::PinnedBuf raw_pin;  // per-call host copy of the chunks' windows
     mutable int cap_hint = 64;    // candidate slots per segment the last scan needed
     ~cmgpu_msv_filter() {
         arena.release();
@@ -709,11 +710,28 @@ int ssv_run(const cmgpu_msv_filter *f, cudaStream_t st, const uint8_t *dsq_all, 
             f->cap_hint = cap;
             continue;
         }
-        std::vector<dev::SsvRaw> hr((size_t)nseg * cap);
-        MSV_TRY(cudaMemcpyAsync(hr.data(), d_raws, sizeof(dev::SsvRaw) * hr.size(), cudaMemcpyDeviceToHost, st));
+        // only each chunk's windows come back (they sit at the chunk's first
+        // segment slot), into pinned memory
+        size_t nall = 0;
+        std::vector<size_t> at(nch);
+        for (int32_t c = 0; c < nch; c++) {
+            at[c] = nall;
+            nall += (size_t)std::max(0, nraw[c]);
+        }
+        dev::SsvRaw *hr = f->raw_pin.get<dev::SsvRaw>(std::max<size_t>(nall, 1));
+        if (!hr) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            set_error("msv: pinned host allocation failed");
+            return CMGPU_ENOMEM;
+        }
+        for (int32_t c = 0; c < nch; c++)
+            if (nraw[c] > 0)
+                MSV_TRY(cudaMemcpyAsync(hr + at[c], d_raws + (size_t)ch[c].seg_first * cap,
+                                        sizeof(dev::SsvRaw) * (size_t)nraw[c], cudaMemcpyDeviceToHost, st));
         MSV_TRY(cudaStreamSynchronize(st));
         for (int32_t c = 0; c < nch; c++) {
-            const dev::SsvRaw *p = hr.data() + (size_t)ch[c].seg_first * cap;
+            const dev::SsvRaw *p = hr + at[c];
             for (int q = 0; q < nraw[c]; q++) raws[c].push_back(RawWin{p[q].n, p[q].length, p[q].k, p[q].score});
         }
         break;
