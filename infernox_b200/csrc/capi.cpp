@@ -568,7 +568,10 @@ static int run_scan(cmgpu_model *m, cmgpu_workspace *ws, int semiring, int qdbid
     if ((rc = ensure_dev(&ws->d_items, &ws->items_cap, items.size()))) return rc;
     CUDA_TRY(cudaMemcpyAsync(ws->d_items, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice,
                              ws->stream));
-    size_t cand_cap = std::max<size_t>(ws->cands_cap, 1 << 16);
+    // Room for one reportable cell per four columns (4 bytes of device memory
+    // per residue): batches with homologs in a tenth of their sequences stay
+    // well inside it, so the scan is not repeated with a larger buffer.
+    const size_t cand_cap = std::max<size_t>({ws->cands_cap, (size_t)1 << 16, (size_t)(total_cols / 4)});
     if ((rc = ensure_dev(&ws->d_cands, &ws->cands_cap, cand_cap))) return rc;
     if (!sweep && !deck_smem && (int64_t)items.size() < best_l) {
         // fewer work items than lanes: no deck for lanes that would stay idle
@@ -644,10 +647,10 @@ static int run_scan(cmgpu_model *m, cmgpu_workspace *ws, int semiring, int qdbid
                 CUDA_TRY(launch(f, n, grid));
                 launches++;
             }
-            ws->stats.kernel_launches = launches;
+            ws->stats.kernel_launches += launches;
         } else {
             CUDA_TRY(launch(0, items.size(), ctas));
-            ws->stats.kernel_launches = 1;
+            ws->stats.kernel_launches += 1;
         }
         CUDA_TRY(cudaEventRecord(ws->ev1, ws->stream));
         CUDA_TRY(cudaMemcpyAsync(ws->h_counters, ws->d_counters, 2 * sizeof(int), cudaMemcpyDeviceToHost,

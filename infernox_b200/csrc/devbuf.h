@@ -81,4 +81,20 @@ inline bool any_code_above_17(const uint8_t *p, int64_t n) {
     return acc != 0;
 }
 
+// Let `kern` take as much dynamic shared memory as the current device allows
+// a block.  The attribute is process-wide per kernel, so every caller sets
+// the same value: host threads launching the same kernel with different
+// shared-memory sizes cannot lower the limit under one another's launch.
+template <class F>
+inline cudaError_t allow_max_dynamic_smem(F kern) {
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes fa;
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, kern);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+    return e;
+}
+
 }  // namespace cmx

@@ -542,7 +542,7 @@ template <int R>
 void launch_msv(const cmgpu_msv_filter *f, cudaStream_t st, const uint8_t *d_dsq, const dev::MsvWin *d_w, int n,
                 int *d_out, int grid) {
     const size_t smem = (size_t)KP * R * 32 * sizeof(uint32_t);
-    cudaFuncSetAttribute(dev::msv_score_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cmx::allow_max_dynamic_smem(dev::msv_score_kernel<R>);
     const MsvHost &h = f->host;
     dev::msv_score_kernel<R><<<grid, 256, smem, st>>>(f->d_negc, h.bias_b, h.tec_b, h.base_b, h.tbm_b, d_dsq, d_w, n,
                                                       d_out);
@@ -553,12 +553,12 @@ void launch_ssv(const cmgpu_msv_filter *f, cudaStream_t st, int xbb, int thr, co
                 const dev::SsvSeg *d_segs, int nseg, const dev::SsvChunk *d_ch, int nch, int cap,
                 dev::SsvCand *d_cands, int *d_counts, dev::SsvRaw *d_raws, int *d_nraw, int *d_need) {
     const size_t smem = (size_t)KP * R * 32 * sizeof(uint32_t);
-    cudaFuncSetAttribute(dev::ssv_scan_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cmx::allow_max_dynamic_smem(dev::ssv_scan_kernel<R>);
     const MsvHost &h = f->host;
     dev::ssv_scan_kernel<R><<<(nseg + 7) / 8, 256, smem, st>>>(f->d_negc, h.bias_b, xbb, thr, d_dsq, d_segs, nseg, cap,
                                                               d_cands, d_counts);
     const size_t rsm = (size_t)(h.M + 1) * KP;
-    cudaFuncSetAttribute(dev::ssv_replay_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsm);
+    cmx::allow_max_dynamic_smem(dev::ssv_replay_kernel<R>);
     dev::ssv_replay_kernel<R><<<(nch + 3) / 4, 128, rsm, st>>>(f->d_negc, f->d_rbv, h.M, h.bias_b, xbb, thr, h.base_b,
                                                             h.tjb_b, h.tbm_b, h.scale_b, d_dsq, d_ch, nch, cap, d_cands,
                                                             d_counts, d_raws, d_nraw, d_need);

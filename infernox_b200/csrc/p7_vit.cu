@@ -554,7 +554,7 @@ extern "C" int cmgpu_vit_score_batch(const cmgpu_vit_filter *f, void *stream_ptr
     if ((e = cudaMemcpyAsync(d_dsq, dsq_all, (size_t)dsq_len, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
         (e = cudaMemcpyAsync(d_w, vw.data(), sizeof(dev::VitWin) * nwin, cudaMemcpyHostToDevice, st)) !=
             cudaSuccess ||
-        (e = cudaFuncSetAttribute(dev::vit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+        (e = cmx::allow_max_dynamic_smem(dev::vit_kernel)) !=
             cudaSuccess) {
         cleanup();
         set_error(std::string("cmgpu_vit_score_batch: ") + cudaGetErrorString(e));
@@ -566,7 +566,7 @@ extern "C" int cmgpu_vit_score_batch(const cmgpu_vit_filter *f, void *stream_ptr
     auto launch_pk = [&](auto kern) {
         const int g = (int)std::min<int64_t>((nwin + 7) / 8, (int64_t)sms * 8);
         const size_t pk_smem = (size_t)18 * NP * 32 * 3 * sizeof(uint32_t);
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pk_smem);
+        cmx::allow_max_dynamic_smem(kern);
         kern<<<g, 256, pk_smem, st>>>(f->d_tab, M, f->host.base_w, f->host.e_move, f->host.e_loop, d_dsq, d_w,
                                       nwin, d_out, d_st);
     };

@@ -38,6 +38,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 
+#include "devbuf.h"
 #include "qdb_kernel.h"
 #include "semiring.cuh"
 
@@ -753,7 +754,7 @@ template <bool INS, bool DS, bool TG>
 static cudaError_t launch_t(const ScanParams &p, int ctas, int threads, cudaStream_t s) {
     auto kern = qdb_scan_kernel<INS, DS, TG>;
     size_t smem = (size_t)p.lay.words * 4;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cmx::allow_max_dynamic_smem(kern);
     if (e != cudaSuccess) return e;
     kern<<<ctas, threads, smem, s>>>(p);
     return cudaGetLastError();
@@ -764,7 +765,7 @@ static int occupancy_t(const ScanParams &p, int threads) {
     int n = 0;
     auto kern = qdb_scan_kernel<INS, DS, TG>;
     size_t smem = (size_t)p.lay.words * 4;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
+    if (cmx::allow_max_dynamic_smem(kern) != cudaSuccess) return 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, threads, smem) != cudaSuccess) return 0;
     return n;
 }

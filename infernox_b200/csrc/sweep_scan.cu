@@ -31,6 +31,7 @@
 #include <climits>
 #include <cstdint>
 
+#include "devbuf.h"
 #include "semiring.cuh"
 #include "sweep_kernel.h"
 
@@ -737,7 +738,7 @@ static int occ_t(const SweepParams &p, int threads) {
     int n = 0;
     auto kern = swdev::sweep_kernel<INS>;
     size_t smem = (size_t)p.lay.words * 4;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
+    if (cmx::allow_max_dynamic_smem(kern) != cudaSuccess) return 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, threads, smem) != cudaSuccess) return 0;
     return n;
 }
@@ -750,7 +751,7 @@ template <bool INS>
 static cudaError_t launch_t(const SweepParams &p, int ctas, cudaStream_t s) {
     auto kern = swdev::sweep_kernel<INS>;
     size_t smem = (size_t)p.lay.words * 4;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cmx::allow_max_dynamic_smem(kern);
     if (e != cudaSuccess) return e;
     kern<<<ctas, p.warps * 32, smem, s>>>(p);
     return cudaGetLastError();

@@ -951,7 +951,7 @@ int trq_batch(const cmgpu_model *mc, cudaStream_t st, int semiring, int qdbidx, 
         ((int64_t)4 * nplane * M * W1 + (int64_t)8 * W1 + (int64_t)3 * (W1 + trq::NW) * nbk * W1 + 63) / 64 * 64;
     const size_t smem = (size_t)(W + 1) * 12 + (ins ? ((size_t)m->ilog_nz * 2 + 16) : 0);
     auto kfn = ins ? trq::trq_kernel<true> : trq::trq_kernel<false>;
-    if (smem > 48 * 1024) TRQ_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    TRQ_TRY(cmx::allow_max_dynamic_smem(kfn));
     int occ = 0, nsm = 0;
     TRQ_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, trq::THREADS, smem));
     TRQ_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device));
