@@ -4,7 +4,8 @@ Other workloads (--workload): "nohmm-cyk-filter" (QDB1 CYK over 100 kb
 chunks), and the filter/banded stages of the default pipeline --
 "f1-ssv" (SSV windows over 100 kb chunks, both strands, of a 4.6 Mb
 sequence, F1 = 0.35), "f2-vit" (Viterbi filter over F1-sized windows),
-"hb-cyk" / "hb-inside" (HMM-banded CYK / float Inside over envelopes with
+"f3-fwd" (local Forward filter and its composition-bias null over the same
+windows), "hb-cyk" / "hb-inside" (HMM-banded CYK / float Inside over envelopes with
 CP9-shaped bands), "hb-trcyk" (truncated HMM-banded CYK, 5'-and-3' pass, all
 four planes), "trq-inside" / "trq-cyk" (the truncated non-banded integer
 TrInside / QDB1 TrCYK window scan, 5'-and-3' pass, over short sequences that
@@ -53,7 +54,7 @@ WORKLOADS = {
     "nohmm-cyk-filter": dict(clen=72, paired=None, nbif=2, sseed=0, pseed=11, semiring=0, band=1,
                              median=100000, sigma=0.0, lo=100000, hi=100000, gc=0.50),
 }
-FILTER_WORKLOADS = ("f1-ssv", "f2-vit", "hb-cyk", "hb-inside", "hb-trcyk", "trq-inside", "trq-cyk")
+FILTER_WORKLOADS = ("f1-ssv", "f2-vit", "f3-fwd", "hb-cyk", "hb-inside", "hb-trcyk", "trq-inside", "trq-cyk")
 OPS_PER_TERM = {0: 2.0, 1: 7.0}   # CYK: FADD + select; Inside: 6 INT + 1 LDS
 OPS_PER_CELL = 2.0                # emission add + store
 CUTOFF_BITS = 15.0                # stands in for the E-value threshold
@@ -547,13 +548,14 @@ def main():
 # HB: per child relaxation 2 (CYK) or 9 (FLogsum), about 3 children per
 # cell, plus emission add and clamp; truncated CYK: the same over the J, L
 # and R planes (T only at bifurcations).
-FILTER_OPS_PER_CELL = {"f1-ssv": 4.0, "f2-vit": 14.0, "hb-cyk": 8.0, "hb-inside": 29.0, "hb-trcyk": 24.0}
+FILTER_OPS_PER_CELL = {"f1-ssv": 4.0, "f2-vit": 14.0, "f3-fwd": 16.0, "hb-cyk": 8.0, "hb-inside": 29.0, "hb-trcyk": 24.0}
 FILTER_METRIC = {"f1-ssv": "F1 SSV window scan Gcells/s", "f2-vit": "F2 Viterbi filter Gcells/s",
+                 "f3-fwd": "F3 Forward filter Gcells/s (with the F3b bias null)",
                  "hb-cyk": "HMM-banded CYK Gcells/s", "hb-inside": "HMM-banded Inside Gcells/s",
                  "hb-trcyk": "truncated HMM-banded CYK Gcells/s (band cells, 4 planes each)",
                  "trq-inside": "truncated non-banded TrInside Gcells/s (J-plane cells, 4 planes each)",
                  "trq-cyk": "truncated QDB TrCYK Gcells/s (J-plane cells, 4 planes each)"}
-FILTER_DTYPE = {"f1-ssv": "u8 (packed s16x2)", "f2-vit": "i16", "hb-cyk": "f32", "hb-inside": "f32",
+FILTER_DTYPE = {"f1-ssv": "u8 (packed s16x2)", "f2-vit": "i16", "f3-fwd": "f32", "hb-cyk": "f32", "hb-inside": "f32",
                 "hb-trcyk": "f32", "trq-inside": "i32", "trq-cyk": "f32"}
 
 
@@ -623,7 +625,7 @@ def filter_main(args):
     from infernox_b200 import hb, model, p7, synth
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     config = {"workload": kind, "parallelism": f"dp{world}", "l2": "flushed (256 MB write) before each timed step"}
-    if kind in ("f1-ssv", "f2-vit"):
+    if kind in ("f1-ssv", "f2-vit", "f3-fwd"):
         M = 120
         prof, cons = p7.synthetic_profile(M, 77, 0.6)
         maxl = int(1.25 * M)
@@ -714,6 +716,14 @@ def filter_main(args):
     elif kind == "f2-vit":
         units = [(int(o), int(j)) for o, _, j in wins]
         one = lambda u: oracle.vit_score_batch(M, prof.mat, prof.trans, buf, [u[0]], [u[1]]) and u[1] * M
+    elif kind == "f3-fwd":
+        units = [(int(o), int(j)) for o, _, j in wins]
+        compo = p7.mean_composition(prof)
+
+        def one(u):
+            oracle.fwd_score_batch(M, prof.mat, prof.trans, buf, [u[0]], [u[1]])
+            oracle.bias_score_batch(compo, M, buf, [u[0]], [u[1]])
+            return u[1] * M
     elif kind in ("trq-inside", "trq-cyk"):
         units = list(range(len(wins)))
         ttab = {"lmesc": tri.lmesc, "rmesc": tri.rmesc, "pty": tri.pty, "ilmesc": tri.ilmesc, "irmesc": tri.irmesc,
@@ -807,6 +817,11 @@ def filter_main(args):
         call = lambda: f.score_batch(buf, wins)
         stats = lambda: p7.vit_stats(f)
         h2d = buf.nbytes + len(wins) * 24
+    elif kind == "f3-fwd":
+        f = p7.FwdFilter(prof, p7.mean_composition(prof), -6.0, 0.69, device=local_rank)
+        call = lambda: f.score_batch(buf, wins)
+        stats = f.stats
+        h2d = buf.nbytes + 2 * len(wins) * 16
     elif kind in ("trq-inside", "trq-cyk"):
         from infernox_b200 import _native as N
         from infernox_b200.scan import Scanner

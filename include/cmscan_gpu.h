@@ -587,6 +587,62 @@ int cmgpu_ssv_diagonals(const cmgpu_msv_filter *f, void *stream, const uint8_t *
  * of the last scoring or scanning call on this filter. */
 int cmgpu_msv_filter_stats(const cmgpu_msv_filter *f, double *kernel_ms, int64_t *cells, int32_t *launches);
 
+/* ---- P7 Forward filter (F3), composition bias (F3b), F1 -> F3b cascade -- */
+typedef struct cmgpu_fwd_filter cmgpu_fwd_filter;
+
+/* build_forward_filter (src/cm_pipeline.rs:969) and build_bias_filter
+ * (:1683) from the p7 filter profile, its mean match composition compo[4]
+ * (P7Profile.compo) and the local Forward exp-tail parameters (evparam
+ * lftau, lflambda).  device < 0: host tables only. */
+int cmgpu_fwd_filter_build(const cmgpu_p7_profile *p, const float *compo, double ftau, double flambda,
+                           int device, cmgpu_fwd_filter **out);
+void cmgpu_fwd_filter_free(cmgpu_fwd_filter *f);
+/* The profile in natural order, for tests: rfv[(M+1)*18] match odds,
+ * tr[(M+1)*8] = tBM, M->M, I->M, D->M (row k: into position k), M->I, I->I,
+ * M->D, D->D (row k: out of position k); bias emission odds eo[18*2] and
+ * state-1 transitions t1[3].  *m_out = M; cap = rows available (>= M+1). */
+int cmgpu_fwd_filter_tables(const cmgpu_fwd_filter *f, float *rfv, float *tr, int32_t cap, int32_t *m_out,
+                            float *eo, float *t1);
+/* forward_filter_score (src/cm_pipeline.rs:1420; the striped engine) and
+ * bias_filter_score (:1722) of residues i0..j0 of every window, in nats;
+ * either output may be NULL. */
+int cmgpu_fwd_score_batch(const cmgpu_fwd_filter *f, void *stream, const uint8_t *dsq_all, int64_t dsq_len,
+                          const cmgpu_window *wins, int32_t nwin, float *fwd_scores, float *bias_scores);
+
+/* The stages and thresholds of one f3_filter_sequence pass
+ * (src/cm_pipeline.rs:1863-1887). */
+typedef struct cmgpu_f3_config {
+    double f1, f1b, f2, f2b, f3, f3b; /* P-value thresholds                  */
+    int64_t cmw;                      /* the CM's W (SSV windows split at 2W) */
+    int64_t maxw;                     /* do_msv == 0: 2*maxw-residue tiles    */
+    int32_t do_msv, do_msvbias, do_vit, do_vitbias, do_fwd, do_fwdbias;
+    double lmmu, lmlambda;            /* local MSV Gumbel (F1b)               */
+    double lvmu, lvlambda;            /* local Viterbi Gumbel (F2, F2b)       */
+} cmgpu_f3_config;
+
+/* F1F3Acct (src/cm_pipeline.rs:1799-1814), summed over the chunks. */
+typedef struct cmgpu_f3_acct {
+    int64_t n_past_msv, pos_past_msv, n_past_msvbias, pos_past_msvbias;
+    int64_t n_past_vit, pos_past_vit, n_past_vitbias, pos_past_vitbias;
+    int64_t n_past_fwd, pos_past_fwd, n_past_fwdbias, pos_past_fwdbias;
+} cmgpu_f3_acct;
+
+/* f3_filter_sequence (src/cm_pipeline.rs:1863-2164) on every chunk (the
+ * chunk's residues are i0..j0 of its window): SSV windows (mf) or tiles,
+ * then the F1b MSV-bias (mf), F2 / F2b Viterbi (vf) and F3 / F3b Forward
+ * gates, and the merge of the survivors.  Windows come back grouped by
+ * chunk in chunk coordinates with the F3b bit score (the reference's wb).
+ * mf may be NULL when do_msv and do_msvbias are 0, vf when do_vit is 0.
+ * CMGPU_EOVERFLOW with the needed count in *n_out when cap is too small.
+ * Device time and launches of the whole pass: cmgpu_fwd_filter_stats. */
+int cmgpu_f3_filter(const cmgpu_fwd_filter *ff, const cmgpu_msv_filter *mf, const cmgpu_vit_filter *vf,
+                    void *stream, const uint8_t *dsq_all, int64_t dsq_len, const cmgpu_window *chunks,
+                    int32_t nchunk, const cmgpu_f3_config *cfg, cmgpu_f1_window *out, int32_t cap,
+                    int32_t *n_out, cmgpu_f3_acct *acct);
+/* Device time, Forward cells (residues x M) and launches of the last
+ * scoring or filtering call on this filter. */
+int cmgpu_fwd_filter_stats(const cmgpu_fwd_filter *f, double *kernel_ms, int64_t *cells, int32_t *launches);
+
 /* Exact counts of cells and terms the reference scanner evaluates for a
  * window of length L (host only; used for Gcells/s). */
 int cmgpu_count_work(const cmgpu_cm *cm, int semiring, int qdbidx, int32_t L,

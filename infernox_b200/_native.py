@@ -78,6 +78,24 @@ class P7Profile(C.Structure):
     _fields_ = [("M", C.c_int32), ("mat", P(C.c_float)), ("trans", P(C.c_float))]
 
 
+class F3Config(C.Structure):
+    """cmgpu_f3_config: stages and thresholds of one f3_filter_sequence pass."""
+    _fields_ = [("f1", C.c_double), ("f1b", C.c_double), ("f2", C.c_double), ("f2b", C.c_double),
+                ("f3", C.c_double), ("f3b", C.c_double), ("cmw", C.c_int64), ("maxw", C.c_int64),
+                ("do_msv", C.c_int32), ("do_msvbias", C.c_int32), ("do_vit", C.c_int32),
+                ("do_vitbias", C.c_int32), ("do_fwd", C.c_int32), ("do_fwdbias", C.c_int32),
+                ("lmmu", C.c_double), ("lmlambda", C.c_double), ("lvmu", C.c_double), ("lvlambda", C.c_double)]
+
+
+F3_ACCT_FIELDS = ("n_past_msv", "pos_past_msv", "n_past_msvbias", "pos_past_msvbias", "n_past_vit", "pos_past_vit",
+                  "n_past_vitbias", "pos_past_vitbias", "n_past_fwd", "pos_past_fwd", "n_past_fwdbias",
+                  "pos_past_fwdbias")
+
+
+class F3Acct(C.Structure):
+    _fields_ = [(k, C.c_int64) for k in F3_ACCT_FIELDS]
+
+
 class Hit(C.Structure):
     _fields_ = [("i", C.c_int32), ("j", C.c_int32), ("score", C.c_float), ("bias", C.c_float)]
 
@@ -226,6 +244,14 @@ def lib() -> C.CDLL:
     L.cmgpu_ssv_diagonals.argtypes = [vp, vp, vp, C.c_int64, vp, C.c_int32, C.c_double, vp, C.c_int32,
                                       P(C.c_int32)]
     L.cmgpu_msv_filter_stats.argtypes = [vp, P(C.c_double), P(C.c_int64), P(C.c_int32)]
+    L.cmgpu_fwd_filter_build.argtypes = [vp, vp, C.c_double, C.c_double, C.c_int, P(vp)]
+    L.cmgpu_fwd_filter_free.argtypes = [vp]
+    L.cmgpu_fwd_filter_free.restype = None
+    L.cmgpu_fwd_filter_tables.argtypes = [vp, vp, vp, C.c_int32, P(C.c_int32), vp, vp]
+    L.cmgpu_fwd_score_batch.argtypes = [vp, vp, vp, C.c_int64, vp, C.c_int32, vp, vp]
+    L.cmgpu_f3_filter.argtypes = [vp, vp, vp, vp, vp, C.c_int64, vp, C.c_int32, P(F3Config), vp, C.c_int32,
+                                  P(C.c_int32), P(F3Acct)]
+    L.cmgpu_fwd_filter_stats.argtypes = [vp, P(C.c_double), P(C.c_int64), P(C.c_int32)]
     L.cmgpu_fast_cyk_scan_hb.argtypes = [vp, P(HbBands), vp, C.c_int32, C.c_int32, C.c_int32, C.c_float,
                                          P(C.c_float), P(C.c_int64), P(C.c_int64)]
     L.cmgpu_hb_scan_hits.argtypes = [vp, C.c_int, P(HbBands), vp, C.c_int32, C.c_int32, C.c_int32, C.c_float,
@@ -276,5 +302,6 @@ EXPORTED = [
     "cmgpu_fast_cyk_scan_hb", "cmgpu_hb_scan_hits", "cmgpu_hb_scan_batch", "cmgpu_hb_stats",
     "cmgpu_tr_scan_hb", "cmgpu_tr_scan_hb_batch", "cmgpu_tr_qdb_scan", "cmgpu_tr_qdb_scan_batch",
     "cmgpu_tr_qdb_stats", "cmgpu_tr_qdb_inject_stall", "cmgpu_genomic_sample", "cmgpu_exp_fit",
-    "cmgpu_calibrate_scan_batch", "cmgpu_calibrate",
+    "cmgpu_calibrate_scan_batch", "cmgpu_calibrate", "cmgpu_fwd_filter_build", "cmgpu_fwd_filter_free",
+    "cmgpu_fwd_filter_tables", "cmgpu_fwd_score_batch", "cmgpu_f3_filter", "cmgpu_fwd_filter_stats",
 ]

@@ -10,7 +10,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libcmscan_gpu.so")
 
-SOURCES = ["qdb_scan.cu", "sweep_scan.cu", "capi.cpp", "cm_prep.cpp", "qdb_plan.cpp", "noalloc.cu", "p7_vit.cu", "p7_msv.cu", "hb_scan.cu", "trq_scan.cu", "calibrate.cpp"]
+SOURCES = ["qdb_scan.cu", "sweep_scan.cu", "capi.cpp", "cm_prep.cpp", "qdb_plan.cpp", "noalloc.cu", "p7_vit.cu", "p7_msv.cu", "hb_scan.cu", "trq_scan.cu", "calibrate.cpp", "p7_fwd.cu"]
 HEADERS = ["devbuf.h", "trunc_report.h", "cm_internal.h", "qdb_plan.h", "qdb_kernel.h", "model_internal.h",
            "semiring.cuh", "sweep_plan.h", "sweep_kernel.h"]
 

@@ -910,6 +910,23 @@ extern "C" int cmgpu_ssv_diagonals(const cmgpu_msv_filter *f, void *stream, cons
     return n > cap ? CMGPU_EOVERFLOW : CMGPU_OK;
 }
 
+namespace cmx {
+// f1_msv_windows on every chunk into a vector (windows grouped by chunk);
+// the chunks have been checked by the caller.
+int f1_msv_windows_vec(const cmgpu_msv_filter *f, cudaStream_t st, const uint8_t *dsq_all, int64_t dsq_len,
+                       const cmgpu_window *chunks, int32_t nchunk, double f1, int64_t cmw,
+                       std::vector<cmgpu_f1_window> &wins) {
+    MSV_TRY(cudaSetDevice(f->device));
+    std::vector<std::vector<RawWin>> raws;
+    int rc = ssv_run(f, st, dsq_all, dsq_len, chunks, nchunk, f1, raws);
+    if (rc) return rc;
+    wins.clear();
+    for (int32_t c = 0; c < nchunk; c++)
+        extend_merge_split(f->host, raws[c], std::max(0, chunks[c].j0 - chunks[c].i0 + 1), cmw, c, wins);
+    return CMGPU_OK;
+}
+}  // namespace cmx
+
 extern "C" int cmgpu_f1_msv_windows(const cmgpu_msv_filter *f, void *stream, const uint8_t *dsq_all, int64_t dsq_len,
                                     const cmgpu_window *chunks, int32_t nchunk, double f1, int64_t cmw,
                                     cmgpu_f1_window *out, int32_t cap, int32_t *n_out) {
@@ -921,13 +938,9 @@ extern "C" int cmgpu_f1_msv_windows(const cmgpu_msv_filter *f, void *stream, con
     }
     int rc = check_windows("cmgpu_f1_msv_windows", dsq_all, dsq_len, chunks, nchunk);
     if (rc) return rc;
-    MSV_TRY(cudaSetDevice(f->device));
-    std::vector<std::vector<RawWin>> raws;
-    rc = ssv_run(f, (cudaStream_t)stream, dsq_all, dsq_len, chunks, nchunk, f1, raws);
-    if (rc) return rc;
     std::vector<cmgpu_f1_window> wins;
-    for (int32_t c = 0; c < nchunk; c++)
-        extend_merge_split(f->host, raws[c], std::max(0, chunks[c].j0 - chunks[c].i0 + 1), cmw, c, wins);
+    rc = cmx::f1_msv_windows_vec(f, (cudaStream_t)stream, dsq_all, dsq_len, chunks, nchunk, f1, cmw, wins);
+    if (rc) return rc;
     *n_out = (int32_t)wins.size();
     if ((int64_t)wins.size() > cap) {
         set_error("cmgpu_f1_msv_windows: output capacity too small");

@@ -7,7 +7,11 @@ Mirrors, over libcmscan_gpu.so:
   * `build_msv_filter(&P7Profile, max_length) -> MsvFilter`,
     `msv_score`, `msv_score_reconfig` and
     `f1_msv_windows(&MsvFilter, dsq, l, f1, cmw) -> Vec<Window>`
-    (src/cm_pipeline.rs:201, :402, :410, :842).
+    (src/cm_pipeline.rs:201, :402, :410, :842);
+  * `build_forward_filter(&P7Profile) -> ForwardFilter`,
+    `build_bias_filter(&compo, m) -> BiasFilter`, `forward_filter_score`,
+    `bias_filter_score` and `f3_filter_sequence` (src/cm_pipeline.rs:969,
+    :1683, :1420, :1722, :1863) as FwdFilter and its functions.
 The batch methods score or scan many windows / chunks in one call.
 """
 from __future__ import annotations
@@ -190,6 +194,125 @@ def f1_msv_windows(f: MsvFilter, dsq, l: int, f1: float, cmw: int):
     """src/cm_pipeline.rs:842 -- [(start, end, score)] of one chunk frame."""
     w = f.f1_windows_batch(np.ascontiguousarray(dsq, np.uint8), np.array([(0, 1, l)], N.WINDOW_DTYPE), f1, cmw)
     return [(int(r["start"]), int(r["end"]), float(r["score"])) for r in w]
+
+
+class FwdFilter:
+    """build_forward_filter(p7) and build_bias_filter(p7.compo, p7.m)
+    (src/cm_pipeline.rs:969, :1683) with the local Forward exp-tail
+    parameters (evparam.lftau / lflambda) of the F3 gate."""
+
+    def __init__(self, p: P7Profile, compo, ftau: float = 0.0, flambda: float = 1.0, device: int = 0):
+        self.p = p
+        self._mat = np.ascontiguousarray(p.mat, np.float32).reshape(p.M + 1, 4)
+        self._trans = np.ascontiguousarray(p.trans, np.float32).reshape(p.M + 1, 7)
+        self._compo = np.ascontiguousarray(compo, np.float32).reshape(4)
+        prof = N.P7Profile(p.M, N.ptr(self._mat, C.c_float), N.ptr(self._trans, C.c_float))
+        self._h = C.c_void_p()
+        N.check(N.lib().cmgpu_fwd_filter_build(C.byref(prof), self._compo.ctypes.data, float(ftau), float(flambda),
+                                               device, C.byref(self._h)))
+
+    def close(self):
+        if self._h:
+            N.lib().cmgpu_fwd_filter_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def tables(self):
+        """(rfv [(M+1), 18], [(M+1), 8] = tBM, MM, IM, DM, MI, II, MD, DD, bias eo [18, 2], t1 [3])."""
+        m = self.p.M
+        rfv = np.zeros((m + 1, 18), np.float32)
+        tr = np.zeros((m + 1, 8), np.float32)
+        eo = np.zeros((18, 2), np.float32)
+        t1 = np.zeros(3, np.float32)
+        n = C.c_int32()
+        N.check(N.lib().cmgpu_fwd_filter_tables(self._h, rfv.ctypes.data, tr.ctypes.data, m + 1, C.byref(n),
+                                                eo.ctypes.data, t1.ctypes.data))
+        return rfv, tr, eo, t1
+
+    def stats(self):
+        """(kernel ms, Forward cells, launches) of the last call."""
+        ms, cells, launches = C.c_double(), C.c_int64(), C.c_int32()
+        N.check(N.lib().cmgpu_fwd_filter_stats(self._h, C.byref(ms), C.byref(cells), C.byref(launches)))
+        return ms.value, cells.value, launches.value
+
+    def score_batch(self, buf: np.ndarray, windows: np.ndarray, fwd: bool = True, bias: bool = True):
+        """(Forward scores, bias-filter scores) in nats per window; either is
+        None when not asked for."""
+        b = np.ascontiguousarray(buf, np.uint8)
+        w = np.ascontiguousarray(windows, N.WINDOW_DTYPE)
+        fs = np.zeros(len(w), np.float32) if fwd else None
+        bs = np.zeros(len(w), np.float32) if bias else None
+        N.check(N.lib().cmgpu_fwd_score_batch(self._h, None, b.ctypes.data, b.size, w.ctypes.data, len(w),
+                                              None if fs is None else fs.ctypes.data,
+                                              None if bs is None else bs.ctypes.data))
+        return fs, bs
+
+
+def forward_filter_score(f: FwdFilter, dsq, l: int) -> float:
+    """src/cm_pipeline.rs:1420 -- the local Forward score (nats) of dsq[1..l]."""
+    return float(f.score_batch(np.ascontiguousarray(dsq, np.uint8), np.array([(0, 1, l)], N.WINDOW_DTYPE),
+                               bias=False)[0][0])
+
+
+def bias_filter_score(f: FwdFilter, dsq, l: int) -> float:
+    """src/cm_pipeline.rs:1722 -- the composition-bias null score (nats)."""
+    return float(f.score_batch(np.ascontiguousarray(dsq, np.uint8), np.array([(0, 1, l)], N.WINDOW_DTYPE),
+                               fwd=False)[1][0])
+
+
+def f3_filter_batch(ff: FwdFilter, buf: np.ndarray, chunks: np.ndarray, f1: float, f3: float, f3b: float, cmw: int,
+                    mf: MsvFilter = None, vf: VitFilter = None, msvbias=None, vit=None, do_fwd: bool = True,
+                    do_fwdbias: bool = True, do_msv: bool = True, maxw: int = 0):
+    """f3_filter_sequence (src/cm_pipeline.rs:1863) on every chunk: the
+    merged survivors (F1_WINDOW_DTYPE, chunk coordinates, F3b bit score) and
+    the summed accounting.  msvbias = (f1b, lmmu, lmlambda) turns F1b on;
+    vit = (f2, do_vitbias, f2b, lvmu, lvlambda) turns F2 / F2b on."""
+    cfg = N.F3Config()
+    cfg.f1, cfg.f3, cfg.f3b, cfg.cmw, cfg.maxw = float(f1), float(f3), float(f3b), int(cmw), int(maxw)
+    cfg.do_msv, cfg.do_fwd, cfg.do_fwdbias = int(do_msv), int(do_fwd), int(do_fwdbias)
+    cfg.f1b = cfg.f2 = cfg.f2b = 1.0
+    if msvbias is not None:
+        cfg.do_msvbias = 1
+        cfg.f1b, cfg.lmmu, cfg.lmlambda = (float(x) for x in msvbias)
+    if vit is not None:
+        cfg.do_vit = 1
+        f2, do_vitbias, f2b, lvmu, lvl = vit
+        cfg.f2, cfg.do_vitbias, cfg.f2b, cfg.lvmu, cfg.lvlambda = float(f2), int(do_vitbias), float(f2b), \
+            float(lvmu), float(lvl)
+    b = np.ascontiguousarray(buf, np.uint8)
+    c = np.ascontiguousarray(chunks, N.WINDOW_DTYPE)
+    acct = N.F3Acct()
+    cap = 1024 + b.size // 256
+    while True:
+        out = np.zeros(cap, F1_WINDOW_DTYPE)
+        n = C.c_int32()
+        rc = N.lib().cmgpu_f3_filter(ff._h, mf._h if mf is not None else None, vf._h if vf is not None else None,
+                                     None, b.ctypes.data, b.size, c.ctypes.data, len(c), C.byref(cfg),
+                                     out.ctypes.data, cap, C.byref(n), C.byref(acct))
+        if rc == N.CMGPU_EOVERFLOW and n.value > cap:
+            cap = n.value
+            continue
+        N.check(rc)
+        return out[: n.value], {k: int(getattr(acct, k)) for k in N.F3_ACCT_FIELDS}
+
+
+def f3_filter_sequence(mf: MsvFilter, ff: FwdFilter, dsq, win_len: int, f1: float, f3: float, f3b: float, cmw: int,
+                       **kw):
+    """src/cm_pipeline.rs:1863 on one chunk frame: ([(start, end, score)], accounting)."""
+    w, acct = f3_filter_batch(ff, np.ascontiguousarray(dsq, np.uint8), np.array([(0, 1, win_len)], N.WINDOW_DTYPE),
+                              f1, f3, f3b, cmw, mf=mf, **kw)
+    return [(int(r["start"]), int(r["end"]), float(r["score"])) for r in w], acct
+
+
+def mean_composition(p: P7Profile) -> np.ndarray:
+    """Mean match emission over the model: the composition a synthetic
+    profile's bias filter uses (profiles read from a file carry their own)."""
+    return np.asarray(p.mat, np.float32)[1:].mean(axis=0).astype(np.float32)
 
 
 def synthetic_profile(m: int, seed: int, peak: float = 0.6):

@@ -1,6 +1,6 @@
 """TEST INFRASTRUCTURE ONLY: ctypes binding of the oracle (qdb_oracle.c,
 hb_oracle.c, tr_oracle.c, trq_oracle.c, p7_oracle.c, msv_oracle.c,
-prep_oracle.c, calib_oracle.c).
+prep_oracle.c, calib_oracle.c, fwd_oracle.c).
 
 Used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as
 the checker of the GPU scanner.  The product package never imports it.
@@ -9,6 +9,7 @@ Build with `make -C oracle` (or oracle.build()).
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 import subprocess
 
@@ -43,7 +44,8 @@ def lib():
     global _lib
     if _lib is None:
         srcs = [os.path.join(HERE, f) for f in ("qdb_oracle.c", "hb_oracle.c", "tr_oracle.c", "trq_oracle.c",
-                                                "p7_oracle.c", "msv_oracle.c", "prep_oracle.c", "calib_oracle.c")]
+                                                "p7_oracle.c", "msv_oracle.c", "prep_oracle.c", "calib_oracle.c",
+                                                "fwd_oracle.c")]
         if not os.path.exists(LIB_PATH) or any(os.path.getmtime(LIB_PATH) < os.path.getmtime(f) for f in srcs):
             native = os.path.basename(os.path.dirname(LIB_PATH)) == "_build_native"
             subprocess.run(["make", "-s", "-C", HERE] + (["native"] if native else []), check=True)
@@ -84,6 +86,10 @@ def lib():
         L.oracle_genomic_sample.argtypes = [C.c_uint32, C.c_int32, C.c_int32, vp]
         L.oracle_exp_fit.argtypes = [vp, C.c_int64, C.c_int, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_float,
                                      C.c_double, vp]
+        L.oracle_fwd_tables.argtypes = [C.c_int, vp, vp, vp, vp]
+        L.oracle_fwd_score_batch.argtypes = [C.c_int, vp, vp, vp, vp, vp, C.c_int32, vp, vp, vp]
+        L.oracle_bias_tables.argtypes = [vp, C.c_int, vp, vp]
+        L.oracle_bias_score_batch.argtypes = [vp, C.c_int, vp, vp, vp, C.c_int32, vp, vp]
         _lib = L
     return _lib
 
@@ -245,6 +251,173 @@ def ssv_threshold(M, mat, trans, max_length, mmu, mlambda, f1):
     mat, trans = _f32(mat), _f32(trans)
     return int(lib().oracle_ssv_threshold(int(M), mat.ctypes.data, trans.ctypes.data, int(max_length), float(mmu),
                                           float(mlambda), float(f1)))
+
+
+def fwd_tables(M, mat, trans):
+    """build_forward_filter restated: (rfv [(M+1), 18], [(M+1), 8] = tbm, amm, aim, adm, tmi, tii, tmd, tdd)."""
+    mat, trans = _f32(mat), _f32(trans)
+    rfv = np.zeros((M + 1) * 18, np.float32)
+    tr = np.zeros((M + 1) * 8, np.float32)
+    lib().oracle_fwd_tables(int(M), mat.ctypes.data, trans.ctypes.data, rfv.ctypes.data, tr.ctypes.data)
+    return rfv.reshape(M + 1, 18), tr.reshape(M + 1, 8)
+
+
+def fwd_score_batch(M, mat, trans, buf, offs, lens):
+    """forward_filter_score (striped engine) per frame: (scores, totscale, xc)."""
+    mat, trans = _f32(mat), _f32(trans)
+    buf = np.ascontiguousarray(buf, np.uint8)
+    offs = np.ascontiguousarray(offs, np.int64)
+    lens = np.ascontiguousarray(lens, np.int32)
+    n = len(lens)
+    sc, ts, xc = (np.zeros(n, np.float32) for _ in range(3))
+    lib().oracle_fwd_score_batch(int(M), mat.ctypes.data, trans.ctypes.data, buf.ctypes.data, offs.ctypes.data,
+                                 lens.ctypes.data, n, sc.ctypes.data, ts.ctypes.data, xc.ctypes.data)
+    return sc, ts, xc
+
+
+def bias_tables(compo, M):
+    compo = _f32(compo)
+    eo = np.zeros(36, np.float32)
+    t1 = np.zeros(3, np.float32)
+    lib().oracle_bias_tables(compo.ctypes.data, int(M), eo.ctypes.data, t1.ctypes.data)
+    return eo.reshape(18, 2), t1
+
+
+def bias_score_batch(compo, M, buf, offs, lens):
+    """bias_filter_score per frame: (scores, the scores before the length term)."""
+    compo = _f32(compo)
+    buf = np.ascontiguousarray(buf, np.uint8)
+    offs = np.ascontiguousarray(offs, np.int64)
+    lens = np.ascontiguousarray(lens, np.int32)
+    n = len(lens)
+    sc, rows = np.zeros(n, np.float32), np.zeros(n, np.float32)
+    lib().oracle_bias_score_batch(compo.ctypes.data, int(M), buf.ctypes.data, offs.ctypes.data, lens.ctypes.data, n,
+                                  sc.ctypes.data, rows.ctypes.data)
+    return sc, rows
+
+
+def _null_one(L):
+    """p7_bg_null_one (src/cm_pipeline.rs:1122-1125)."""
+    p1 = L / (L + 1.0)
+    return L * math.log(p1) + math.log(1.0 - p1)
+
+
+def _exp_surv(x, mu, lam):
+    """esl_exp_surv (src/cp9.rs:6531-6537)."""
+    return 1.0 if x < mu else math.exp(-lam * (x - mu))
+
+
+def _gumbel_surv(x, mu, lam):
+    """esl_gumbel_surv (src/cm_pipeline.rs:1852-1861)."""
+    y = lam * (x - mu)
+    ey = -math.exp(-y)
+    return -ey if abs(ey) < 5e-9 else 1.0 - math.exp(ey)
+
+
+def f3_filter_sequence(p7, compo, ftau, flambda, chunk, f1, f3, f3b, cmw, msvbias=None, vit=None, do_fwd=True,
+                       do_fwdbias=True, do_msv=True, maxw=0, max_length=0, mmu=0.0, mlambda=0.0):
+    """f3_filter_sequence (src/cm_pipeline.rs:1863-2164) on one chunk (a frame
+    [255, residues, 255]): the merged surviving windows [(start, end, score)]
+    and the accounting dict.  p7 = (M, mat, trans); msvbias = (f1b, lmmu,
+    lmlambda) or None; vit = (f2, do_vitbias, f2b, lvmu, lvlambda) or None."""
+    M, mat, trans = p7
+    chunk = np.ascontiguousarray(chunk, np.uint8)
+    win_len = len(chunk) - 2
+    ln2 = math.log(2.0)
+    if do_msv:
+        w, _, _, _ = f1_msv_windows(M, mat, trans, max_length, mmu, mlambda, chunk, [0], [win_len], f1, cmw)
+        wins = [(int(s), int(e)) for _, s, e in w]
+    else:
+        n, mw = win_len, maxw
+        nwin = 1
+        if n > 2 * mw:
+            nwin += (n - 2 * mw) // (mw + 1)
+            if (n - 2 * mw) % (mw + 1) > 0:
+                nwin += 1
+        wins = [(1 + i * (mw + 1), min(1 + i * (mw + 1) + 2 * mw - 1, n)) for i in range(nwin)]
+    nwin = len(wins)
+    # one frame per window: [255, residues ws..we, 255]
+    frames, offs, lens = [], [], []
+    pos = 0
+    for ws, we in wins:
+        f = np.concatenate([[255], chunk[ws:we + 1], [255]]).astype(np.uint8)
+        frames.append(f)
+        offs.append(pos)
+        lens.append(we - ws + 1)
+        pos += len(f)
+    buf = np.concatenate(frames) if frames else np.zeros(0, np.uint8)
+    bias = bias_score_batch(compo, M, buf, offs, lens)[0] if nwin else np.zeros(0, np.float32)
+    fwd = fwd_score_batch(M, mat, trans, buf, offs, lens)[0] if nwin and do_fwd else np.zeros(nwin, np.float32)
+    msv = msv_score_batch(M, mat, trans, max_length, buf, offs, lens, lens) if nwin and msvbias else None
+    vsc = vit_score_batch(M, mat, trans, buf, offs, lens) if nwin and vit else None
+    s_f1b = [True] * nwin
+    s_f2 = [True] * nwin
+    s_f2b = [True] * nwin
+    s_f3 = [False] * nwin
+    s_f3b = [False] * nwin
+    wb = [np.float32(-999.0)] * nwin
+    for i in range(nwin):
+        wlen = lens[i]
+        nullsc = _null_one(wlen)
+        if msvbias is not None and msv[1][i]:
+            f1b, lmmu, lml = msvbias
+            if _gumbel_surv((float(msv[0][i]) - float(bias[i])) / ln2, lmmu, lml) > f1b:
+                s_f1b[i] = False
+                continue
+        if vit is not None and vsc[1][i]:
+            f2, do_vitbias, f2b, lvmu, lvl = vit
+            vf = float(vsc[0][i])
+            if _gumbel_surv((vf - nullsc) / ln2, lvmu, lvl) > f2:
+                s_f2[i] = s_f2b[i] = False
+                continue
+            if do_vitbias and _gumbel_surv((vf - float(bias[i])) / ln2, lvmu, lvl) > f2b:
+                s_f2b[i] = False
+                continue
+        if do_fwd:
+            wsc = (float(fwd[i]) - nullsc) / ln2
+            wb[i] = np.float32(wsc)
+            if _exp_surv(wsc, ftau, flambda) > f3:
+                continue
+        s_f3[i] = True
+        if do_fwd and do_fwdbias:
+            wsc = (float(fwd[i]) - float(bias[i])) / ln2
+            wb[i] = np.float32(wsc)
+            if _exp_surv(wsc, ftau, flambda) > f3b:
+                continue
+        s_f3b[i] = True
+    ns = [wins[i][0] for i in range(nwin) if s_f3b[i]]
+    ne = [wins[i][1] for i in range(nwin) if s_f3b[i]]
+    nb = [wb[i] for i in range(nwin) if s_f3b[i]]
+    out = []
+    i = 0
+    while i < len(ns):
+        i2 = i + 1
+        while i2 < len(ns) and ne[i] + 1 >= ns[i2]:
+            ne[i] = ne[i2]
+            nb[i] = max(nb[i], nb[i2])
+            i2 += 1
+        out.append((ns[i], ne[i], np.float32(nb[i])))
+        i = i2
+    acct = dict.fromkeys(("n_past_msv", "pos_past_msv", "n_past_msvbias", "pos_past_msvbias", "n_past_vit",
+                          "pos_past_vit", "n_past_vitbias", "pos_past_vitbias", "n_past_fwd", "pos_past_fwd",
+                          "n_past_fwdbias", "pos_past_fwdbias"), 0)
+    acct["n_past_msv"] = nwin
+    stages = (("msvbias", s_f1b), ("vit", s_f2), ("vitbias", s_f2b), ("fwd", s_f3), ("fwdbias", s_f3b))
+    for i in range(nwin):
+        wlen = lens[i]
+        acct["pos_past_msv"] += wlen
+        for name, s in stages:
+            if s[i]:
+                acct["n_past_" + name] += 1
+                acct["pos_past_" + name] += wlen
+        if i > 0:
+            ov = wins[i - 1][1] - wins[i][0] + 1
+            if ov > 0:
+                acct["pos_past_msv"] -= ov
+                for name, s in stages:
+                    if s[i] and s[i - 1]:
+                        acct["pos_past_" + name] -= ov
+    return out, acct
 
 
 def hb_scan(cm, inside, bands, dsq, i0, j0, env_cutoff, report, cutoff, do_null3):
