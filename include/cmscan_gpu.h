@@ -639,6 +639,13 @@ int cmgpu_f3_filter(const cmgpu_fwd_filter *ff, const cmgpu_msv_filter *mf, cons
                     void *stream, const uint8_t *dsq_all, int64_t dsq_len, const cmgpu_window *chunks,
                     int32_t nchunk, const cmgpu_f3_config *cfg, cmgpu_f1_window *out, int32_t cap,
                     int32_t *n_out, cmgpu_f3_acct *acct);
+/* Forward kernels (cmgpu_fwd_filter_set_kernel); both give the same bits.
+ * AUTO keeps each lane's segment of the rows in registers where it fits
+ * (nq = (M-1)/4+1 <= 32), else in shared memory; SHARED always uses the
+ * shared-memory kernel. */
+#define CMGPU_FWD_KERNEL_AUTO 0
+#define CMGPU_FWD_KERNEL_SHARED 1
+int cmgpu_fwd_filter_set_kernel(cmgpu_fwd_filter *f, int kernel);
 /* Device time, Forward cells (residues x M) and launches of the last
  * scoring or filtering call on this filter. */
 int cmgpu_fwd_filter_stats(const cmgpu_fwd_filter *f, double *kernel_ms, int64_t *cells, int32_t *launches);

@@ -252,6 +252,7 @@ def lib() -> C.CDLL:
     L.cmgpu_f3_filter.argtypes = [vp, vp, vp, vp, vp, C.c_int64, vp, C.c_int32, P(F3Config), vp, C.c_int32,
                                   P(C.c_int32), P(F3Acct)]
     L.cmgpu_fwd_filter_stats.argtypes = [vp, P(C.c_double), P(C.c_int64), P(C.c_int32)]
+    L.cmgpu_fwd_filter_set_kernel.argtypes = [vp, C.c_int]
     L.cmgpu_fast_cyk_scan_hb.argtypes = [vp, P(HbBands), vp, C.c_int32, C.c_int32, C.c_int32, C.c_float,
                                          P(C.c_float), P(C.c_int64), P(C.c_int64)]
     L.cmgpu_hb_scan_hits.argtypes = [vp, C.c_int, P(HbBands), vp, C.c_int32, C.c_int32, C.c_int32, C.c_float,
@@ -303,5 +304,5 @@ EXPORTED = [
     "cmgpu_tr_scan_hb", "cmgpu_tr_scan_hb_batch", "cmgpu_tr_qdb_scan", "cmgpu_tr_qdb_scan_batch",
     "cmgpu_tr_qdb_stats", "cmgpu_tr_qdb_inject_stall", "cmgpu_genomic_sample", "cmgpu_exp_fit",
     "cmgpu_calibrate_scan_batch", "cmgpu_calibrate", "cmgpu_fwd_filter_build", "cmgpu_fwd_filter_free",
-    "cmgpu_fwd_filter_tables", "cmgpu_fwd_score_batch", "cmgpu_f3_filter", "cmgpu_fwd_filter_stats",
+    "cmgpu_fwd_filter_tables", "cmgpu_fwd_score_batch", "cmgpu_f3_filter", "cmgpu_fwd_filter_stats", "cmgpu_fwd_filter_set_kernel",
 ]

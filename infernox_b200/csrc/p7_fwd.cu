@@ -69,6 +69,7 @@ struct FwdHost {
     std::vector<float> rfv;   // [(M+1)][KP] match odds, natural order
     std::vector<float> tr;    // [(M+1)][8]: tbm, amm, aim, adm, tmi, tii, tmd, tdd
     std::vector<float> stab;  // device layout: [nq][T_N][4], then rfv [KP][rq][4]
+    std::vector<float> ptab;  // register kernel: [nq][4][T_N] (a lane's eight values together), then rfv as above
     float eo[KP * 2] = {};
     float t1[3] = {};
     double ftau = 0, flambda = 0;
@@ -127,6 +128,12 @@ void build_host(const cmgpu_p7_profile *p, const float *compo, FwdHost &h) {
             for (int x = 0; x < KP; x++)
                 h.stab[(size_t)nq * T_N * 4 + ((size_t)x * rq + q) * 4 + zz] = h.rfv[(size_t)pos * KP + x];
         }
+    h.ptab.assign(h.stab.size(), 0.0f);
+    for (int q = 0; q < nq; q++)
+        for (int zz = 0; zz < 4; zz++)
+            for (int r = 0; r < T_N; r++)
+                h.ptab[((size_t)q * 4 + zz) * T_N + r] = h.stab[((size_t)q * T_N + r) * 4 + zz];
+    std::copy(h.stab.begin() + (size_t)nq * T_N * 4, h.stab.end(), h.ptab.begin() + (size_t)nq * T_N * 4);
     // bias filter (src/cm_pipeline.rs:1683-1720)
     const float bg = 0.25f;
     const float l1 = (float)m / 8.0f;
@@ -155,6 +162,8 @@ struct cmgpu_fwd_filter {
     int device = 0;
     FwdHost host;
     float *d_tab = nullptr;
+    float *d_ptab = nullptr;
+    int kernel = CMGPU_FWD_KERNEL_AUTO;
     double last_ms = 0;
     int64_t last_cells = 0;
     int32_t last_launches = 0;
@@ -162,6 +171,7 @@ struct cmgpu_fwd_filter {
     ~cmgpu_fwd_filter() {
         arena.release();
         cudaFree(d_tab);
+        cudaFree(d_ptab);
     }
 };
 
@@ -290,6 +300,132 @@ __global__ void __launch_bounds__(256) fwd_kernel(const float *__restrict__ tab,
                     dmr[q * 4 + z] *= inv;
                     imr[q * 4 + z] *= inv;
                 }
+                tot += (float)log((double)xe);
+            }
+        }
+        if (z == 0) out[w] = make_float2(tot, xc);
+    }
+}
+
+// The same recurrence with a lane's segment of the M, D and I rows in
+// registers (nq <= NQ; the loops run to NQ with the cells past nq
+// skipped), the lane's eight transition values of a cell read as two
+// 16-byte words, and its D->D values held in registers for the window.
+template <int NQ>
+__global__ void __launch_bounds__(128) fwd_kernel_reg(const float *__restrict__ ptab, int M, int nq, int rq,
+                                                      const uint8_t *__restrict__ dsq,
+                                                      const FwdWin *__restrict__ wins, int nwin,
+                                                      int *__restrict__ next, float2 *__restrict__ out) {
+    extern __shared__ __align__(16) float sm[];
+    const int tabn = nq * T_N * 4 + KP * rq * 4;
+    for (int q = threadIdx.x; q < tabn; q += blockDim.x) sm[q] = ptab[q];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, z = lane & 3;
+    const unsigned gmask = 0xFu << (lane & ~3);
+    const float4 *T4 = reinterpret_cast<const float4 *>(sm);
+    const float *R0 = sm + nq * T_N * 4;
+    const bool lazy = M >= 100;
+    float tdd[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; q++) tdd[q] = q < nq ? sm[(q * 4 + z) * T_N + T_DD] : 0.0f;
+    float mmv[NQ], dmv[NQ], imv[NQ];
+    for (;;) {
+        int w = 0;
+        if (z == 0) w = atomicAdd(next, 1);
+        w = __shfl_sync(gmask, w, lane & ~3);
+        if (w >= nwin) break;
+        const FwdWin win = wins[w];
+        const uint8_t *d = dsq + win.first - 1;
+        const int L = win.L;
+#pragma unroll
+        for (int q = 0; q < NQ; q++) mmv[q] = dmv[q] = imv[q] = 0.0f;
+        float lastm = 0.0f, lastd = 0.0f, lasti = 0.0f;  // the cells at q = nq - 1
+        const float pmove = 3.0f / ((float)L + 2.0f + 1.0f);
+        const float ploop = 1.0f - pmove;
+        float xn = 1.0f, xj = 0.0f, xb = pmove, xc = 0.0f, tot = 0.0f;
+        for (int i = 1; i <= L; i++) {
+            const float *rf = R0 + (int)d[i] * rq * 4 + z;
+            float mpv = lane_shift(gmask, lastm, z);
+            float dpv = lane_shift(gmask, lastd, z);
+            float ipv = lane_shift(gmask, lasti, z);
+            float dcv = 0.0f, xev = 0.0f;
+#pragma unroll
+            for (int q = 0; q < NQ; q++) {
+                if (q < nq) {
+                    const float4 ta = T4[(q * 4 + z) * 2], tb = T4[(q * 4 + z) * 2 + 1];
+                    float sv = xb * ta.x;
+                    sv = sv + mpv * ta.y;
+                    sv = sv + ipv * ta.z;
+                    sv = sv + dpv * ta.w;
+                    sv = sv * rf[q * 4];
+                    xev = xev + sv;
+                    mpv = mmv[q];
+                    dpv = dmv[q];
+                    ipv = imv[q];
+                    mmv[q] = sv;
+                    dmv[q] = dcv;
+                    dcv = sv * tb.x;
+                    imv[q] = mpv * tb.y + ipv * tb.z;
+                    if (q == nq - 1) {
+                        lastm = mmv[q];
+                        lasti = imv[q];
+                    }
+                }
+            }
+            dcv = lane_shift(gmask, dcv, z);
+            dmv[0] = 0.0f;
+#pragma unroll
+            for (int q = 0; q < NQ; q++)
+                if (q < nq) {
+                    const float dd = dcv + dmv[q];
+                    dmv[q] = dd;
+                    dcv = dd * tdd[q];
+                }
+            for (int j = 1; j < 4; j++) {
+                dcv = lane_shift(gmask, dcv, z);
+                int changed = 0;
+#pragma unroll
+                for (int q = 0; q < NQ; q++)
+                    if (q < nq) {
+                        const float old = dmv[q];
+                        const float dd = dcv + old;
+                        changed |= dd > old;
+                        dmv[q] = dd;
+                        dcv = dcv * tdd[q];
+                    }
+                if (lazy) {
+                    changed |= __shfl_xor_sync(gmask, changed, 1, 4);
+                    changed |= __shfl_xor_sync(gmask, changed, 2, 4);
+                    if (!changed) break;
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < NQ; q++)
+                if (q < nq) {
+                    xev = xev + dmv[q];
+                    if (q == nq - 1) lastd = dmv[q];
+                }
+            const float h = xev + __shfl_sync(gmask, xev, (z + 1) & 3, 4);
+            const float xe = __shfl_sync(gmask, h, 0, 4) + __shfl_sync(gmask, h, 2, 4);
+            xn = xn * ploop;
+            xc = (xc * ploop) + (xe * 0.5f);
+            xj = (xj * ploop) + (xe * 0.5f);
+            xb = (xj * pmove) + (xn * pmove);
+            if (xe > 1.0e4f) {
+                const float inv = __fdiv_rn(1.0f, xe);
+                xn *= inv;
+                xc *= inv;
+                xj *= inv;
+                xb *= inv;
+#pragma unroll
+                for (int q = 0; q < NQ; q++) {
+                    mmv[q] *= inv;
+                    dmv[q] *= inv;
+                    imv[q] *= inv;
+                }
+                lastm *= inv;
+                lastd *= inv;
+                lasti *= inv;
                 tot += (float)log((double)xe);
             }
         }
@@ -436,7 +572,21 @@ int score_windows(const cmgpu_fwd_filter *f, cudaStream_t st, const uint8_t *dsq
     FWD_TRY(cudaEventCreate(&ev0));
     FWD_TRY(cudaEventCreate(&ev1));
     FWD_TRY(cudaEventRecord(ev0, st));
-    if (nf > 0) {
+    const bool regs = nq <= 32 && f->kernel != CMGPU_FWD_KERNEL_SHARED;
+    if (nf > 0 && regs) {
+        // the segment of each lane fits in registers
+        auto kern = nq <= 8 ? cmx::dev::fwd_kernel_reg<8>
+                  : nq <= 16 ? cmx::dev::fwd_kernel_reg<16>
+                  : nq <= 24 ? cmx::dev::fwd_kernel_reg<24> : cmx::dev::fwd_kernel_reg<32>;
+        const size_t rsmem = (size_t)(nq * T_N * 4 + KP * h.rq * 4) * sizeof(float);
+        FWD_TRY(cmx::allow_max_dynamic_smem(kern));
+        int per_sm = 0;
+        FWD_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, rsmem));
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((nf + 31) / 32, (int64_t)sms * std::max(per_sm, 1)));
+        kern<<<grid, 128, rsmem, st>>>(f->d_ptab, h.M, nq, h.rq, d_dsq, d_w, nf, d_next, d_out);
+        FWD_TRY(cudaGetLastError());
+        mf->last_launches++;
+    } else if (nf > 0) {
         auto kern = ts ? cmx::dev::fwd_kernel<true> : cmx::dev::fwd_kernel<false>;
         FWD_TRY(cmx::allow_max_dynamic_smem(kern));
         int per_sm = 0;
@@ -511,6 +661,8 @@ extern "C" int cmgpu_fwd_filter_build(const cmgpu_p7_profile *p, const float *co
         const size_t bytes = f->host.stab.size() * sizeof(float);
         if (e == cudaSuccess) e = cudaMalloc(&f->d_tab, bytes);
         if (e == cudaSuccess) e = cudaMemcpy(f->d_tab, f->host.stab.data(), bytes, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMalloc(&f->d_ptab, bytes);
+        if (e == cudaSuccess) e = cudaMemcpy(f->d_ptab, f->host.ptab.data(), bytes, cudaMemcpyHostToDevice);
         if (e != cudaSuccess) {
             set_error(std::string("cmgpu_fwd_filter_build: ") + cudaGetErrorString(e));
             delete f;
@@ -558,6 +710,12 @@ extern "C" int cmgpu_fwd_score_batch(const cmgpu_fwd_filter *f, void *stream, co
         if (fwd_scores) fwd_scores[k] = fwd_final(ts[k], xc[k], L);
         if (bias_scores) bias_scores[k] = bias_final(rows[k], L);
     }
+    return CMGPU_OK;
+}
+
+extern "C" int cmgpu_fwd_filter_set_kernel(cmgpu_fwd_filter *f, int kernel) {
+    if (!f || kernel < CMGPU_FWD_KERNEL_AUTO || kernel > CMGPU_FWD_KERNEL_SHARED) return CMGPU_EINVAL;
+    f->kernel = kernel;
     return CMGPU_OK;
 }
 

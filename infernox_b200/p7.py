@@ -234,6 +234,10 @@ class FwdFilter:
                                                 eo.ctypes.data, t1.ctypes.data))
         return rfv, tr, eo, t1
 
+    def set_kernel(self, shared: bool):
+        """Force the shared-memory Forward kernel (True) or let the filter pick (False)."""
+        N.check(N.lib().cmgpu_fwd_filter_set_kernel(self._h, 1 if shared else 0))
+
     def stats(self):
         """(kernel ms, Forward cells, launches) of the last call."""
         ms, cells, launches = C.c_double(), C.c_int64(), C.c_int32()

@@ -9,6 +9,9 @@
 * genomic_kat.json: the random genomic sequences of cmcalibrate's generator
   for seed 181 that the reference's test `rng_sample_matches_c` pins against
   C Infernal (src/cm_calibrate.rs:1253-1268).
+* cm_file_kat.json: the two model texts of the reference's CM reader tests
+  (`test_minimal_cm_parse`, `test_v1_1_cm_parse`, src/cm_file.rs:2155-2212)
+  with the name / states / nodes / clen those tests assert.
 * scan_small.json: the oracle's hits on one fixed seeded model and sequence,
   a regression lock for the oracle itself.
 
@@ -63,6 +66,19 @@ def genomic_kats():
     return {"source": "src/cm_calibrate.rs:1253-1268", "seed": seed, "L": length, "sequences": seqs}
 
 
+def cm_file_kats():
+    src = open(os.path.join(REF, "src", "cm_file.rs")).read()
+    out = []
+    for test in ("fn test_minimal_cm_parse", "fn test_v1_1_cm_parse"):
+        body = src[src.index(test):]
+        body = body[: body.index("\n    }\n")]
+        text = re.search(r'let cm_text = r#"(.*?)"#;', body, re.S).group(1)
+        want = dict(re.findall(r"assert_eq!\(cm\.(\w+), ([^)]+)\);", body))
+        out.append({"test": test[3:], "text": text, "name": want["name"].strip('"'), "M": int(want["m"]),
+                    "nodes": int(want["nodes"]), "clen": int(want["clen"])})
+    return {"source": "src/cm_file.rs:2155-2212", "models": out}
+
+
 def scan_small():
     sys.path.insert(0, ROOT)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -90,6 +106,8 @@ def main():
             json.dump(state_delta_kats(), f, indent=1)
         with open(os.path.join(HERE, "genomic_kat.json"), "w") as f:
             json.dump(genomic_kats(), f, indent=1)
+        with open(os.path.join(HERE, "cm_file_kat.json"), "w") as f:
+            json.dump(cm_file_kats(), f, indent=1)
     with open(os.path.join(HERE, "scan_small.json"), "w") as f:
         json.dump(scan_small(), f, indent=1)
 

@@ -37,12 +37,14 @@ def bits(a):
     return np.ascontiguousarray(a, np.float32).view(np.uint32)
 
 
-def test_fwd_and_bias_match_oracle_on_reference_grid():
+@pytest.mark.parametrize("shared", [False, True], ids=["auto", "shared"])
+def test_fwd_and_bias_match_oracle_on_reference_grid(shared):
     n = 0
     for p, seqs in reference_grid():
         buf, wins, offs, lens = frames_of(seqs)
         compo = mean_composition(p)
         f = FwdFilter(p, compo)
+        f.set_kernel(shared)
         fs, bs = f.score_batch(buf, wins)
         ofs, _, _ = oracle.fwd_score_batch(p.M, p.mat, p.trans, buf, offs, lens)
         obs, _ = oracle.bias_score_batch(compo, p.M, buf, offs, lens)
@@ -53,8 +55,9 @@ def test_fwd_and_bias_match_oracle_on_reference_grid():
     assert n == 21 * 8 * len(LS)
 
 
-@pytest.mark.parametrize("m", [99, 100, 120, 256, 400, 1500])
-def test_fwd_long_windows_planted_homologs(m):
+@pytest.mark.parametrize("shared", [False, True], ids=["auto", "shared"])
+@pytest.mark.parametrize("m", [29, 99, 100, 120, 128, 256, 400, 1500])
+def test_fwd_long_windows_planted_homologs(m, shared):
     """Long windows with planted consensus runs: the Forward mass grows past
     the 1e4 rescaling threshold many times; M = 99 / 100 straddle the switch
     from four fixed D passes to the early-stopping ones."""
@@ -64,6 +67,7 @@ def test_fwd_long_windows_planted_homologs(m):
     buf, wins, offs, lens = frames_of(seqs)
     compo = mean_composition(p)
     f = FwdFilter(p, compo)
+    f.set_kernel(shared)
     fs, bs = f.score_batch(buf, wins)
     ofs, ots, _ = oracle.fwd_score_batch(m, p.mat, p.trans, buf, offs, lens)
     obs, _ = oracle.bias_score_batch(compo, m, buf, offs, lens)
