@@ -5,7 +5,8 @@ chunks), and the filter/banded stages of the default pipeline --
 "f1-ssv" (SSV windows over 100 kb chunks, both strands, of a 4.6 Mb
 sequence, F1 = 0.35), "f2-vit" (Viterbi filter over F1-sized windows),
 "f3-fwd" (local Forward filter and its composition-bias null over the same
-windows), "hb-cyk" / "hb-inside" (HMM-banded CYK / float Inside over envelopes with
+windows), "f3-cascade" (the whole F1 -> F3b pass of f3_filter_sequence over
+the 4.6 Mb sequence), "hb-cyk" / "hb-inside" (HMM-banded CYK / float Inside over envelopes with
 CP9-shaped bands), "hb-trcyk" (truncated HMM-banded CYK, 5'-and-3' pass, all
 four planes), "trq-inside" / "trq-cyk" (the truncated non-banded integer
 TrInside / QDB1 TrCYK window scan, 5'-and-3' pass, over short sequences that
@@ -54,7 +55,7 @@ WORKLOADS = {
     "nohmm-cyk-filter": dict(clen=72, paired=None, nbif=2, sseed=0, pseed=11, semiring=0, band=1,
                              median=100000, sigma=0.0, lo=100000, hi=100000, gc=0.50),
 }
-FILTER_WORKLOADS = ("f1-ssv", "f2-vit", "f3-fwd", "hb-cyk", "hb-inside", "hb-trcyk", "trq-inside", "trq-cyk")
+FILTER_WORKLOADS = ("f1-ssv", "f2-vit", "f3-fwd", "f3-cascade", "hb-cyk", "hb-inside", "hb-trcyk", "trq-inside", "trq-cyk")
 OPS_PER_TERM = {0: 2.0, 1: 7.0}   # CYK: FADD + select; Inside: 6 INT + 1 LDS
 OPS_PER_CELL = 2.0                # emission add + store
 CUTOFF_BITS = 15.0                # stands in for the E-value threshold
@@ -551,11 +552,12 @@ def main():
 FILTER_OPS_PER_CELL = {"f1-ssv": 4.0, "f2-vit": 14.0, "f3-fwd": 16.0, "hb-cyk": 8.0, "hb-inside": 29.0, "hb-trcyk": 24.0}
 FILTER_METRIC = {"f1-ssv": "F1 SSV window scan Gcells/s", "f2-vit": "F2 Viterbi filter Gcells/s",
                  "f3-fwd": "F3 Forward filter Gcells/s (with the F3b bias null)",
+                 "f3-cascade": "F1 -> F3b filter pass Mres/s (f3_filter_sequence, both strands)",
                  "hb-cyk": "HMM-banded CYK Gcells/s", "hb-inside": "HMM-banded Inside Gcells/s",
                  "hb-trcyk": "truncated HMM-banded CYK Gcells/s (band cells, 4 planes each)",
                  "trq-inside": "truncated non-banded TrInside Gcells/s (J-plane cells, 4 planes each)",
                  "trq-cyk": "truncated QDB TrCYK Gcells/s (J-plane cells, 4 planes each)"}
-FILTER_DTYPE = {"f1-ssv": "u8 (packed s16x2)", "f2-vit": "i16", "f3-fwd": "f32", "hb-cyk": "f32", "hb-inside": "f32",
+FILTER_DTYPE = {"f1-ssv": "u8 (packed s16x2)", "f2-vit": "i16", "f3-fwd": "f32", "f3-cascade": "u8/f32", "hb-cyk": "f32", "hb-inside": "f32",
                 "hb-trcyk": "f32", "trq-inside": "i32", "trq-cyk": "f32"}
 
 
@@ -625,12 +627,21 @@ def filter_main(args):
     from infernox_b200 import hb, model, p7, synth
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     config = {"workload": kind, "parallelism": f"dp{world}", "l2": "flushed (256 MB write) before each timed step"}
-    if kind in ("f1-ssv", "f2-vit", "f3-fwd"):
+    unit, div = ("Mres/s", 1e6) if kind == "f3-cascade" else ("Gcells/s", 1e9)
+    if kind in ("f1-ssv", "f2-vit", "f3-fwd", "f3-cascade"):
         M = 120
         prof, cons = p7.synthetic_profile(M, 77, 0.6)
         maxl = int(1.25 * M)
         mmu, mlam, f1 = -8.0, 0.693, 0.35
-        if kind == "f1-ssv":
+        if kind == "f3-cascade":
+            buf, wins = _chunks(4_600_000, 100_000, rng, cons, 40, 0.508)
+            f3, f3b, ftau, flam, cmw = 0.02, 0.02, -6.0, 0.69, 148
+            compo = p7.mean_composition(prof)
+            config.update({"model": f"synthetic p7 profile M={M} (peak 0.6)",
+                           "sequence": "4.6 Mb, both strands, 100 kb chunks, 40 planted consensus runs",
+                           "stages": "F1 SSV windows (F1 = 0.35), F3 Forward and F3b bias (0.02, the <2 Mb "
+                                     "thresholds), merge", "lftau": ftau, "lflambda": flam, "cmw": cmw})
+        elif kind == "f1-ssv":
             buf, wins = _chunks(4_600_000, 100_000, rng, cons, 40, 0.508)
             config.update({"model": f"synthetic p7 profile M={M} (peak 0.6)",
                            "sequence": "4.6 Mb, both strands, 100 kb chunks, 40 planted consensus runs",
@@ -639,7 +650,7 @@ def filter_main(args):
             buf, wins = _chunks(2_000_000, 2 * maxl, rng, cons, 40, 0.508)
             config.update({"model": f"synthetic p7 profile M={M} (peak 0.6)",
                            "windows": f"{len(wins)} windows of {2 * maxl} residues (2 Mb, both strands)"})
-        cells_step = int((wins["j0"] - wins["i0"] + 1).sum()) * M
+        cells_step = int((wins["j0"] - wins["i0"] + 1).sum()) * (1 if kind == "f3-cascade" else M)
     elif kind in ("trq-inside", "trq-cyk"):
         cmw = WORKLOADS["batched-uneven-max"]
         cm_s = synth.synth_cm(synth.structure(cmw["clen"], cmw["paired"], cmw["nbif"], cmw["sseed"]), cmw["pseed"],
@@ -716,6 +727,13 @@ def filter_main(args):
     elif kind == "f2-vit":
         units = [(int(o), int(j)) for o, _, j in wins]
         one = lambda u: oracle.vit_score_batch(M, prof.mat, prof.trans, buf, [u[0]], [u[1]]) and u[1] * M
+    elif kind == "f3-cascade":
+        units = [(int(o), int(j)) for o, _, j in wins]
+
+        def one(u):
+            oracle.f3_filter_sequence((M, prof.mat, prof.trans), compo, ftau, flam, buf[u[0]:u[0] + u[1] + 2], f1,
+                                      f3, f3b, cmw, max_length=maxl, mmu=mmu, mlambda=mlam)
+            return u[1]
     elif kind == "f3-fwd":
         units = [(int(o), int(j)) for o, _, j in wins]
         compo = p7.mean_composition(prof)
@@ -776,7 +794,7 @@ def filter_main(args):
             for _ in range(cores):
                 ex.submit(worker)
         dt = time.perf_counter() - t0
-        return {"value": st["cells"] / dt / 1e9, "unit": "Gcells/s", "cores": cores, "kind": "port",
+        return {"value": st["cells"] / dt / div, "unit": unit, "cores": cores, "kind": "port",
                 "sample": f"{st['n']} of {len(units)} units of one step's inputs, {dt:.1f} s on {cores} threads",
                 "cells": st["cells"], "seconds": dt}
 
@@ -788,16 +806,16 @@ def filter_main(args):
             cpu_sample(per_step)
         samples = [cpu_sample(per_step) for _ in range(args.steps)]
         cells, secs = sum(x["cells"] for x in samples), sum(x["seconds"] for x in samples)
-        val = cells / secs / 1e9
-        cb = {"value": val, "unit": "Gcells/s", "cores": cores, "kind": "port",
+        val = cells / secs / div
+        cb = {"value": val, "unit": unit, "cores": cores, "kind": "port",
               "sample": f"{args.steps} steps of {per_step:.1f} s, each a bounded sample of one step's units "
                         f"on {cores} threads (after {args.warmup} warm-up samples)"}
-        print(json.dumps({"impl": "reference", "metric": FILTER_METRIC[kind], "value": val, "unit": "Gcells/s",
+        print(json.dumps({"impl": "reference", "metric": FILTER_METRIC[kind], "value": val, "unit": unit,
                           "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                           "ms_per_step": 1e3 * secs / max(1, args.steps), "higher_is_better": True,
                           "scaling": "weak", "vs_baseline": None, "dtype": FILTER_DTYPE[kind], "data": "synthetic",
                           "config": config, "cpu_baseline": cb,
-                          "e2e": {"value": val, "unit": "Gcells/s", "h2d_bytes_per_step": 0,
+                          "e2e": {"value": val, "unit": unit, "h2d_bytes_per_step": 0,
                                   "d2h_bytes_per_step": 0}}))
         return
 
@@ -817,6 +835,12 @@ def filter_main(args):
         call = lambda: f.score_batch(buf, wins)
         stats = lambda: p7.vit_stats(f)
         h2d = buf.nbytes + len(wins) * 24
+    elif kind == "f3-cascade":
+        mf = p7.MsvFilter(prof, maxl, mmu, mlam, device=local_rank)
+        f = p7.FwdFilter(prof, compo, ftau, flam, device=local_rank)
+        call = lambda: p7.f3_filter_batch(f, buf, wins, f1, f3, f3b, cmw, mf=mf)[0]
+        stats = f.stats
+        h2d = 2 * buf.nbytes + len(wins) * 16
     elif kind == "f3-fwd":
         f = p7.FwdFilter(prof, p7.mean_composition(prof), -6.0, 0.69, device=local_rank)
         call = lambda: f.score_batch(buf, wins)
@@ -870,26 +894,30 @@ def filter_main(args):
     if not _same(out, ref):
         raise RuntimeError("results differ between steps")
     kernel_ms = sum(kms) / len(kms)
-    value = cells_step / (kernel_ms / 1e3) / 1e9
-    e2e = cells_step / (statistics.mean(times) / 1e3) / 1e9
+    value = cells_step / (kernel_ms / 1e3) / div
+    e2e = cells_step / (statistics.mean(times) / 1e3) / div
     sm_mhz = clk["sm_mhz"] or 1965.0
     nsm = torch.cuda.get_device_properties(local_rank).multi_processor_count
     peak = nsm * 128 * sm_mhz * 1e6 / 1e9
     achieved = FILTER_OPS_PER_CELL[kind] * cells_step / (kernel_ms / 1e3) / 1e9
     cb = cpu_sample(args.cpu_seconds)
     metric = FILTER_METRIC[kind]
-    line = {"metric": metric, "value": value, "unit": "Gcells/s", "n_gpus": world, "steps": args.steps,
+    line = {"metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": statistics.mean(times), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
             "dtype": FILTER_DTYPE[kind],
             "data": "synthetic", "config": config,
-            "e2e": {"value": e2e, "unit": "Gcells/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": None},
+            "e2e": {"value": e2e, "unit": unit, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": None},
             "gpu_launches": launches,
             "roofline": {"bound": "issue", "achieved": achieved, "peak": peak, "unit": "Gop/s",
                          "frac": achieved / peak, "traffic": None,
                          "note": f"{FILTER_OPS_PER_CELL[kind]:.0f} lane-ops per cell; {nsm} SMs x 128 lanes x "
                                  f"{sm_mhz:.0f} MHz"},
             "cpu_baseline": cb, "clocks": clk}
+    if kind == "f3-cascade":
+        # several kernels (SSV scan and replay, Forward, bias): the kernel roofline
+        # lines belong to f1-ssv and f3-fwd
+        line["roofline"] = None
     if rank == 0:
         print(json.dumps(line))
 

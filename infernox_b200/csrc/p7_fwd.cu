@@ -22,10 +22,13 @@
 // M < 100, stopping at the first pass that changes no cell of the group for
 // M >= 100), the horizontal sum (x0 + x1) + (x2 + x3), the N/C/J/B specials
 // and the sparse rescaling at xE > 1e4, whose logarithm is taken in double
-// precision.  The rows of the window's M, D and I cells live in shared
-// memory, each group at a stride of 4 (mod 32) words so that the 32 threads
-// of a warp touch 32 banks.  Groups take windows from a device counter,
-// longest first.
+// precision.  Models with nq <= 32 keep a lane's segment of the window's M,
+// D and I rows in registers (fwd_kernel_reg); longer ones keep the rows in
+// shared memory, each group at a stride of 4 (mod 32) words so that the 32
+// threads of a warp touch 32 banks (fwd_kernel).  Groups take windows from a
+// device counter, longest first.  A D pass "changes" a cell when its bits
+// change: D values are sums of products of probabilities, never negative,
+// so that is the reference's d > old.
 //
 // Device side, bias: one thread per window, the two-state forward with
 // per-row max rescaling (:1722-1790); the length term is added on the host
@@ -271,7 +274,7 @@ __global__ void __launch_bounds__(256) fwd_kernel(const float *__restrict__ tab,
                 for (int q = 0; q < nq; q++) {
                     const float old = dmr[q * 4 + z];
                     const float dd = dcv + old;
-                    changed |= dd > old;
+                    changed |= __float_as_int(dd) ^ __float_as_int(old);  // dcv >= 0: differs iff dd > old
                     dmr[q * 4 + z] = dd;
                     dcv = dcv * T[q * (T_N * 4) + T_DD * 4 + z];
                 }
@@ -389,7 +392,7 @@ __global__ void __launch_bounds__(128) fwd_kernel_reg(const float *__restrict__ 
                     if (q < nq) {
                         const float old = dmv[q];
                         const float dd = dcv + old;
-                        changed |= dd > old;
+                        changed |= __float_as_int(dd) ^ __float_as_int(old);
                         dmv[q] = dd;
                         dcv = dcv * tdd[q];
                     }
