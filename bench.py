@@ -549,7 +549,7 @@ def main():
 # HB: per child relaxation 2 (CYK) or 9 (FLogsum), about 3 children per
 # cell, plus emission add and clamp; truncated CYK: the same over the J, L
 # and R planes (T only at bifurcations).
-FILTER_OPS_PER_CELL = {"f1-ssv": 4.0, "f2-vit": 14.0, "f3-fwd": 16.0, "hb-cyk": 8.0, "hb-inside": 29.0, "hb-trcyk": 24.0}
+FILTER_OPS_PER_CELL = {"f1-ssv": 4.0, "f2-vit": 14.0, "f3-fwd": 16.0, "f3-cascade": 0.0, "hb-cyk": 8.0, "hb-inside": 29.0, "hb-trcyk": 24.0}
 FILTER_METRIC = {"f1-ssv": "F1 SSV window scan Gcells/s", "f2-vit": "F2 Viterbi filter Gcells/s",
                  "f3-fwd": "F3 Forward filter Gcells/s (with the F3b bias null)",
                  "f3-cascade": "F1 -> F3b filter pass Mres/s (f3_filter_sequence, both strands)",

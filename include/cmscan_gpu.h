@@ -495,6 +495,10 @@ int cmgpu_tr_qdb_scan_batch(const cmgpu_model *m, void *stream, int semiring, in
  * the call fails with CMGPU_ETIMEOUT instead of hanging; -1 clears it.  The
  * model stays usable. */
 int cmgpu_tr_qdb_inject_stall(cmgpu_model *m, int32_t column);
+/* Device memory the truncated QDB scan may hold in window decks at once
+ * (each resident window has its own; the grid is cut to fit).  0 restores
+ * the default, 4 GiB. */
+int cmgpu_tr_qdb_set_deck_budget(cmgpu_model *m, int64_t bytes);
 /* Device time, J-plane cells and launches of the last truncated QDB call. */
 int cmgpu_tr_qdb_stats(const cmgpu_model *m, double *kernel_ms, int64_t *cells, int32_t *launches);
 

@@ -273,6 +273,7 @@ def lib() -> C.CDLL:
                                           vp, C.c_int32, C.c_float, vp, vp, C.c_int64, P(C.c_int64)]
     L.cmgpu_tr_qdb_stats.argtypes = [vp, P(C.c_double), P(C.c_int64), P(C.c_int32)]
     L.cmgpu_tr_qdb_inject_stall.argtypes = [vp, C.c_int32]
+    L.cmgpu_tr_qdb_set_deck_budget.argtypes = [vp, C.c_int64]
     L.cmgpu_count_work.argtypes = [P(Cm), C.c_int, C.c_int, C.c_int32, P(C.c_double),
                                    P(C.c_double)]
     L.cmgpu_genomic_sample.argtypes = [C.c_uint32, C.c_int32, C.c_int32, vp]
@@ -302,7 +303,7 @@ EXPORTED = [
     "cmgpu_msv_score_batch", "cmgpu_f1_msv_windows", "cmgpu_ssv_diagonals", "cmgpu_msv_filter_stats",
     "cmgpu_fast_cyk_scan_hb", "cmgpu_hb_scan_hits", "cmgpu_hb_scan_batch", "cmgpu_hb_stats",
     "cmgpu_tr_scan_hb", "cmgpu_tr_scan_hb_batch", "cmgpu_tr_qdb_scan", "cmgpu_tr_qdb_scan_batch",
-    "cmgpu_tr_qdb_stats", "cmgpu_tr_qdb_inject_stall", "cmgpu_genomic_sample", "cmgpu_exp_fit",
+    "cmgpu_tr_qdb_stats", "cmgpu_tr_qdb_inject_stall", "cmgpu_tr_qdb_set_deck_budget", "cmgpu_genomic_sample", "cmgpu_exp_fit",
     "cmgpu_calibrate_scan_batch", "cmgpu_calibrate", "cmgpu_fwd_filter_build", "cmgpu_fwd_filter_free",
     "cmgpu_fwd_filter_tables", "cmgpu_fwd_score_batch", "cmgpu_f3_filter", "cmgpu_fwd_filter_stats", "cmgpu_fwd_filter_set_kernel",
 ]

@@ -39,6 +39,7 @@
 #include <cmath>
 #include <cstring>
 #include <numeric>
+#include <utility>
 #include <string>
 #include <vector>
 
@@ -311,26 +312,24 @@ __global__ void __launch_bounds__(256) fwd_kernel(const float *__restrict__ tab,
 }
 
 // The same recurrence with a lane's segment of the M, D and I rows in
-// registers (nq <= NQ; the loops run to NQ with the cells past nq
-// skipped), the lane's eight transition values of a cell read as two
-// 16-byte words, and its D->D values held in registers for the window.
-template <int NQ>
-__global__ void __launch_bounds__(128) fwd_kernel_reg(const float *__restrict__ ptab, int M, int nq, int rq,
+// registers: NQ = nq exactly (one instantiation per segment length, so no
+// cell needs a bounds test), the lane's seven transition values of a cell
+// read from shared memory as two 16-byte words, D->D read per pass.  LAZY:
+// M >= 100, the D passes stop at the first one that changes no cell.
+template <int NQ, bool LAZY>
+__global__ void __launch_bounds__(128, 3) fwd_kernel_reg(const float *__restrict__ ptab, int rq,
                                                       const uint8_t *__restrict__ dsq,
                                                       const FwdWin *__restrict__ wins, int nwin,
                                                       int *__restrict__ next, float2 *__restrict__ out) {
     extern __shared__ __align__(16) float sm[];
-    const int tabn = nq * T_N * 4 + KP * rq * 4;
+    const int tabn = NQ * T_N * 4 + KP * rq * 4;
     for (int q = threadIdx.x; q < tabn; q += blockDim.x) sm[q] = ptab[q];
     __syncthreads();
     const int lane = threadIdx.x & 31, z = lane & 3;
     const unsigned gmask = 0xFu << (lane & ~3);
-    const float4 *T4 = reinterpret_cast<const float4 *>(sm);
-    const float *R0 = sm + nq * T_N * 4;
-    const bool lazy = M >= 100;
-    float tdd[NQ];
-#pragma unroll
-    for (int q = 0; q < NQ; q++) tdd[q] = q < nq ? sm[(q * 4 + z) * T_N + T_DD] : 0.0f;
+    const float4 *T4 = reinterpret_cast<const float4 *>(sm) + z * 2;
+    const float *TD = sm + z * T_N + T_DD;
+    const float *R0 = sm + NQ * T_N * 4 + z;
     float mmv[NQ], dmv[NQ], imv[NQ];
     for (;;) {
         int w = 0;
@@ -342,72 +341,59 @@ __global__ void __launch_bounds__(128) fwd_kernel_reg(const float *__restrict__ 
         const int L = win.L;
 #pragma unroll
         for (int q = 0; q < NQ; q++) mmv[q] = dmv[q] = imv[q] = 0.0f;
-        float lastm = 0.0f, lastd = 0.0f, lasti = 0.0f;  // the cells at q = nq - 1
         const float pmove = 3.0f / ((float)L + 2.0f + 1.0f);
         const float ploop = 1.0f - pmove;
         float xn = 1.0f, xj = 0.0f, xb = pmove, xc = 0.0f, tot = 0.0f;
         for (int i = 1; i <= L; i++) {
-            const float *rf = R0 + (int)d[i] * rq * 4 + z;
-            float mpv = lane_shift(gmask, lastm, z);
-            float dpv = lane_shift(gmask, lastd, z);
-            float ipv = lane_shift(gmask, lasti, z);
+            const float *rf = R0 + (int)d[i] * rq * 4;
+            float mpv = lane_shift(gmask, mmv[NQ - 1], z);
+            float dpv = lane_shift(gmask, dmv[NQ - 1], z);
+            float ipv = lane_shift(gmask, imv[NQ - 1], z);
             float dcv = 0.0f, xev = 0.0f;
 #pragma unroll
             for (int q = 0; q < NQ; q++) {
-                if (q < nq) {
-                    const float4 ta = T4[(q * 4 + z) * 2], tb = T4[(q * 4 + z) * 2 + 1];
-                    float sv = xb * ta.x;
-                    sv = sv + mpv * ta.y;
-                    sv = sv + ipv * ta.z;
-                    sv = sv + dpv * ta.w;
-                    sv = sv * rf[q * 4];
-                    xev = xev + sv;
-                    mpv = mmv[q];
-                    dpv = dmv[q];
-                    ipv = imv[q];
-                    mmv[q] = sv;
-                    dmv[q] = dcv;
-                    dcv = sv * tb.x;
-                    imv[q] = mpv * tb.y + ipv * tb.z;
-                    if (q == nq - 1) {
-                        lastm = mmv[q];
-                        lasti = imv[q];
-                    }
-                }
+                const float4 ta = T4[q * 8], tb = T4[q * 8 + 1];
+                float sv = xb * ta.x;
+                sv = sv + mpv * ta.y;
+                sv = sv + ipv * ta.z;
+                sv = sv + dpv * ta.w;
+                sv = sv * rf[q * 4];
+                xev = xev + sv;
+                mpv = mmv[q];
+                dpv = dmv[q];
+                ipv = imv[q];
+                mmv[q] = sv;
+                dmv[q] = dcv;
+                dcv = sv * tb.x;
+                imv[q] = mpv * tb.y + ipv * tb.z;
             }
             dcv = lane_shift(gmask, dcv, z);
             dmv[0] = 0.0f;
 #pragma unroll
-            for (int q = 0; q < NQ; q++)
-                if (q < nq) {
-                    const float dd = dcv + dmv[q];
-                    dmv[q] = dd;
-                    dcv = dd * tdd[q];
-                }
+            for (int q = 0; q < NQ; q++) {
+                const float dd = dcv + dmv[q];
+                dmv[q] = dd;
+                dcv = dd * TD[q * 32];
+            }
             for (int j = 1; j < 4; j++) {
                 dcv = lane_shift(gmask, dcv, z);
                 int changed = 0;
 #pragma unroll
-                for (int q = 0; q < NQ; q++)
-                    if (q < nq) {
-                        const float old = dmv[q];
-                        const float dd = dcv + old;
-                        changed |= __float_as_int(dd) ^ __float_as_int(old);
-                        dmv[q] = dd;
-                        dcv = dcv * tdd[q];
-                    }
-                if (lazy) {
+                for (int q = 0; q < NQ; q++) {
+                    const float old = dmv[q];
+                    const float dd = dcv + old;
+                    if (LAZY) changed |= __float_as_int(dd) ^ __float_as_int(old);
+                    dmv[q] = dd;
+                    dcv = dcv * TD[q * 32];
+                }
+                if (LAZY) {
                     changed |= __shfl_xor_sync(gmask, changed, 1, 4);
                     changed |= __shfl_xor_sync(gmask, changed, 2, 4);
                     if (!changed) break;
                 }
             }
 #pragma unroll
-            for (int q = 0; q < NQ; q++)
-                if (q < nq) {
-                    xev = xev + dmv[q];
-                    if (q == nq - 1) lastd = dmv[q];
-                }
+            for (int q = 0; q < NQ; q++) xev = xev + dmv[q];
             const float h = xev + __shfl_sync(gmask, xev, (z + 1) & 3, 4);
             const float xe = __shfl_sync(gmask, h, 0, 4) + __shfl_sync(gmask, h, 2, 4);
             xn = xn * ploop;
@@ -426,14 +412,21 @@ __global__ void __launch_bounds__(128) fwd_kernel_reg(const float *__restrict__ 
                     dmv[q] *= inv;
                     imv[q] *= inv;
                 }
-                lastm *= inv;
-                lastd *= inv;
-                lasti *= inv;
                 tot += (float)log((double)xe);
             }
         }
         if (z == 0) out[w] = make_float2(tot, xc);
     }
+}
+
+typedef void (*FwdRegFn)(const float *, int, const uint8_t *, const FwdWin *, int, int *, float2 *);
+
+// the register kernel for segment length nq (2..32) and the D-pass rule
+template <int... Q>
+FwdRegFn fwd_reg_kernel(int nq, bool lazy, std::integer_sequence<int, Q...>) {
+    static const FwdRegFn fixed[] = {fwd_kernel_reg<Q + 2, false>...};
+    static const FwdRegFn early[] = {fwd_kernel_reg<Q + 2, true>...};
+    return (lazy ? early : fixed)[nq - 2];
 }
 
 // bias_filter_score before its length term, one thread per window
@@ -578,15 +571,13 @@ int score_windows(const cmgpu_fwd_filter *f, cudaStream_t st, const uint8_t *dsq
     const bool regs = nq <= 32 && f->kernel != CMGPU_FWD_KERNEL_SHARED;
     if (nf > 0 && regs) {
         // the segment of each lane fits in registers
-        auto kern = nq <= 8 ? cmx::dev::fwd_kernel_reg<8>
-                  : nq <= 16 ? cmx::dev::fwd_kernel_reg<16>
-                  : nq <= 24 ? cmx::dev::fwd_kernel_reg<24> : cmx::dev::fwd_kernel_reg<32>;
+        auto kern = cmx::dev::fwd_reg_kernel(nq, h.M >= 100, std::make_integer_sequence<int, 31>());
         const size_t rsmem = (size_t)(nq * T_N * 4 + KP * h.rq * 4) * sizeof(float);
         FWD_TRY(cmx::allow_max_dynamic_smem(kern));
         int per_sm = 0;
         FWD_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, rsmem));
         const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((nf + 31) / 32, (int64_t)sms * std::max(per_sm, 1)));
-        kern<<<grid, 128, rsmem, st>>>(f->d_ptab, h.M, nq, h.rq, d_dsq, d_w, nf, d_next, d_out);
+        kern<<<grid, 128, rsmem, st>>>(f->d_ptab, h.rq, d_dsq, d_w, nf, d_next, d_out);
         FWD_TRY(cudaGetLastError());
         mf->last_launches++;
     } else if (nf > 0) {

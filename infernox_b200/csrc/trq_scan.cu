@@ -77,6 +77,7 @@ struct TrqDev {
     int64_t last_cells = 0;
     int32_t last_launches = 0;
     int32_t stall_col = -1;  // test hook: this column never publishes its progress (next call only)
+    int64_t deck_budget = (int64_t)4 << 30;  // bytes of decks resident at once (bounds the grid)
 };
 
 void trq_free(TrqDev *t) {
@@ -959,7 +960,7 @@ int trq_batch(const cmgpu_model *mc, cudaStream_t st, int semiring, int qdbidx, 
         set_error("truncated QDB scan: the kernel does not fit on an SM (W too large)");
         return CMGPU_EINVAL;
     }
-    const int64_t budget = (int64_t)4 << 30;  // bytes of decks
+    const int64_t budget = q->deck_budget;  // bytes of decks
     int64_t grid = std::min<int64_t>({(int64_t)nw, (int64_t)occ * nsm, std::max<int64_t>(1, budget / (deck_stride * 4))});
 
     DevArena &ar = q->arena;
@@ -1141,6 +1142,15 @@ extern "C" int cmgpu_tr_qdb_inject_stall(cmgpu_model *m, int32_t column) {
     int rc = trq_prepare(m, &q);
     if (rc) return rc;
     q->stall_col = column;
+    return CMGPU_OK;
+}
+
+extern "C" int cmgpu_tr_qdb_set_deck_budget(cmgpu_model *m, int64_t bytes) {
+    if (!m || bytes < 0) return CMGPU_EINVAL;
+    TrqDev *q = nullptr;
+    int rc = trq_prepare(m, &q);
+    if (rc) return rc;
+    q->deck_budget = bytes > 0 ? bytes : ((int64_t)4 << 30);
     return CMGPU_OK;
 }
 

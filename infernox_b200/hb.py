@@ -406,3 +406,9 @@ def tr_inputs(cm_s, cfg, pass_idx: int, local: bool) -> TrInputs:
     r = PTY_ROW[int(pass_idx)]
     return TrInputs(t["lmesc"], t["rmesc"], t["pty"][r].copy(), t["lpos"], t["rpos"], int(cfg.clen), bool(local),
                     t["ilmesc"], t["irmesc"], t["ipty"][r].copy())
+
+
+def tr_qdb_set_deck_budget(sc: Scanner, nbytes: int) -> None:
+    """Device memory the truncated QDB scan may hold in window decks at once
+    (0: the default, 4 GiB)."""
+    N.check(N.lib().cmgpu_tr_qdb_set_deck_budget(sc._model, int(nbytes)))
