@@ -31,7 +31,8 @@
 // so that is the reference's d > old.
 //
 // Device side, bias: one thread per window, the two-state forward with
-// per-row max rescaling (:1722-1790); the length term is added on the host
+// per-row max rescaling (:1722-1790), on a second stream of the filter so it
+// runs beside the Forward kernel; the length term is added on the host
 // (glibc logf, as the reference).
 #include <cuda_runtime.h>
 
@@ -168,6 +169,8 @@ struct cmgpu_fwd_filter {
     float *d_tab = nullptr;
     float *d_ptab = nullptr;
     int kernel = CMGPU_FWD_KERNEL_AUTO;
+    cudaStream_t side = nullptr;  // the bias kernel runs here, beside the Forward kernel
+    cudaEvent_t fork = nullptr, join = nullptr;
     double last_ms = 0;
     int64_t last_cells = 0;
     int32_t last_launches = 0;
@@ -176,6 +179,9 @@ struct cmgpu_fwd_filter {
         arena.release();
         cudaFree(d_tab);
         cudaFree(d_ptab);
+        if (fork) cudaEventDestroy(fork);
+        if (join) cudaEventDestroy(join);
+        if (side) cudaStreamDestroy(side);
     }
 };
 
@@ -568,6 +574,18 @@ int score_windows(const cmgpu_fwd_filter *f, cudaStream_t st, const uint8_t *dsq
     FWD_TRY(cudaEventCreate(&ev0));
     FWD_TRY(cudaEventCreate(&ev1));
     FWD_TRY(cudaEventRecord(ev0, st));
+    if (bias_rows) {
+        // the bias null (one thread per window, a few CTAs) beside the Forward kernel
+        cmx::dev::BiasParams bp;
+        std::memcpy(bp.eo, h.eo, sizeof bp.eo);
+        std::memcpy(bp.t1, h.t1, sizeof bp.t1);
+        FWD_TRY(cudaEventRecord(f->fork, st));
+        FWD_TRY(cudaStreamWaitEvent(f->side, f->fork, 0));
+        cmx::dev::bias_kernel<<<(nwin + 127) / 128, 128, 0, f->side>>>(bp, d_dsq, d_w + nf, nwin, d_rows);
+        FWD_TRY(cudaGetLastError());
+        FWD_TRY(cudaEventRecord(f->join, f->side));
+        mf->last_launches++;
+    }
     const bool regs = nq <= 32 && f->kernel != CMGPU_FWD_KERNEL_SHARED;
     if (nf > 0 && regs) {
         // the segment of each lane fits in registers
@@ -592,14 +610,7 @@ int score_windows(const cmgpu_fwd_filter *f, cudaStream_t st, const uint8_t *dsq
         FWD_TRY(cudaGetLastError());
         mf->last_launches++;
     }
-    if (bias_rows) {
-        cmx::dev::BiasParams bp;
-        std::memcpy(bp.eo, h.eo, sizeof bp.eo);
-        std::memcpy(bp.t1, h.t1, sizeof bp.t1);
-        cmx::dev::bias_kernel<<<(nwin + 127) / 128, 128, 0, st>>>(bp, d_dsq, d_w + nf, nwin, d_rows);
-        FWD_TRY(cudaGetLastError());
-        mf->last_launches++;
-    }
+    if (bias_rows) FWD_TRY(cudaStreamWaitEvent(st, f->join, 0));
     FWD_TRY(cudaEventRecord(ev1, st));
     std::vector<float2> out((size_t)nf);
     if (nf > 0) FWD_TRY(cudaMemcpyAsync(out.data(), d_out, sizeof(float2) * nf, cudaMemcpyDeviceToHost, st));
@@ -657,6 +668,9 @@ extern "C" int cmgpu_fwd_filter_build(const cmgpu_p7_profile *p, const float *co
         if (e == cudaSuccess) e = cudaMemcpy(f->d_tab, f->host.stab.data(), bytes, cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMalloc(&f->d_ptab, bytes);
         if (e == cudaSuccess) e = cudaMemcpy(f->d_ptab, f->host.ptab.data(), bytes, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&f->side, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&f->fork, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&f->join, cudaEventDisableTiming);
         if (e != cudaSuccess) {
             set_error(std::string("cmgpu_fwd_filter_build: ") + cudaGetErrorString(e));
             delete f;
