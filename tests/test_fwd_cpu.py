@@ -98,3 +98,36 @@ def test_build_rejects_empty_model():
     p = P7Profile(0, np.zeros((1, 4), np.float32), np.zeros((1, 7), np.float32))
     with pytest.raises(N.CmgpuError):
         FwdFilter(p, np.full(4, 0.25, np.float32), device=-1)
+
+
+def test_oracle_cascade_merge_and_accounting():
+    """The oracle's f3_filter_sequence: survivors merged into disjoint,
+    non-abutting windows inside the chunk; with every gate open (P <= 1)
+    the result is the merge of all F1 windows and every stage counts them
+    all; tightening F3 only removes windows."""
+    from p7_helpers import peaked_profile, planted_frame
+    m = 80
+    p, cons = peaked_profile(3, m, peak=0.6)
+    fr = planted_frame(9, 20000, cons, 5)
+    kw = dict(max_length=100, mmu=-9.0, mlambda=0.69)
+    compo = mean_composition(p)
+    open_w, open_a = oracle.f3_filter_sequence((m, p.mat, p.trans), compo, -6.0, 0.69, fr, 0.5, 1.0, 1.0, 96, **kw)
+    f1w, _, _, _ = oracle.f1_msv_windows(m, p.mat, p.trans, 100, -9.0, 0.69, fr, [0], [20000], 0.5, 96)
+    assert open_a["n_past_msv"] == len(f1w) == open_a["n_past_fwd"] == open_a["n_past_fwdbias"]
+    assert open_a["pos_past_fwdbias"] == open_a["pos_past_msv"]
+    merged = []
+    for _, s, e in f1w:
+        if merged and merged[-1][1] + 1 >= s:
+            merged[-1][1] = e  # the reference takes the later window's end
+        else:
+            merged.append([s, e])
+    assert [(s, e) for s, e, _ in open_w] == [tuple(x) for x in merged]
+    tight_w, tight_a = oracle.f3_filter_sequence((m, p.mat, p.trans), compo, -6.0, 0.69, fr, 0.5, 0.01, 0.01, 96,
+                                                 **kw)
+    assert tight_a["n_past_fwdbias"] <= tight_a["n_past_fwd"] <= tight_a["n_past_msv"]
+    assert 0 < len(tight_w) <= len(open_w)
+    for (s, e, _), (s2, _, _) in zip(tight_w, tight_w[1:]):
+        assert 1 <= s <= e <= 20000 and e + 1 < s2
+    # every survivor lies inside a window of the open pass
+    for s, e, _ in tight_w:
+        assert any(a <= s and e <= b for a, b, _ in open_w)
