@@ -313,6 +313,41 @@ def f3_filter_sequence(mf: MsvFilter, ff: FwdFilter, dsq, win_len: int, f1: floa
     return [(int(r["start"]), int(r["end"]), float(r["score"])) for r in w], acct
 
 
+def pipeline_thresholds(z_residues: float) -> dict:
+    """CmPipeline::new_default (src/cm_pipeline.rs:73-112): the filter
+    thresholds and stages of the default pipeline for a database of
+    z_residues residues (both strands)."""
+    z_mb = z_residues / 1.0e6
+    t = dict(f1=0.35, f1b=1.0, f2=1.0, f2b=1.0, f3=0.02, f3b=0.02, f4=0.02, f4b=0.02, f5=0.02, f5b=1.0, f6=0.0001,
+             do_msv=True, do_msvbias=False, do_vit=True, do_vitbias=True, do_fwd=True, do_fwdbias=True)
+    if z_mb >= 20000.0:
+        t.update(f1=0.06, f2=0.02, f2b=0.02, f3=0.0002, f3b=0.0002, f4=0.0002, f4b=0.0002, f5=0.0002)
+    elif z_mb >= 2000.0:
+        t.update(f1=0.15, f2=0.15, f2b=0.15, f3=0.0002, f3b=0.0002, f4=0.0002, f4b=0.0002, f5=0.0002)
+    elif z_mb >= 200.0:
+        t.update(f1=0.15, f2=0.15, f2b=0.15, f3=0.0008, f3b=0.0008, f4=0.0008, f4b=0.0008, f5=0.0008)
+    elif z_mb >= 20.0:
+        t.update(f1=0.35, f2=0.15, f2b=0.15, f3=0.003, f3b=0.003, f4=0.003, f4b=0.003, f5=0.003)
+    elif z_mb >= 2.0:
+        t.update(f1=0.35, do_vit=False, do_vitbias=False, f2=1.0, f2b=1.0, f3=0.005, f3b=0.005, f4=0.005,
+                 f4b=0.005, f5=0.005)
+    else:
+        t.update(f1=0.35, do_vit=False, do_vitbias=False, f2=1.0, f2b=1.0, f3=0.02, f3b=0.02, f4=0.02, f4b=0.02,
+                 f5=0.02)
+    return t
+
+
+def f3_pass_for_database(ff: FwdFilter, mf: MsvFilter, vf: VitFilter, buf, chunks, z_residues: float, cmw: int,
+                         lvmu: float = 0.0, lvlambda: float = 1.0):
+    """The F1 -> F3b pass of the default pipeline for a database of
+    z_residues residues: thresholds and stages from pipeline_thresholds (the
+    Viterbi stage from 20 Mb up), then f3_filter_batch."""
+    t = pipeline_thresholds(z_residues)
+    vit = (t["f2"], t["do_vitbias"], t["f2b"], lvmu, lvlambda) if t["do_vit"] else None
+    return f3_filter_batch(ff, buf, chunks, t["f1"], t["f3"], t["f3b"], cmw, mf=mf, vf=vf if vit else None, vit=vit,
+                           do_fwd=t["do_fwd"], do_fwdbias=t["do_fwdbias"])
+
+
 def mean_composition(p: P7Profile) -> np.ndarray:
     """Mean match emission over the model: the composition a synthetic
     profile's bias filter uses (profiles read from a file carry their own)."""

@@ -12,6 +12,9 @@
 * cm_file_kat.json: the two model texts of the reference's CM reader tests
   (`test_minimal_cm_parse`, `test_v1_1_cm_parse`, src/cm_file.rs:2155-2212)
   with the name / states / nodes / clen those tests assert.
+* pipeline_kat.json: the filter thresholds per database size that the
+  reference's `thresholds_match_c_table` test asserts
+  (src/cm_pipeline.rs:2170-2187).
 * scan_small.json: the oracle's hits on one fixed seeded model and sequence,
   a regression lock for the oracle itself.
 
@@ -79,6 +82,22 @@ def cm_file_kats():
     return {"source": "src/cm_file.rs:2155-2212", "models": out}
 
 
+def pipeline_kats():
+    src = open(os.path.join(REF, "src", "cm_pipeline.rs")).read()
+    body = src[src.index("fn thresholds_match_c_table"):]
+    body = body[: body.index("\n    }\n")]
+    cases = []
+    for blk in body.split("let p = CmPipeline::new_default(")[1:]:
+        z = float(blk[: blk.index(")")])
+        want = {}
+        for k, v in re.findall(r"assert_eq!\(p\.(\w+), ([0-9.e-]+)\);", blk):
+            want[k] = float(v)
+        for neg, k in re.findall(r"assert!\((!?)p\.(\w+)\);", blk):
+            want[k] = not neg
+        cases.append({"z": z, "want": want})
+    return {"source": "src/cm_pipeline.rs:2170-2187", "cases": cases}
+
+
 def scan_small():
     sys.path.insert(0, ROOT)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -108,6 +127,8 @@ def main():
             json.dump(genomic_kats(), f, indent=1)
         with open(os.path.join(HERE, "cm_file_kat.json"), "w") as f:
             json.dump(cm_file_kats(), f, indent=1)
+        with open(os.path.join(HERE, "pipeline_kat.json"), "w") as f:
+            json.dump(pipeline_kats(), f, indent=1)
     with open(os.path.join(HERE, "scan_small.json"), "w") as f:
         json.dump(scan_small(), f, indent=1)
 

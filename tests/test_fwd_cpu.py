@@ -131,3 +131,19 @@ def test_oracle_cascade_merge_and_accounting():
     # every survivor lies inside a window of the open pass
     for s, e, _ in tight_w:
         assert any(a <= s and e <= b for a, b, _ in open_w)
+
+
+def test_pipeline_thresholds_match_reference_test():
+    """The reference's own thresholds_match_c_table cases (C's
+    cm_pipeline_Create table), and the band edges of that table."""
+    import json
+    import os
+    from infernox_b200.p7 import pipeline_thresholds
+    kat = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "pipeline_kat.json")))
+    assert len(kat["cases"]) == 3
+    for c in kat["cases"]:
+        t = pipeline_thresholds(c["z"])
+        for k, v in c["want"].items():
+            assert t[k] == v, (c["z"], k)
+    assert pipeline_thresholds(1.999e6)["f3"] == 0.02 and pipeline_thresholds(2.0e6)["f3"] == 0.005
+    assert pipeline_thresholds(20e9)["f1"] == 0.06 and pipeline_thresholds(19.9e9)["f1"] == 0.15
