@@ -171,6 +171,7 @@ struct cmgpu_fwd_filter {
     int kernel = CMGPU_FWD_KERNEL_AUTO;
     cudaStream_t side = nullptr;  // the bias kernel runs here, beside the Forward kernel
     cudaEvent_t fork = nullptr, join = nullptr;
+    cudaEvent_t t0 = nullptr, t1 = nullptr;  // device time of a call
     double last_ms = 0;
     int64_t last_cells = 0;
     int32_t last_launches = 0;
@@ -181,6 +182,8 @@ struct cmgpu_fwd_filter {
         cudaFree(d_ptab);
         if (fork) cudaEventDestroy(fork);
         if (join) cudaEventDestroy(join);
+        if (t0) cudaEventDestroy(t0);
+        if (t1) cudaEventDestroy(t1);
         if (side) cudaStreamDestroy(side);
     }
 };
@@ -570,9 +573,7 @@ int score_windows(const cmgpu_fwd_filter *f, cudaStream_t st, const uint8_t *dsq
         return CMGPU_ENOSPACE;
     }
     const size_t smem = smem_words(threads) * 4;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    FWD_TRY(cudaEventCreate(&ev0));
-    FWD_TRY(cudaEventCreate(&ev1));
+    cudaEvent_t ev0 = f->t0, ev1 = f->t1;
     FWD_TRY(cudaEventRecord(ev0, st));
     if (bias_rows) {
         // the bias null (one thread per window, a few CTAs) beside the Forward kernel
@@ -621,8 +622,6 @@ int score_windows(const cmgpu_fwd_filter *f, cudaStream_t st, const uint8_t *dsq
     FWD_TRY(cudaStreamSynchronize(st));
     float ms = 0;
     cudaEventElapsedTime(&ms, ev0, ev1);
-    cudaEventDestroy(ev0);
-    cudaEventDestroy(ev1);
     mf->last_ms = ms;
     if (fwd_ts) {
         fwd_ts->assign(nwin, 0.0f);
@@ -671,6 +670,8 @@ extern "C" int cmgpu_fwd_filter_build(const cmgpu_p7_profile *p, const float *co
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&f->side, cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&f->fork, cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&f->join, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreate(&f->t0);
+        if (e == cudaSuccess) e = cudaEventCreate(&f->t1);
         if (e != cudaSuccess) {
             set_error(std::string("cmgpu_fwd_filter_build: ") + cudaGetErrorString(e));
             delete f;
