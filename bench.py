@@ -1,7 +1,9 @@
 """Benchmark of the batched QDB/Inside window scan (one JSON line on rank 0).
 
 Other workloads (--workload): "nohmm-cyk-filter" (QDB1 CYK over 100 kb
-chunks), and the filter/banded stages of the default pipeline --
+chunks), "cfg3-cyk" (the 1,500-column, 25-bifurcation model shape: QDB1 CYK
+over 1 kb windows, batched against one launch per window), and the
+filter/banded stages of the default pipeline --
 "f1-ssv" (SSV windows over 100 kb chunks, both strands, of a 4.6 Mb
 sequence, F1 = 0.35), "f2-vit" (Viterbi filter over F1-sized windows),
 "f3-fwd" (local Forward filter and its composition-bias null over the same
@@ -54,6 +56,11 @@ WORKLOADS = {
                                median=1500, sigma=0.78, lo=200, hi=20000, gc=0.45),
     "nohmm-cyk-filter": dict(clen=72, paired=None, nbif=2, sseed=0, pseed=11, semiring=0, band=1,
                              median=100000, sigma=0.0, lo=100000, hi=100000, gc=0.50),
+    # the bifurcation-heavy model shape (1,500 columns, 60% paired, 25
+    # bifurcations, W = 1,551): the QDB1 CYK filter scan over 1 kb windows,
+    # batched against the plain one-launch-per-window path
+    "cfg3-cyk": dict(clen=1500, paired=0.6, nbif=25, sseed=31, pseed=33, semiring=0, band=1,
+                     median=1000, sigma=0.0, lo=1000, hi=1000, gc=0.45),
 }
 FILTER_WORKLOADS = ("f1-ssv", "f2-vit", "f3-fwd", "f3-cascade", "hb-cyk", "hb-inside", "hb-trcyk", "trq-inside", "trq-cyk")
 OPS_PER_TERM = {0: 2.0, 1: 7.0}   # CYK: FADD + select; Inside: 6 INT + 1 LDS

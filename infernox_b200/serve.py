@@ -78,6 +78,13 @@ def _pad_merge(hits, W: int, n: int):
     return out
 
 
+def library_from_cm_file(src, local: bool = True) -> list:
+    """The configured CMs of a CM file -- cmscan's CM database -- in file
+    order, each keeping the W its file states (cmfile.read_cms)."""
+    from . import cmfile, model
+    return [model.configure(f.cm, local=local, W=f.W) for f in cmfile.read_cms(src)]
+
+
 class Server:
     """The request loop over a library of configured CMs on one GPU."""
 

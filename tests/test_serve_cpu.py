@@ -48,3 +48,19 @@ def test_envelopes_pad_and_merge():
     assert serve._pad_merge([(10, 20), (12, 22)], 10, 300) == [(11, 21)]
     assert serve._pad_merge([(1, 5)], 50, 30) == [(1, 30)]
     assert serve._pad_merge([], 10, 100) == []
+
+
+def test_library_from_cm_file():
+    """cmscan's CM database: a file of several models becomes the serving
+    library, each model configured locally with the W its file states."""
+    from infernox_b200 import cmfile, model, synth
+    cms = [synth.synth_cm(synth.structure(c, 0.4, b, s), s, name=f"lib{s}") for c, b, s in
+           ((40, 0, 1), (90, 1, 2), (60, 2, 3))]
+    text = "".join(cmfile.write_cm(cm) for cm in cms)
+    lib = serve.library_from_cm_file(text)
+    assert [m.name for m in lib] == ["lib1", "lib2", "lib3"]
+    assert all(m.local for m in lib)
+    assert [m.W for m in lib] == [model.configure(cm, local=False).W for cm in cms]
+    s = serve.Server(lib, budget_residues=10_000)
+    assert s.submit(_req(1, 100)) == serve.OK
+    s.close()
