@@ -15,6 +15,9 @@
 * pipeline_kat.json: the filter thresholds per database size that the
   reference's `thresholds_match_c_table` test asserts
   (src/cm_pipeline.rs:2170-2187).
+* histogram_kat.json: the exponential tail fit of the reference's
+  `test_cmcalibrate_sequence` (src/easel/histogram.rs:543-586), whose mu and
+  lambda the reference pins to a probe of C libeasel.
 * scan_small.json: the oracle's hits on one fixed seeded model and sequence,
   a regression lock for the oracle itself.
 
@@ -98,6 +101,19 @@ def pipeline_kats():
     return {"source": "src/cm_pipeline.rs:2170-2187", "cases": cases}
 
 
+def histogram_kats():
+    src = open(os.path.join(REF, "src", "easel", "histogram.rs")).read()
+    body = src[src.index("fn test_cmcalibrate_sequence"):]
+    body = body[: body.index("\n    }\n")]
+    scores = [float(x) for x in re.search(r"let scores = \[(.*?)\];", body, re.S).group(1).replace("\n", " ").split(",")
+              if x.strip()]
+    mass = float(re.search(r"get_tail_by_mass\(([0-9.]+)\)", body).group(1))
+    mu = re.search(r"assert_eq!\(mu, ([0-9.e-]+)\);", body).group(1)
+    lam = re.search(r"assert_eq!\(lambda, ([0-9.e-]+)\);", body).group(1)
+    return {"source": "src/easel/histogram.rs:543-586", "scores": scores, "tail_mass": mass, "mu": mu,
+            "lambda": lam}
+
+
 def scan_small():
     sys.path.insert(0, ROOT)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -129,6 +145,8 @@ def main():
             json.dump(cm_file_kats(), f, indent=1)
         with open(os.path.join(HERE, "pipeline_kat.json"), "w") as f:
             json.dump(pipeline_kats(), f, indent=1)
+        with open(os.path.join(HERE, "histogram_kat.json"), "w") as f:
+            json.dump(histogram_kats(), f, indent=1)
     with open(os.path.join(HERE, "scan_small.json"), "w") as f:
         json.dump(scan_small(), f, indent=1)
 

@@ -87,3 +87,34 @@ def test_n_sequences_rounds_like_reference():
     assert cal.n_sequences(cal.CalibrateConfig(l_mb=0.02)) == 2
     assert cal.n_sequences(cal.CalibrateConfig(l_mb=0.005)) == 1
     assert cal.n_sequences(cal.CalibrateConfig(l_mb=0.004)) == 0
+
+
+def _fit_complete(xs):
+    """esl_exp_FitComplete (src/easel/exponential.rs:67-89): mu = the lowest
+    tail score, lambda = 1 / mean(x - mu), summed in tail order."""
+    mu = min(xs)
+    mean = 0.0
+    for x in xs:
+        mean += x - mu
+    return mu, 1.0 / (mean / len(xs))
+
+
+def test_tail_fit_matches_the_libeasel_probe():
+    """The reference's test_cmcalibrate_sequence: the tail of mass 0.5 of its
+    20 scores fitted by esl_exp_FitComplete gives the mu and lambda it pins to
+    a probe of C libeasel.  The formula reproduces them bit for bit on those
+    (double) scores, and the library's tail fit -- fed the same scores as the
+    floats cmcalibrate's scans produce -- returns that formula's value on the
+    floats, in every exp mode."""
+    kat = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "histogram_kat.json")))
+    s64 = kat["scores"]
+    n = int(len(s64) * kat["tail_mass"])
+    mu, lam = _fit_complete(sorted(s64)[len(s64) - n:])
+    assert mu == float(kat["mu"]) and lam == float(kat["lambda"])
+    s32 = np.asarray(s64, np.float32)
+    fmu, flam = _fit_complete(sorted(float(x) for x in s32)[len(s64) - n:])
+    for mode in range(4):
+        r = cal.fit_histogram(s32, mode, 1, 10000, tailp=kat["tail_mass"], dbsize=1.0)
+        assert np.float64(r["mu_orig"]).tobytes() == np.float64(fmu).tobytes()
+        assert np.float64(r["lambda_"]).tobytes() == np.float64(flam).tobytes()
+        assert r["nrandhits"] == len(s64)
