@@ -732,8 +732,11 @@ def filter_main(args):
         one = lambda u: oracle.f1_msv_windows(M, prof.mat, prof.trans, maxl, mmu, mlam, buf, [u[0]], [u[1]], f1,
                                               maxl) and u[1] * M
     elif kind == "f2-vit":
-        units = [(int(o), int(j)) for o, _, j in wins]
-        one = lambda u: oracle.vit_score_batch(M, prof.mat, prof.trans, buf, [u[0]], [u[1]]) and u[1] * M
+        # 64 windows per oracle call: the filter is built once per call, as the
+        # reference builds it once per search
+        units = [(wins["dsq_offset"][a:a + 64].astype(np.int64), wins["j0"][a:a + 64].astype(np.int32))
+                 for a in range(0, len(wins), 64)]
+        one = lambda u: oracle.vit_score_batch(M, prof.mat, prof.trans, buf, u[0], u[1]) and int(u[1].sum()) * M
     elif kind == "f3-cascade":
         units = [(int(o), int(j)) for o, _, j in wins]
 
@@ -742,13 +745,15 @@ def filter_main(args):
                                       f3, f3b, cmw, max_length=maxl, mmu=mmu, mlambda=mlam)
             return u[1]
     elif kind == "f3-fwd":
-        units = [(int(o), int(j)) for o, _, j in wins]
+        # 64 windows per oracle call (the SSE2 engine, the reference's x86 path)
+        units = [(wins["dsq_offset"][a:a + 64].astype(np.int64), wins["j0"][a:a + 64].astype(np.int32))
+                 for a in range(0, len(wins), 64)]
         compo = p7.mean_composition(prof)
 
         def one(u):
-            oracle.fwd_score_batch(M, prof.mat, prof.trans, buf, [u[0]], [u[1]])
-            oracle.bias_score_batch(compo, M, buf, [u[0]], [u[1]])
-            return u[1] * M
+            oracle.fwd_score_batch(M, prof.mat, prof.trans, buf, u[0], u[1])
+            oracle.bias_score_batch(compo, M, buf, u[0], u[1])
+            return int(u[1].sum()) * M
     elif kind in ("trq-inside", "trq-cyk"):
         units = list(range(len(wins)))
         ttab = {"lmesc": tri.lmesc, "rmesc": tri.rmesc, "pty": tri.pty, "ilmesc": tri.ilmesc, "irmesc": tri.irmesc,

@@ -206,6 +206,126 @@ static float fwd_score(const fwdf *f, const uint8_t *dsq, int L, float *ret_tots
     return (float)((double)totscale + log((double)xc * (double)pmove));
 }
 
+#ifdef __SSE2__
+#include <emmintrin.h>
+
+/* The same engine on 128-bit vectors, as the reference runs it on x86: the
+ * striped tables are packed once per profile (tmain[q][7][4] = BM, MM, IM,
+ * DM, MD, MI, II; tdd[q][4]; rfv[x][q][4]) and every step above is one
+ * packed op over the four lanes.  Bit-identical to fwd_score (the lanes are
+ * independent except at the same shifts and sums); the timed CPU baseline. */
+typedef struct {
+    int m, nq;
+    float *tmain, *tdd, *rfv;
+} fwdv;
+
+static void fwdv_build(const fwdf *f, fwdv *v) {
+    const int m = f->m, nq = fwd_nq(m);
+    v->m = m;
+    v->nq = nq;
+    v->tmain = (float *)aligned_alloc(16, sizeof(float) * (size_t)nq * 28);
+    v->tdd = (float *)aligned_alloc(16, sizeof(float) * (size_t)nq * 4);
+    v->rfv = (float *)aligned_alloc(16, sizeof(float) * (size_t)KP * nq * 4);
+    const float *src[7] = {f->tbm, f->amm, f->aim, f->adm, f->tmd, f->tmi, f->tii};
+    for (int q = 0; q < nq; q++)
+        for (int zz = 0; zz < 4; zz++) {
+            const int p = q + 1 + zz * nq;
+            for (int t = 0; t < 7; t++) v->tmain[q * 28 + t * 4 + zz] = at(src[t], m, p);
+            v->tdd[q * 4 + zz] = at(f->tdd, m, p);
+            for (int x = 0; x < KP; x++) v->rfv[(x * nq + q) * 4 + zz] = p <= m ? f->rfv[p * KP + x] : 0.0f;
+        }
+}
+
+static void fwdv_free(fwdv *v) {
+    free(v->tmain);
+    free(v->tdd);
+    free(v->rfv);
+}
+
+static __m128 vshift(__m128 a) { return _mm_castsi128_ps(_mm_slli_si128(_mm_castps_si128(a), 4)); }
+
+static float fwd_score_sse(const fwdv *v, const uint8_t *dsq, int L, float *ret_totscale, float *ret_xc) {
+    const int m = v->m, nq = v->nq;
+    const float nj = 1.0f;
+    const float pmove = (2.0f + nj) / ((float)L + 2.0f + nj);
+    const float ploop = 1.0f - pmove;
+    __m128 *mm = (__m128 *)aligned_alloc(16, sizeof(__m128) * (size_t)nq);
+    __m128 *dm = (__m128 *)aligned_alloc(16, sizeof(__m128) * (size_t)nq);
+    __m128 *im = (__m128 *)aligned_alloc(16, sizeof(__m128) * (size_t)nq);
+    const __m128 zero = _mm_setzero_ps();
+    for (int q = 0; q < nq; q++) mm[q] = dm[q] = im[q] = zero;
+    const __m128 *tm = (const __m128 *)v->tmain, *td = (const __m128 *)v->tdd;
+    float xn = 1.0f, xj = 0.0f, xb = pmove, xc = 0.0f, totscale = 0.0f;
+    for (int i = 1; i <= L; i++) {
+        const __m128 *rf = (const __m128 *)v->rfv + (size_t)dsq[i] * nq;
+        const __m128 xbv = _mm_set1_ps(xb);
+        __m128 dcv = zero, xev = zero;
+        __m128 mpv = vshift(mm[nq - 1]), dpv = vshift(dm[nq - 1]), ipv = vshift(im[nq - 1]);
+        for (int q = 0; q < nq; q++) {
+            const __m128 *t = tm + q * 7;
+            __m128 sv = _mm_mul_ps(xbv, t[0]);
+            sv = _mm_add_ps(sv, _mm_mul_ps(mpv, t[1]));
+            sv = _mm_add_ps(sv, _mm_mul_ps(ipv, t[2]));
+            sv = _mm_add_ps(sv, _mm_mul_ps(dpv, t[3]));
+            sv = _mm_mul_ps(sv, rf[q]);
+            xev = _mm_add_ps(xev, sv);
+            mpv = mm[q];
+            dpv = dm[q];
+            ipv = im[q];
+            mm[q] = sv;
+            dm[q] = dcv;
+            dcv = _mm_mul_ps(sv, t[4]);
+            im[q] = _mm_add_ps(_mm_mul_ps(mpv, t[5]), _mm_mul_ps(ipv, t[6]));
+        }
+        dcv = vshift(dcv);
+        dm[0] = zero;
+        for (int q = 0; q < nq; q++) {
+            dm[q] = _mm_add_ps(dcv, dm[q]);
+            dcv = _mm_mul_ps(dm[q], td[q]);
+        }
+        for (int j = 1; j < 4; j++) {
+            __m128 cv = zero;
+            dcv = vshift(dcv);
+            for (int q = 0; q < nq; q++) {
+                const __m128 d = _mm_add_ps(dcv, dm[q]);
+                cv = _mm_or_ps(cv, _mm_cmpgt_ps(d, dm[q]));
+                dm[q] = d;
+                dcv = _mm_mul_ps(dcv, td[q]);
+            }
+            if (m >= 100 && _mm_movemask_ps(cv) == 0) break;
+        }
+        for (int q = 0; q < nq; q++) xev = _mm_add_ps(xev, dm[q]);
+        xev = _mm_add_ps(xev, _mm_shuffle_ps(xev, xev, 0x39));
+        xev = _mm_add_ps(xev, _mm_shuffle_ps(xev, xev, 0x4E));
+        const float xe = _mm_cvtss_f32(xev);
+        xn = xn * ploop;
+        xc = (xc * ploop) + (xe * 0.5f);
+        xj = (xj * ploop) + (xe * 0.5f);
+        xb = (xj * pmove) + (xn * pmove);
+        if (xe > 1.0e4f) {
+            const float inv = 1.0f / xe;
+            xn *= inv;
+            xc *= inv;
+            xj *= inv;
+            xb *= inv;
+            const __m128 iv = _mm_set1_ps(inv);
+            for (int q = 0; q < nq; q++) {
+                mm[q] = _mm_mul_ps(mm[q], iv);
+                dm[q] = _mm_mul_ps(dm[q], iv);
+                im[q] = _mm_mul_ps(im[q], iv);
+            }
+            totscale += (float)log((double)xe);
+        }
+    }
+    free(mm);
+    free(dm);
+    free(im);
+    if (ret_totscale) *ret_totscale = totscale;
+    if (ret_xc) *ret_xc = xc;
+    return (float)((double)totscale + log((double)xc * (double)pmove));
+}
+#endif
+
 /* build_bias_filter (src/cm_pipeline.rs:1683-1720) */
 static void bias_build(const float *compo, int m, float *eo /* [KP][2] */, float *t1 /* [3] */) {
     const float bg = 0.25f;
@@ -283,15 +403,35 @@ int oracle_fwd_tables(int m, const float *mat, const float *trans, float *rfv, f
 }
 
 /* forward_filter_score on residues 1..lens[w] of the frame at buf + offs[w]
- * (index 0 is the leading sentinel); totscale / xc may be NULL */
-int oracle_fwd_score_batch(int m, const float *mat, const float *trans, const uint8_t *buf, const int64_t *offs,
-                           const int32_t *lens, int32_t n, float *scores, float *totscale, float *xc) {
+ * (index 0 is the leading sentinel); totscale / xc may be NULL.  The
+ * vectorised engine where the compiler has SSE2 (every x86-64), else the
+ * lane-by-lane one; oracle_fwd_score_batch_scalar always the latter. */
+int oracle_fwd_score_batch_scalar(int m, const float *mat, const float *trans, const uint8_t *buf,
+                                  const int64_t *offs, const int32_t *lens, int32_t n, float *scores, float *totscale,
+                                  float *xc) {
     fwdf f;
     fwd_build(m, mat, trans, &f);
     for (int32_t w = 0; w < n; w++)
         scores[w] = fwd_score(&f, buf + offs[w], lens[w], totscale ? totscale + w : NULL, xc ? xc + w : NULL);
     fwd_free(&f);
     return 0;
+}
+
+int oracle_fwd_score_batch(int m, const float *mat, const float *trans, const uint8_t *buf, const int64_t *offs,
+                           const int32_t *lens, int32_t n, float *scores, float *totscale, float *xc) {
+#ifdef __SSE2__
+    fwdf f;
+    fwdv v;
+    fwd_build(m, mat, trans, &f);
+    fwdv_build(&f, &v);
+    for (int32_t w = 0; w < n; w++)
+        scores[w] = fwd_score_sse(&v, buf + offs[w], lens[w], totscale ? totscale + w : NULL, xc ? xc + w : NULL);
+    fwdv_free(&v);
+    fwd_free(&f);
+    return 0;
+#else
+    return oracle_fwd_score_batch_scalar(m, mat, trans, buf, offs, lens, n, scores, totscale, xc);
+#endif
 }
 
 int oracle_bias_tables(const float *compo, int m, float *eo, float *t1) {

@@ -88,6 +88,7 @@ def lib():
                                      C.c_double, vp]
         L.oracle_fwd_tables.argtypes = [C.c_int, vp, vp, vp, vp]
         L.oracle_fwd_score_batch.argtypes = [C.c_int, vp, vp, vp, vp, vp, C.c_int32, vp, vp, vp]
+        L.oracle_fwd_score_batch_scalar.argtypes = [C.c_int, vp, vp, vp, vp, vp, C.c_int32, vp, vp, vp]
         L.oracle_bias_tables.argtypes = [vp, C.c_int, vp, vp]
         L.oracle_bias_score_batch.argtypes = [vp, C.c_int, vp, vp, vp, C.c_int32, vp, vp]
         _lib = L
@@ -262,16 +263,18 @@ def fwd_tables(M, mat, trans):
     return rfv.reshape(M + 1, 18), tr.reshape(M + 1, 8)
 
 
-def fwd_score_batch(M, mat, trans, buf, offs, lens):
-    """forward_filter_score (striped engine) per frame: (scores, totscale, xc)."""
+def fwd_score_batch(M, mat, trans, buf, offs, lens, scalar=False):
+    """forward_filter_score (striped engine) per frame: (scores, totscale, xc);
+    scalar: the lane-by-lane emulation instead of the SSE2 one."""
     mat, trans = _f32(mat), _f32(trans)
     buf = np.ascontiguousarray(buf, np.uint8)
     offs = np.ascontiguousarray(offs, np.int64)
     lens = np.ascontiguousarray(lens, np.int32)
     n = len(lens)
     sc, ts, xc = (np.zeros(n, np.float32) for _ in range(3))
-    lib().oracle_fwd_score_batch(int(M), mat.ctypes.data, trans.ctypes.data, buf.ctypes.data, offs.ctypes.data,
-                                 lens.ctypes.data, n, sc.ctypes.data, ts.ctypes.data, xc.ctypes.data)
+    fn = lib().oracle_fwd_score_batch_scalar if scalar else lib().oracle_fwd_score_batch
+    fn(int(M), mat.ctypes.data, trans.ctypes.data, buf.ctypes.data, offs.ctypes.data, lens.ctypes.data, n,
+       sc.ctypes.data, ts.ctypes.data, xc.ctypes.data)
     return sc, ts, xc
 
 

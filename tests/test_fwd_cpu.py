@@ -147,3 +147,23 @@ def test_pipeline_thresholds_match_reference_test():
             assert t[k] == v, (c["z"], k)
     assert pipeline_thresholds(1.999e6)["f3"] == 0.02 and pipeline_thresholds(2.0e6)["f3"] == 0.005
     assert pipeline_thresholds(20e9)["f1"] == 0.06 and pipeline_thresholds(19.9e9)["f1"] == 0.15
+
+
+def test_oracle_sse_engine_equals_lane_by_lane():
+    """The oracle's SSE2 engine (the timed CPU baseline, the reference's own
+    x86 code path) gives the lane-by-lane emulation's bits: on the reference
+    test's grid and on long windows with planted homologs around the M = 100
+    switch of the D passes."""
+    from p7_helpers import peaked_profile, planted_frame
+    for p, seqs in reference_grid(reps=2):
+        for d in seqs:
+            L = len(d) - 2
+            a = oracle.fwd_score_batch(p.M, p.mat, p.trans, d, [0], [L])
+            b = oracle.fwd_score_batch(p.M, p.mat, p.trans, d, [0], [L], scalar=True)
+            assert all(x.tobytes() == y.tobytes() for x, y in zip(a, b)), (p.M, L)
+    for m in (99, 100, 257):
+        p, cons = peaked_profile(5 + m, m, peak=0.7)
+        fr = planted_frame(m, 3000, cons, 3)
+        a = oracle.fwd_score_batch(m, p.mat, p.trans, fr, [0], [3000])
+        b = oracle.fwd_score_batch(m, p.mat, p.trans, fr, [0], [3000], scalar=True)
+        assert all(x.tobytes() == y.tobytes() for x, y in zip(a, b)) and a[1][0] > 0
