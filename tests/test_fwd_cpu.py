@@ -161,7 +161,7 @@ def test_oracle_sse_engine_equals_lane_by_lane():
             a = oracle.fwd_score_batch(p.M, p.mat, p.trans, d, [0], [L])
             b = oracle.fwd_score_batch(p.M, p.mat, p.trans, d, [0], [L], scalar=True)
             assert all(x.tobytes() == y.tobytes() for x, y in zip(a, b)), (p.M, L)
-    for m in (99, 100, 257):
+    for m in (29, 99, 100, 128, 257, 400, 1500):
         p, cons = peaked_profile(5 + m, m, peak=0.7)
         fr = planted_frame(m, 3000, cons, 3)
         a = oracle.fwd_score_batch(m, p.mat, p.trans, fr, [0], [3000])
