@@ -60,6 +60,7 @@ def lib():
         L.oracle_final_stage_inside_opt.argtypes = [vp, P(C.c_uint8), vp, C.c_int32, C.c_float,
                                                     C.c_int, C.c_int, vp, C.c_int32, P(C.c_int32)]
         L.oracle_vit_score_batch.argtypes = [C.c_int, vp, vp, vp, vp, vp, C.c_int32, vp, vp]
+        L.oracle_vit_score_batch_scalar.argtypes = [C.c_int, vp, vp, vp, vp, vp, C.c_int32, vp, vp]
         L.oracle_vit_tables.argtypes = [C.c_int, vp, vp, vp, vp]
         L.oracle_msv_tables.argtypes = [C.c_int, vp, vp, C.c_int, vp, vp, vp, vp, vp]
         L.oracle_msv_score_batch.argtypes = [C.c_int, vp, vp, C.c_int, vp, vp, vp, vp, C.c_int32, vp, vp]
@@ -170,8 +171,9 @@ def ilogsum(a, b):
     return int(lib().oracle_ilogsum(a, b))
 
 
-def vit_score_batch(M, mat, trans, buf, offs, lens):
-    """vit_score_scalar on each sequence: (scores f32, scored u8; 0 = overflow)."""
+def vit_score_batch(M, mat, trans, buf, offs, lens, scalar=False):
+    """vit_score on each sequence: (scores f32, scored u8; 0 = overflow);
+    scalar: the scalar sweep (vit_score_scalar) instead of the SSE2 engine."""
     mat = np.ascontiguousarray(mat, np.float32)
     trans = np.ascontiguousarray(trans, np.float32)
     buf = np.ascontiguousarray(buf, np.uint8)
@@ -179,8 +181,9 @@ def vit_score_batch(M, mat, trans, buf, offs, lens):
     lens = np.ascontiguousarray(lens, np.int32)
     sc = np.zeros(len(lens), np.float32)
     ok = np.zeros(len(lens), np.uint8)
-    lib().oracle_vit_score_batch(int(M), mat.ctypes.data, trans.ctypes.data, buf.ctypes.data, offs.ctypes.data,
-                                 lens.ctypes.data, len(lens), sc.ctypes.data, ok.ctypes.data)
+    fn = lib().oracle_vit_score_batch_scalar if scalar else lib().oracle_vit_score_batch
+    fn(int(M), mat.ctypes.data, trans.ctypes.data, buf.ctypes.data, offs.ctypes.data, lens.ctypes.data, len(lens),
+       sc.ctypes.data, ok.ctypes.data)
     return sc, ok
 
 

@@ -161,18 +161,167 @@ static int vit_score(const vitf *f, const uint8_t *dsq, int l, float *score) {
     return ok;
 }
 
-/* exported: score a batch of sequences (frames with sentinels) */
-int oracle_vit_score_batch(int m, const float *mat, const float *trans, const uint8_t *buf, const int64_t *offs,
-                           const int32_t *lens, int32_t n, float *scores, uint8_t *scored) {
+#ifdef __SSE2__
+#include <emmintrin.h>
+
+/* The same score on eight int16 lanes, striped the way the reference's SSE
+ * engine lays a profile out (Q = max(2, (m-1)/8+1) vectors, lane z of vector
+ * q = position q + 1 + z*Q, -32768 beyond m): M and I cells from the previous
+ * row, D cells first from this row's M cells, then passes that carry D along
+ * each lane and across lanes until no cell changes.  Every step is a
+ * saturating add or an exact max, so the cells equal the scalar sweep's; the
+ * timed CPU baseline. */
+typedef struct {
+    int m, q;
+    __m128i *rw;                      /* [KP][Q] emissions */
+    __m128i *bm, *mm, *im, *dm;       /* into position k: entry, and from k-1 */
+    __m128i *mi, *ii, *md, *dd;       /* out of position k */
+} vitv;
+
+static void vitv_build(const vitf *f, vitv *v) {
+    const int m = f->m, Q = m >= 1 ? ((m - 1) / 8 + 1 < 2 ? 2 : (m - 1) / 8 + 1) : 2;
+    v->m = m;
+    v->q = Q;
+    __m128i **arr[9] = {&v->rw, &v->bm, &v->mm, &v->im, &v->dm, &v->mi, &v->ii, &v->md, &v->dd};
+    for (int a = 0; a < 9; a++) *arr[a] = (__m128i *)aligned_alloc(16, sizeof(__m128i) * (size_t)Q * (a ? 1 : KP));
+    for (int q = 0; q < Q; q++) {
+        int16_t l[9][8], rw[KP][8];
+        for (int z = 0; z < 8; z++) {
+            const int k = q + 1 + z * Q;
+            const int in = k <= m;
+            l[1][z] = in ? f->vbm[k] : NEGINF;
+            l[2][z] = in ? f->tmm[k - 1] : NEGINF;
+            l[3][z] = in ? f->tim[k - 1] : NEGINF;
+            l[4][z] = in ? f->tdm[k - 1] : NEGINF;
+            l[5][z] = in ? f->tmi[k] : NEGINF;
+            l[6][z] = in ? f->tii[k] : NEGINF;
+            l[7][z] = in ? f->tmd[k] : NEGINF;
+            l[8][z] = in ? f->tdd[k] : NEGINF;
+            for (int x = 0; x < KP; x++) rw[x][z] = in ? f->rwv[k * KP + x] : NEGINF;
+        }
+        for (int a = 1; a < 9; a++) (*arr[a])[q] = _mm_loadu_si128((const __m128i *)l[a]);
+        for (int x = 0; x < KP; x++) v->rw[x * Q + q] = _mm_loadu_si128((const __m128i *)rw[x]);
+    }
+}
+
+static void vitv_free(vitv *v) {
+    __m128i *arr[9] = {v->rw, v->bm, v->mm, v->im, v->dm, v->mi, v->ii, v->md, v->dd};
+    for (int a = 0; a < 9; a++) free(arr[a]);
+}
+
+/* lane z takes lane z-1's value, lane 0 takes -infinity */
+static __m128i vshift16(__m128i a) {
+    return _mm_or_si128(_mm_slli_si128(a, 2), _mm_cvtsi32_si128(0x8000));
+}
+
+static int16_t hmax16(__m128i a) {
+    a = _mm_max_epi16(a, _mm_shuffle_epi32(a, 0x4E));
+    a = _mm_max_epi16(a, _mm_shuffle_epi32(a, 0xB1));
+    a = _mm_max_epi16(a, _mm_shufflelo_epi16(a, 0xB1));
+    return (int16_t)_mm_extract_epi16(a, 0);
+}
+
+static int vit_score_sse(const vitf *f, const vitv *v, const uint8_t *dsq, int l, float *score) {
+    const int Q = v->q;
+    const float pmove = 3.0f / ((float)l + 3.0f);
+    const int16_t xw_move = wordify(f->scale_w, logf(pmove));
+    __m128i *M = (__m128i *)aligned_alloc(16, sizeof(__m128i) * (size_t)Q * 3), *I = M + Q, *D = M + 2 * Q;
+    const __m128i ninf = _mm_set1_epi16(NEGINF);
+    for (int q = 0; q < Q; q++) M[q] = I[q] = D[q] = ninf;
+    int16_t xn = f->base_w, xb = adds(xn, xw_move), xj = NEGINF, xc = NEGINF;
+    int ok = 1;
+    for (int i = 1; i <= l; i++) {
+        const __m128i *rw = v->rw + (size_t)dsq[i] * Q;
+        const __m128i xbv = _mm_set1_epi16(xb);
+        __m128i mpv = vshift16(M[Q - 1]), ipv = vshift16(I[Q - 1]), dpv = vshift16(D[Q - 1]);
+        __m128i dcv = ninf, xev = ninf;
+        for (int q = 0; q < Q; q++) {
+            __m128i sc = _mm_adds_epi16(xbv, v->bm[q]);
+            sc = _mm_max_epi16(sc, _mm_adds_epi16(mpv, v->mm[q]));
+            sc = _mm_max_epi16(sc, _mm_adds_epi16(ipv, v->im[q]));
+            sc = _mm_max_epi16(sc, _mm_adds_epi16(dpv, v->dm[q]));
+            sc = _mm_adds_epi16(sc, rw[q]);
+            xev = _mm_max_epi16(xev, sc);
+            mpv = M[q];
+            ipv = I[q];
+            dpv = D[q];
+            M[q] = sc;
+            I[q] = _mm_max_epi16(_mm_adds_epi16(mpv, v->mi[q]), _mm_adds_epi16(ipv, v->ii[q]));
+            D[q] = dcv;
+            dcv = _mm_adds_epi16(sc, v->md[q]);
+        }
+        /* D chains across the lanes: repeat until a pass changes nothing */
+        for (int changed = 1; changed;) {
+            changed = 0;
+            dcv = vshift16(dcv);
+            for (int q = 0; q < Q; q++) {
+                const __m128i d = _mm_max_epi16(D[q], dcv);
+                changed |= _mm_movemask_epi8(_mm_cmpeq_epi16(d, D[q])) != 0xFFFF;
+                D[q] = d;
+                dcv = _mm_adds_epi16(d, v->dd[q]);
+            }
+        }
+        const int16_t xe = hmax16(xev);
+        if (xe >= 32767) {
+            ok = 0;
+            break;
+        }
+        xn = adds(xn, 0);
+        xc = max16(xc, adds(xe, f->e_move));
+        xj = max16(xj, adds(xe, f->e_loop));
+        xb = max16(adds(xj, xw_move), adds(xn, xw_move));
+    }
+    if (ok) {
+        if (xc > NEGINF) {
+            float ret = (float)xc + (float)xw_move - (float)f->base_w;
+            ret /= f->scale_w;
+            *score = ret - 3.0f;
+        } else {
+            *score = -INFINITY;
+        }
+    }
+    free(M);
+    return ok;
+}
+#endif
+
+static int vit_batch(int m, const float *mat, const float *trans, const uint8_t *buf, const int64_t *offs,
+                     const int32_t *lens, int32_t n, float *scores, uint8_t *scored, int scalar) {
     vitf f;
     vit_build(m, mat, trans, &f);
+#ifdef __SSE2__
+    vitv v;
+    if (!scalar) vitv_build(&f, &v);
+#endif
     for (int32_t q = 0; q < n; q++) {
         float s = NAN;
+#ifdef __SSE2__
+        scored[q] = (uint8_t)(scalar ? vit_score(&f, buf + offs[q], lens[q], &s)
+                                     : vit_score_sse(&f, &v, buf + offs[q], lens[q], &s));
+#else
         scored[q] = (uint8_t)vit_score(&f, buf + offs[q], lens[q], &s);
+#endif
         scores[q] = scored[q] ? s : NAN;
     }
+#ifdef __SSE2__
+    if (!scalar) vitv_free(&v);
+#endif
     vit_free(&f);
     return 0;
+}
+
+/* exported: score a batch of sequences (frames with sentinels); the
+ * vectorised engine where the compiler has SSE2, the scalar sweep in
+ * oracle_vit_score_batch_scalar */
+int oracle_vit_score_batch(int m, const float *mat, const float *trans, const uint8_t *buf, const int64_t *offs,
+                           const int32_t *lens, int32_t n, float *scores, uint8_t *scored) {
+    return vit_batch(m, mat, trans, buf, offs, lens, n, scores, scored, 0);
+}
+
+int oracle_vit_score_batch_scalar(int m, const float *mat, const float *trans, const uint8_t *buf,
+                                  const int64_t *offs, const int32_t *lens, int32_t n, float *scores,
+                                  uint8_t *scored) {
+    return vit_batch(m, mat, trans, buf, offs, lens, n, scores, scored, 1);
 }
 
 /* exported: the filter tables in the product's layout [(m+1)][26] */

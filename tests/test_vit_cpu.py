@@ -55,3 +55,30 @@ def test_vit_oracle_sanity():
         off += len(d)
     sc, ok = oracle.vit_score_batch(40, p.mat, p.trans, np.concatenate(bufs), offs, lens)
     assert ok.all() and np.isfinite(sc).all()
+
+
+def test_oracle_sse_engine_equals_scalar_sweep():
+    """The reference's own sse_matches_scalar property (src/p7_vitfilter.rs:
+    603-635) on the oracle: its SSE2 striped engine (the timed CPU baseline)
+    and its scalar sweep give the same score bits and overflow flags on the
+    test's whole grid, and on long windows of larger models."""
+    import numpy as np
+    import oracle
+    from p7_helpers import Lcg, random_profile, reference_grid
+    n = 0
+    for p, seqs in reference_grid():
+        for d in seqs:
+            L = len(d) - 2
+            a = oracle.vit_score_batch(p.M, p.mat, p.trans, d, [0], [L])
+            b = oracle.vit_score_batch(p.M, p.mat, p.trans, d, [0], [L], scalar=True)
+            assert np.array_equal(a[1], b[1]) and a[0].tobytes() == b[0].tobytes(), (p.M, L)
+            n += 1
+    assert n == 1176
+    for m in (97, 257, 1500):
+        p = random_profile(Lcg(1000 + m), m)
+        r = np.random.default_rng(m)
+        d = np.full(5002, 255, np.uint8)
+        d[1:-1] = r.integers(0, 18, 5000)
+        a = oracle.vit_score_batch(m, p.mat, p.trans, d, [0], [5000])
+        b = oracle.vit_score_batch(m, p.mat, p.trans, d, [0], [5000], scalar=True)
+        assert np.array_equal(a[1], b[1]) and a[0].tobytes() == b[0].tobytes(), m
