@@ -15,7 +15,13 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_lib", "libcmscan_gpu.so")
 
 CMGPU_OK = 0
+CMGPU_EINVAL = -1
+CMGPU_ENOMEM = -2
+CMGPU_EDEVICE = -3
 CMGPU_EOVERFLOW = -4
+CMGPU_ERANGE = -5
+CMGPU_ETIMEOUT = -6
+CMGPU_ENOSPACE = -7
 CYK_F32, INSIDE_I32, INSIDE_F32 = 0, 1, 2
 NOQDB, QDB1, QDB2 = 0, 1, 2
 KERNEL_AUTO, KERNEL_LEVEL, KERNEL_SWEEP = 0, 1, 2

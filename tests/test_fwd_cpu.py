@@ -167,3 +167,31 @@ def test_oracle_sse_engine_equals_lane_by_lane():
         a = oracle.fwd_score_batch(m, p.mat, p.trans, fr, [0], [3000])
         b = oracle.fwd_score_batch(m, p.mat, p.trans, fr, [0], [3000], scalar=True)
         assert all(x.tobytes() == y.tobytes() for x, y in zip(a, b)) and a[1][0] > 0
+
+
+def test_abi_refuses_bad_arguments_before_any_device_work():
+    """The Forward filter's entry points check their arguments first: null
+    pointers, empty models, a stage without its filter, a host-only filter
+    asked to score -- each an error code, no device touched."""
+    import ctypes as C
+    from p7_helpers import random_profile, Lcg
+    L = N.lib()
+    assert L.cmgpu_fwd_filter_build(None, None, 0.0, 1.0, -1, None) == N.CMGPU_EINVAL
+    assert L.cmgpu_fwd_score_batch(None, None, None, 0, None, 0, None, None) == N.CMGPU_EINVAL
+    p = random_profile(Lcg(3), 12)
+    f = FwdFilter(p, np.full(4, 0.25, np.float32), device=-1)  # host tables only
+    buf = np.full(12, 255, np.uint8)
+    buf[1:11] = 1
+    w = np.array([(0, 1, 10)], N.WINDOW_DTYPE)
+    out = np.zeros(1, np.float32)
+    assert L.cmgpu_fwd_score_batch(f._h, None, buf.ctypes.data, buf.size, w.ctypes.data, 1, out.ctypes.data,
+                                   None) == N.CMGPU_EINVAL
+    assert b"without a device" in L.cmgpu_last_error()
+    cfg = N.F3Config()
+    cfg.do_msv, cfg.cmw, cfg.do_fwd = 1, 30, 1
+    n = C.c_int32()
+    assert L.cmgpu_f3_filter(f._h, None, None, None, buf.ctypes.data, buf.size, w.ctypes.data, 1, C.byref(cfg),
+                             None, 0, C.byref(n), None) == N.CMGPU_EINVAL
+    assert b"without its filter" in L.cmgpu_last_error()
+    assert L.cmgpu_fwd_filter_set_kernel(f._h, 7) == N.CMGPU_EINVAL
+    f.close()
