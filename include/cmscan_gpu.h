@@ -165,6 +165,27 @@ int cmgpu_prep_configure(const cmgpu_cm_params *p, int local, int32_t W_in,
                          double beta1, double beta2, double betaW,
                          cmgpu_cm_scores *out);
 
+/* The CP9 HMM of a CM (cp9_build_and_configure, src/cp9.rs:2212-2232): the
+ * profile HMM that HMM-banded search derives its bands from, built from the
+ * global CM and put in local mode (begins and ends at pbegin, end-local
+ * exits at pend).  Caller-allocated, M = the CM's consensus length:
+ * mat / ins [(M+1)*4] emissions, t [(M+1)*10] transitions MM MI MD MEL IM II
+ * ID DM DI DD, begin / end [M+1], msc / isc [(M+1)*18] integer emission
+ * scores, otsc [(M+1)*12] integer transition scores in the DP's order MM IM
+ * DM BM MI II DI MD ID DD ME MEL, has_el [M+1] (an end-local exit leaves
+ * node k), hns2cs [(M+1)*3*2] the CM states behind node k's match, insert
+ * and delete states (-1: none). */
+typedef struct cmgpu_cp9 {
+    int32_t M;
+    float *mat, *ins, *t, *begin, *end;
+    int32_t *msc, *isc, *otsc;
+    uint8_t *has_el;
+    int32_t *hns2cs;
+    float el_self;          /* out */
+    int32_t el_selfsc;      /* out */
+} cmgpu_cp9;
+int cmgpu_prep_cp9(const cmgpu_cm_params *p, cmgpu_cp9 *out);
+
 /* Inputs of the truncated scanners for a configured CM, all caller
  * allocated: the marginal emission scores (fill_marginal_emissions,
  * src/cp9.rs:4441) lmesc/rmesc and ilmesc/irmesc [M*18]; the truncated-begin

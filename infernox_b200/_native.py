@@ -84,6 +84,14 @@ class P7Profile(C.Structure):
     _fields_ = [("M", C.c_int32), ("mat", P(C.c_float)), ("trans", P(C.c_float))]
 
 
+class Cp9(C.Structure):
+    """cmgpu_cp9: the CP9 HMM of a CM (caller-allocated arrays)."""
+    _fields_ = [("M", C.c_int32), ("mat", P(C.c_float)), ("ins", P(C.c_float)), ("t", P(C.c_float)),
+                ("begin", P(C.c_float)), ("end", P(C.c_float)), ("msc", P(C.c_int32)), ("isc", P(C.c_int32)),
+                ("otsc", P(C.c_int32)), ("has_el", P(C.c_uint8)), ("hns2cs", P(C.c_int32)),
+                ("el_self", C.c_float), ("el_selfsc", C.c_int32)]
+
+
 class F3Config(C.Structure):
     """cmgpu_f3_config: stages and thresholds of one f3_filter_sequence pass."""
     _fields_ = [("f1", C.c_double), ("f1b", C.c_double), ("f2", C.c_double), ("f2b", C.c_double),
@@ -250,6 +258,7 @@ def lib() -> C.CDLL:
     L.cmgpu_ssv_diagonals.argtypes = [vp, vp, vp, C.c_int64, vp, C.c_int32, C.c_double, vp, C.c_int32,
                                       P(C.c_int32)]
     L.cmgpu_msv_filter_stats.argtypes = [vp, P(C.c_double), P(C.c_int64), P(C.c_int32)]
+    L.cmgpu_prep_cp9.argtypes = [P(CmParams), P(Cp9)]
     L.cmgpu_fwd_filter_build.argtypes = [vp, vp, C.c_double, C.c_double, C.c_int, P(vp)]
     L.cmgpu_fwd_filter_free.argtypes = [vp]
     L.cmgpu_fwd_filter_free.restype = None
@@ -311,5 +320,5 @@ EXPORTED = [
     "cmgpu_tr_scan_hb", "cmgpu_tr_scan_hb_batch", "cmgpu_tr_qdb_scan", "cmgpu_tr_qdb_scan_batch",
     "cmgpu_tr_qdb_stats", "cmgpu_tr_qdb_inject_stall", "cmgpu_tr_qdb_set_deck_budget", "cmgpu_genomic_sample", "cmgpu_exp_fit",
     "cmgpu_calibrate_scan_batch", "cmgpu_calibrate", "cmgpu_fwd_filter_build", "cmgpu_fwd_filter_free",
-    "cmgpu_fwd_filter_tables", "cmgpu_fwd_score_batch", "cmgpu_f3_filter", "cmgpu_fwd_filter_stats", "cmgpu_fwd_filter_set_kernel",
+    "cmgpu_prep_cp9", "cmgpu_fwd_filter_tables", "cmgpu_fwd_score_batch", "cmgpu_f3_filter", "cmgpu_fwd_filter_stats", "cmgpu_fwd_filter_set_kernel",
 ]

@@ -9,8 +9,11 @@
 //   localisation        src/cp9.rs:4193-4258  (cm_config_local)
 //   QDB band engine     src/cm_qdband.rs:258-549, wrapper :554-592
 //   ILogsum / FLogsum   src/cp9.rs:28-44, :5391-5400
+//   CP9 HMM of a CM     src/cp9.rs:275-427, :1000-1255, :2212-2232, :2532-2841
 // Compiled with -ffp-contract=off: no multiply-add is fused, as in Rust.
 #include <algorithm>
+#include <array>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -728,5 +731,483 @@ extern "C" int cmgpu_prep_truncated(const cmgpu_cm_params *p, int local, cmgpu_t
         out->lpos[v] = (t == MATP_ND || t == MATL_ND) ? elpos[nd] : elpos[nd] + 1;
         out->rpos[v] = (t == MATP_ND || t == MATR_ND) ? erpos[nd] : erpos[nd] - 1;
     }
+    return CMGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// The CP9 HMM of a CM: the first step of HMM-banded search
+// (cp9_build_and_configure, src/cp9.rs:2212-2232): the CM <-> HMM state map
+// (CP9_map_cm2hmm, :275-427), occupancy-weighted emissions (:2558-2612) and
+// transitions summed over CM subpaths (:2615-2841), renormalisation (:1000),
+// end-local states (:1042), local begins and ends (:1097, :1121) and the
+// integer log-odds scores (:1176-1255).
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int CT_MM = 0, CT_MI = 1, CT_MD = 2, CT_MEL = 3, CT_IM = 4, CT_II = 5, CT_ID = 6, CT_DM = 7, CT_DI = 8,
+              CT_DD = 9, CT_N = 10;
+constexpr int HM = 0, HI = 1, HD = 2;  // HMM match, insert, delete
+constexpr int CP9_INFTY = 987654321;
+
+struct Cp9Map {
+    int hmm_m = 0;
+    std::vector<int> nd2lpos, nd2rpos, pos2nd;
+    std::vector<std::array<std::array<int, 2>, 3>> hns2cs;  // [k][ks][0..1]
+    std::vector<std::array<int, 2>> cs2hn, cs2hs;          // [v][0..1]
+};
+
+struct Cp9 {
+    int M = 0;
+    std::vector<std::array<float, 4>> mat, ins;
+    std::vector<std::array<float, CT_N>> t;
+    std::vector<float> begin, end;
+    std::vector<uint8_t> has_el;
+    float null[4] = {};
+    float el_self = 0.0f;
+};
+
+// Prob2Score of the CP9 (src/cp9.rs:977-998): the ratio in float, sreLOG2
+// (ln x * 1.44269504) in double, floor(0.5 + 1000 x), never below -INFTY.
+int cp9_prob2score(float p, float null) {
+    if (p == 0.0f) return -CP9_INFTY;
+    const float ratio = p / null;
+    const double l2 = ratio > 0.0f ? std::log((double)ratio) * 1.44269504 : -1e36;
+    const double v = std::floor(0.5 + 1000.0 * l2);
+    if (!std::isfinite(v) || v <= -(double)CP9_INFTY) return -CP9_INFTY;
+    return (int)v;
+}
+
+void fnorm_f(float *v, int n) {
+    const float s = kahan_fsum(v, n);
+    for (int i = 0; i < n; i++) v[i] = s != 0.0f ? v[i] / s : 1.0f / (float)n;
+}
+
+bool map_helper(const Model &cm, Cp9Map &m, int k, int ks, int v) {
+    // a detached insert (the state after it an END_E) maps to no HMM state
+    if (ks == HI && (v + 1 >= cm.M ? EL_ST : cm.sttype[v + 1]) == E_ST) return true;
+    if (m.cs2hn[v][0] == -1) {
+        m.cs2hn[v][0] = k;
+        m.cs2hs[v][0] = ks;
+    } else if (m.cs2hn[v][1] == -1) {
+        m.cs2hn[v][1] = k;
+        m.cs2hs[v][1] = ks;
+    } else {
+        return false;
+    }
+    auto &h = m.hns2cs[k][ks];
+    if (h[0] == -1) {
+        h[0] = v;
+    } else if (h[1] == -1) {
+        h[1] = v;
+    } else {
+        return false;
+    }
+    return true;
+}
+
+// the insert state modelling the column after HMM node k, looked up from the
+// node of column k+1 (or ROOT_IR after the last column)
+bool map_right_insert(const Model &cm, Cp9Map &m, int k) {
+    if (k == m.hmm_m) return map_helper(cm, m, k, HI, 2);  // ROOT_IR
+    const int nn = m.pos2nd[k + 1];
+    if (m.nd2lpos[nn] == k + 1) {
+        int b = nn;
+        while (b >= 0 && cm.ndtype[b] != BEGR_ND) b--;
+        if (b < 0) return false;
+        return map_helper(cm, m, k, HI, cm.nodemap[b] + 1);  // BEGR_IL
+    }
+    if (m.nd2rpos[nn] == k + 1) {
+        if (cm.ndtype[nn] == MATP_ND) return map_helper(cm, m, k, HI, cm.nodemap[nn] + 5);  // MATP_IR
+        if (cm.ndtype[nn] == MATR_ND) return map_helper(cm, m, k, HI, cm.nodemap[nn] + 2);  // MATR_IR
+    }
+    return true;
+}
+
+bool map_cm2hmm(const Model &cm, const std::vector<int> &lpos, const std::vector<int> &rpos, Cp9Map &m) {
+    m.hmm_m = 0;
+    for (int v = 0; v < cm.M; v++) {
+        if (cm.stid[v] == ID_MATP_MP) m.hmm_m += 2;
+        else if (cm.stid[v] == ID_MATL_ML || cm.stid[v] == ID_MATR_MR) m.hmm_m += 1;
+    }
+    const int H = m.hmm_m;
+    m.nd2lpos.assign(cm.nodes, -1);
+    m.nd2rpos.assign(cm.nodes, -1);
+    m.pos2nd.assign(H + 1, -1);
+    std::array<std::array<int, 2>, 3> none;
+    for (auto &a : none) a = {-1, -1};
+    m.hns2cs.assign(H + 1, none);
+    m.cs2hn.assign(cm.M + 1, {-1, -1});
+    m.cs2hs.assign(cm.M + 1, {-1, -1});
+    for (int n = 0; n < cm.nodes; n++) {
+        const int t = cm.ndtype[n];
+        if (t == MATP_ND || t == MATL_ND) {
+            m.nd2lpos[n] = lpos[n];
+            m.pos2nd[lpos[n]] = n;
+        }
+        if (t == MATP_ND || t == MATR_ND) {
+            m.nd2rpos[n] = rpos[n];
+            m.pos2nd[rpos[n]] = n;
+        }
+    }
+    bool ok = map_helper(cm, m, 0, HM, 0) && map_helper(cm, m, 0, HI, 1);  // ROOT_S, ROOT_IL
+    for (int k = 1; ok && k <= H; k++) {
+        const int n = m.pos2nd[k];
+        if (n < 0) return false;
+        const int t = cm.ndtype[n], nm = cm.nodemap[n];
+        if (t == MATP_ND && m.nd2lpos[n] == k) {
+            ok = map_helper(cm, m, k, HM, nm) && map_helper(cm, m, k, HM, nm + 1) &&
+                 map_helper(cm, m, k, HI, nm + 4) && map_helper(cm, m, k, HD, nm + 2) &&
+                 map_helper(cm, m, k, HD, nm + 3);
+        } else if (t == MATP_ND) {
+            ok = map_helper(cm, m, k, HM, nm) && map_helper(cm, m, k, HM, nm + 2) && map_right_insert(cm, m, k);
+            const int pk = m.pos2nd[k - 1];
+            if (ok && m.nd2lpos[pk] == k - 1) {
+                if (cm.ndtype[pk] != MATL_ND && cm.ndtype[pk] != MATP_ND) return false;
+                ok = map_helper(cm, m, k - 1, HI, nm + 5);  // MATP_IR
+            }
+            ok = ok && map_helper(cm, m, k, HD, nm + 1) && map_helper(cm, m, k, HD, nm + 3);
+        } else if (t == MATL_ND) {
+            ok = map_helper(cm, m, k, HM, nm) && map_helper(cm, m, k, HI, nm + 2) &&
+                 map_helper(cm, m, k, HD, nm + 1);
+            if (ok && k == H) ok = map_helper(cm, m, k, HI, 2);  // ROOT_IR
+        } else if (t == MATR_ND) {
+            ok = map_helper(cm, m, k, HM, nm) && map_right_insert(cm, m, k);
+            if (ok && m.nd2lpos[m.pos2nd[k - 1]] == k - 1) return false;
+            ok = ok && map_helper(cm, m, k, HD, nm + 1);
+        } else {
+            return false;
+        }
+    }
+    return ok;
+}
+
+// probability that CM state x emits residue i at HMM node k (a pair state
+// marginalised over its other half), cm2hmm_emit_prob (src/cp9.rs:2532-2553)
+float emit_prob(const Model &cm, const Cp9Map &m, int x, int i, int k) {
+    const float *e = &cm.e[(size_t)x * 16];
+    if (cm.stid[x] != ID_MATP_MP) return e[i];
+    float r = 0.0f;
+    if (m.nd2lpos[m.pos2nd[k]] == k) {
+        for (int j = i * K; j < (i + 1) * K; j++) r += e[j];
+    } else {
+        for (int j = i; j < K * K; j += K) r += e[j];
+    }
+    return r;
+}
+
+void add_emission(float &cell, double psi, float p) { cell = (float)((double)cell + psi * (double)p); }
+
+void cp9_emissions(const Model &cm, const Cp9Map &m, const std::vector<double> &psi, Cp9 &h) {
+    const int H = m.hmm_m;
+    for (int i = 0; i < K; i++) {
+        h.null[i] = cm.null[i];
+        h.ins[0][i] = cm.e[(size_t)1 * 16 + i];  // node 0's insert is ROOT_IL
+    }
+    for (int k = 1; k <= H; k++) {
+        for (int ks : {HM, HI}) {
+            const int a0 = m.hns2cs[k][ks][0], a1 = m.hns2cs[k][ks][1];
+            auto &row = ks == HM ? h.mat[k] : h.ins[k];
+            for (int i = 0; i < K; i++) {
+                add_emission(row[i], psi[a0], emit_prob(cm, m, a0, i, k));
+                if (a1 != -1) add_emission(row[i], psi[a1], emit_prob(cm, m, a1, i, k));
+            }
+        }
+    }
+}
+
+// the nodes with an end-local exit: MATP/MATL/MATR/BEGL/BEGR not followed by END
+bool has_exit(const Model &cm, int nd) {
+    const int t = cm.ndtype[nd];
+    return (t == MATP_ND || t == MATL_ND || t == MATR_ND || t == BEGL_ND || t == BEGR_ND) && nd + 1 < cm.nodes &&
+           cm.ndtype[nd + 1] != END_ND;
+}
+
+// transition index from parent x to its child v (the reference's transition
+// map: a bifurcation's two children are both its transition 0)
+int child_index(const Model &cm, int x, int v) { return cm.sttype[x] == B_ST ? 0 : v - cm.cfirst[x]; }
+
+// cm_sum_subpaths_cp9 (src/cp9.rs:2615-2693): summed probability of the CM
+// subpaths from start to end
+float sum_subpaths(const Model &cm, const int32_t *plast, const int32_t *pnum, const Cp9Map &m, int start, int end,
+                   int k, const std::vector<double> &psi) {
+    auto is_ins = [&](int v) { return cm.sttype[v] == IL_ST || cm.sttype[v] == IR_ST; };
+    if (start == end) return is_ins(start) ? cm.t[(size_t)start * MAXC] : 1.0f;
+    std::vector<double> sub(end - start + 1, 0.0);
+    sub[0] = 1.0;
+    if (!is_ins(start) && !is_ins(end)) {
+        double to_start = 0.0;
+        const int h0 = m.hns2cs[k][HI][0], h1 = m.hns2cs[k][HI][1];
+        if (h0 < start) to_start = psi[h0] * (double)sum_subpaths(cm, plast, pnum, m, h0, start, k, psi);
+        if (h1 != -1 && h1 < start)
+            to_start += psi[h1] * (double)sum_subpaths(cm, plast, pnum, m, h1, start, k, psi);
+        sub[0] -= to_start / psi[start];
+    }
+    for (int v = start + 1; v <= end; v++) {
+        const int vi = v - start, ins = is_ins(v) ? 1 : 0;
+        if (cm.sttype[v] == S_ST) sub[vi] = sub[vi - 1] * 1.0;
+        if (v != end && ins && (m.cs2hn[v][0] == k || m.cs2hn[v][1] == k)) continue;
+        for (int y = pnum[v] - 1; y >= ins; y--) {
+            const int x = plast[v] - y;
+            if (x - start >= 0) sub[vi] += sub[x - start] * (double)cm.t[(size_t)x * MAXC + child_index(cm, x, v)];
+        }
+        if (v != end && ins) {
+            const double t0 = (double)cm.t[(size_t)v * MAXC];
+            sub[vi] += sub[vi] * (t0 / (1.0 - t0));
+        }
+    }
+    return (float)sub[end - start];
+}
+
+void add_trans(const Model &cm, const int32_t *plast, const int32_t *pnum, const Cp9Map &m, Cp9 &h, int a, int b,
+               int k, int idx, const std::vector<double> &psi) {
+    if (a == -1 || b == -1) return;
+    const int lo = a <= b ? a : b, hi = a <= b ? b : a;
+    const float sub = sum_subpaths(cm, plast, pnum, m, lo, hi, k, psi);
+    h.t[k][idx] = (float)((double)h.t[k][idx] + psi[lo] * (double)sub);
+}
+
+void add4(const Model &cm, const int32_t *plast, const int32_t *pnum, const Cp9Map &m, Cp9 &h,
+          const std::array<int, 2> &ap, const std::array<int, 2> &bp, int k, int idx, const std::vector<double> &psi) {
+    for (int i : {0, 1})
+        for (int j : {0, 1}) add_trans(cm, plast, pnum, m, h, ap[i], bp[j], k, idx, psi);
+}
+
+void fscale_f(float *v, int n, float s) {
+    for (int i = 0; i < n; i++) v[i] *= s;
+}
+
+void cp9_transitions(const Model &cm, const int32_t *plast, const int32_t *pnum, const Cp9Map &m,
+                     const std::vector<double> &psi, Cp9 &h) {
+    const int H = m.hmm_m;
+    auto &c = m.hns2cs;
+    // into node 1 (src/cp9.rs:2742-2770)
+    add4(cm, plast, pnum, m, h, c[0][HM], c[1][HM], 0, CT_MM, psi);
+    h.begin[1] = h.t[0][CT_MM];
+    h.t[0][CT_MM] = 0.0f;
+    add4(cm, plast, pnum, m, h, c[0][HM], c[0][HI], 0, CT_MI, psi);
+    add4(cm, plast, pnum, m, h, c[0][HM], c[1][HD], 0, CT_MD, psi);
+    add4(cm, plast, pnum, m, h, c[0][HI], c[1][HM], 0, CT_IM, psi);
+    add4(cm, plast, pnum, m, h, c[0][HI], c[0][HI], 0, CT_II, psi);
+    add4(cm, plast, pnum, m, h, c[0][HI], c[1][HD], 0, CT_ID, psi);
+    h.t[0][CT_DM] = h.t[0][CT_DI] = h.t[0][CT_DD] = 0.0f;
+    float d = kahan_fsum(&h.begin[1], H) + h.t[0][CT_MI] + h.t[0][CT_MD];
+    fscale_f(&h.begin[1], H, 1.0f / d);
+    h.t[0][CT_MI] /= d;
+    h.t[0][CT_MD] /= d;
+    fnorm_f(&h.t[0][CT_IM], 3);
+    // out of node M (:2772-2800)
+    const std::array<int, 2> end_e{cm.M - 1, -1};
+    add4(cm, plast, pnum, m, h, c[H][HM], end_e, H, CT_MM, psi);
+    h.end[H] = h.t[H][CT_MM];
+    h.t[H][CT_MM] = 0.0f;
+    add4(cm, plast, pnum, m, h, c[H][HM], c[H][HI], H, CT_MI, psi);
+    h.t[H][CT_MD] = 0.0f;
+    add4(cm, plast, pnum, m, h, c[H][HI], end_e, H, CT_IM, psi);
+    add4(cm, plast, pnum, m, h, c[H][HI], c[H][HI], H, CT_II, psi);
+    h.t[H][CT_ID] = 0.0f;
+    add4(cm, plast, pnum, m, h, c[H][HD], end_e, H, CT_DM, psi);
+    add4(cm, plast, pnum, m, h, c[H][HD], c[H][HI], H, CT_DI, psi);
+    h.t[H][CT_DD] = 0.0f;
+    d = kahan_fsum(&h.t[H][0], 4) + h.end[H];
+    fscale_f(&h.t[H][0], 4, 1.0f / d);
+    h.end[H] /= d;
+    fnorm_f(&h.t[H][CT_IM], 3);
+    fnorm_f(&h.t[H][CT_DM], 3);
+    // interior nodes (:2803-2826)
+    for (int k = 1; k < H; k++) {
+        const auto &hm = c[k][HM], &hi = c[k][HI], &hd = c[k][HD], &nm = c[k + 1][HM], &nd = c[k + 1][HD];
+        add4(cm, plast, pnum, m, h, hm, nm, k, CT_MM, psi);
+        add4(cm, plast, pnum, m, h, hm, hi, k, CT_MI, psi);
+        add4(cm, plast, pnum, m, h, hm, nd, k, CT_MD, psi);
+        add4(cm, plast, pnum, m, h, hi, nm, k, CT_IM, psi);
+        add4(cm, plast, pnum, m, h, hi, hi, k, CT_II, psi);
+        add4(cm, plast, pnum, m, h, hi, nd, k, CT_ID, psi);
+        add4(cm, plast, pnum, m, h, hd, nm, k, CT_DM, psi);
+        add4(cm, plast, pnum, m, h, hd, hi, k, CT_DI, psi);
+        add4(cm, plast, pnum, m, h, hd, nd, k, CT_DD, psi);
+        d = kahan_fsum(&h.t[k][0], 4) + h.end[k];
+        fscale_f(&h.t[k][0], 4, 1.0f / d);
+        h.end[k] /= d;
+        fnorm_f(&h.t[k][CT_IM], 3);
+        fnorm_f(&h.t[k][CT_DM], 3);
+    }
+}
+
+// CPlan9Renormalize (src/cp9.rs:1000-1040)
+void cp9_renormalize(Cp9 &h) {
+    const int H = h.M;
+    h.mat[0] = {0.0f, 0.0f, 0.0f, 0.0f};
+    for (int k = 1; k <= H; k++) fnorm_f(h.mat[k].data(), K);
+    for (int k = 0; k <= H; k++) fnorm_f(h.ins[k].data(), K);
+    const float d = kahan_fsum(&h.begin[1], H) + h.t[0][CT_MI] + h.t[0][CT_MD] + h.t[0][CT_MEL];
+    fscale_f(&h.begin[1], H, 1.0f / d);
+    h.t[0][CT_MI] /= d;
+    h.t[0][CT_MD] /= d;
+    h.t[0][CT_MEL] /= d;
+    fnorm_f(&h.t[0][CT_IM], 3);
+    h.t[0][CT_DM] = h.t[0][CT_DI] = h.t[0][CT_DD] = 0.0f;
+    for (int k = 1; k <= H; k++) {
+        const float dk = kahan_fsum(&h.t[k][0], 4) + h.end[k];
+        fscale_f(&h.t[k][0], 4, 1.0f / dk);
+        h.end[k] /= dk;
+        fnorm_f(&h.t[k][CT_IM], 3);
+        fnorm_f(&h.t[k][CT_DM], 3);
+    }
+    fnorm_f(h.null, K);
+}
+
+// CPlan9InitEL, the score-relevant part (src/cp9.rs:1042-1077)
+void cp9_init_el(const Model &cm, const std::vector<int> &lpos, Cp9 &h) {
+    h.el_self = (float)std::exp((double)cm.el_selfsc * 0.69314718);
+    std::fill(h.has_el.begin(), h.has_el.end(), 0);
+    for (int nd = 0; nd < cm.nodes; nd++)
+        if (has_exit(cm, nd)) h.has_el[lpos[nd]] = 1;
+}
+
+// cp9_renormalize_exits (src/cp9.rs:1079-1095)
+void cp9_renormalize_exits(Cp9 &h) {
+    const int H = h.M;
+    for (int k = 1; k < H; k++) {
+        const float d = kahan_fsum(&h.t[k][0], 4);
+        fscale_f(&h.t[k][0], 4, (1.0f - h.end[k]) / d);
+    }
+    const float d = h.t[H][CT_MI] + h.t[H][CT_MEL];
+    if (std::fabs(d - 0.0f) >= 5e-9f) {
+        const float f = (1.0f - h.end[H]) / d;
+        h.t[H][CT_MI] *= f;
+        h.t[H][CT_MEL] *= f;
+    }
+}
+
+// cp9_sw_config (src/cp9.rs:1097-1119), entry and exit pbegin
+void cp9_sw_config(Cp9 &h, float pentry, float pexit) {
+    const int H = h.M;
+    const float s = h.t[0][CT_MI] + h.t[0][CT_MD] + h.t[0][CT_MEL];
+    h.begin[1] = (1.0f - pentry) * (1.0f - s);
+    const float val = (pentry * (1.0f - s)) / ((float)H - 1.0f);
+    for (int k = 2; k <= H; k++) h.begin[k] = val;
+    const float basep = pexit / ((float)H - 1.0f);
+    for (int k = 1; k < H; k++) h.end[k] = basep / (1.0f - basep * ((float)k - 1.0f));
+    cp9_renormalize_exits(h);
+}
+
+// cp9_EL_local_ends_config (src/cp9.rs:1121-1147), on the global CM
+void cp9_el_local_ends(const Model &cm, Cp9 &h) {
+    int nexits = 0;
+    for (int nd = 1; nd < cm.nodes; nd++)
+        if (has_exit(cm, nd)) nexits++;
+    const float to_el = cm.pend / (float)nexits;
+    h.t[0][CT_MEL] = 0.0f;
+    for (int k = 1; k <= h.M; k++) {
+        if (!h.has_el[k]) continue;
+        h.t[k][CT_MEL] = to_el;
+        const float nf = 1.0f - (h.t[k][CT_MEL] / (1.0f - h.end[k]));
+        h.t[k][CT_MM] *= nf;
+        h.t[k][CT_MI] *= nf;
+        h.t[k][CT_MD] *= nf;
+    }
+}
+
+// esl_abc_IExpectScore with the CP9's null (src/cp9.rs:1152-1173)
+int cp9_iexpect(int x, const int *sc, const float *p) {
+    if (!is_residue(x)) return 0;
+    float r = 0.0f, den = 0.0f;
+    for (int i = 0; i < K; i++)
+        if (degen(x, i)) {
+            r += (float)sc[i] * p[i];
+            den += p[i];
+        }
+    r /= den;
+    return r < 0.0f ? (int)(r - 0.5f) : (int)(r + 0.5f);
+}
+
+void cp9_emission_scores(const std::array<float, 4> &pr, const float *null, int32_t *out) {
+    int sc[KP];
+    for (int x = 0; x < K; x++) sc[x] = cp9_prob2score(pr[x], null[x]);
+    sc[K] = sc[KP - 2] = sc[KP - 1] = -CP9_INFTY;
+    for (int x = K + 1; x <= KP - 3; x++) sc[x] = cp9_iexpect(x, sc, null);
+    std::copy(sc, sc + KP, out);
+}
+
+}  // namespace
+
+extern "C" int cmgpu_prep_cp9(const cmgpu_cm_params *p, cmgpu_cp9 *out) {
+    if (!p || !out || p->M < 2 || p->nodes < 2 || !p->sttype || !p->t || !p->e || !p->plast || !p->pnum ||
+        !p->ndidx || !out->mat || !out->ins || !out->t || !out->begin || !out->end || !out->msc || !out->isc ||
+        !out->otsc || !out->has_el || !out->hns2cs || out->M != p->clen) {
+        cmx::set_error("cmgpu_prep_cp9: bad arguments (out->M must be the CM's consensus length)");
+        return CMGPU_EINVAL;
+    }
+    Model cm = load(p);
+    std::vector<int32_t> ndidx(p->ndidx, p->ndidx + cm.M);
+    std::vector<int> lpos, rpos;
+    emit_map(cm, ndidx, lpos, rpos);
+    Cp9Map m;
+    if (!map_cm2hmm(cm, lpos, rpos, m) || m.hmm_m != p->clen || m.hmm_m < 2) {
+        cmx::set_error("cmgpu_prep_cp9: the CM's nodes do not map onto a CP9 HMM");
+        return CMGPU_EINVAL;
+    }
+    for (int k = 0; k <= m.hmm_m; k++)
+        if (m.hns2cs[k][HI][0] == -1 || m.hns2cs[k][HM][0] == -1) {
+            cmx::set_error("cmgpu_prep_cp9: HMM node " + std::to_string(k) + " has no CM match or insert state");
+            return CMGPU_EINVAL;
+        }
+    std::vector<double> psi;
+    if (!state_occupancy(cm, p->plast, p->pnum, psi)) {
+        cmx::set_error("cmgpu_prep_cp9: a parent does not list the state among its children");
+        return CMGPU_EINVAL;
+    }
+    const int H = m.hmm_m;
+    Cp9 h;
+    h.M = H;
+    h.mat.assign(H + 1, {0.0f, 0.0f, 0.0f, 0.0f});
+    h.ins.assign(H + 1, {0.0f, 0.0f, 0.0f, 0.0f});
+    std::array<float, CT_N> zt{};
+    h.t.assign(H + 1, zt);
+    h.begin.assign(H + 1, 0.0f);
+    h.end.assign(H + 1, 0.0f);
+    h.has_el.assign(H + 1, 0);
+    cp9_emissions(cm, m, psi, h);
+    cp9_init_el(cm, lpos, h);
+    cp9_transitions(cm, p->plast, p->pnum, m, psi, h);
+    cp9_renormalize(h);
+    cp9_sw_config(h, cm.pbegin, cm.pbegin);
+    cp9_el_local_ends(cm, h);
+    // CP9Logoddsify (src/cp9.rs:1176-1255), transitions in the DP's order
+    for (int k = 0; k <= H; k++) {
+        std::copy(h.mat[k].begin(), h.mat[k].end(), out->mat + (size_t)k * 4);
+        std::copy(h.ins[k].begin(), h.ins[k].end(), out->ins + (size_t)k * 4);
+        std::copy(h.t[k].begin(), h.t[k].end(), out->t + (size_t)k * CT_N);
+        out->begin[k] = h.begin[k];
+        out->end[k] = h.end[k];
+        out->has_el[k] = h.has_el[k];
+        cp9_emission_scores(h.ins[k], h.null, out->isc + (size_t)k * KP);
+        if (k == 0) {
+            std::fill(out->msc, out->msc + KP, 0);
+        } else {
+            cp9_emission_scores(h.mat[k], h.null, out->msc + (size_t)k * KP);
+        }
+        auto ts = [&](int c) { return cp9_prob2score(h.t[k][c], 1.0f); };
+        const int bsc = k == 0 ? -CP9_INFTY : cp9_prob2score(h.begin[k], 1.0f);
+        const int esc = k == 0 ? -CP9_INFTY : cp9_prob2score(h.end[k], 1.0f);
+        const bool k0 = k == 0;
+        int32_t *o = out->otsc + (size_t)k * 12;
+        o[0] = ts(CT_MM);
+        o[1] = ts(CT_IM);
+        o[2] = k0 ? -CP9_INFTY : ts(CT_DM);
+        o[3] = bsc;
+        o[4] = ts(CT_MI);
+        o[5] = ts(CT_II);
+        o[6] = k0 ? -CP9_INFTY : ts(CT_DI);
+        o[7] = ts(CT_MD);
+        o[8] = ts(CT_ID);
+        o[9] = k0 ? -CP9_INFTY : ts(CT_DD);
+        o[10] = esc;
+        o[11] = ts(CT_MEL);
+        for (int ks = 0; ks < 3; ks++)
+            for (int j = 0; j < 2; j++) out->hns2cs[((size_t)k * 3 + ks) * 2 + j] = m.hns2cs[k][ks][j];
+    }
+    out->el_self = h.el_self;
+    out->el_selfsc = cp9_prob2score(h.el_self, 1.0f);
     return CMGPU_OK;
 }

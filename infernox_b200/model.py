@@ -159,3 +159,27 @@ def configure(cm: SynthCM, local: bool = True, W: int = 0, beta1: float = DEFAUL
         null=np.asarray(cm.null, np.float32), n3_omega=float(np.float32(cm.n3_omega)),
         **out,
     )
+
+
+def cp9(cm: SynthCM) -> dict:
+    """The CP9 HMM of a CM (cmgpu_prep_cp9; cp9_build_and_configure,
+    src/cp9.rs:2212-2232): probabilities, integer scores and the HMM -> CM
+    state map, as numpy arrays keyed by field name."""
+    H = cm.clen
+    p, keep = params_struct(cm)
+    out = dict(mat=np.zeros((H + 1, 4), np.float32), ins=np.zeros((H + 1, 4), np.float32),
+               t=np.zeros((H + 1, 10), np.float32), begin=np.zeros(H + 1, np.float32),
+               end=np.zeros(H + 1, np.float32), msc=np.zeros((H + 1, 18), np.int32),
+               isc=np.zeros((H + 1, 18), np.int32), otsc=np.zeros((H + 1, 12), np.int32),
+               has_el=np.zeros(H + 1, np.uint8), hns2cs=np.zeros((H + 1, 3, 2), np.int32))
+    s = N.Cp9()
+    s.M = H
+    for k, ct in (("mat", C.c_float), ("ins", C.c_float), ("t", C.c_float), ("begin", C.c_float),
+                  ("end", C.c_float), ("msc", C.c_int32), ("isc", C.c_int32), ("otsc", C.c_int32),
+                  ("has_el", C.c_uint8), ("hns2cs", C.c_int32)):
+        setattr(s, k, N.ptr(out[k], ct))
+    N.check(N.lib().cmgpu_prep_cp9(C.byref(p), C.byref(s)))
+    del keep
+    out["el_self"] = float(s.el_self)
+    out["el_selfsc"] = int(s.el_selfsc)
+    return out

@@ -557,6 +557,34 @@ def prep_truncated(cm_s, local):
     return out
 
 
+def prep_cp9(cm_s):
+    """The oracle's CP9 HMM of a CM (the fields of cmgpu_cp9)."""
+    from infernox_b200 import _native as N
+    from infernox_b200.model import params_struct
+    H = cm_s.clen
+    out = dict(mat=np.zeros((H + 1, 4), np.float32), ins=np.zeros((H + 1, 4), np.float32),
+               t=np.zeros((H + 1, 10), np.float32), begin=np.zeros(H + 1, np.float32),
+               end=np.zeros(H + 1, np.float32), msc=np.zeros((H + 1, 18), np.int32),
+               isc=np.zeros((H + 1, 18), np.int32), otsc=np.zeros((H + 1, 12), np.int32),
+               has_el=np.zeros(H + 1, np.uint8), hns2cs=np.zeros((H + 1, 3, 2), np.int32))
+    p, keep = params_struct(cm_s)
+    s = N.Cp9()
+    s.M = H
+    for k, ct in (("mat", C.c_float), ("ins", C.c_float), ("t", C.c_float), ("begin", C.c_float),
+                  ("end", C.c_float), ("msc", C.c_int32), ("isc", C.c_int32), ("otsc", C.c_int32),
+                  ("has_el", C.c_uint8), ("hns2cs", C.c_int32)):
+        setattr(s, k, N.ptr(out[k], ct))
+    L = lib()
+    L.oracle_prep_cp9.argtypes = [C.c_void_p, C.c_void_p]
+    rc = L.oracle_prep_cp9(C.byref(p), C.byref(s))
+    if rc != 0:
+        raise RuntimeError(f"oracle_prep_cp9: {rc}")
+    del keep
+    out["el_self"] = float(s.el_self)
+    out["el_selfsc"] = int(s.el_selfsc)
+    return out
+
+
 # ---- cmcalibrate (calib_oracle.c, oracle_calib_scan in qdb_oracle.c) ------
 
 EXP_DTYPE = np.dtype([("lambda", np.float64), ("mu", np.float64), ("dbsize", np.float64), ("mu_orig", np.float64),

@@ -618,3 +618,427 @@ int oracle_prep_truncated(const cmgpu_cm_params *p, int local, cmgpu_tr_prep *o)
     free(il);
     return rc;
 }
+
+/* ---- the CP9 HMM of a CM (cp9_build_and_configure, src/cp9.rs:2212) ---- */
+
+#define C9N 10 /* MM MI MD MEL IM II ID DM DI DD */
+enum { cMM = 0, cMI, cMD, cMEL, cIM, cII, cID, cDM, cDI, cDD };
+
+typedef struct {
+    const cmgpu_cm_params *p;
+    int H;
+    int *nd2l, *nd2r, *pos2nd; /* [nodes], [nodes], [H+1] */
+    int *hns;                  /* [H+1][3][2] */
+    int *csn, *css;            /* [M+1][2] */
+    const double *psi;
+    float *mat, *ins, *t, *beg, *end; /* [H+1][4], [H+1][4], [H+1][10], [H+1], [H+1] */
+} c9;
+
+#define HNS(m, k, s, j) (m)->hns[((k) * 3 + (s)) * 2 + (j)]
+
+static int c9_sttype(const c9 *m, int v) { return v < m->p->M ? m->p->sttype[v] : 9; /* EL */ }
+
+/* map_helper (src/cp9.rs:247-273) */
+static int c9_map(c9 *m, int k, int ks, int v) {
+    if (ks == 1 && c9_sttype(m, v + 1) == pE) return 0; /* detached insert */
+    if (m->csn[v * 2] == -1) {
+        m->csn[v * 2] = k;
+        m->css[v * 2] = ks;
+    } else if (m->csn[v * 2 + 1] == -1) {
+        m->csn[v * 2 + 1] = k;
+        m->css[v * 2 + 1] = ks;
+    } else
+        return -1;
+    if (HNS(m, k, ks, 0) == -1)
+        HNS(m, k, ks, 0) = v;
+    else if (HNS(m, k, ks, 1) == -1)
+        HNS(m, k, ks, 1) = v;
+    else
+        return -1;
+    return 0;
+}
+
+/* the insert for the column right of k (the MATP-right and MATR cases of
+ * CP9_map_cm2hmm, src/cp9.rs:331-356, :383-404) */
+static int c9_right_insert(c9 *m, int k) {
+    const cmgpu_cm_params *p = m->p;
+    if (k == m->H) return c9_map(m, k, 1, 2);
+    int nn = m->pos2nd[k + 1];
+    if (m->nd2l[nn] == k + 1) {
+        int b = nn;
+        while (b >= 0 && p->ndtype[b] != nBEGR) b--;
+        if (b < 0) return -1;
+        return c9_map(m, k, 1, p->nodemap[b] + 1);
+    }
+    if (m->nd2r[nn] == k + 1) {
+        if (p->ndtype[nn] == nMATP) return c9_map(m, k, 1, p->nodemap[nn] + 5);
+        if (p->ndtype[nn] == nMATR) return c9_map(m, k, 1, p->nodemap[nn] + 2);
+    }
+    return 0;
+}
+
+/* CP9_map_cm2hmm (src/cp9.rs:275-427) */
+static int c9_mapping(c9 *m, const int *lpos, const int *rpos) {
+    const cmgpu_cm_params *p = m->p;
+    int rc = 0;
+    for (int n = 0; n < p->nodes; n++) {
+        m->nd2l[n] = m->nd2r[n] = -1;
+        if (p->ndtype[n] == nMATP || p->ndtype[n] == nMATL) {
+            m->nd2l[n] = lpos[n];
+            m->pos2nd[lpos[n]] = n;
+        }
+        if (p->ndtype[n] == nMATP || p->ndtype[n] == nMATR) {
+            m->nd2r[n] = rpos[n];
+            m->pos2nd[rpos[n]] = n;
+        }
+    }
+    rc |= c9_map(m, 0, 0, 0);
+    rc |= c9_map(m, 0, 1, 1);
+    for (int k = 1; k <= m->H && rc == 0; k++) {
+        const int n = m->pos2nd[k], nm = p->nodemap[n], t = p->ndtype[n];
+        if (t == nMATP && m->nd2l[n] == k) {
+            rc |= c9_map(m, k, 0, nm);
+            rc |= c9_map(m, k, 0, nm + 1);
+            rc |= c9_map(m, k, 1, nm + 4);
+            rc |= c9_map(m, k, 2, nm + 2);
+            rc |= c9_map(m, k, 2, nm + 3);
+        } else if (t == nMATP) {
+            rc |= c9_map(m, k, 0, nm);
+            rc |= c9_map(m, k, 0, nm + 2);
+            rc |= c9_right_insert(m, k);
+            const int pk = m->pos2nd[k - 1];
+            if (m->nd2l[pk] == k - 1) {
+                if (p->ndtype[pk] != nMATL && p->ndtype[pk] != nMATP) return -1;
+                rc |= c9_map(m, k - 1, 1, nm + 5);
+            }
+            rc |= c9_map(m, k, 2, nm + 1);
+            rc |= c9_map(m, k, 2, nm + 3);
+        } else if (t == nMATL) {
+            rc |= c9_map(m, k, 0, nm);
+            rc |= c9_map(m, k, 1, nm + 2);
+            rc |= c9_map(m, k, 2, nm + 1);
+            if (k == m->H) rc |= c9_map(m, k, 1, 2);
+        } else if (t == nMATR) {
+            rc |= c9_map(m, k, 0, nm);
+            rc |= c9_right_insert(m, k);
+            if (m->nd2l[m->pos2nd[k - 1]] == k - 1) return -1;
+            rc |= c9_map(m, k, 2, nm + 1);
+        } else
+            return -1;
+    }
+    return rc;
+}
+
+static float c9_emit(const c9 *m, int x, int i, int k) {
+    const cmgpu_cm_params *p = m->p;
+    const float *e = p->e + (size_t)x * 16;
+    if (p->stid[x] != uMATP_MP) return e[i];
+    float r = 0.0f;
+    if (m->nd2l[m->pos2nd[k]] == k)
+        for (int j = i * PK; j < (i + 1) * PK; j++) r += e[j];
+    else
+        for (int j = i; j < PK * PK; j += PK) r += e[j];
+    return r;
+}
+
+static int c9_is_ins(const cmgpu_cm_params *p, int v) { return p->sttype[v] == pIL || p->sttype[v] == pIR; }
+
+/* cm_sum_subpaths_cp9 (src/cp9.rs:2615-2693) */
+static float c9_subpaths(const c9 *m, int start, int end, int k) {
+    const cmgpu_cm_params *p = m->p;
+    if (start == end) return c9_is_ins(p, start) ? p->t[start * 6] : 1.0f;
+    double *sp = calloc((size_t)(end - start + 1), sizeof(double));
+    sp[0] = 1.0;
+    if (!c9_is_ins(p, start) && !c9_is_ins(p, end)) {
+        double its = 0.0;
+        const int h0 = HNS(m, k, 1, 0), h1 = HNS(m, k, 1, 1);
+        if (h0 < start) its = m->psi[h0] * (double)c9_subpaths(m, h0, start, k);
+        if (h1 != -1 && h1 < start) its += m->psi[h1] * (double)c9_subpaths(m, h1, start, k);
+        sp[0] -= its / m->psi[start];
+    }
+    for (int v = start + 1; v <= end; v++) {
+        const int vi = v - start, isi = c9_is_ins(p, v);
+        if (p->sttype[v] == pS) sp[vi] = sp[vi - 1] * 1.0;
+        if (v != end && isi && (m->csn[v * 2] == k || m->csn[v * 2 + 1] == k)) continue;
+        for (int y = p->pnum[v] - 1; y >= isi; y--) {
+            const int x = p->plast[v] - y;
+            const int ti = p->sttype[x] == pB ? 0 : v - p->cfirst[x]; /* transition map */
+            if (x - start >= 0) sp[vi] += sp[x - start] * (double)p->t[x * 6 + ti];
+        }
+        if (v != end && isi) sp[vi] += sp[vi] * ((double)p->t[v * 6] / (1.0 - (double)p->t[v * 6]));
+    }
+    const float r = (float)sp[end - start];
+    free(sp);
+    return r;
+}
+
+static void c9_add(c9 *m, int a, int b, int k, int idx) {
+    if (a == -1 || b == -1) return;
+    float *c = &m->t[k * C9N + idx];
+    if (a <= b)
+        *c = (float)((double)*c + m->psi[a] * (double)c9_subpaths(m, a, b, k));
+    else
+        *c = (float)((double)*c + m->psi[b] * (double)c9_subpaths(m, b, a, k));
+}
+
+static void c9_add4(c9 *m, int ka, int sa, int kb, int sb, int k, int idx) {
+    for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 2; j++) c9_add(m, HNS(m, ka, sa, i), HNS(m, kb, sb, j), k, idx);
+}
+
+/* the END_E state paired with nothing, as the second operand */
+static void c9_add_end(c9 *m, int ka, int sa, int k, int idx) {
+    for (int i = 0; i < 2; i++) c9_add(m, HNS(m, ka, sa, i), m->p->M - 1, k, idx);
+}
+
+static float c9_ksum(const float *v, int n) {
+    float s = 0.0f, c = 0.0f;
+    for (int i = 0; i < n; i++) {
+        float y = v[i] - c, t = s + y;
+        c = (t - s) - y;
+        s = t;
+    }
+    return s;
+}
+static void c9_norm(float *v, int n) {
+    const float s = c9_ksum(v, n);
+    for (int i = 0; i < n; i++) v[i] = s != 0.0f ? v[i] / s : 1.0f / (float)n;
+}
+static void c9_scale(float *v, int n, float f) {
+    for (int i = 0; i < n; i++) v[i] *= f;
+}
+static int c9_exit(const cmgpu_cm_params *p, int nd) {
+    const int t = p->ndtype[nd];
+    return (t == nMATP || t == nMATL || t == nMATR || t == nBEGL || t == nBEGR) && nd + 1 < p->nodes &&
+           p->ndtype[nd + 1] != nEND;
+}
+
+static int c9_iexp(int x, const int *sc, const float *nul) {
+    if (!is_res(x)) return 0;
+    float r = 0.0f, d = 0.0f;
+    for (int i = 0; i < PK; i++)
+        if (DEG[x][i]) {
+            r += (float)sc[i] * nul[i];
+            d += nul[i];
+        }
+    r /= d;
+    return r < 0.0f ? (int)(r - 0.5f) : (int)(r + 0.5f);
+}
+
+static void c9_scores(const float *pr, const float *nul, int32_t *out) {
+    int sc[PKP];
+    for (int x = 0; x < PK; x++) sc[x] = p2s_cp9(pr[x], nul[x]);
+    sc[PK] = sc[PKP - 2] = sc[PKP - 1] = -PINF;
+    for (int x = PK + 1; x <= PKP - 3; x++) sc[x] = c9_iexp(x, sc, nul);
+    for (int x = 0; x < PKP; x++) out[x] = sc[x];
+}
+
+/* exported: cp9_build_and_configure into the product's cmgpu_cp9 layout */
+int oracle_prep_cp9(const cmgpu_cm_params *p, cmgpu_cp9 *o) {
+    const int M = p->M;
+    int H = 0;
+    for (int v = 0; v < M; v++) H += p->stid[v] == uMATP_MP ? 2 : (p->stid[v] == uMATL_ML || p->stid[v] == uMATR_MR);
+    if (H != o->M) return -1;
+    c9 m;
+    m.p = p;
+    m.H = H;
+    m.nd2l = malloc(sizeof(int) * (size_t)p->nodes);
+    m.nd2r = malloc(sizeof(int) * (size_t)p->nodes);
+    m.pos2nd = malloc(sizeof(int) * (size_t)(H + 1));
+    m.hns = malloc(sizeof(int) * 6 * (size_t)(H + 1));
+    m.csn = malloc(sizeof(int) * 2 * (size_t)(M + 1));
+    m.css = malloc(sizeof(int) * 2 * (size_t)(M + 1));
+    for (int i = 0; i <= H; i++) m.pos2nd[i] = -1;
+    for (int i = 0; i < 6 * (H + 1); i++) m.hns[i] = -1;
+    for (int i = 0; i < 2 * (M + 1); i++) m.csn[i] = m.css[i] = -1;
+    int *lpos = malloc(sizeof(int) * (size_t)p->nodes), *rpos = malloc(sizeof(int) * (size_t)p->nodes);
+    double *psi = malloc(sizeof(double) * (size_t)M);
+    emitmap(p, lpos, rpos);
+    int rc = c9_mapping(&m, lpos, rpos);
+    if (rc == 0) rc = occupancy(p, psi);
+    for (int k = 0; rc == 0 && k <= H; k++)
+        if (HNS(&m, k, 0, 0) == -1 || HNS(&m, k, 1, 0) == -1) rc = -1;
+    m.psi = psi;
+    m.mat = calloc((size_t)(H + 1) * 4, sizeof(float));
+    m.ins = calloc((size_t)(H + 1) * 4, sizeof(float));
+    m.t = calloc((size_t)(H + 1) * C9N, sizeof(float));
+    m.beg = calloc((size_t)(H + 1), sizeof(float));
+    m.end = calloc((size_t)(H + 1), sizeof(float));
+    unsigned char *hel = calloc((size_t)(H + 1), 1);
+    float nul[PK];
+    if (rc == 0) {
+        /* emissions (src/cp9.rs:2558-2612) */
+        for (int i = 0; i < PK; i++) {
+            nul[i] = p->null[i];
+            m.ins[i] = p->e[1 * 16 + i];
+        }
+        for (int k = 1; k <= H; k++) {
+            for (int i = 0; i < PK; i++) {
+                for (int j = 0; j < 2; j++) {
+                    const int a = HNS(&m, k, 0, j);
+                    if (a != -1) m.mat[k * 4 + i] = (float)((double)m.mat[k * 4 + i] + psi[a] * (double)c9_emit(&m, a, i, k));
+                }
+            }
+            for (int i = 0; i < PK; i++) {
+                for (int j = 0; j < 2; j++) {
+                    const int b = HNS(&m, k, 1, j);
+                    if (b != -1) m.ins[k * 4 + i] = (float)((double)m.ins[k * 4 + i] + psi[b] * (double)c9_emit(&m, b, i, k));
+                }
+            }
+        }
+        /* end-local states (:1042-1077) */
+        const float el_self = (float)exp((double)p->el_selfsc * 0.69314718);
+        for (int nd = 0; nd < p->nodes; nd++)
+            if (c9_exit(p, nd)) hel[lpos[nd]] = 1;
+        /* transitions (:2742-2841) */
+        float *T = m.t;
+        c9_add4(&m, 0, 0, 1, 0, 0, cMM);
+        m.beg[1] = T[cMM];
+        T[cMM] = 0.0f;
+        c9_add4(&m, 0, 0, 0, 1, 0, cMI);
+        c9_add4(&m, 0, 0, 1, 2, 0, cMD);
+        c9_add4(&m, 0, 1, 1, 0, 0, cIM);
+        c9_add4(&m, 0, 1, 0, 1, 0, cII);
+        c9_add4(&m, 0, 1, 1, 2, 0, cID);
+        T[cDM] = T[cDI] = T[cDD] = 0.0f;
+        float d = c9_ksum(m.beg + 1, H) + T[cMI] + T[cMD];
+        c9_scale(m.beg + 1, H, 1.0f / d);
+        T[cMI] /= d;
+        T[cMD] /= d;
+        c9_norm(T + cIM, 3);
+        float *TH = m.t + H * C9N;
+        c9_add_end(&m, H, 0, H, cMM);
+        m.end[H] = TH[cMM];
+        TH[cMM] = 0.0f;
+        c9_add4(&m, H, 0, H, 1, H, cMI);
+        TH[cMD] = 0.0f;
+        c9_add_end(&m, H, 1, H, cIM);
+        c9_add4(&m, H, 1, H, 1, H, cII);
+        TH[cID] = 0.0f;
+        c9_add_end(&m, H, 2, H, cDM);
+        c9_add4(&m, H, 2, H, 1, H, cDI);
+        TH[cDD] = 0.0f;
+        d = c9_ksum(TH, 4) + m.end[H];
+        c9_scale(TH, 4, 1.0f / d);
+        m.end[H] /= d;
+        c9_norm(TH + cIM, 3);
+        c9_norm(TH + cDM, 3);
+        for (int k = 1; k < H; k++) {
+            float *Tk = m.t + k * C9N;
+            c9_add4(&m, k, 0, k + 1, 0, k, cMM);
+            c9_add4(&m, k, 0, k, 1, k, cMI);
+            c9_add4(&m, k, 0, k + 1, 2, k, cMD);
+            c9_add4(&m, k, 1, k + 1, 0, k, cIM);
+            c9_add4(&m, k, 1, k, 1, k, cII);
+            c9_add4(&m, k, 1, k + 1, 2, k, cID);
+            c9_add4(&m, k, 2, k + 1, 0, k, cDM);
+            c9_add4(&m, k, 2, k, 1, k, cDI);
+            c9_add4(&m, k, 2, k + 1, 2, k, cDD);
+            d = c9_ksum(Tk, 4) + m.end[k];
+            c9_scale(Tk, 4, 1.0f / d);
+            m.end[k] /= d;
+            c9_norm(Tk + cIM, 3);
+            c9_norm(Tk + cDM, 3);
+        }
+        /* CPlan9Renormalize (:1000-1040) */
+        for (int i = 0; i < PK; i++) m.mat[i] = 0.0f;
+        for (int k = 1; k <= H; k++) c9_norm(m.mat + k * 4, PK);
+        for (int k = 0; k <= H; k++) c9_norm(m.ins + k * 4, PK);
+        d = c9_ksum(m.beg + 1, H) + T[cMI] + T[cMD] + T[cMEL];
+        c9_scale(m.beg + 1, H, 1.0f / d);
+        T[cMI] /= d;
+        T[cMD] /= d;
+        T[cMEL] /= d;
+        c9_norm(T + cIM, 3);
+        T[cDM] = T[cDI] = T[cDD] = 0.0f;
+        for (int k = 1; k <= H; k++) {
+            float *Tk = m.t + k * C9N;
+            const float dk = c9_ksum(Tk, 4) + m.end[k];
+            c9_scale(Tk, 4, 1.0f / dk);
+            m.end[k] /= dk;
+            c9_norm(Tk + cIM, 3);
+            c9_norm(Tk + cDM, 3);
+        }
+        c9_norm(nul, PK);
+        /* local begins and ends, pentry = pexit = pbegin (:1097-1119, :1079) */
+        const float pb = p->pbegin;
+        const float s = T[cMI] + T[cMD] + T[cMEL];
+        m.beg[1] = (1.0f - pb) * (1.0f - s);
+        for (int k = 2; k <= H; k++) m.beg[k] = (pb * (1.0f - s)) / ((float)H - 1.0f);
+        const float basep = pb / ((float)H - 1.0f);
+        for (int k = 1; k < H; k++) m.end[k] = basep / (1.0f - basep * ((float)k - 1.0f));
+        for (int k = 1; k < H; k++) {
+            float *Tk = m.t + k * C9N;
+            const float dk = c9_ksum(Tk, 4);
+            c9_scale(Tk, 4, (1.0f - m.end[k]) / dk);
+        }
+        const float dm = TH[cMI] + TH[cMEL];
+        if (fabsf(dm - 0.0f) >= 5e-9f) {
+            const float f = (1.0f - m.end[H]) / dm;
+            TH[cMI] *= f;
+            TH[cMEL] *= f;
+        }
+        /* end-local exits (:1121-1147) */
+        int nexits = 0;
+        for (int nd = 1; nd < p->nodes; nd++) nexits += c9_exit(p, nd);
+        const float to_el = p->pend / (float)nexits;
+        T[cMEL] = 0.0f;
+        for (int k = 1; k <= H; k++) {
+            float *Tk = m.t + k * C9N;
+            if (!hel[k]) continue;
+            Tk[cMEL] = to_el;
+            const float nf = 1.0f - (Tk[cMEL] / (1.0f - m.end[k]));
+            Tk[cMM] *= nf;
+            Tk[cMI] *= nf;
+            Tk[cMD] *= nf;
+        }
+        /* CP9Logoddsify (:1176-1255) into the product's layout */
+        for (int k = 0; k <= H; k++) {
+            const float *Tk = m.t + k * C9N;
+            memcpy(o->mat + k * 4, m.mat + k * 4, sizeof(float) * 4);
+            memcpy(o->ins + k * 4, m.ins + k * 4, sizeof(float) * 4);
+            memcpy(o->t + k * C9N, Tk, sizeof(float) * C9N);
+            o->begin[k] = m.beg[k];
+            o->end[k] = m.end[k];
+            o->has_el[k] = hel[k];
+            c9_scores(m.ins + k * 4, nul, o->isc + k * PKP);
+            if (k == 0)
+                for (int x = 0; x < PKP; x++) o->msc[x] = 0;
+            else
+                c9_scores(m.mat + k * 4, nul, o->msc + k * PKP);
+            int32_t *ot = o->otsc + k * 12;
+            ot[0] = p2s_cp9(Tk[cMM], 1.0f);
+            ot[1] = p2s_cp9(Tk[cIM], 1.0f);
+            ot[2] = k ? p2s_cp9(Tk[cDM], 1.0f) : -PINF;
+            ot[3] = k ? p2s_cp9(m.beg[k], 1.0f) : -PINF;
+            ot[4] = p2s_cp9(Tk[cMI], 1.0f);
+            ot[5] = p2s_cp9(Tk[cII], 1.0f);
+            ot[6] = k ? p2s_cp9(Tk[cDI], 1.0f) : -PINF;
+            ot[7] = p2s_cp9(Tk[cMD], 1.0f);
+            ot[8] = p2s_cp9(Tk[cID], 1.0f);
+            ot[9] = k ? p2s_cp9(Tk[cDD], 1.0f) : -PINF;
+            ot[10] = k ? p2s_cp9(m.end[k], 1.0f) : -PINF;
+            ot[11] = p2s_cp9(Tk[cMEL], 1.0f);
+            for (int s2 = 0; s2 < 3; s2++)
+                for (int j = 0; j < 2; j++) o->hns2cs[(k * 3 + s2) * 2 + j] = HNS(&m, k, s2, j);
+        }
+        o->el_self = el_self;
+        o->el_selfsc = p2s_cp9(el_self, 1.0f);
+    }
+    free(m.nd2l);
+    free(m.nd2r);
+    free(m.pos2nd);
+    free(m.hns);
+    free(m.csn);
+    free(m.css);
+    free(lpos);
+    free(rpos);
+    free(psi);
+    free(m.mat);
+    free(m.ins);
+    free(m.t);
+    free(m.beg);
+    free(m.end);
+    free(hel);
+    return rc;
+}

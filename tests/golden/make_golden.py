@@ -18,6 +18,8 @@
 * histogram_kat.json: the exponential tail fit of the reference's
   `test_cmcalibrate_sequence` (src/easel/histogram.rs:543-586), whose mu and
   lambda the reference pins to a probe of C libeasel.
+* tmap_kat.json: the CM transition map (cm_create_transition_map,
+  src/cp9.rs:480-740), which state occupancy and the CP9 subpath sums index.
 * scan_small.json: the oracle's hits on one fixed seeded model and sequence,
   a regression lock for the oracle itself.
 
@@ -114,6 +116,22 @@ def histogram_kats():
             "lambda": lam}
 
 
+def tmap_kats():
+    """cm_create_transition_map's table (src/cp9.rs:480-740) as
+    [parent unique state, node type, child unique state, transition]."""
+    src = open(os.path.join(REF, "src", "cp9.rs")).read()
+    body = src[src.index("pub fn cm_create_transition_map"):]
+    body = body[: body.index("\n}\n")]
+    ids = {"ROOT_S": 0, "ROOT_IL": 1, "ROOT_IR": 2, "BEGL_S": 3, "BEGR_S": 4, "BEGR_IL": 5, "MATP_MP": 6,
+           "MATP_ML": 7, "MATP_MR": 8, "MATP_D": 9, "MATP_IL": 10, "MATP_IR": 11, "MATL_ML": 12, "MATL_D": 13,
+           "MATL_IL": 14, "MATR_MR": 15, "MATR_D": 16, "MATR_IR": 17, "BIF_B": 18, "END_E": 19}
+    nds = {"BIF_ND": 0, "MATP_ND": 1, "MATL_ND": 2, "MATR_ND": 3, "BEGL_ND": 4, "BEGR_ND": 5, "ROOT_ND": 6,
+           "END_ND": 7}
+    rows = [[ids[a], nds[b], ids[c], int(n)] for a, b, c, n in
+            re.findall(r"tmap\[(\w+) as usize\]\[(\w+) as usize\]\[(\w+) as usize\] = (\d+);", body)]
+    return {"source": "src/cp9.rs:480-740", "entries": rows}
+
+
 def scan_small():
     sys.path.insert(0, ROOT)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -147,6 +165,8 @@ def main():
             json.dump(pipeline_kats(), f, indent=1)
         with open(os.path.join(HERE, "histogram_kat.json"), "w") as f:
             json.dump(histogram_kats(), f, indent=1)
+        with open(os.path.join(HERE, "tmap_kat.json"), "w") as f:
+            json.dump(tmap_kats(), f)
     with open(os.path.join(HERE, "scan_small.json"), "w") as f:
         json.dump(scan_small(), f, indent=1)
 
