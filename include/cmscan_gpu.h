@@ -174,13 +174,17 @@ int cmgpu_prep_configure(const cmgpu_cm_params *p, int local, int32_t W_in,
  * scores, otsc [(M+1)*12] integer transition scores in the DP's order MM IM
  * DM BM MI II DI MD ID DD ME MEL, has_el [M+1] (an end-local exit leaves
  * node k), hns2cs [(M+1)*3*2] the CM states behind node k's match, insert
- * and delete states (-1: none). */
+ * and delete states (-1: none), el_pairs [nodes*2] the (source, destination)
+ * HMM nodes of every end-local exit in CM node order (CPlan9InitEL's
+ * el_from_idx lists, src/cp9.rs:1061-1075), their count in n_el. */
 typedef struct cmgpu_cp9 {
     int32_t M;
     float *mat, *ins, *t, *begin, *end;
     int32_t *msc, *isc, *otsc;
     uint8_t *has_el;
     int32_t *hns2cs;
+    int32_t *el_pairs;
+    int32_t n_el;           /* out */
     float el_self;          /* out */
     int32_t el_selfsc;      /* out */
 } cmgpu_cp9;

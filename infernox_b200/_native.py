@@ -89,7 +89,7 @@ class Cp9(C.Structure):
     _fields_ = [("M", C.c_int32), ("mat", P(C.c_float)), ("ins", P(C.c_float)), ("t", P(C.c_float)),
                 ("begin", P(C.c_float)), ("end", P(C.c_float)), ("msc", P(C.c_int32)), ("isc", P(C.c_int32)),
                 ("otsc", P(C.c_int32)), ("has_el", P(C.c_uint8)), ("hns2cs", P(C.c_int32)),
-                ("el_self", C.c_float), ("el_selfsc", C.c_int32)]
+                ("el_pairs", P(C.c_int32)), ("n_el", C.c_int32), ("el_self", C.c_float), ("el_selfsc", C.c_int32)]
 
 
 class F3Config(C.Structure):

@@ -1134,7 +1134,7 @@ void cp9_emission_scores(const std::array<float, 4> &pr, const float *null, int3
 extern "C" int cmgpu_prep_cp9(const cmgpu_cm_params *p, cmgpu_cp9 *out) {
     if (!p || !out || p->M < 2 || p->nodes < 2 || !p->sttype || !p->t || !p->e || !p->plast || !p->pnum ||
         !p->ndidx || !out->mat || !out->ins || !out->t || !out->begin || !out->end || !out->msc || !out->isc ||
-        !out->otsc || !out->has_el || !out->hns2cs || out->M != p->clen) {
+        !out->otsc || !out->has_el || !out->hns2cs || !out->el_pairs || out->M != p->clen) {
         cmx::set_error("cmgpu_prep_cp9: bad arguments (out->M must be the CM's consensus length)");
         return CMGPU_EINVAL;
     }
@@ -1207,6 +1207,13 @@ extern "C" int cmgpu_prep_cp9(const cmgpu_cm_params *p, cmgpu_cp9 *out) {
         for (int ks = 0; ks < 3; ks++)
             for (int j = 0; j < 2; j++) out->hns2cs[((size_t)k * 3 + ks) * 2 + j] = m.hns2cs[k][ks][j];
     }
+    out->n_el = 0;
+    for (int nd = 0; nd < cm.nodes; nd++)
+        if (has_exit(cm, nd)) {
+            out->el_pairs[2 * out->n_el] = lpos[nd];
+            out->el_pairs[2 * out->n_el + 1] = rpos[nd];
+            out->n_el++;
+        }
     out->el_self = h.el_self;
     out->el_selfsc = cp9_prob2score(h.el_self, 1.0f);
     return CMGPU_OK;

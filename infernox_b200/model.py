@@ -171,15 +171,17 @@ def cp9(cm: SynthCM) -> dict:
                t=np.zeros((H + 1, 10), np.float32), begin=np.zeros(H + 1, np.float32),
                end=np.zeros(H + 1, np.float32), msc=np.zeros((H + 1, 18), np.int32),
                isc=np.zeros((H + 1, 18), np.int32), otsc=np.zeros((H + 1, 12), np.int32),
-               has_el=np.zeros(H + 1, np.uint8), hns2cs=np.zeros((H + 1, 3, 2), np.int32))
+               has_el=np.zeros(H + 1, np.uint8), hns2cs=np.zeros((H + 1, 3, 2), np.int32),
+               el_pairs=np.zeros((cm.st.nodes, 2), np.int32))
     s = N.Cp9()
     s.M = H
     for k, ct in (("mat", C.c_float), ("ins", C.c_float), ("t", C.c_float), ("begin", C.c_float),
                   ("end", C.c_float), ("msc", C.c_int32), ("isc", C.c_int32), ("otsc", C.c_int32),
-                  ("has_el", C.c_uint8), ("hns2cs", C.c_int32)):
+                  ("has_el", C.c_uint8), ("hns2cs", C.c_int32), ("el_pairs", C.c_int32)):
         setattr(s, k, N.ptr(out[k], ct))
     N.check(N.lib().cmgpu_prep_cp9(C.byref(p), C.byref(s)))
     del keep
+    out["el_pairs"] = out["el_pairs"][: s.n_el]
     out["el_self"] = float(s.el_self)
     out["el_selfsc"] = int(s.el_selfsc)
     return out

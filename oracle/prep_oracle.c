@@ -1022,6 +1022,13 @@ int oracle_prep_cp9(const cmgpu_cm_params *p, cmgpu_cp9 *o) {
             for (int s2 = 0; s2 < 3; s2++)
                 for (int j = 0; j < 2; j++) o->hns2cs[(k * 3 + s2) * 2 + j] = HNS(&m, k, s2, j);
         }
+        o->n_el = 0;
+        for (int nd = 0; nd < p->nodes; nd++) {
+            if (!c9_exit(p, nd)) continue;
+            o->el_pairs[2 * o->n_el] = lpos[nd];
+            o->el_pairs[2 * o->n_el + 1] = rpos[nd];
+            o->n_el++;
+        }
         o->el_self = el_self;
         o->el_selfsc = p2s_cp9(el_self, 1.0f);
     }

@@ -66,6 +66,10 @@ def test_cp9_is_a_local_probability_model(name):
     assert (h["begin"][1:] > 0).all() and (h["end"][1:] > 0).all()
     el = h["has_el"][1:] == 1  # node 0's flag (a bifurcation at the first column) takes no exit
     assert el.sum() > 0 and (t[1:][el, 3] > 0).all() and (t[1:][~el, 3] == 0).all()
+    # the exits' sources are the flagged nodes; each exit lands to the right of its source
+    pairs = h["el_pairs"]
+    assert set(pairs[:, 0].tolist()) == set(np.nonzero(h["has_el"])[0].tolist())
+    assert (pairs[:, 1] > pairs[:, 0]).all() and (pairs[:, 1] <= H + 1).all()
     # every HMM node's match and insert states come from the CM
     assert (h["hns2cs"][:, 0, 0] >= 0).all() and (h["hns2cs"][:, 1, 0] >= 0).all()
     assert (h["hns2cs"][1:, 2, 0] >= 0).all()
